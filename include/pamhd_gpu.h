@@ -1,0 +1,220 @@
+/*
+pamhd_gpu.h - C ABI of the B200 (sm_100a) finite-volume MHD step.
+
+This is the drop-in boundary for PAMHD's cell-centred ("Mode C") MHD step
+on uniform Cartesian grids: the conservative state (mass density, momentum
+density, total energy density, magnetic field), the Rusanov / HLL / HLLD /
+Roe face fluxes, flux application and the lagged CFL timestep rule.
+Host code (C or C++) calls these entry points with plain pointers and
+sizes; no C++ types, exceptions or torch types cross this boundary.
+
+Conventions
+  - Every function returns an int status: PAMHD_OK (0) or a PAMHD_ERR_*.
+  - Arrays of cell data are structure-of-arrays: eight arrays, one per
+    conservative variable in the order of the reference's detail::MHD
+    (mhd/variables.hpp:240): rho, mom_x, mom_y, mom_z, E, B_x, B_y, B_z.
+    Each holds n[0]*n[1]*n[2] doubles, x fastest (index i + n0*(j + n1*k)),
+    the order of dccrg's level-0 cell ids on a uniform grid.
+  - Host arrays passed in are caller-owned and copied; device arrays are
+    owned by the context.
+  - A context is bound to one CUDA device and one CUDA stream and is not
+    thread-safe; different contexts may be used from different threads.
+  - All arithmetic is IEEE FP64.
+*/
+#ifndef PAMHD_GPU_H
+#define PAMHD_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PAMHD_GPU_ABI_VERSION 1
+
+/* Return codes. */
+enum {
+	PAMHD_OK = 0,
+	PAMHD_ERR_ARGUMENT = 1,  /* invalid argument or configuration */
+	PAMHD_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+	PAMHD_ERR_PHYSICS = 3,   /* a solver met a state the reference throws on
+	                            (see pamhd_gpu_status for which and where) */
+	PAMHD_ERR_STATE = 4,     /* call made in the wrong order */
+	PAMHD_ERR_TIMEOUT = 5    /* a bounded device-side wait gave up */
+};
+
+/*
+Riemann solver ids, in the numeric order of the reference's
+enum class Solver (mhd/common.hpp:54-61).  rusanov_staggered is accepted by
+the reference's option parser but aborts in its dispatcher
+(mhd/solve.hpp:150-153); here it is rejected with PAMHD_ERR_ARGUMENT.
+*/
+enum {
+	PAMHD_RUSANOV = 0,
+	PAMHD_RUSANOV_STAGGERED = 1,
+	PAMHD_HLL_ATHENA = 2,
+	PAMHD_HLLD_ATHENA = 3,
+	PAMHD_ROE_ATHENA = 4
+};
+
+/*
+Boundary kinds per grid side.  PERIODIC must be given on both sides of a
+dimension.  COPY fills a ghost from its inward face neighbour (density,
+velocity, thermal pressure and magnetic field copied; mhd/boundaries.hpp:
+818-1030).  VALUE holds a fixed conservative state (value boundaries,
+mhd/boundaries.hpp:760-880, and the solar-wind inflow of
+mhd/solar_wind_box.hpp:227).
+*/
+enum {
+	PAMHD_BC_PERIODIC = 0,
+	PAMHD_BC_COPY = 1,
+	PAMHD_BC_VALUE = 2
+};
+
+/*
+Status flag bits reported by pamhd_gpu_status() and by
+pamhd_gpu_face_flux().  Each matches a std::domain_error the reference
+throws (and then aborts on, mhd/solve.hpp:156-181).
+*/
+enum {
+	PAMHD_FLAG_DENSITY = 1u << 0,        /* non-positive or non-normal mass density */
+	PAMHD_FLAG_PRESSURE = 1u << 1,       /* non-positive or non-normal thermal pressure */
+	PAMHD_FLAG_WAVE_SPEED = 1u << 2,     /* invalid fast magnetosonic / signal speed */
+	PAMHD_FLAG_FLUX = 1u << 3,           /* non-finite flux or momentum */
+	PAMHD_FLAG_ROE_DENSITY = 1u << 4,    /* roe_athena.hpp:505: intermediate density */
+	PAMHD_FLAG_ROE_PRESSURE = 1u << 5,   /* roe_athena.hpp:523: intermediate pressure */
+	PAMHD_FLAG_NEW_STATE = 1u << 6,      /* common.hpp:728-742: updated state invalid */
+	PAMHD_FLAG_TIMEOUT = 1u << 7         /* a bounded device wait expired */
+};
+
+/*
+Grid configuration.  Replaces the parts of the reference's JSON options
+that the step reads: the solver (mhd/options.hpp:97-112), the timestep
+factor (mhd/options.hpp:119-132, "mhd-time-step-factor"), the adiabatic
+index and vacuum permeability (simulation_options.hpp:59-60), the uniform
+cell size (grid/options.hpp) and the boundary kinds.
+A dimension with n == 1 is inactive: it has no faces and does not enter
+the timestep.
+*/
+typedef struct pamhd_cfg {
+	int32_t n[3];                /* interior cells in x, y, z */
+	int32_t solver;              /* PAMHD_RUSANOV ... PAMHD_ROE_ATHENA */
+	double cell_length[3];       /* dx, dy, dz */
+	double adiabatic_index;      /* gamma */
+	double vacuum_permeability;  /* mu0 */
+	double time_step_factor;     /* CFL number */
+	int32_t bc_lo[3];            /* PAMHD_BC_* of the -x, -y, -z sides */
+	int32_t bc_hi[3];            /* PAMHD_BC_* of the +x, +y, +z sides */
+	double value_lo[3][8];       /* ghost state of VALUE sides (rho, mom, E, B) */
+	double value_hi[3][8];
+	int32_t device;              /* CUDA device ordinal */
+	int32_t reserved;            /* must be 0 */
+} pamhd_cfg;
+
+typedef struct pamhd_ctx pamhd_ctx;
+
+/* ABI version of the loaded library (PAMHD_GPU_ABI_VERSION). */
+int pamhd_gpu_abi_version(void);
+
+/* Text of a return code. */
+const char* pamhd_gpu_errstr(int code);
+
+/*
+Creates a context: allocates the state (two copies, ping-pong) and the
+reduction buffers on cfg->device.  Replaces the dccrg grid set-up and the
+cell-data allocation of tests/mhd/test.cpp:330-444 for uniform grids.
+*/
+int pamhd_gpu_create(const pamhd_cfg* cfg, pamhd_ctx** ctx);
+
+/* Frees everything the context owns. */
+int pamhd_gpu_destroy(pamhd_ctx* ctx);
+
+/*
+Copies the interior state in from eight host arrays and fills the ghost
+cells (apply_boundaries, mhd/boundaries.hpp:1261).  Marks the context as
+not primed: the next step is the dt = 0 priming step.
+*/
+int pamhd_gpu_set_state(pamhd_ctx* ctx, const double* const soa[8]);
+
+/* Copies the interior state out to eight host arrays (synchronises). */
+int pamhd_gpu_get_state(pamhd_ctx* ctx, double* const soa[8]);
+
+/* As set/get_state but with device pointers, ordered on the context's stream. */
+int pamhd_gpu_set_state_device(pamhd_ctx* ctx, const double* const soa[8]);
+int pamhd_gpu_get_state_device(pamhd_ctx* ctx, double* const soa[8]);
+
+/*
+One step of the lagged-CFL rule; replaces pamhd::mhd::timestep()
+(mhd/solve.hpp:1837-1924) in its Mode C, no-substepping form:
+  dt = min over faces of CFL * dx_d / s_face from the previous step's face
+  speeds (0 if any face speed <= 0), capped by max_dt
+  (substepping.hpp:285-338, solve.hpp:1933-2007);
+  fluxes for every face, scaled by dt (solve.hpp:217-392);
+  U += (F- - F+)/dx, then y, then z (solve.hpp:1543-1587);
+  ghost refresh.
+The first step after create/set_state is the reference's dt = 0 priming
+step whatever max_dt is (tests/mhd/test.cpp:462-470).
+Synchronises; *dt_taken receives the step length.
+Returns PAMHD_ERR_PHYSICS if any face met an invalid state.
+*/
+int pamhd_gpu_step(pamhd_ctx* ctx, double max_dt, double* dt_taken);
+
+/*
+Runs nsteps steps without host synchronisation (captured in a CUDA graph
+after the first call), each capped so that simulation time does not pass
+t_end, as the loop of tests/mhd/test.cpp:514-530 does.  Primes first if
+needed.  Does not wait for the GPU; use pamhd_gpu_sync() and
+pamhd_gpu_time() to collect the result.
+*/
+int pamhd_gpu_steps(pamhd_ctx* ctx, int32_t nsteps, double t_end);
+
+/* Waits for the context's stream; returns PAMHD_ERR_PHYSICS if a face failed. */
+int pamhd_gpu_sync(pamhd_ctx* ctx);
+
+/* Simulation time, number of steps taken and the last dt (synchronises). */
+int pamhd_gpu_time(pamhd_ctx* ctx, double* time, int64_t* steps, double* last_dt);
+
+/*
+Copies the dt of the last min(count, recorded) steps (oldest first) out
+(synchronises); *written receives how many.
+*/
+int pamhd_gpu_dt_history(pamhd_ctx* ctx, double* dt, int32_t count, int32_t* written);
+
+/*
+Error state of the context: OR of PAMHD_FLAG_* seen since the last
+set_state, and the first failing face in x-fastest cell order:
+cell index (interior numbering, ghosts as -1/n) and face direction
+(+1, +2, +3) — the face at which the reference would have aborted
+(mhd/solve.hpp:156-181).
+*/
+int pamhd_gpu_status(pamhd_ctx* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
+
+/*
+Conserved totals over interior cells: sum of rho, mom[3], E, B[3] times the
+cell volume, summed in a fixed order (deterministic).
+*/
+int pamhd_gpu_totals(pamhd_ctx* ctx, double totals[8]);
+
+/*
+Solver-level entry point: the face flux and max signal speed of n
+independent face problems, each given as the two states in the face frame
+(x = face normal) and the face's background field.  Replaces the compile
+time plugin get_flux_X<Mas, Mom, Nrj, Mag>(state_neg, state_pos, bg_face_B,
+gamma, mu0) -> tuple<MHD, Scalar> of mhd/rusanov.hpp:67,
+mhd/hll_athena.hpp:65, mhd/hlld_athena.hpp:62 and mhd/roe_athena.hpp:575.
+Host arrays: neg, pos and flux hold n*8 doubles (cell-major), bg n*3 (NULL
+means zero), speed n, flags n (0 or PAMHD_FLAG_* of the first check that
+failed).  Runs on `device`; returns PAMHD_ERR_PHYSICS if any face failed.
+*/
+int pamhd_gpu_face_flux(
+	int32_t device, int32_t solver, int64_t n,
+	const double* neg, const double* pos, const double* bg,
+	double adiabatic_index, double vacuum_permeability,
+	double* flux, double* speed, uint32_t* flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

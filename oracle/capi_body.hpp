@@ -1,0 +1,169 @@
+/*
+C entry points of the CPU oracle, shared by the two oracle libraries:
+  oracle/_build/liboracle.so   - the restated solvers of mhd_oracle.hpp
+  oracle/_ref/libpamhd_ref.so  - the reference's own solver headers
+Both drive them with the same Mode C grid restatement (mode_c.hpp).
+
+TEST INFRASTRUCTURE - see mhd_oracle.hpp for who may use this.
+
+The including file defines ORACLE_API(name) (the exported symbol name) and
+ORACLE_FLUX (the solver dispatch functor type).
+*/
+#include <cstdio>
+#include <cstring>
+
+#include "mode_c.hpp"
+
+namespace {
+
+using Grid = oracle::Mode_C_Grid<ORACLE_FLUX>;
+
+thread_local std::string last_error;
+
+int fail_with(const char* what)
+{
+	last_error = what;
+	return PAMHD_ERR_ARGUMENT;
+}
+
+} // namespace
+
+extern "C" {
+
+// text of the last argument error of this thread
+const char* ORACLE_API(last_error)(void)
+{
+	return last_error.c_str();
+}
+
+/*
+Face fluxes of n independent face problems in the face frame; see
+pamhd_gpu_face_flux in include/pamhd_gpu.h for the layout.  flags[i]
+receives the PAMHD_FLAG_* of the exception the solver threw, or 0.
+Returns the number of failed faces.
+*/
+int64_t ORACLE_API(face_flux)(
+	int32_t solver, int64_t n, const double* neg, const double* pos, const double* bg,
+	double gamma, double mu0, double* flux, double* speed, uint32_t* flags)
+{
+	const ORACLE_FLUX solve{};
+	int64_t failed = 0;
+	for (int64_t i = 0; i < n; i++) {
+		oracle::MHD a, b;
+		const double* x = neg + 8 * i;
+		const double* y = pos + 8 * i;
+		a.rho = x[0]; a.mom = {x[1], x[2], x[3]}; a.nrj = x[4]; a.mag = {x[5], x[6], x[7]};
+		b.rho = y[0]; b.mom = {y[1], y[2], y[3]}; b.nrj = y[4]; b.mag = {y[5], y[6], y[7]};
+		oracle::Vec3 g{0, 0, 0};
+		if (bg != nullptr) g = {bg[3 * i], bg[3 * i + 1], bg[3 * i + 2]};
+		double* out = flux + 8 * i;
+		try {
+			const oracle::Face_Flux r = solve(solver, a, b, g, gamma, mu0);
+			const double row[8] = {
+				r.flux.rho, r.flux.mom[0], r.flux.mom[1], r.flux.mom[2],
+				r.flux.nrj, r.flux.mag[0], r.flux.mag[1], r.flux.mag[2]};
+			std::memcpy(out, row, sizeof row);
+			speed[i] = r.speed;
+			flags[i] = 0;
+		} catch (const oracle::Domain_Error& e) {
+			for (int k = 0; k < 8; k++) out[k] = 0;
+			speed[i] = 0;
+			flags[i] = e.flag;
+			failed++;
+		} catch (const std::exception&) {
+			for (int k = 0; k < 8; k++) out[k] = 0;
+			speed[i] = 0;
+			flags[i] = 0x80000000u;
+			failed++;
+		}
+	}
+	return failed;
+}
+
+// a Mode C grid; returns NULL on an invalid configuration
+void* ORACLE_API(grid_create)(const pamhd_cfg* cfg)
+{
+	try {
+		return new Grid(*cfg);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return nullptr;
+	}
+}
+
+void ORACLE_API(grid_destroy)(void* grid)
+{
+	delete static_cast<Grid*>(grid);
+}
+
+void ORACLE_API(grid_set_threads)(void* grid, int32_t threads)
+{
+	static_cast<Grid*>(grid)->threads = threads < 1 ? 1 : threads;
+}
+
+int ORACLE_API(grid_set_state)(void* grid, const double* const soa[8])
+{
+	try {
+		static_cast<Grid*>(grid)->set_interior(soa);
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+int ORACLE_API(grid_get_state)(void* grid, double* const soa[8])
+{
+	static_cast<Grid*>(grid)->get_interior(soa);
+	return PAMHD_OK;
+}
+
+/*
+One step (see Mode_C_Grid::step).  On a solver failure returns
+PAMHD_ERR_PHYSICS with the flag, the failing cell (interior coordinates;
+ghosts are -1 or n) and the face direction (+1..+3); the state is left as
+it was before the step's update.
+*/
+int ORACLE_API(grid_step)(void* grid, double max_dt, double* dt_taken,
+                          uint32_t* flag, int32_t cell[3], int32_t* dir)
+{
+	Grid& g = *static_cast<Grid*>(grid);
+	*flag = 0;
+	try {
+		*dt_taken = g.step(max_dt);
+	} catch (const oracle::Domain_Error& e) {
+		*flag = e.flag;
+		int c[3];
+		g.coords(size_t(g.failure.cell), c);
+		for (int d = 0; d < 3; d++) cell[d] = c[d];
+		*dir = g.failure.dir;
+		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+// runs steps until t reaches t_end or max_steps steps were taken; returns steps taken or -1
+int64_t ORACLE_API(grid_run)(void* grid, double t_start, double t_end, int64_t max_steps,
+                             double* t_reached, double* dt_history)
+{
+	Grid& g = *static_cast<Grid*>(grid);
+	double t = t_start;
+	int64_t steps = 0;
+	try {
+		while (t < t_end and steps < max_steps) {
+			const double dt = g.step(t_end - t);
+			if (dt_history != nullptr) dt_history[steps] = dt;
+			t += dt;
+			steps++;
+		}
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		*t_reached = t;
+		return -1;
+	}
+	*t_reached = t;
+	return steps;
+}
+
+} // extern "C"

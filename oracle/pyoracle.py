@@ -1,0 +1,214 @@
+"""ctypes access to the CPU oracle libraries.
+
+TEST INFRASTRUCTURE: only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg may import this module.  It is the checker, never the
+thing measured or shipped.
+
+Two libraries expose the same entry points (oracle/capi_body.hpp):
+  port       oracle/_build/liboracle.so   restated solvers (mhd_oracle.hpp)
+  reference  oracle/_ref/libpamhd_ref.so  the reference's own solver headers
+Both drive the solvers with the same Mode C grid restatement (mode_c.hpp).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+REF_LIB = os.path.join(ORACLE_DIR, "_ref", "libpamhd_ref.so")
+REF_EXE = os.path.join(ORACLE_DIR, "_ref", "reference.exe")
+
+RUSANOV, RUSANOV_STAGGERED, HLL, HLLD, ROE = 0, 1, 2, 3, 4
+SOLVERS = {"rusanov": RUSANOV, "hll_athena": HLL, "hlld_athena": HLLD, "roe_athena": ROE}
+BC_PERIODIC, BC_COPY, BC_VALUE = 0, 1, 2
+
+
+class Cfg(ctypes.Structure):
+    """Layout of pamhd_cfg (include/pamhd_gpu.h)."""
+
+    _fields_ = [
+        ("n", ctypes.c_int32 * 3),
+        ("solver", ctypes.c_int32),
+        ("cell_length", ctypes.c_double * 3),
+        ("adiabatic_index", ctypes.c_double),
+        ("vacuum_permeability", ctypes.c_double),
+        ("time_step_factor", ctypes.c_double),
+        ("bc_lo", ctypes.c_int32 * 3),
+        ("bc_hi", ctypes.c_int32 * 3),
+        ("value_lo", (ctypes.c_double * 8) * 3),
+        ("value_hi", (ctypes.c_double * 8) * 3),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+def make_cfg(n, solver, cell_length, gamma, mu0, cfl, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0),
+             value_lo=None, value_hi=None, device=0) -> Cfg:
+    c = Cfg()
+    for d in range(3):
+        c.n[d] = int(n[d])
+        c.cell_length[d] = float(cell_length[d])
+        c.bc_lo[d] = int(bc_lo[d])
+        c.bc_hi[d] = int(bc_hi[d])
+        for k in range(8):
+            c.value_lo[d][k] = 0.0 if value_lo is None or value_lo[d] is None else float(value_lo[d][k])
+            c.value_hi[d][k] = 0.0 if value_hi is None or value_hi[d] is None else float(value_hi[d][k])
+    c.solver = int(solver)
+    c.adiabatic_index = float(gamma)
+    c.vacuum_permeability = float(mu0)
+    c.time_step_factor = float(cfl)
+    c.device = int(device)
+    c.reserved = 0
+    return c
+
+
+def build(quiet: bool = True) -> None:
+    """Runs oracle/Makefile (the reference targets only where the reference tree exists)."""
+    out = subprocess.run(["make", "-C", ORACLE_DIR], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+_P = ctypes.POINTER
+_D = ctypes.c_double
+_DP = _P(ctypes.c_double)
+
+
+def _soa_in(arrays):
+    ptrs = (ctypes.c_void_p * 8)()
+    keep = []
+    for k in range(8):
+        a = np.ascontiguousarray(arrays[k], dtype=np.float64)
+        keep.append(a)
+        ptrs[k] = a.ctypes.data
+    return ptrs, keep
+
+
+class Oracle:
+    """One oracle library: 'port' (restated solvers) or 'reference' (reference headers)."""
+
+    def __init__(self, kind: str = "port"):
+        path = PORT_LIB if kind == "port" else REF_LIB
+        if not os.path.exists(path):
+            build()
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing (the reference build needs the reference tree)")
+        self.kind = kind
+        self.lib = ctypes.CDLL(path)
+        p = "oracle_" if kind == "port" else "ref_"
+        L = self.lib
+        self._face_flux = getattr(L, p + "face_flux")
+        self._face_flux.restype = ctypes.c_int64
+        self._face_flux.argtypes = [ctypes.c_int32, ctypes.c_int64, _DP, _DP, _DP, _D, _D, _DP, _DP,
+                                    _P(ctypes.c_uint32)]
+        self._create = getattr(L, p + "grid_create")
+        self._create.restype = ctypes.c_void_p
+        self._create.argtypes = [_P(Cfg)]
+        self._destroy = getattr(L, p + "grid_destroy")
+        self._destroy.argtypes = [ctypes.c_void_p]
+        self._threads = getattr(L, p + "grid_set_threads")
+        self._threads.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        self._set = getattr(L, p + "grid_set_state")
+        self._set.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._get = getattr(L, p + "grid_get_state")
+        self._get.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._step = getattr(L, p + "grid_step")
+        self._step.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
+                               _P(ctypes.c_int32)]
+        self._run = getattr(L, p + "grid_run")
+        self._run.restype = ctypes.c_int64
+        self._run.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int64, _DP, _DP]
+        self._last_error = getattr(L, p + "last_error")
+        self._last_error.restype = ctypes.c_char_p
+        if kind == "port":
+            self._ref1d = L.oracle_reference_1d
+            self._ref1d.restype = ctypes.c_int32
+            self._ref1d.argtypes = [ctypes.c_int32, ctypes.c_int32, _D, _D, _DP]
+
+    def last_error(self) -> str:
+        return self._last_error().decode()
+
+    def face_flux(self, solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0):
+        """neg, pos: (n, 8); bg: (n, 3) or None.  Returns flux (n, 8), speed (n,), flags (n,)."""
+        neg = np.ascontiguousarray(neg, dtype=np.float64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        n = neg.shape[0]
+        flux = np.zeros((n, 8))
+        speed = np.zeros(n)
+        flags = np.zeros(n, dtype=np.uint32)
+        bgp = None
+        if bg is not None:
+            bg = np.ascontiguousarray(bg, dtype=np.float64)
+            bgp = bg.ctypes.data_as(_DP)
+        self._face_flux(solver, n, neg.ctypes.data_as(_DP), pos.ctypes.data_as(_DP), bgp, gamma, mu0,
+                        flux.ctypes.data_as(_DP), speed.ctypes.data_as(_DP),
+                        flags.ctypes.data_as(_P(ctypes.c_uint32)))
+        return flux, speed, flags
+
+    def reference_1d(self, solver, cells=1002, t_end=1.0, length=1e5):
+        out = np.zeros((cells, 8))
+        steps = self._ref1d(solver, cells, t_end, length, out.ctypes.data_as(_DP))
+        if steps < 0:
+            raise RuntimeError(self.last_error())
+        return out, steps
+
+    def grid(self, cfg: Cfg, threads: int = 1) -> "OracleGrid":
+        return OracleGrid(self, cfg, threads)
+
+
+class OracleGrid:
+    """A Mode C grid in the oracle; state arrays are (8, nz, ny, nx)."""
+
+    def __init__(self, oracle: Oracle, cfg: Cfg, threads: int = 1):
+        self.o = oracle
+        self.cfg = cfg
+        self.shape = (cfg.n[2], cfg.n[1], cfg.n[0])
+        self.h = oracle._create(ctypes.byref(cfg))
+        if not self.h:
+            raise ValueError(oracle.last_error())
+        oracle._threads(self.h, threads)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.o._destroy(h)
+            self.h = None
+
+    def set_state(self, U):
+        ptrs, keep = _soa_in([U[k].reshape(-1) for k in range(8)])
+        rc = self.o._set(self.h, ptrs)
+        if rc != 0:
+            raise ValueError(self.o.last_error())
+
+    def get_state(self):
+        U = np.zeros((8,) + self.shape)
+        ptrs = (ctypes.c_void_p * 8)()
+        for k in range(8):
+            ptrs[k] = U[k].ctypes.data
+        self.o._get(self.h, ptrs)
+        return U
+
+    def step(self, max_dt):
+        """Returns (dt, flag, cell, dir); flag != 0 when a face failed (state not updated)."""
+        dt = ctypes.c_double(0)
+        flag = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.o._step(self.h, max_dt, ctypes.byref(dt), ctypes.byref(flag), cell, ctypes.byref(d))
+        if rc not in (0, 3):
+            raise ValueError(self.o.last_error())
+        return dt.value, flag.value, tuple(cell), d.value
+
+    def run(self, t_start, t_end, max_steps):
+        hist = np.zeros(max_steps)
+        t = ctypes.c_double(0)
+        steps = self.o._run(self.h, t_start, t_end, max_steps, ctypes.byref(t), hist.ctypes.data_as(_DP))
+        if steps < 0:
+            raise RuntimeError(self.o.last_error())
+        return t.value, hist[:steps]

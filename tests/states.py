@@ -1,0 +1,181 @@
+"""Seeded MHD states and grids shared by the tests, the fixture generator and
+the benchmark inputs (numpy only)."""
+from __future__ import annotations
+
+import numpy as np
+
+GAMMA_53 = 5.0 / 3.0
+
+
+def energy(rho, v, p, B, gamma, mu0=1.0):
+    """Total energy density from primitives (get_total_energy_density, mhd/common.hpp:258)."""
+    return p / (gamma - 1) + 0.5 * rho * (v ** 2).sum(axis=0) + 0.5 / mu0 * (B ** 2).sum(axis=0)
+
+
+def random_face_states(n, rng, gamma=GAMMA_53, spread=1.0):
+    """(n, 8) conservative states: rho in [0.1, 3], |v| ~ N(0, spread), B ~ N(0, 1), p in [0.05, 2]."""
+    rho = rng.uniform(0.1, 3.0, n)
+    v = rng.normal(0.0, spread, (3, n))
+    B = rng.normal(0.0, 1.0, (3, n))
+    p = rng.uniform(0.05, 2.0, n)
+    s = np.zeros((n, 8))
+    s[:, 0] = rho
+    s[:, 1:4] = (v * rho).T
+    s[:, 4] = energy(rho, v, p, B, gamma)
+    s[:, 5:8] = B.T
+    return s
+
+
+def nearby_face_states(n, rng, gamma=GAMMA_53, jump=0.05):
+    """Pairs of states that differ by a few percent: the smooth-flow regime of a resolved run."""
+    a = random_face_states(n, rng, gamma)
+    rho = a[:, 0] * (1 + jump * rng.normal(size=n)).clip(0.5, 1.5)
+    v = a[:, 1:4] / a[:, 0:1] + jump * rng.normal(size=(n, 3))
+    B = a[:, 5:8] + jump * rng.normal(size=(n, 3))
+    p_a = (gamma - 1) * (a[:, 4] - 0.5 * (a[:, 1:4] ** 2).sum(1) / a[:, 0] - 0.5 * (a[:, 5:8] ** 2).sum(1))
+    p = p_a * (1 + jump * rng.normal(size=n)).clip(0.5, 1.5)
+    b = np.zeros_like(a)
+    b[:, 0] = rho
+    b[:, 1:4] = v * rho[:, None]
+    b[:, 4] = energy(rho, v.T, p, B.T, gamma)
+    b[:, 5:8] = B
+    return a, b
+
+
+def edge_case_face_states(gamma=GAMMA_53):
+    """Hand-made face problems covering the branches of the four solvers."""
+    def st(rho, v, p, B):
+        v = np.asarray(v, float)
+        B = np.asarray(B, float)
+        return np.array([rho, *(rho * v), energy(rho, v[:, None], p, B[:, None], gamma)[0], *B])
+
+    cases = [
+        # Brio-Wu interface (gamma 2 in the config; here the library gamma)
+        (st(1.0, [0, 0, 0], 1.0, [0.75, 1, 0]), st(0.125, [0, 0, 0], 0.1, [0.75, -1, 0])),
+        # identical states
+        (st(1.0, [0.3, -0.2, 0.1], 0.5, [0.4, 0.2, -0.1]),) * 2,
+        # no field at all: fast speed = sound speed
+        (st(1.0, [0.1, 0, 0], 1.0, [0, 0, 0]), st(0.5, [-0.1, 0, 0], 0.4, [0, 0, 0])),
+        # zero normal field: HLLD double-star states collapse, Roe sign branch
+        (st(1.0, [0.0, 0.5, 0], 1.0, [0, 1, 0.5]), st(0.8, [0.0, -0.5, 0], 0.8, [0, -1, 0.2])),
+        # purely normal field
+        (st(1.0, [0.2, 0, 0], 1.0, [1.0, 0, 0]), st(0.9, [0.1, 0, 0], 0.9, [1.0, 0, 0])),
+        # supersonic to +x and to -x (upwind returns)
+        (st(1.0, [20.0, 0.1, 0], 1.0, [0.5, 0.2, 0]), st(0.9, [19.0, 0.0, 0], 0.9, [0.5, 0.1, 0])),
+        (st(1.0, [-20.0, 0.1, 0], 1.0, [0.5, 0.2, 0]), st(0.9, [-19.0, 0.0, 0], 0.9, [0.5, 0.1, 0])),
+        # strong shear
+        (st(1.0, [0.0, 5.0, -3.0], 1.0, [0.3, 2.0, 1.0]), st(1.0, [0.0, -5.0, 3.0], 1.0, [0.3, -2.0, -1.0])),
+        # strong rarefaction
+        (st(1.0, [-2.0, 0, 0], 1.0, [0.5, 0.5, 0]), st(1.0, [2.0, 0, 0], 1.0, [0.5, 0.5, 0])),
+        # tiny pressure, strong field
+        (st(1.0, [0.1, 0, 0], 1e-4, [3.0, 4.0, 0]), st(1.0, [0.0, 0, 0], 1e-4, [3.0, 3.5, 0])),
+    ]
+    neg = np.array([c[0] for c in cases])
+    pos = np.array([c[-1] for c in cases])
+    # invalid inputs: negative density, negative pressure, NaN momentum
+    bad_neg = neg[:3].copy()
+    bad_pos = pos[:3].copy()
+    bad_neg[0, 0] = -1.0
+    bad_pos[1, 4] = 0.5 * (bad_pos[1, 1:4] ** 2).sum() / bad_pos[1, 0] + 0.5 * (bad_pos[1, 5:8] ** 2).sum() - 0.01
+    bad_neg[2, 1] = np.nan
+    return np.vstack([neg, bad_neg]), np.vstack([pos, bad_pos])
+
+
+def orszag_tang(n, gamma=GAMMA_53):
+    """Orszag-Tang vortex on [0,1]^2 with n x n cells (rho 25/(36 pi), p 5/(12 pi), mu0 = 1).
+    Returns (8, 1, n, n)."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="xy")  # arrays indexed [y, x]
+    rho = np.full_like(X, 25.0 / (36.0 * np.pi))
+    p = np.full_like(X, 5.0 / (12.0 * np.pi))
+    v = np.stack([-np.sin(2 * np.pi * Y), np.sin(2 * np.pi * X), np.zeros_like(X)])
+    B = np.stack([-np.sin(2 * np.pi * Y), np.sin(4 * np.pi * X), np.zeros_like(X)]) / np.sqrt(4 * np.pi)
+    U = np.zeros((8, 1, n, n))
+    U[0, 0] = rho
+    U[1:4, 0] = v * rho
+    U[4, 0] = energy(rho, v, p, B, gamma)
+    U[5:8, 0] = B
+    return U
+
+
+def brio_wu(n=1000, gamma=2.0):
+    """Brio-Wu shock tube on [0,1] with n cells; returns (8, 1, 1, n) and the two edge states."""
+    x = (np.arange(n) + 0.5) / n
+    left = x < 0.5
+    rho = np.where(left, 1.0, 0.125)
+    p = np.where(left, 1.0, 0.1)
+    v = np.zeros((3, n))
+    B = np.stack([np.full(n, 0.75), np.where(left, 1.0, -1.0), np.zeros(n)])
+    U = np.zeros((8, 1, 1, n))
+    U[0, 0, 0] = rho
+    U[4, 0, 0] = energy(rho, v, p, B, gamma)
+    U[5:8, 0, 0] = B
+    return U
+
+
+def smooth_3d(shape, rng, gamma=GAMMA_53, amp=0.1):
+    """Smooth periodic 3-D state (8, nz, ny, nx): a few random Fourier modes on a uniform background."""
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz) / nz, np.arange(ny) / ny, np.arange(nx) / nx, indexing="ij")
+
+    def field(base):
+        f = np.full(shape, base, float)
+        for _ in range(3):
+            k = rng.integers(-2, 3, 3)
+            ph = rng.uniform(0, 2 * np.pi)
+            f += amp * rng.normal() * np.cos(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + ph)
+        return f
+
+    rho = field(1.0)
+    p = field(0.6)
+    v = np.stack([field(0.1), field(-0.05), field(0.02)])
+    B = np.stack([field(0.5), field(0.3), field(-0.2)])
+    U = np.zeros((8,) + tuple(shape))
+    U[0] = rho
+    U[1:4] = v * rho
+    U[4] = energy(rho, v, p, B, gamma)
+    U[5:8] = B
+    return U
+
+
+def blast_wave(n, seed=20261203, gamma=GAMMA_53, amp=0.01, kmax=8):
+    """Magnetised blast wave on [-0.5, 0.5]^3 with n^3 cells: rho 1, p 0.1 (10 inside r < 0.1),
+    B0 = (1, 1, 0)/sqrt(2) plus a divergence-free perturbation dB = curl A built from random-phase
+    modes with integer wavenumbers |k| in [1, kmax] (2 pi units), scaled so rms|dB| = amp |B0|.
+    Returns (8, n, n, n) float64."""
+    rng = np.random.default_rng(seed)
+    c = (np.arange(n) + 0.5) / n - 0.5
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    B0 = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
+    dB = np.zeros((3, n, n, n))
+    modes = []
+    for kx in range(-kmax, kmax + 1):
+        for ky in range(-kmax, kmax + 1):
+            for kz in range(0, kmax + 1):
+                k2 = kx * kx + ky * ky + kz * kz
+                if 1 <= k2 <= kmax * kmax and (kz > 0 or ky > 0 or (ky == 0 and kx > 0)):
+                    modes.append((kx, ky, kz))
+    sel = rng.choice(len(modes), size=min(48, len(modes)), replace=False)
+    for m in sel:
+        k = 2 * np.pi * np.array(modes[m], float)
+        a = rng.normal(size=3)
+        a -= k * (a @ k) / (k @ k)  # transverse amplitude
+        ph = rng.uniform(0, 2 * np.pi)
+        arg = k[0] * X + k[1] * Y + k[2] * Z + ph
+        # A = a cos(k.x + ph)  ->  curl A = -sin(k.x + ph) (k x a)
+        kxa = np.cross(k, a)
+        s = np.sin(arg)
+        for d in range(3):
+            dB[d] -= kxa[d] * s
+    rms = np.sqrt((dB ** 2).sum(0).mean())
+    dB *= amp * np.linalg.norm(B0) / rms
+    B = B0[:, None, None, None] + dB
+    rho = np.ones((n, n, n))
+    r = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
+    p = np.where(r < 0.1, 10.0, 0.1)
+    v = np.zeros((3, n, n, n))
+    U = np.zeros((8, n, n, n))
+    U[0] = rho
+    U[4] = energy(rho, v, p, B, gamma)
+    U[5:8] = B
+    return U

@@ -1,0 +1,210 @@
+"""Pins the CPU oracle to the reference (CPU only).
+
+The oracle (oracle/mhd_oracle.hpp, oracle/mode_c.hpp) restates the
+reference's solvers and step.  These tests hold it to:
+  - the fixtures in tests/golden, made by tests/golden/make_golden.py from
+    the reference's own solver headers and its tests/mhd/reference.cpp;
+  - the live reference build (oracle/_ref) where the reference tree exists;
+  - the reference's shipped goldens tests/mhd/mhd_{rusanov,hll_athena}.ref at
+    the reference's own tolerance (tests/mhd/reference.cpp:637-640);
+  - rotation symmetry, the property mhd_diff.py --rotate checks.
+Bit-for-bit equality is required wherever both sides run the same
+arithmetic (the oracle is built with -ffp-contract=off, as the reference).
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+import states
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+REF_TESTS = "/root/reference/tests/mhd"
+
+
+def _load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_face_flux_matches_reference_fixture(port, solver):
+    g = _load("face_flux.npz")
+    flux, speed, flags = port.face_flux(po.SOLVERS[solver], g["neg"], g["pos"], g["bg"])
+    np.testing.assert_array_equal(flags, g[f"{solver}_flags"])
+    np.testing.assert_array_equal(flux, g[f"{solver}_flux"])
+    np.testing.assert_array_equal(speed, g[f"{solver}_speed"])
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_face_flux_matches_live_reference(port, ref, solver):
+    rng = np.random.default_rng(7)
+    neg = states.random_face_states(4000, rng)
+    pos = states.random_face_states(4000, rng)
+    a, b = states.nearby_face_states(4000, rng)
+    neg = np.vstack([neg, a])
+    pos = np.vstack([pos, b])
+    bg = rng.normal(0, 0.3, (neg.shape[0], 3))
+    for mu0 in (1.0, 4e-7 * np.pi):
+        scale = np.ones(8)
+        if mu0 != 1.0:
+            scale[5:8] = np.sqrt(mu0)  # same Alfven speeds in SI field units
+        f1, s1, g1 = port.face_flux(po.SOLVERS[solver], neg * scale, pos * scale, bg * scale[5:8], 5 / 3, mu0)
+        f2, s2, g2 = ref.face_flux(po.SOLVERS[solver], neg * scale, pos * scale, bg * scale[5:8], 5 / 3, mu0)
+        np.testing.assert_array_equal(g1, g2)
+        np.testing.assert_array_equal(f1, f2)
+        np.testing.assert_array_equal(s1, s2)
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena"])
+def test_reference_1d_matches_reference_program(port, solver):
+    out, steps = port.reference_1d(po.SOLVERS[solver])
+    assert steps == {"rusanov": 944, "hll_athena": 945}[solver]
+    np.testing.assert_array_equal(out, _load("ref1d.npz")[solver])
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena"])
+def test_reference_1d_matches_shipped_golden(port, solver):
+    path = os.path.join(REF_TESTS, f"mhd_{solver}.ref")
+    if not os.path.exists(path):
+        pytest.skip("reference tree not present")
+    gold = np.loadtxt(path)
+    out, _ = port.reference_1d(po.SOLVERS[solver])
+    # verify_mhd: relative error <= 1e-6 where either value exceeds 1e-25 (reference.cpp:637-742)
+    big = (out > 1e-25) | (gold > 1e-25)
+    rel = np.abs(out - gold) / np.maximum(np.abs(out), np.abs(gold)).clip(1e-300)
+    assert rel[big].max() <= 1e-6
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena"])
+def test_reference_program_passes_its_own_golden(solver):
+    if not (os.path.exists(po.REF_EXE) and os.path.isdir(REF_TESTS)):
+        pytest.skip("reference build not present")
+    r = subprocess.run([po.REF_EXE, "--solver", solver], cwd=REF_TESTS, capture_output=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+
+
+def _run(o, key, solver):
+    rng = np.random.default_rng(20261203 + 1)
+    if key == "periodic":
+        U0 = states.smooth_3d((4, 5, 6), rng)
+        cfg = po.make_cfg((6, 5, 4), solver, (1 / 6, 1 / 5, 1 / 4), 5 / 3, 1.0, 0.4)
+        steps, max_dt = 4, 1.0
+    elif key == "bounded":
+        U0 = states.smooth_3d((4, 5, 6), rng)
+        inflow = np.array([1.2, 0.3 * 1.2, 0.2 * 1.2, 0.0,
+                           states.energy(1.2, np.array([[0.3], [0.2], [0.0]]), 0.7,
+                                         np.array([[0.4], [0.1], [-0.2]]), 5 / 3)[0], 0.4, 0.1, -0.2])
+        cfg = po.make_cfg((6, 5, 4), solver, (0.2, 0.25, 0.3), 5 / 3, 1.0, 0.4,
+                          bc_lo=(po.BC_COPY, po.BC_VALUE, po.BC_PERIODIC),
+                          bc_hi=(po.BC_COPY, po.BC_COPY, po.BC_PERIODIC), value_lo=[None, inflow, None])
+        steps, max_dt = 4, 1.0
+    else:
+        U0 = states.brio_wu(64)
+        cfg = po.make_cfg((64, 1, 1), solver, (1 / 64, 1, 1), 2.0, 1.0, 0.5,
+                          bc_lo=(po.BC_COPY, 0, 0), bc_hi=(po.BC_COPY, 0, 0))
+        steps, max_dt = 12, 0.1
+    g = o.grid(cfg)
+    g.set_state(U0)
+    traj, dts = [U0], []
+    for _ in range(steps):
+        dt, flag, _, _ = g.step(max_dt)
+        if flag:
+            break
+        dts.append(dt)
+        traj.append(g.get_state())
+    return np.array(traj), np.array(dts)
+
+
+@pytest.mark.parametrize("key,solver", [("periodic", s) for s in po.SOLVERS]
+                         + [("bounded", "hll_athena"), ("bounded", "hlld_athena")]
+                         + [("briowu", s) for s in po.SOLVERS])
+def test_mode_c_matches_reference_fixture(port, key, solver):
+    g = _load("mode_c.npz")
+    traj, dts = _run(port, key, po.SOLVERS[solver])
+    np.testing.assert_array_equal(dts, g[f"{key}_{solver}_dt"])
+    np.testing.assert_array_equal(traj, g[f"{key}_{solver}_traj"])
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+@pytest.mark.parametrize("axis", [1, 2])
+def test_mode_c_rotation_symmetry(port, solver, axis):
+    """A 1-D tube along y or z equals the tube along x with vector components rotated
+    (get_rotated_vector, mhd/common.hpp:612), bit for bit."""
+    n = 48
+    Ux = states.brio_wu(n)
+    ext = [1, 1, 1]
+    ext[axis] = n
+    lens = [1.0, 1.0, 1.0]
+    lens[axis] = 1 / n
+    perm = {1: [2, 0, 1], 2: [1, 2, 0]}[axis]  # component c of the rotated tube = component perm[c] of x
+    U = np.zeros((8, ext[2], ext[1], ext[0]))
+    line = Ux[:, 0, 0, :]
+    for c in range(3):
+        U[1 + c].reshape(-1)[:] = line[1 + perm[c]]
+        U[5 + c].reshape(-1)[:] = line[5 + perm[c]]
+    U[0].reshape(-1)[:] = line[0]
+    U[4].reshape(-1)[:] = line[4]
+    bc_lo = [0, 0, 0]
+    bc_hi = [0, 0, 0]
+    cfg_x = po.make_cfg((n, 1, 1), po.SOLVERS[solver], (1 / n, 1, 1), 2.0, 1.0, 0.5,
+                        bc_lo=(po.BC_COPY, 0, 0), bc_hi=(po.BC_COPY, 0, 0))
+    bc_lo[axis] = po.BC_COPY
+    bc_hi[axis] = po.BC_COPY
+    cfg_r = po.make_cfg(ext, po.SOLVERS[solver], lens, 2.0, 1.0, 0.5, bc_lo=bc_lo, bc_hi=bc_hi)
+    gx, gr = port.grid(cfg_x), port.grid(cfg_r)
+    gx.set_state(Ux)
+    gr.set_state(U)
+    for _ in range(8):
+        dx = gx.step(0.1)
+        dr = gr.step(0.1)
+        assert dx[0] == dr[0] and dx[1] == dr[1]
+        if dx[1]:
+            break
+        a = gx.get_state()[:, 0, 0, :]
+        b = gr.get_state().reshape(8, -1)
+        for c in range(3):
+            np.testing.assert_array_equal(b[1 + c], a[1 + perm[c]])
+            np.testing.assert_array_equal(b[5 + c], a[5 + perm[c]])
+        np.testing.assert_array_equal(b[[0, 4]], a[[0, 4]])
+
+
+def test_mode_c_threads_do_not_change_bits(port):
+    rng = np.random.default_rng(3)
+    U0 = states.smooth_3d((16, 12, 10), rng)
+    cfg = po.make_cfg((10, 12, 16), po.HLLD, (0.1, 0.1, 0.1), 5 / 3, 1.0, 0.4)
+    a, b = port.grid(cfg, threads=1), port.grid(cfg, threads=4)
+    a.set_state(U0)
+    b.set_state(U0)
+    for _ in range(3):
+        assert a.step(1.0)[0] == b.step(1.0)[0]
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+
+
+def test_mode_c_conserves_totals_on_periodic_grid(port):
+    rng = np.random.default_rng(4)
+    U0 = states.smooth_3d((8, 8, 8), rng)
+    cfg = po.make_cfg((8, 8, 8), po.HLLD, (1 / 8, 1 / 8, 1 / 8), 5 / 3, 1.0, 0.4)
+    g = port.grid(cfg)
+    g.set_state(U0)
+    for _ in range(5):
+        g.step(1.0)
+    U = g.get_state()
+    t0 = U0.reshape(8, -1).sum(1)
+    t1 = U.reshape(8, -1).sum(1)
+    scale = np.abs(U0).reshape(8, -1).sum(1)
+    assert np.all(np.abs(t1 - t0) <= 1e-13 * scale)
+
+
+def test_invalid_state_reports_first_failing_face(port):
+    rng = np.random.default_rng(5)
+    U0 = states.smooth_3d((4, 4, 4), rng)
+    U0[4, 2, 1, 3] = 0.0  # negative pressure in cell (x=3, y=1, z=2)
+    cfg = po.make_cfg((4, 4, 4), po.HLLD, (0.25, 0.25, 0.25), 5 / 3, 1.0, 0.4)
+    g = port.grid(cfg)
+    g.set_state(U0)
+    dt, flag, cell, d = g.step(0.0)
+    assert flag == 2  # PAMHD_FLAG_PRESSURE
+    # first face in x-fastest cell order touching the bad cell: the +z face of (3, 1, 1)
+    assert cell == (3, 1, 1) and d == 3
