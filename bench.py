@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the fused FP64 finite-volume MHD step on B200.
+
+Workload (one line of JSON on rank 0): the 3-D magnetised blast wave,
+256^3 periodic cells on [-0.5, 0.5]^3, gamma 5/3, mu0 1, HLLD, CFL 0.4:
+rho 1, p 0.1 (10 inside r < 0.1), B0 = (1, 1, 0)/sqrt(2) plus a seeded
+random-phase divergence-free perturbation of 1% over wavenumbers 1-8.
+A step is one pass of the fused kernel over all 256^3 cells.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value    cell-updates/s, K steps with the state resident in HBM, timed by
+         CUDA events on the context's stream (max over ranks; N ranks run
+         N independent 256^3 boxes: weak scaling, no collective in the step)
+e2e      the same metric through the C ABI with host buffers: set_state
+         from pinned host arrays, K steps, get_state back, all timed
+roofline achieved HBM GB/s at the algorithmic 128 B per cell-update (8 FP64
+         values read, 8 written) over the mean kernel duration, against the
+         measured copy bandwidth
+cpu_baseline  the reference's own solver code (oracle/_ref, compiled from
+         the reference headers) on the host cores, on a bounded sample
+--impl reference  that CPU path alone, timed per step on the sample
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "HLLD FP64 cell-updates/s at 256³ (% HBM peak); batched vs plain; adjoint/fwd cost"
+UNIT = "cell-updates/s"
+T_END = 1e30
+BYTES_PER_CELL_UPDATE = 128  # 8 FP64 read + 8 FP64 written
+CFL = 0.4
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--n", type=int, default=256, help="cells per dimension")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(n):
+    return {
+        "workload": f"3-D magnetised blast wave, {n}^3 periodic, gamma 5/3, HLLD, CFL {CFL}, FP64",
+        "cells": n ** 3,
+        "solver": "hlld_athena",
+        "inputs": "synthetic seeded (seed 20261203): rho 1, p 0.1 / 10 in r<0.1, B0 (1,1,0)/sqrt2 + 1% dB",
+        "l2": f"state {8 * 8 * n ** 3 / 1e9:.2f} GB per copy > 126 MB L2: no flush needed",
+    }
+
+
+def blast_state(n):
+    import states
+    return states.blast_wave(n)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(n):
+    """dram bytes per launch of the step kernel from the committed ncu summary, scaled to n^3."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "step_kernel_hlld":
+                cells, dram = float(parts[1]), float(parts[2])
+                return dram * (n ** 3) / cells
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons with NVML while the timed region runs."""
+
+    def __init__(self, device):
+        self.samples, self.reasons = [], set()
+        self.stop = threading.Event()
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+        self.t = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        if self.nv is None:
+            return
+        names = {
+            0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+            0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown",
+        }
+        while not self.stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in names.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def __enter__(self):
+        self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.t.join()
+
+    def summary(self):
+        return {
+            "sm_mhz": float(np.median(self.samples)) if self.samples else None,
+            "sm_max_mhz": self.max_mhz,
+            "reasons": sorted(self.reasons),
+            "samples": len(self.samples),
+        }
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_sample_run(U_full, n, planes, steps, threads):
+    """Times `steps` HLLD steps of the reference solver code (oracle/_ref) on a periodic slab of
+    `planes` z-planes of the workload's initial state, after one priming step."""
+    from oracle import pyoracle as po
+    kind = "reference"
+    try:
+        o = po.Oracle("reference")
+    except Exception:
+        o = po.Oracle("port")
+        kind = "port"
+    z0 = (n - planes) // 2
+    U = np.ascontiguousarray(U_full[:, z0:z0 + planes])
+    cfg = po.make_cfg((n, n, planes), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL)
+    g = o.grid(cfg, threads=threads)
+    g.set_state(U)
+    g.step(1.0)  # priming
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt, flag, _, _ = g.step(T_END)
+        if flag:
+            raise RuntimeError("CPU sample failed")
+    el = time.perf_counter() - t0
+    return n * n * planes * steps / el, kind, el
+
+
+def cpu_baseline(U_full, n):
+    threads = cpu_threads()
+    planes = 16
+    rate, kind, el = cpu_sample_run(U_full, n, planes, 1, threads)
+    # aim at ~10 s of wall time (not more than 8 steps)
+    steps = int(max(1, min(8, 10.0 / max(el, 1e-3))))
+    rate, kind, el = cpu_sample_run(U_full, n, planes, steps, threads)
+    return {
+        "value": rate,
+        "unit": UNIT,
+        "cores": threads,
+        "kind": kind,
+        "sample": f"{steps} HLLD steps on a {n}x{n}x{planes} periodic slab of the blast initial state "
+                  f"({el:.1f} s wall on {threads} threads, std::thread over cells)",
+    }
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def run_reference(a):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    n = a.n
+    U = blast_state(n)
+    threads = cpu_threads()
+    planes = 16
+    from oracle import pyoracle as po
+    kind = "reference"
+    try:
+        o = po.Oracle("reference")
+    except Exception:
+        o = po.Oracle("port")
+        kind = "port"
+    z0 = (n - planes) // 2
+    Us = np.ascontiguousarray(U[:, z0:z0 + planes])
+    cfg = po.make_cfg((n, n, planes), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL)
+    g = o.grid(cfg, threads=threads)
+    g.set_state(Us)
+    for _ in range(a.warmup):
+        g.step(T_END)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        dt, flag, _, _ = g.step(T_END)
+        if flag:
+            raise RuntimeError("reference step failed")
+    el = time.perf_counter() - t0
+    value = n * n * planes * a.steps / el
+    sample = f"each step: one HLLD step on a {n}x{n}x{planes} periodic slab of the blast initial state"
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": dict(workload(n), sample=sample),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(a):
+    import torch
+    import pamhd_b200 as pg
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    n = a.n
+    U = blast_state(n)
+    cells = n ** 3
+    cfg = pg.Config(n=(n, n, n), solver=pg.HLLD, cell_length=(1 / n,) * 3, adiabatic_index=5 / 3,
+                    vacuum_permeability=1.0, time_step_factor=CFL, device=local)
+    ctx = pg.Context(cfg)
+
+    # pinned host buffers for the end-to-end measurement
+    host_in = torch.from_numpy(U.reshape(8, -1)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # ---- device-resident throughput
+    ctx.set_state(host_in.numpy().reshape(U.shape))
+    ctx.steps(a.warmup, T_END)
+    ctx.sync()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        ctx.steps(a.steps, T_END)
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ctx.sync()  # raises if any face met an invalid state
+    ms = max_over_ranks(start.elapsed_time(end))
+    t_sim, nsteps, _ = ctx.time()
+    value = world * cells * a.steps / (ms / 1e3)
+    kernel_ms = ms / a.steps  # one fused kernel per step (periodic grid: no boundary kernel)
+
+    # ---- end to end through the C ABI with host buffers
+    ptr_in = [host_in[k].data_ptr() for k in range(8)]
+    ptr_out = [host_out[k].data_ptr() for k in range(8)]
+    L = pg.lib()
+    barrier()
+    torch.cuda.synchronize()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    rc = L.pamhd_gpu_set_state(ctx.h, pg._pointers(ptr_in))
+    assert rc == 0, rc
+    ctx.steps(a.steps, T_END)
+    rc = L.pamhd_gpu_get_state(ctx.h, pg._pointers(ptr_out))
+    assert rc == 0, rc
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e_ms = max_over_ranks(e_start.elapsed_time(e_end))
+    e2e = world * cells * a.steps / (e_ms / 1e3)
+    state_bytes = 8 * 8 * cells
+
+    peak, peak_kind = peaks()
+    achieved = BYTES_PER_CELL_UPDATE * cells / (kernel_ms / 1e3) / 1e9
+    traffic = ncu_traffic(n)
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": a.steps,
+        "warmup": a.warmup,
+        "ms_per_step": ms / a.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": dict(workload(n), parallelism=f"{world} independent {n}^3 boxes, one per GPU",
+                       simulated_time=t_sim, steps_on_context=nsteps),
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": traffic,
+            "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+            "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
+            "kernel_ms": kernel_ms,
+        },
+        "e2e": {
+            "value": e2e,
+            "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes / a.steps,
+            "d2h_bytes_per_step": state_bytes / a.steps,
+            "what": f"set_state from pinned host arrays + {a.steps} steps + get_state to pinned host arrays "
+                    f"({state_bytes / 1e9:.2f} GB each way per run, amortised per step)",
+        },
+        "gpu_launches": a.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(U, n)
+        except Exception as e:  # a missing oracle build must not hide the GPU number
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable",
+                                    "sample": str(e)}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_b200(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

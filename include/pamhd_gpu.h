@@ -169,6 +169,13 @@ pamhd_gpu_time() to collect the result.
 */
 int pamhd_gpu_steps(pamhd_ctx* ctx, int32_t nsteps, double t_end);
 
+/*
+The CUDA stream (a cudaStream_t) every kernel of the context runs on, so
+that callers can order their own work with it or time it with CUDA events.
+No reference counterpart (the reference has no device streams).
+*/
+int pamhd_gpu_get_stream(pamhd_ctx* ctx, void** stream);
+
 /* Waits for the context's stream; returns PAMHD_ERR_PHYSICS if a face failed. */
 int pamhd_gpu_sync(pamhd_ctx* ctx);
 

@@ -1,0 +1,274 @@
+"""Python binding of the B200 finite-volume MHD step (libpamhd_gpu.so).
+
+Every call goes through the C ABI of include/pamhd_gpu.h; there is no
+Python or CPU implementation of the step here.  If the library is missing
+the import of a context fails loudly (build it with `python -m
+pamhd_b200.build`).
+
+    from pamhd_b200 import Context, Config, HLLD
+    ctx = Context(Config(n=(256, 256, 256), solver=HLLD, cell_length=(1/256,)*3,
+                         adiabatic_index=5/3, vacuum_permeability=1.0, time_step_factor=0.4))
+    ctx.set_state(U)            # (8, nz, ny, nx) float64: rho, mom xyz, E, B xyz
+    ctx.step(0.0)               # dt = 0 priming step, as tests/mhd/test.cpp:462
+    ctx.steps(200, t_end=1e9)   # 200 steps, no host synchronisation
+    U = ctx.get_state()
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libpamhd_gpu.so")
+
+RUSANOV, RUSANOV_STAGGERED, HLL, HLLD, ROE = 0, 1, 2, 3, 4
+SOLVERS = {"rusanov": RUSANOV, "hll_athena": HLL, "hlld_athena": HLLD, "roe_athena": ROE}
+BC_PERIODIC, BC_COPY, BC_VALUE = 0, 1, 2
+
+OK, ERR_ARGUMENT, ERR_CUDA, ERR_PHYSICS, ERR_STATE, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
+FLAG_DENSITY, FLAG_PRESSURE, FLAG_WAVE_SPEED, FLAG_FLUX = 1, 2, 4, 8
+FLAG_ROE_DENSITY, FLAG_ROE_PRESSURE, FLAG_NEW_STATE, FLAG_TIMEOUT = 16, 32, 64, 128
+
+
+class PamhdError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {errstr(code)} ({code})")
+        self.code = code
+
+
+class PhysicsError(PamhdError):
+    """A face met a state the reference would throw std::domain_error on."""
+
+    def __init__(self, code, what, flags=0, cell=(0, 0, 0), direction=0):
+        super().__init__(code, what)
+        self.flags = flags
+        self.cell = cell
+        self.direction = direction
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int32 * 3),
+        ("solver", ctypes.c_int32),
+        ("cell_length", ctypes.c_double * 3),
+        ("adiabatic_index", ctypes.c_double),
+        ("vacuum_permeability", ctypes.c_double),
+        ("time_step_factor", ctypes.c_double),
+        ("bc_lo", ctypes.c_int32 * 3),
+        ("bc_hi", ctypes.c_int32 * 3),
+        ("value_lo", (ctypes.c_double * 8) * 3),
+        ("value_hi", (ctypes.c_double * 8) * 3),
+        ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+@dataclass
+class Config:
+    """pamhd_cfg of include/pamhd_gpu.h."""
+
+    n: tuple
+    solver: int
+    cell_length: tuple
+    adiabatic_index: float = 5.0 / 3.0
+    vacuum_permeability: float = 1.0
+    time_step_factor: float = 0.5
+    bc_lo: tuple = (BC_PERIODIC, BC_PERIODIC, BC_PERIODIC)
+    bc_hi: tuple = (BC_PERIODIC, BC_PERIODIC, BC_PERIODIC)
+    value_lo: list = field(default_factory=lambda: [None, None, None])
+    value_hi: list = field(default_factory=lambda: [None, None, None])
+    device: int = 0
+
+    def to_c(self) -> _Cfg:
+        c = _Cfg()
+        for d in range(3):
+            c.n[d] = int(self.n[d])
+            c.cell_length[d] = float(self.cell_length[d])
+            c.bc_lo[d] = int(self.bc_lo[d])
+            c.bc_hi[d] = int(self.bc_hi[d])
+            for k in range(8):
+                c.value_lo[d][k] = 0.0 if self.value_lo[d] is None else float(self.value_lo[d][k])
+                c.value_hi[d][k] = 0.0 if self.value_hi[d] is None else float(self.value_hi[d][k])
+        c.solver = int(self.solver)
+        c.adiabatic_index = float(self.adiabatic_index)
+        c.vacuum_permeability = float(self.vacuum_permeability)
+        c.time_step_factor = float(self.time_step_factor)
+        c.device = int(self.device)
+        c.reserved = 0
+        return c
+
+
+_lib = None
+_P = ctypes.POINTER
+_D = ctypes.c_double
+_DP = _P(ctypes.c_double)
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libpamhd_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m pamhd_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.pamhd_gpu_abi_version.restype = ctypes.c_int
+    L.pamhd_gpu_errstr.restype = ctypes.c_char_p
+    L.pamhd_gpu_errstr.argtypes = [ctypes.c_int]
+    L.pamhd_gpu_create.argtypes = [_P(_Cfg), _P(ctypes.c_void_p)]
+    L.pamhd_gpu_destroy.argtypes = [ctypes.c_void_p]
+    for name in ("pamhd_gpu_set_state", "pamhd_gpu_get_state", "pamhd_gpu_set_state_device",
+                 "pamhd_gpu_get_state_device"):
+        getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.pamhd_gpu_step.argtypes = [ctypes.c_void_p, _D, _DP]
+    L.pamhd_gpu_steps.argtypes = [ctypes.c_void_p, ctypes.c_int32, _D]
+    L.pamhd_gpu_sync.argtypes = [ctypes.c_void_p]
+    L.pamhd_gpu_get_stream.argtypes = [ctypes.c_void_p, _P(ctypes.c_void_p)]
+    L.pamhd_gpu_time.argtypes = [ctypes.c_void_p, _DP, _P(ctypes.c_int64), _DP]
+    L.pamhd_gpu_dt_history.argtypes = [ctypes.c_void_p, _DP, ctypes.c_int32, _P(ctypes.c_int32)]
+    L.pamhd_gpu_status.argtypes = [ctypes.c_void_p, _P(ctypes.c_uint32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
+    L.pamhd_gpu_totals.argtypes = [ctypes.c_void_p, _DP]
+    L.pamhd_gpu_face_flux.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _DP, _DP, _DP, _D, _D,
+                                      _DP, _DP, _P(ctypes.c_uint32)]
+    if L.pamhd_gpu_abi_version() != 1:
+        raise ImportError("libpamhd_gpu.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+def errstr(code: int) -> str:
+    try:
+        return lib().pamhd_gpu_errstr(code).decode()
+    except ImportError:
+        return "unknown"
+
+
+def _pointers(arrays):
+    ptrs = (ctypes.c_void_p * 8)()
+    for k in range(8):
+        ptrs[k] = arrays[k]
+    return ptrs
+
+
+class Context:
+    """A pamhd_ctx: one uniform grid on one GPU."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.L = lib()
+        self.shape = (int(cfg.n[2]), int(cfg.n[1]), int(cfg.n[0]))
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        rc = self.L.pamhd_gpu_create(ctypes.byref(self._c), ctypes.byref(h))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pamhd_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == ERR_PHYSICS:
+            flags, cell, d = self.status()
+            raise PhysicsError(rc, what, flags, cell, d)
+        if rc != OK:
+            raise PamhdError(rc, what)
+
+    def set_state(self, U: np.ndarray):
+        """U: (8, nz, ny, nx) float64 host array."""
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shape)
+        self._check(self.L.pamhd_gpu_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_set_state")
+
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        U = np.empty((8,) + self.shape) if out is None else out
+        self._check(self.L.pamhd_gpu_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_get_state")
+        return U
+
+    def set_state_device(self, ptrs):
+        """ptrs: eight device pointers (ints), e.g. torch tensor data_ptr()s."""
+        self._check(self.L.pamhd_gpu_set_state_device(self.h, _pointers(ptrs)), "pamhd_gpu_set_state_device")
+
+    def get_state_device(self, ptrs):
+        self._check(self.L.pamhd_gpu_get_state_device(self.h, _pointers(ptrs)), "pamhd_gpu_get_state_device")
+
+    def step(self, max_dt: float) -> float:
+        dt = ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_step(self.h, max_dt, ctypes.byref(dt)), "pamhd_gpu_step")
+        return dt.value
+
+    def steps(self, n: int, t_end: float):
+        self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
+
+    def stream(self) -> int:
+        """The cudaStream_t of the context, as an integer handle."""
+        s = ctypes.c_void_p()
+        self._check(self.L.pamhd_gpu_get_stream(self.h, ctypes.byref(s)), "pamhd_gpu_get_stream")
+        return int(s.value or 0)
+
+    def sync(self):
+        self._check(self.L.pamhd_gpu_sync(self.h), "pamhd_gpu_sync")
+
+    def time(self):
+        t, n, dt = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_time(self.h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(dt)),
+                    "pamhd_gpu_time")
+        return t.value, n.value, dt.value
+
+    def dt_history(self, count: int) -> np.ndarray:
+        out = np.zeros(count)
+        w = ctypes.c_int32(0)
+        self._check(self.L.pamhd_gpu_dt_history(self.h, out.ctypes.data_as(_DP), count, ctypes.byref(w)),
+                    "pamhd_gpu_dt_history")
+        return out[: w.value]
+
+    def status(self):
+        f = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.L.pamhd_gpu_status(self.h, ctypes.byref(f), cell, ctypes.byref(d))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_status")
+        return f.value, tuple(cell), d.value
+
+    def totals(self) -> np.ndarray:
+        out = np.zeros(8)
+        self._check(self.L.pamhd_gpu_totals(self.h, out.ctypes.data_as(_DP)), "pamhd_gpu_totals")
+        return out
+
+
+def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
+    """Solver-level entry point (pamhd_gpu_face_flux).  neg, pos: (n, 8); bg: (n, 3) or None.
+    Returns flux (n, 8), speed (n,), flags (n,); failed faces have flags != 0 (no exception)."""
+    L = lib()
+    neg = np.ascontiguousarray(neg, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n = neg.shape[0]
+    flux = np.zeros((n, 8))
+    speed = np.zeros(n)
+    flags = np.zeros(n, dtype=np.uint32)
+    bgp = None
+    if bg is not None:
+        bg = np.ascontiguousarray(bg, dtype=np.float64)
+        bgp = bg.ctypes.data_as(_DP)
+    rc = L.pamhd_gpu_face_flux(device, solver, n, neg.ctypes.data_as(_DP), pos.ctypes.data_as(_DP), bgp,
+                               gamma, mu0, flux.ctypes.data_as(_DP), speed.ctypes.data_as(_DP),
+                               flags.ctypes.data_as(_P(ctypes.c_uint32)))
+    if rc not in (OK, ERR_PHYSICS):
+        raise PamhdError(rc, "pamhd_gpu_face_flux")
+    return flux, speed, flags

@@ -1,0 +1,547 @@
+/*
+Host side of the C ABI in include/pamhd_gpu.h: the context (device
+buffers, stream, CUDA graph) and every exported entry point.
+
+A context owns two copies of the state (ping-pong: a step reads one and
+writes the other), a three-slot ring of speed reductions and clocks, the
+error status and a dt history, all on one device and one stream.  Steps
+are issued without host synchronisation; because the kernel parameters of
+a step depend only on the step index modulo 6 (state parity x ring phase),
+six consecutive steps are captured once into a CUDA graph and replayed.
+*/
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "step.cuh"
+
+using namespace pamhd_b200;
+
+struct pamhd_ctx {
+	pamhd_cfg cfg;
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	Layout L;
+	Step_Params base;
+	double* state[2] = {nullptr, nullptr};
+	int cur = 0;
+	Speed_Max* red = nullptr;
+	Clock* clock = nullptr;
+	Status* status = nullptr;
+	Control* control = nullptr;
+	double* dt_hist = nullptr;
+	int hist_len = 1 << 16;
+	long long steps = 0;
+	double* staging = nullptr;
+	double* partial = nullptr;
+	int partial_blocks = 296;
+	bool needs_boundary_speeds = false;
+	cudaGraphExec_t graph = nullptr;
+	bool loaded = false;
+};
+
+namespace {
+
+constexpr int GRAPH_STEPS = 6;
+
+int check(const cudaError_t e)
+{
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+#define PAMHD_TRY(expr) do { const int rc_ = (expr); if (rc_ != PAMHD_OK) return rc_; } while (0)
+
+int validate(const pamhd_cfg& c)
+{
+	if (c.reserved != 0) return PAMHD_ERR_ARGUMENT;
+	if (c.solver != PAMHD_RUSANOV and c.solver != PAMHD_HLL_ATHENA and c.solver != PAMHD_HLLD_ATHENA
+		and c.solver != PAMHD_ROE_ATHENA) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	for (int d = 0; d < 3; d++) {
+		if (c.n[d] < 1) return PAMHD_ERR_ARGUMENT;
+		if (not (c.cell_length[d] > 0.0) or not std::isfinite(c.cell_length[d])) return PAMHD_ERR_ARGUMENT;
+		for (const int b: {c.bc_lo[d], c.bc_hi[d]}) {
+			if (b != PAMHD_BC_PERIODIC and b != PAMHD_BC_COPY and b != PAMHD_BC_VALUE) return PAMHD_ERR_ARGUMENT;
+		}
+		if (c.n[d] > 1 and ((c.bc_lo[d] == PAMHD_BC_PERIODIC) != (c.bc_hi[d] == PAMHD_BC_PERIODIC))) {
+			return PAMHD_ERR_ARGUMENT;
+		}
+	}
+	// active dimensions must be x, x-y or x-y-z
+	if (c.n[0] < 2) return PAMHD_ERR_ARGUMENT;
+	if (c.n[1] < 2 and c.n[2] > 1) return PAMHD_ERR_ARGUMENT;
+	if (not (c.adiabatic_index > 1.0) or not (c.vacuum_permeability > 0.0) or not (c.time_step_factor > 0.0)) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	return PAMHD_OK;
+}
+
+Layout make_layout(const pamhd_cfg& c)
+{
+	Layout L;
+	for (int d = 0; d < 3; d++) {
+		L.n[d] = c.n[d];
+		L.g[d] = c.n[d] > 1 ? 1 : 0;
+	}
+	L.xoff = 4;  // ghost column at 3: interior rows start 32-byte aligned
+	L.pitch = ((L.xoff + L.n[0] + 1) + 3) / 4 * 4;
+	L.rows = L.n[1] + 2 * L.g[1];
+	L.planes = L.n[2] + 2 * L.g[2];
+	L.plane = (long long)L.pitch * L.rows;
+	L.var = (L.plane * L.planes + 31) / 32 * 32;
+	return L;
+}
+
+void set_params(pamhd_ctx& x)
+{
+	const pamhd_cfg& c = x.cfg;
+	Step_Params& P = x.base;
+	std::memset(&P, 0, sizeof P);
+	P.L = x.L;
+	P.gas.gamma = c.adiabatic_index;
+	P.gas.mu0 = c.vacuum_permeability;
+	P.gas.inv_mu0 = 1.0 / c.vacuum_permeability;
+	P.gas.sqrt_mu0 = std::sqrt(c.vacuum_permeability);
+	P.gas.inv_sqrt_mu0 = 1.0 / std::sqrt(c.vacuum_permeability);
+	P.cfl = c.time_step_factor;
+	x.needs_boundary_speeds = false;
+	int active_count = 0;
+	for (int d = 0; d < 3; d++) {
+		P.len[d] = c.cell_length[d];
+		P.inv_len[d] = 1.0 / c.cell_length[d];
+		P.active[d] = c.n[d] > 1;
+		P.periodic[d] = P.active[d] and c.bc_lo[d] == PAMHD_BC_PERIODIC;
+		P.bc_lo[d] = c.bc_lo[d];
+		P.bc_hi[d] = c.bc_hi[d];
+		P.ext[d] = (P.active[d] and not P.periodic[d]) ? 1 : 0;
+		active_count += P.active[d];
+	}
+	for (int d = 0; d < 3; d++) {
+		if (P.active[d] and not P.periodic[d] and active_count > 1) x.needs_boundary_speeds = true;
+	}
+	P.red = x.red;
+	P.clock = x.clock;
+	P.status = x.status;
+	P.control = x.control;
+	P.dt_hist = x.dt_hist;
+	P.hist_len = x.hist_len;
+	// z planes per block: enough blocks for several waves on 148 SMs, few redundant z faces
+	const int ty = P.active[1] ? 8 : 1;
+	const long long tiles = (long long)((c.n[0] + 31) / 32) * ((c.n[1] + ty - 1) / ty);
+	long long chunks = (2368 + tiles - 1) / tiles;
+	chunks = std::max(1LL, std::min(chunks, (long long)std::max(1, c.n[2] / 16)));
+	P.kchunk = int((c.n[2] + chunks - 1) / chunks);
+}
+
+Step_Params params_for(const pamhd_ctx& x, const long long step, const int cur)
+{
+	Step_Params P = x.base;
+	P.in = x.state[cur];
+	P.out = x.state[cur ^ 1];
+	P.phase = int(step % 3);
+	return P;
+}
+
+int issue_step(pamhd_ctx& x)
+{
+	const Step_Params P = params_for(x, x.steps, x.cur);
+	if (x.needs_boundary_speeds) PAMHD_TRY(launch_boundary_speeds(P, x.cfg.solver, x.stream));
+	PAMHD_TRY(launch_step(P, x.cfg.solver, x.stream));
+	x.cur ^= 1;
+	x.steps++;
+	return PAMHD_OK;
+}
+
+int reset_run_state(pamhd_ctx& x)
+{
+	PAMHD_TRY(check(cudaMemsetAsync(x.red, 0, 3 * sizeof(Speed_Max), x.stream)));
+	PAMHD_TRY(check(cudaMemsetAsync(x.clock, 0, 3 * sizeof(Clock), x.stream)));
+	Status s;
+	s.flags = 0;
+	s.pad = 0;
+	s.first = ~0ull;
+	PAMHD_TRY(check(cudaMemcpyAsync(x.status, &s, sizeof s, cudaMemcpyHostToDevice, x.stream)));
+	x.steps = 0;
+	x.cur = 0;
+	return PAMHD_OK;
+}
+
+int read_status(pamhd_ctx& x, Status& s)
+{
+	PAMHD_TRY(check(cudaMemcpyAsync(&s, x.status, sizeof s, cudaMemcpyDeviceToHost, x.stream)));
+	return check(cudaStreamSynchronize(x.stream));
+}
+
+int set_control(pamhd_ctx& x, const double max_dt, const double t_end)
+{
+	Control c;
+	c.max_dt = max_dt;
+	c.t_end = t_end;
+	PAMHD_TRY(check(cudaMemcpyAsync(x.control, &c, sizeof c, cudaMemcpyHostToDevice, x.stream)));
+	// the copy reads from this stack variable: wait for it
+	return check(cudaStreamSynchronize(x.stream));
+}
+
+int fill_ghosts(pamhd_ctx& x)
+{
+	const Step_Params P = x.base;
+	PAMHD_TRY(launch_fill_ghosts_values(P, x.state[0], x.cfg.value_lo, x.cfg.value_hi, x.stream));
+	return launch_fill_ghosts_values(P, x.state[1], x.cfg.value_lo, x.cfg.value_hi, x.stream);
+}
+
+int capture_graph(pamhd_ctx& x)
+{
+	if (x.graph != nullptr) return PAMHD_OK;
+	cudaGraph_t g = nullptr;
+	PAMHD_TRY(check(cudaStreamBeginCapture(x.stream, cudaStreamCaptureModeThreadLocal)));
+	const long long steps0 = x.steps;
+	const int cur0 = x.cur;
+	int rc = PAMHD_OK;
+	for (int s = 0; s < GRAPH_STEPS and rc == PAMHD_OK; s++) rc = issue_step(x);
+	x.steps = steps0;
+	x.cur = cur0;
+	const cudaError_t e = cudaStreamEndCapture(x.stream, &g);
+	if (rc != PAMHD_OK or e != cudaSuccess) {
+		if (g != nullptr) cudaGraphDestroy(g);
+		return rc != PAMHD_OK ? rc : PAMHD_ERR_CUDA;
+	}
+	const cudaError_t ie = cudaGraphInstantiate(&x.graph, g, 0);
+	cudaGraphDestroy(g);
+	return check(ie);
+}
+
+} // namespace
+
+extern "C" {
+
+int pamhd_gpu_abi_version(void)
+{
+	return PAMHD_GPU_ABI_VERSION;
+}
+
+const char* pamhd_gpu_errstr(const int code)
+{
+	switch (code) {
+	case PAMHD_OK: return "ok";
+	case PAMHD_ERR_ARGUMENT: return "invalid argument or configuration";
+	case PAMHD_ERR_CUDA: return "CUDA runtime error";
+	case PAMHD_ERR_PHYSICS: return "a face met an invalid state (see pamhd_gpu_status)";
+	case PAMHD_ERR_STATE: return "call made in the wrong order";
+	case PAMHD_ERR_TIMEOUT: return "a bounded device wait expired";
+	default: return "unknown error";
+	}
+}
+
+int pamhd_gpu_create(const pamhd_cfg* cfg, pamhd_ctx** out)
+{
+	if (cfg == nullptr or out == nullptr) return PAMHD_ERR_ARGUMENT;
+	*out = nullptr;
+	PAMHD_TRY(validate(*cfg));
+	pamhd_ctx* x = new (std::nothrow) pamhd_ctx;
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	x->cfg = *cfg;
+	x->device = cfg->device;
+	x->L = make_layout(*cfg);
+	auto fail = [&](const int rc) {
+		pamhd_gpu_destroy(x);
+		return rc;
+	};
+	if (cudaSetDevice(x->device) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+	if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+	const size_t state_bytes = size_t(8) * x->L.var * sizeof(double);
+	const size_t cells = size_t(x->L.n[0]) * x->L.n[1] * x->L.n[2];
+	if (cudaMalloc(&x->state[0], state_bytes) != cudaSuccess
+		or cudaMalloc(&x->state[1], state_bytes) != cudaSuccess
+		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
+		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
+		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess
+		or cudaMalloc(&x->control, sizeof(Control)) != cudaSuccess
+		or cudaMalloc(&x->dt_hist, x->hist_len * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->staging, cells * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->partial, 8 * x->partial_blocks * sizeof(double)) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	if (cudaMemsetAsync(x->state[0], 0, state_bytes, x->stream) != cudaSuccess
+		or cudaMemsetAsync(x->state[1], 0, state_bytes, x->stream) != cudaSuccess
+		or cudaMemsetAsync(x->dt_hist, 0, x->hist_len * sizeof(double), x->stream) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	set_params(*x);
+	// kernel attributes are set here, outside any stream capture
+	if (prepare_step_kernels(cfg->solver, cfg->n[1] > 1) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+	if (reset_run_state(*x) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+	if (cudaStreamSynchronize(x->stream) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+	*out = x;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_destroy(pamhd_ctx* x)
+{
+	if (x == nullptr) return PAMHD_OK;
+	cudaSetDevice(x->device);
+	if (x->stream != nullptr) cudaStreamSynchronize(x->stream);
+	if (x->graph != nullptr) cudaGraphExecDestroy(x->graph);
+	cudaFree(x->state[0]);
+	cudaFree(x->state[1]);
+	cudaFree(x->red);
+	cudaFree(x->clock);
+	cudaFree(x->status);
+	cudaFree(x->control);
+	cudaFree(x->dt_hist);
+	cudaFree(x->staging);
+	cudaFree(x->partial);
+	if (x->stream != nullptr) cudaStreamDestroy(x->stream);
+	delete x;
+	return PAMHD_OK;
+}
+
+static int set_state_impl(pamhd_ctx* x, const double* const soa[8], const cudaMemcpyKind kind)
+{
+	if (x == nullptr or soa == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	const size_t bytes = size_t(x->L.n[0]) * x->L.n[1] * x->L.n[2] * sizeof(double);
+	for (int v = 0; v < 8; v++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(x->staging, soa[v], bytes, kind, x->stream)));
+		PAMHD_TRY(launch_scatter(x->staging, x->state[0] + v * x->L.var, x->L, x->stream));
+	}
+	PAMHD_TRY(fill_ghosts(*x));
+	PAMHD_TRY(reset_run_state(*x));
+	x->loaded = true;
+	return check(cudaStreamSynchronize(x->stream));
+}
+
+static int get_state_impl(pamhd_ctx* x, double* const soa[8], const cudaMemcpyKind kind)
+{
+	if (x == nullptr or soa == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	const size_t bytes = size_t(x->L.n[0]) * x->L.n[1] * x->L.n[2] * sizeof(double);
+	for (int v = 0; v < 8; v++) {
+		PAMHD_TRY(launch_gather(x->state[x->cur] + v * x->L.var, x->staging, x->L, x->stream));
+		PAMHD_TRY(check(cudaMemcpyAsync(soa[v], x->staging, bytes, kind, x->stream)));
+	}
+	return check(cudaStreamSynchronize(x->stream));
+}
+
+int pamhd_gpu_set_state(pamhd_ctx* x, const double* const soa[8])
+{
+	return set_state_impl(x, soa, cudaMemcpyHostToDevice);
+}
+
+int pamhd_gpu_get_state(pamhd_ctx* x, double* const soa[8])
+{
+	return get_state_impl(x, soa, cudaMemcpyDeviceToHost);
+}
+
+int pamhd_gpu_set_state_device(pamhd_ctx* x, const double* const soa[8])
+{
+	return set_state_impl(x, soa, cudaMemcpyDeviceToDevice);
+}
+
+int pamhd_gpu_get_state_device(pamhd_ctx* x, double* const soa[8])
+{
+	return get_state_impl(x, soa, cudaMemcpyDeviceToDevice);
+}
+
+int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (not (max_dt >= 0.0)) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(set_control(*x, max_dt, 0.0));
+	PAMHD_TRY(issue_step(*x));
+	Clock c;
+	PAMHD_TRY(check(cudaMemcpyAsync(&c, x->clock + x->steps % 3, sizeof c, cudaMemcpyDeviceToHost, x->stream)));
+	Status s;
+	PAMHD_TRY(read_status(*x, s));
+	if (dt_taken != nullptr) *dt_taken = c.dt;
+	return s.flags != 0 ? PAMHD_ERR_PHYSICS : PAMHD_OK;
+}
+
+int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
+{
+	if (x == nullptr or nsteps < 0) return PAMHD_ERR_ARGUMENT;
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(set_control(*x, -1.0, t_end));
+	int left = nsteps;
+	while (left > 0 and x->steps % GRAPH_STEPS != 0) {
+		PAMHD_TRY(issue_step(*x));
+		left--;
+	}
+	if (left >= GRAPH_STEPS) {
+		PAMHD_TRY(capture_graph(*x));
+		while (left >= GRAPH_STEPS) {
+			PAMHD_TRY(check(cudaGraphLaunch(x->graph, x->stream)));
+			x->steps += GRAPH_STEPS;  // the state parity is unchanged after an even number of steps
+			left -= GRAPH_STEPS;
+		}
+	}
+	while (left > 0) {
+		PAMHD_TRY(issue_step(*x));
+		left--;
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_get_stream(pamhd_ctx* x, void** stream)
+{
+	if (x == nullptr or stream == nullptr) return PAMHD_ERR_ARGUMENT;
+	*stream = static_cast<void*>(x->stream);
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_sync(pamhd_ctx* x)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	Status s;
+	PAMHD_TRY(read_status(*x, s));
+	return s.flags != 0 ? PAMHD_ERR_PHYSICS : PAMHD_OK;
+}
+
+int pamhd_gpu_time(pamhd_ctx* x, double* time, int64_t* steps, double* last_dt)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	Clock c;
+	PAMHD_TRY(check(cudaMemcpyAsync(&c, x->clock + x->steps % 3, sizeof c, cudaMemcpyDeviceToHost, x->stream)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	if (time != nullptr) *time = c.t;
+	if (steps != nullptr) *steps = c.steps;
+	if (last_dt != nullptr) *last_dt = c.dt;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_dt_history(pamhd_ctx* x, double* dt, const int32_t count, int32_t* written)
+{
+	if (x == nullptr or dt == nullptr or count < 0) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	std::vector<double> all(x->hist_len);
+	PAMHD_TRY(check(cudaMemcpyAsync(all.data(), x->dt_hist, x->hist_len * sizeof(double),
+	                                cudaMemcpyDeviceToHost, x->stream)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	const long long have = std::min<long long>(x->steps, x->hist_len);
+	const long long n = std::min<long long>(have, count);
+	for (long long i = 0; i < n; i++) {
+		const long long step = x->steps - n + i;
+		dt[i] = all[step % x->hist_len];
+	}
+	if (written != nullptr) *written = int32_t(n);
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_status(pamhd_ctx* x, uint32_t* flags, int32_t cell[3], int32_t* dir)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	Status s;
+	PAMHD_TRY(read_status(*x, s));
+	if (flags != nullptr) *flags = s.flags;
+	int32_t c[3] = {0, 0, 0};
+	int32_t d = 0;
+	if (s.flags != 0 and s.first != ~0ull) {
+		const unsigned long long key = s.first >> 8;
+		d = int32_t(key & 3ull);
+		unsigned long long lin = key >> 2;
+		const Step_Params& P = x->base;
+		const unsigned long long nx = x->L.n[0] + 2 * P.ext[0], ny = x->L.n[1] + 2 * P.ext[1];
+		c[0] = int32_t(lin % nx) - P.ext[0];
+		lin /= nx;
+		c[1] = int32_t(lin % ny) - P.ext[1];
+		c[2] = int32_t(lin / ny) - P.ext[2];
+	}
+	if (cell != nullptr) {
+		cell[0] = c[0];
+		cell[1] = c[1];
+		cell[2] = c[2];
+	}
+	if (dir != nullptr) *dir = d;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_totals(pamhd_ctx* x, double totals[8])
+{
+	if (x == nullptr or totals == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(launch_totals(x->state[x->cur], x->L, 0.0, x->partial, x->partial_blocks, x->stream));
+	std::vector<double> part(8 * x->partial_blocks);
+	PAMHD_TRY(check(cudaMemcpyAsync(part.data(), x->partial, part.size() * sizeof(double),
+	                                cudaMemcpyDeviceToHost, x->stream)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	const double volume = x->cfg.cell_length[0] * x->cfg.cell_length[1] * x->cfg.cell_length[2];
+	for (int v = 0; v < 8; v++) {
+		double sum = 0.0, comp = 0.0;
+		for (int b = 0; b < x->partial_blocks; b++) {
+			const double y = part[8 * b + v] - comp;
+			const double t = sum + y;
+			comp = (t - sum) - y;
+			sum = t;
+		}
+		totals[v] = sum * volume;
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_face_flux(const int32_t device, const int32_t solver, const int64_t n, const double* neg,
+                        const double* pos, const double* bg, const double adiabatic_index,
+                        const double vacuum_permeability, double* flux, double* speed, uint32_t* flags)
+{
+	if (n < 0 or neg == nullptr or pos == nullptr or flux == nullptr or speed == nullptr or flags == nullptr) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	if (solver != PAMHD_RUSANOV and solver != PAMHD_HLL_ATHENA and solver != PAMHD_HLLD_ATHENA
+		and solver != PAMHD_ROE_ATHENA) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	if (not (adiabatic_index > 1.0) or not (vacuum_permeability > 0.0)) return PAMHD_ERR_ARGUMENT;
+	if (n == 0) return PAMHD_OK;
+	PAMHD_TRY(check(cudaSetDevice(device)));
+	Gas g;
+	g.gamma = adiabatic_index;
+	g.mu0 = vacuum_permeability;
+	g.inv_mu0 = 1.0 / vacuum_permeability;
+	g.sqrt_mu0 = std::sqrt(vacuum_permeability);
+	g.inv_sqrt_mu0 = 1.0 / g.sqrt_mu0;
+	double *dn = nullptr, *dp = nullptr, *db = nullptr, *df = nullptr, *ds = nullptr;
+	uint32_t* dg = nullptr;
+	int rc = PAMHD_OK;
+	const size_t s8 = size_t(n) * 8 * sizeof(double);
+	if (cudaMalloc(&dn, s8) != cudaSuccess or cudaMalloc(&dp, s8) != cudaSuccess
+		or cudaMalloc(&df, s8) != cudaSuccess or cudaMalloc(&ds, n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&dg, n * sizeof(uint32_t)) != cudaSuccess
+		or (bg != nullptr and cudaMalloc(&db, size_t(n) * 3 * sizeof(double)) != cudaSuccess)) {
+		rc = PAMHD_ERR_CUDA;
+	}
+	if (rc == PAMHD_OK) {
+		rc = check(cudaMemcpy(dn, neg, s8, cudaMemcpyHostToDevice));
+		if (rc == PAMHD_OK) rc = check(cudaMemcpy(dp, pos, s8, cudaMemcpyHostToDevice));
+		if (rc == PAMHD_OK and bg != nullptr) {
+			rc = check(cudaMemcpy(db, bg, size_t(n) * 3 * sizeof(double), cudaMemcpyHostToDevice));
+		}
+	}
+	if (rc == PAMHD_OK) rc = launch_face_flux(solver, n, dn, dp, db, g, df, ds, dg, nullptr);
+	if (rc == PAMHD_OK) rc = check(cudaMemcpy(flux, df, s8, cudaMemcpyDeviceToHost));
+	if (rc == PAMHD_OK) rc = check(cudaMemcpy(speed, ds, n * sizeof(double), cudaMemcpyDeviceToHost));
+	if (rc == PAMHD_OK) rc = check(cudaMemcpy(flags, dg, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+	cudaFree(dn);
+	cudaFree(dp);
+	cudaFree(db);
+	cudaFree(df);
+	cudaFree(ds);
+	cudaFree(dg);
+	if (rc != PAMHD_OK) return rc;
+	for (int64_t i = 0; i < n; i++) {
+		if (flags[i] != 0) return PAMHD_ERR_PHYSICS;
+	}
+	return PAMHD_OK;
+}
+
+} // extern "C"

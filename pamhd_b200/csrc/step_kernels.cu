@@ -1,0 +1,788 @@
+/*
+Kernels of the fused finite-volume MHD step (sm_100a, FP64 CUDA cores).
+
+step_kernel<SOLVER, TY> - one launch = one whole step (the reference's
+  get_all_fluxes + update_mhd_state + minimize_timestep, mhd/solve.hpp:
+  1702-1811, :1518-1614, :1933-2014, in their cell-centred form):
+  * a block owns a 32 x TY column tile and marches along z through a chunk
+    of planes ("2.5-D blocking");
+  * each plane of the tile plus a one-cell halo in x and y is read once
+    from HBM (coalesced along x), its derived quantities (1/rho, pressure,
+    fast speeds along x, y, z) computed once per cell into shared memory;
+  * every x and y face of the tile is solved once from shared memory and
+    its dt-scaled flux kept in shared memory; the z face between the
+    previous and the current plane is solved by the thread owning the
+    column and kept in registers, so every z face is solved once;
+  * the new state of a cell is written as soon as its last (+z) face is
+    known, plus its periodic image or COPY ghost (so no separate ghost
+    fill pass is needed);
+  * the face signal speeds are max-reduced per axis (warp shuffles, then
+    one atomicMax per block on the bits of the non-negative double) into a
+    three-slot ring; the next step's dt is computed from that ring by
+    every block at kernel start, so consecutive steps never wait on the
+    host and can be replayed from a CUDA graph.
+Only the redundant halo faces of each tile (1/32 + 1/TY of the x/y faces)
+and one z plane per chunk are solved twice.
+*/
+#include <cuda_runtime.h>
+
+#include "step.cuh"
+
+namespace pamhd_b200 {
+
+constexpr int TX = 32;
+constexpr int NV = 13;  // record: rho, mom xyz, E, B xyz, 1/rho, p, cf x, cf y, cf z
+enum { R_RINV = 8, R_P = 9, R_CF = 10 };
+
+template <int TY> struct Tile {
+	static constexpr int JO = (TY > 1) ? 1 : 0;            // halo rows exist when y is active
+	static constexpr int W = TX + 2;                       // record row width (halo columns)
+	static constexpr int H = TY + 2 * JO;                  // record rows
+	static constexpr int CELLS = W * H;
+	static constexpr int REC = NV * CELLS;                 // doubles per plane slot
+	static constexpr int FXN = TY * (TX + 1);              // x faces of a plane
+	static constexpr int FYN = (TY > 1) ? (TY + 1) * TX : 0;
+	static constexpr size_t BYTES = size_t(2 * REC + 8 * FXN + 8 * FYN) * 8 + size_t(2 * CELLS) * 4;
+};
+
+int step_smem_bytes(const int ty)
+{
+	return ty == 1 ? int(Tile<1>::BYTES) : int(Tile<8>::BYTES);
+}
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ double warp_max(double v)
+{
+	#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+
+/*
+dt of the step from the previous step's face speeds: the minimum over
+faces of CFL * d_len / s (solve.hpp:1983-2003), which equals
+CFL * d_len / max(s) per axis because rounding is monotonic; 0 when any
+face speed was <= 0; replaced by the cap when cap <= that minimum
+(substepping.hpp:331-338).
+*/
+__device__ __forceinline__ double step_dt(const Step_Params& P)
+{
+	const Speed_Max& r = P.red[P.phase];
+	bool zero = r.zero != 0;
+	double smallest = 1.7976931348623157e308;
+	#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		if (not P.active[d]) continue;
+		const double s = __longlong_as_double((long long)r.smax[d]);
+		if (not (s > 0.0)) {
+			zero = true;
+		} else {
+			smallest = fmin(smallest, (P.cfl * P.len[d]) / s);
+		}
+	}
+	if (zero) smallest = 0.0;
+	const double t = P.clock[P.phase].t;
+	const double cap = P.control->max_dt >= 0.0 ? P.control->max_dt : P.control->t_end - t;
+	return (cap <= smallest) ? cap : smallest;
+}
+
+// block-wide start of a step: every block computes dt; block 0 advances the clock ring
+__device__ __forceinline__ double begin_step(const Step_Params& P, double* s_dt, const bool first_block)
+{
+	if (threadIdx.x == 0 and threadIdx.y == 0) {
+		const double dt = step_dt(P);
+		*s_dt = dt;
+		if (first_block) {
+			const Clock c = P.clock[P.phase];
+			Clock& next = P.clock[(P.phase + 1) % 3];
+			next.t = c.t + dt;
+			next.dt = dt;
+			next.steps = c.steps + 1;
+			if (P.dt_hist != nullptr) P.dt_hist[c.steps % P.hist_len] = dt;
+			Speed_Max& z = P.red[(P.phase + 2) % 3];
+			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
+			z.zero = 0u;
+		}
+	}
+	__syncthreads();
+	return *s_dt;
+}
+
+// the first failing face, numbered as the oracle's extended grid (x fastest)
+__device__ void record_failure(const Step_Params& P, const uint32_t flag, const int i, const int j,
+                               const int k, const int dir)
+{
+	int c[3] = {i, j, k};
+	#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		if (P.periodic[d] and c[d] < 0) c[d] += P.L.n[d];
+	}
+	const unsigned long long nx = P.L.n[0] + 2 * P.ext[0], ny = P.L.n[1] + 2 * P.ext[1];
+	const unsigned long long lin = (unsigned long long)(c[0] + P.ext[0])
+		+ nx * ((unsigned long long)(c[1] + P.ext[1]) + ny * (unsigned long long)(c[2] + P.ext[2]));
+	atomicOr(&P.status->flags, flag);
+	atomicMin(&P.status->first, ((lin * 4ull + (unsigned long long)dir) << 8) | flag);
+}
+
+__device__ __forceinline__ void flush_speeds(const Step_Params& P, double smax[3], bool zero)
+{
+	__shared__ double part[3][32];
+	__shared__ int part_zero[32];
+	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+	const int warp = tid >> 5, lane = tid & 31, warps = (blockDim.x * blockDim.y + 31) >> 5;
+	#pragma unroll
+	for (int d = 0; d < 3; d++) smax[d] = warp_max(smax[d]);
+	const int z = __any_sync(0xffffffffu, zero);
+	if (lane == 0) {
+		part[0][warp] = smax[0];
+		part[1][warp] = smax[1];
+		part[2][warp] = smax[2];
+		part_zero[warp] = z;
+	}
+	__syncthreads();
+	if (tid == 0) {
+		Speed_Max& r = P.red[(P.phase + 1) % 3];
+		int any_zero = 0;
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			double m = 0.0;
+			for (int w = 0; w < warps; w++) m = fmax(m, part[d][w]);
+			if (P.active[d] and m > 0.0) {
+				atomicMax(&r.smax[d], (unsigned long long)__double_as_longlong(m));
+			}
+		}
+		for (int w = 0; w < warps; w++) any_zero |= part_zero[w];
+		if (any_zero) atomicOr(&r.zero, 1u);
+	}
+}
+
+// ghost copy of COPY sides: density, velocity, pressure and field of the neighbour
+// (mhd/boundaries.hpp:818-1030 with the constant-pressure field copy)
+__device__ __forceinline__ void copy_state(const double U[8], const Gas& g, double C[8])
+{
+	const double ir = 1.0 / U[0];
+	const double vx = U[1] * ir, vy = U[2] * ir, vz = U[3] * ir;
+	const double b2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+	const double p = (U[4] - 0.5 * ir * (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) - 0.5 * g.inv_mu0 * b2)
+		* (g.gamma - 1.0);
+	C[0] = U[0];
+	C[1] = U[0] * vx;
+	C[2] = U[0] * vy;
+	C[3] = U[0] * vz;
+	const double ic = 1.0 / C[0];
+	const double wx = C[1] * ic, wy = C[2] * ic, wz = C[3] * ic;
+	C[4] = p / (g.gamma - 1.0) + 0.5 * C[0] * (wx * wx + wy * wy + wz * wz) + 0.5 * g.inv_mu0 * b2;
+	C[5] = U[5];
+	C[6] = U[6];
+	C[7] = U[7];
+}
+
+__device__ __forceinline__ void store_cell(double* out, const Layout& L, const int i, const int j,
+                                           const int k, const double U[8])
+{
+	const long long off = L.offset(i, j, k);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) out[v * L.var + off] = U[v];
+}
+
+// new state of an interior cell plus its periodic image / COPY ghost
+__device__ void write_cell(const Step_Params& P, const int i, const int j, const int k, const double U[8])
+{
+	store_cell(P.out, P.L, i, j, k, U);
+	const int c[3] = {i, j, k};
+	#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		if (not P.active[d]) continue;
+		const int n = P.L.n[d];
+		int t[3] = {i, j, k};
+		if (c[d] == 0) {
+			if (P.periodic[d]) {
+				t[d] = n;
+				store_cell(P.out, P.L, t[0], t[1], t[2], U);
+			} else if (P.bc_lo[d] == PAMHD_BC_COPY) {
+				double C[8];
+				copy_state(U, P.gas, C);
+				t[d] = -1;
+				store_cell(P.out, P.L, t[0], t[1], t[2], C);
+			}
+		}
+		if (c[d] == n - 1) {
+			t[0] = i; t[1] = j; t[2] = k;
+			if (P.periodic[d]) {
+				t[d] = -1;
+				store_cell(P.out, P.L, t[0], t[1], t[2], U);
+			} else if (P.bc_hi[d] == PAMHD_BC_COPY) {
+				double C[8];
+				copy_state(U, P.gas, C);
+				t[d] = n;
+				store_cell(P.out, P.L, t[0], t[1], t[2], C);
+			}
+		}
+	}
+}
+
+// read a cell from HBM, derive its per-cell quantities into a record slot
+template <bool CX, bool CY, bool CZ>
+__device__ __forceinline__ void load_record(const Step_Params& P, double* rec, uint32_t* bad, const int cells,
+                                            const int ri, const int i, const int j, const int k)
+{
+	const long long off = P.L.offset(i, j, k);
+	double U[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) U[v] = __ldg(P.in + v * P.L.var + off);
+	const Derived d = derive<CX, CY, CZ>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) rec[v * cells + ri] = U[v];
+	rec[R_RINV * cells + ri] = d.rinv;
+	rec[R_P * cells + ri] = d.p;
+	if (CX) rec[(R_CF + 0) * cells + ri] = d.cf[0];
+	if (CY) rec[(R_CF + 1) * cells + ri] = d.cf[1];
+	if (CZ) rec[(R_CF + 2) * cells + ri] = d.cf[2];
+	bad[ri] = d.bad;
+}
+
+template <int A>
+__device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, const int cells, const int ri)
+{
+	Side s;
+	s.rho = rec[ri];
+	rotate<A>(rec[1 * cells + ri], rec[2 * cells + ri], rec[3 * cells + ri], s.m0, s.m1, s.m2);
+	s.E = rec[4 * cells + ri];
+	rotate<A>(rec[5 * cells + ri], rec[6 * cells + ri], rec[7 * cells + ri], s.b0, s.b1, s.b2);
+	s.rinv = rec[R_RINV * cells + ri];
+	s.p = rec[R_P * cells + ri];
+	s.cf = rec[(R_CF + A) * cells + ri];
+	s.v0 = s.m0 * s.rinv;
+	s.v1 = s.m1 * s.rinv;
+	s.v2 = s.m2 * s.rinv;
+	s.bad = bad[ri];
+	return s;
+}
+
+// solve one face, fold its speed into the running max, store dt * F in the xyz frame
+template <int SOLVER, int A>
+__device__ __forceinline__ void face(const Step_Params& P, const Side& L, const Side& R, const double dt,
+                                     double* dst, const int stride, double smax[3], bool& zero,
+                                     const int i, const int j, const int k)
+{
+	double F[8];
+	uint32_t flag = 0;
+	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
+	if (flag != 0) record_failure(P, flag, i, j, k, A + 1);
+	smax[A] = fmax(smax[A], s);
+	zero = zero or not (s > 0.0);
+	double m0, m1, m2, b0, b1, b2;
+	unrotate<A>(F[1], F[2], F[3], m0, m1, m2);
+	unrotate<A>(F[5], F[6], F[7], b0, b1, b2);
+	dst[0 * stride] = dt * F[0];
+	dst[1 * stride] = dt * m0;
+	dst[2 * stride] = dt * m1;
+	dst[3 * stride] = dt * m2;
+	dst[4 * stride] = dt * F[4];
+	dst[5 * stride] = dt * b0;
+	dst[6 * stride] = dt * b1;
+	dst[7 * stride] = dt * b2;
+}
+
+// ------------------------------------------------------------------ the step
+
+template <int SOLVER, int TY>
+__global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
+{
+	using T = Tile<TY>;
+	extern __shared__ __align__(16) double smem[];
+	__shared__ double s_dt;
+	double* const rec_base = smem;
+	double* const fx = smem + 2 * T::REC;        // [8][TY][TX + 1]
+	double* const fy = fx + 8 * T::FXN;          // [8][TY + 1][TX]
+	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(fy + 8 * T::FYN);
+
+	const bool first_block = blockIdx.x == 0 and blockIdx.y == 0 and blockIdx.z == 0;
+	const double dt = begin_step(P, &s_dt, first_block);
+
+	constexpr bool YACT = TY > 1;
+	const bool zact = P.active[2] != 0;
+	const int nx = P.L.n[0], ny = P.L.n[1];
+	const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+	const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
+	const int gx = gx0 + tx, gy = gy0 + ty;
+	const bool own = gx < nx and gy < ny;
+	const int kb = blockIdx.z * P.kchunk;
+	const int ke = min(P.L.n[2], kb + P.kchunk);
+	const int kfirst = zact ? kb - 1 : kb;
+	const int klast = zact ? ke : ke - 1;
+	const int ri = (ty + T::JO) * T::W + tx + 1;
+
+	double smax[3] = {0.0, 0.0, 0.0};
+	bool zero = false;
+	double Up[8], Fzm[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) Up[v] = Fzm[v] = 0.0;
+
+	for (int k = kfirst; k <= klast; k++) {
+		const int slot = (k - kfirst) & 1;
+		double* const rec = rec_base + slot * T::REC;
+		uint32_t* const bad = bad_base + slot * T::CELLS;
+		const double* const prev = rec_base + (slot ^ 1) * T::REC;
+		const uint32_t* const prev_bad = bad_base + (slot ^ 1) * T::CELLS;
+		const bool inner = k >= kb and k < ke;
+
+		// (a) stage the plane: own cells, and the halo for planes with x / y faces
+		if (own) load_record<true, YACT, true>(P, rec, bad, T::CELLS, ri, gx, gy, k);
+		if (inner) {
+			if (tid < 2 * TY) {
+				const int row = tid % TY;
+				const bool right = tid >= TY;
+				const int hx = right ? gx0 + TX : gx0 - 1;
+				if (gy0 + row < ny and hx <= nx) {
+					const int hri = (row + T::JO) * T::W + (right ? TX + 1 : 0);
+					load_record<true, false, false>(P, rec, bad, T::CELLS, hri, hx, gy0 + row, k);
+				}
+			} else if (YACT and tid < 2 * TY + 2 * TX) {
+				const int col = (tid - 2 * TY) % TX;
+				const bool top = tid >= 2 * TY + TX;
+				const int hy = top ? gy0 + TY : gy0 - 1;
+				if (gx0 + col < nx and hy <= ny) {
+					const int hri = (top ? TY + 1 : 0) * T::W + col + 1;
+					load_record<false, true, false>(P, rec, bad, T::CELLS, hri, gx0 + col, hy, k);
+				}
+			}
+		}
+		__syncthreads();
+
+		// (b) faces
+		double Fz[8];
+		if (inner) {
+			if (gx0 + tx <= nx and gy < ny) {
+				const Side L = side_at<0>(rec, bad, T::CELLS, ri - 1);
+				const Side R = side_at<0>(rec, bad, T::CELLS, ri);
+				face<SOLVER, 0>(P, L, R, dt, fx + ty * (TX + 1) + tx, T::FXN, smax, zero, gx - 1, gy, k);
+			}
+			if (YACT and gy0 + ty <= ny and gx < nx) {
+				const Side L = side_at<1>(rec, bad, T::CELLS, ri - T::W);
+				const Side R = side_at<1>(rec, bad, T::CELLS, ri);
+				face<SOLVER, 1>(P, L, R, dt, fy + ty * TX + tx, T::FYN, smax, zero, gx, gy - 1, k);
+			}
+			if (tid < TY) {
+				// the +x face of the tile's last column
+				const int row = tid;
+				if (gx0 + TX <= nx and gy0 + row < ny) {
+					const int r2 = (row + T::JO) * T::W + TX;
+					const Side L = side_at<0>(rec, bad, T::CELLS, r2);
+					const Side R = side_at<0>(rec, bad, T::CELLS, r2 + 1);
+					face<SOLVER, 0>(P, L, R, dt, fx + row * (TX + 1) + TX, T::FXN, smax, zero,
+					                gx0 + TX - 1, gy0 + row, k);
+				}
+			} else if (YACT and tid < TY + TX) {
+				// the +y face of the tile's last row
+				const int col = tid - TY;
+				if (gy0 + TY <= ny and gx0 + col < nx) {
+					const int r2 = TY * T::W + col + 1;
+					const Side L = side_at<1>(rec, bad, T::CELLS, r2);
+					const Side R = side_at<1>(rec, bad, T::CELLS, r2 + T::W);
+					face<SOLVER, 1>(P, L, R, dt, fy + TY * TX + col, T::FYN, smax, zero,
+					                gx0 + col, gy0 + TY - 1, k);
+				}
+			}
+		}
+		if (zact and k > kfirst and own) {
+			const Side L = side_at<2>(prev, prev_bad, T::CELLS, ri);
+			const Side R = side_at<2>(rec, bad, T::CELLS, ri);
+			face<SOLVER, 2>(P, L, R, dt, Fz, 1, smax, zero, gx, gy, k - 1);
+		}
+		__syncthreads();
+
+		// (c) update: U += (F- - F+)/dx, then y, then z (solve.hpp:1551-1587)
+		if (own) {
+			if (zact and k > kb) {
+				double Un[8];
+				#pragma unroll
+				for (int v = 0; v < 8; v++) Un[v] = Up[v] + (Fzm[v] - Fz[v]) * P.inv_len[2];
+				write_cell(P, gx, gy, k - 1, Un);
+			}
+			if (inner) {
+				#pragma unroll
+				for (int v = 0; v < 8; v++) {
+					const double* f = fx + v * T::FXN + ty * (TX + 1) + tx;
+					Up[v] = rec[v * T::CELLS + ri] + (f[0] - f[1]) * P.inv_len[0];
+				}
+				if (YACT) {
+					#pragma unroll
+					for (int v = 0; v < 8; v++) {
+						const double* f = fy + v * T::FYN + ty * TX + tx;
+						Up[v] += (f[0] - f[TX]) * P.inv_len[1];
+					}
+				}
+				if (zact) {
+					#pragma unroll
+					for (int v = 0; v < 8; v++) Fzm[v] = Fz[v];
+				} else {
+					write_cell(P, gx, gy, k, Up);
+				}
+			}
+		}
+	}
+	flush_speeds(P, smax, zero);
+}
+
+/*
+Speeds of the faces between two boundary ghosts of a non-periodic side
+(cells of class 0 on both sides).  The reference solves those faces too
+(mhd/solve.hpp:254-311 visits every cell of class >= 0) and their speeds
+enter the timestep (:1965-2005); their fluxes change nothing.
+blockIdx.y enumerates (ghost dimension d, side, tangential axis e).
+*/
+template <int SOLVER>
+__global__ void boundary_speed_kernel(const Step_Params P)
+{
+	__shared__ double s_dt;
+	(void)s_dt;
+	int combos[12][3];
+	int nc = 0;
+	for (int d = 0; d < 3; d++) {
+		if (not P.active[d] or P.periodic[d]) continue;
+		for (int side = 0; side < 2; side++) {
+			for (int e = 0; e < 3; e++) {
+				if (e == d or not P.active[e]) continue;
+				combos[nc][0] = d; combos[nc][1] = side; combos[nc][2] = e;
+				nc++;
+			}
+		}
+	}
+	double smax[3] = {0.0, 0.0, 0.0};
+	bool zero = false;
+	if ((int)blockIdx.y < nc) {
+		const int d = combos[blockIdx.y][0], side = combos[blockIdx.y][1], e = combos[blockIdx.y][2];
+		const int f = 3 - d - e;
+		const int ne = P.periodic[e] ? P.L.n[e] : P.L.n[e] - 1;
+		const int nf = P.L.n[f];
+		const long long count = (long long)ne * nf;
+		for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
+		     t += (long long)gridDim.x * blockDim.x) {
+			int a[3], b[3];
+			a[d] = b[d] = side ? P.L.n[d] : -1;
+			a[e] = int(t % ne);
+			b[e] = a[e] + 1 == P.L.n[e] ? 0 : a[e] + 1;
+			a[f] = b[f] = int(t / ne);
+			double UA[8], UB[8];
+			const long long oa = P.L.offset(a[0], a[1], a[2]), ob = P.L.offset(b[0], b[1], b[2]);
+			#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				UA[v] = P.in[v * P.L.var + oa];
+				UB[v] = P.in[v * P.L.var + ob];
+			}
+			const Derived da = derive<true, true, true>(UA[0], UA[1], UA[2], UA[3], UA[4], UA[5], UA[6], UA[7], P.gas);
+			const Derived db = derive<true, true, true>(UB[0], UB[1], UB[2], UB[3], UB[4], UB[5], UB[6], UB[7], P.gas);
+			Side L, R;
+			auto fill = [e](Side& s, const double U[8], const Derived& dd) {
+				s.rho = U[0];
+				s.E = U[4];
+				double m[3] = {U[1], U[2], U[3]}, B[3] = {U[5], U[6], U[7]};
+				const int i0 = e, i1 = (e + 1) % 3, i2 = (e + 2) % 3;
+				s.m0 = m[i0]; s.m1 = m[i1]; s.m2 = m[i2];
+				s.b0 = B[i0]; s.b1 = B[i1]; s.b2 = B[i2];
+				s.rinv = dd.rinv;
+				s.v0 = s.m0 * s.rinv; s.v1 = s.m1 * s.rinv; s.v2 = s.m2 * s.rinv;
+				s.p = dd.p;
+				s.cf = dd.cf[e];
+				s.bad = dd.bad;
+			};
+			fill(L, UA, da);
+			fill(R, UB, db);
+			double F[8];
+			uint32_t flag = 0;
+			const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
+			if (flag != 0) record_failure(P, flag, a[0], a[1], a[2], e + 1);
+			smax[e] = fmax(smax[e], s);
+			zero = zero or not (s > 0.0);
+		}
+	}
+	flush_speeds(P, smax, zero);
+}
+
+// ------------------------------------------------------------------ layout and ghosts
+
+__global__ void scatter_kernel(const double* __restrict__ packed, double* __restrict__ var, const Layout L)
+{
+	const long long n = (long long)L.n[0] * L.n[1] * L.n[2];
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int i = int(t % L.n[0]);
+		const int j = int((t / L.n[0]) % L.n[1]);
+		const int k = int(t / ((long long)L.n[0] * L.n[1]));
+		var[L.offset(i, j, k)] = packed[t];
+	}
+}
+
+__global__ void gather_kernel(const double* __restrict__ var, double* __restrict__ packed, const Layout L)
+{
+	const long long n = (long long)L.n[0] * L.n[1] * L.n[2];
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const int i = int(t % L.n[0]);
+		const int j = int((t / L.n[0]) % L.n[1]);
+		const int k = int(t / ((long long)L.n[0] * L.n[1]));
+		packed[t] = var[L.offset(i, j, k)];
+	}
+}
+
+/*
+Fills every face ghost of `state` from its interior (periodic image, COPY)
+or the configured VALUE state (apply_boundaries, mhd/boundaries.hpp:1261).
+value_lo/hi are passed through the params of the host context.
+*/
+struct Ghost_Values {
+	double lo[3][8];
+	double hi[3][8];
+};
+
+__global__ void fill_ghosts_kernel(const Step_Params P, double* state, const Ghost_Values V)
+{
+	for (int d = 0; d < 3; d++) {
+		if (not P.active[d]) continue;
+		const int e = (d + 1) % 3, f = (d + 2) % 3;
+		const long long count = (long long)P.L.n[e] * P.L.n[f];
+		for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 2 * count;
+		     t += (long long)gridDim.x * blockDim.x) {
+			const int side = int(t / count);
+			const long long r = t % count;
+			int c[3];
+			c[e] = int(r % P.L.n[e]);
+			c[f] = int(r / P.L.n[e]);
+			c[d] = side ? P.L.n[d] : -1;
+			int s[3] = {c[0], c[1], c[2]};
+			double U[8];
+			const int kind = side ? P.bc_hi[d] : P.bc_lo[d];
+			if (P.periodic[d]) {
+				s[d] = side ? 0 : P.L.n[d] - 1;
+				const long long o = P.L.offset(s[0], s[1], s[2]);
+				for (int v = 0; v < 8; v++) U[v] = state[v * P.L.var + o];
+			} else if (kind == PAMHD_BC_COPY) {
+				s[d] = side ? P.L.n[d] - 1 : 0;
+				const long long o = P.L.offset(s[0], s[1], s[2]);
+				double W[8];
+				for (int v = 0; v < 8; v++) W[v] = state[v * P.L.var + o];
+				copy_state(W, P.gas, U);
+			} else {
+				for (int v = 0; v < 8; v++) U[v] = side ? V.hi[d][v] : V.lo[d][v];
+			}
+			store_cell(state, P.L, c[0], c[1], c[2], U);
+		}
+	}
+}
+
+// ------------------------------------------------------------------ solver-level entry
+
+__device__ __forceinline__ Side face_side(const double* s, const double* bg, const bool use_bg, const Gas& g)
+{
+	Side out;
+	out.rho = s[0]; out.m0 = s[1]; out.m1 = s[2]; out.m2 = s[3]; out.E = s[4];
+	out.b0 = s[5]; out.b1 = s[6]; out.b2 = s[7];
+	const Derived d = derive<true, false, false>(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], g);
+	out.rinv = d.rinv;
+	out.v0 = d.vx; out.v1 = d.vy; out.v2 = d.vz;
+	out.p = d.p;
+	out.cf = d.cf[0];
+	out.bad = d.bad;
+	if (use_bg) {
+		// fast speed with the total field (get_fast_magnetosonic_speed, mhd/common.hpp:433-490)
+		const double t0 = s[5] + bg[0], t1 = s[6] + bg[1], t2 = s[7] + bg[2];
+		const double t2s = t0 * t0 + t1 * t1 + t2 * t2;
+		const double cs2 = g.gamma * d.p * d.rinv;
+		if (t2s > 0.0) {
+			const double va2 = t2s * g.inv_mu0 * d.rinv;
+			const double sum2 = cs2 + va2;
+			const double to_sqrt = cs2 * cs2 + va2 * va2 + 2.0 * cs2 * va2 * (1.0 - 2.0 * (t0 * t0 / t2s));
+			if (out.bad == 0 and not (is_normal(sum2) and to_sqrt > 0.0 and is_normal(to_sqrt))) {
+				out.bad = PAMHD_FLAG_WAVE_SPEED;
+			}
+			out.cf = sqrt(0.5 * (sum2 + sqrt(fmax(to_sqrt, 0.0))));
+		} else {
+			out.cf = sqrt(fmax(cs2, 0.0));
+		}
+	}
+	return out;
+}
+
+template <int SOLVER>
+__global__ void face_flux_kernel(long long n, const double* __restrict__ neg, const double* __restrict__ pos,
+                                 const double* __restrict__ bg, const Gas g, double* __restrict__ flux,
+                                 double* __restrict__ speed, uint32_t* __restrict__ flags)
+{
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+		const bool use_bg = bg != nullptr and (SOLVER == PAMHD_RUSANOV or SOLVER == PAMHD_HLL_ATHENA);
+		const double zero3[3] = {0.0, 0.0, 0.0};
+		const double* b = use_bg ? bg + 3 * t : zero3;
+		const Side L = face_side(neg + 8 * t, b, use_bg, g);
+		const Side R = face_side(pos + 8 * t, b, use_bg, g);
+		double F[8];
+		uint32_t flag = L.bad | R.bad;
+		if (flag & PAMHD_FLAG_DENSITY) flag = PAMHD_FLAG_DENSITY;
+		else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
+		double s;
+		if (SOLVER == PAMHD_RUSANOV) s = use_bg ? flux_rusanov<true>(L, R, g, F, flag, b) : flux_rusanov<false>(L, R, g, F, flag);
+		else if (SOLVER == PAMHD_HLL_ATHENA) s = use_bg ? flux_hll<true>(L, R, g, F, flag, b) : flux_hll<false>(L, R, g, F, flag);
+		else if (SOLVER == PAMHD_HLLD_ATHENA) s = flux_hlld(L, R, g, F, flag);
+		else s = flux_roe(L, R, g, F, flag);
+		for (int v = 0; v < 8; v++) flux[8 * t + v] = flag ? 0.0 : F[v];
+		speed[t] = flag ? 0.0 : s;
+		flags[t] = flag;
+	}
+}
+
+// ------------------------------------------------------------------ conserved totals
+
+/*
+Per-block partial sums of the eight conserved variables over interior
+cells (compensated summation inside a thread, a fixed-order tree across
+the block), so that totals are deterministic run to run.
+*/
+__global__ void totals_kernel(const double* __restrict__ state, const Layout L, double* __restrict__ partial)
+{
+	__shared__ double red[8][256];
+	const long long n = (long long)L.n[0] * L.n[1] * L.n[2];
+	const long long per = (n + gridDim.x - 1) / gridDim.x;
+	const long long a = blockIdx.x * per, b = min(n, a + per);
+	double sum[8], comp[8];
+	for (int v = 0; v < 8; v++) sum[v] = comp[v] = 0.0;
+	for (long long t = a + threadIdx.x; t < b; t += blockDim.x) {
+		const int i = int(t % L.n[0]);
+		const int j = int((t / L.n[0]) % L.n[1]);
+		const int k = int(t / ((long long)L.n[0] * L.n[1]));
+		const long long o = L.offset(i, j, k);
+		for (int v = 0; v < 8; v++) {
+			const double y = state[v * L.var + o] - comp[v];
+			const double s = sum[v] + y;
+			comp[v] = (s - sum[v]) - y;
+			sum[v] = s;
+		}
+	}
+	for (int v = 0; v < 8; v++) red[v][threadIdx.x] = sum[v];
+	__syncthreads();
+	for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+		if ((int)threadIdx.x < w) {
+			for (int v = 0; v < 8; v++) red[v][threadIdx.x] += red[v][threadIdx.x + w];
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		for (int v = 0; v < 8; v++) partial[8 * blockIdx.x + v] = red[v][0];
+	}
+}
+
+// ------------------------------------------------------------------ launchers
+
+template <int SOLVER, int TY>
+static int prepare_t()
+{
+	const cudaError_t e = cudaFuncSetAttribute(step_kernel<SOLVER, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                           int(Tile<TY>::BYTES));
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int prepare_step_kernels(const int solver, const bool y)
+{
+	switch (solver) {
+	case PAMHD_RUSANOV: return y ? prepare_t<PAMHD_RUSANOV, 8>() : prepare_t<PAMHD_RUSANOV, 1>();
+	case PAMHD_HLL_ATHENA: return y ? prepare_t<PAMHD_HLL_ATHENA, 8>() : prepare_t<PAMHD_HLL_ATHENA, 1>();
+	case PAMHD_HLLD_ATHENA: return y ? prepare_t<PAMHD_HLLD_ATHENA, 8>() : prepare_t<PAMHD_HLLD_ATHENA, 1>();
+	case PAMHD_ROE_ATHENA: return y ? prepare_t<PAMHD_ROE_ATHENA, 8>() : prepare_t<PAMHD_ROE_ATHENA, 1>();
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+template <int SOLVER, int TY>
+static int launch_step_t(const Step_Params& P, cudaStream_t stream)
+{
+	const size_t smem = Tile<TY>::BYTES;
+	const dim3 block(TX, TY);
+	const dim3 grid((P.L.n[0] + TX - 1) / TX, (P.L.n[1] + TY - 1) / TY,
+	                (P.L.n[2] + P.kchunk - 1) / P.kchunk);
+	step_kernel<SOLVER, TY><<<grid, block, smem, stream>>>(P);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_step(const Step_Params& P, const int solver, cudaStream_t stream)
+{
+	const bool y = P.active[1] != 0;
+	switch (solver) {
+	case PAMHD_RUSANOV: return y ? launch_step_t<PAMHD_RUSANOV, 8>(P, stream) : launch_step_t<PAMHD_RUSANOV, 1>(P, stream);
+	case PAMHD_HLL_ATHENA: return y ? launch_step_t<PAMHD_HLL_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_HLL_ATHENA, 1>(P, stream);
+	case PAMHD_HLLD_ATHENA: return y ? launch_step_t<PAMHD_HLLD_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_HLLD_ATHENA, 1>(P, stream);
+	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+int launch_boundary_speeds(const Step_Params& P, const int solver, cudaStream_t stream)
+{
+	int combos = 0, largest = 0;
+	for (int d = 0; d < 3; d++) {
+		if (not P.active[d] or P.periodic[d]) continue;
+		for (int e = 0; e < 3; e++) {
+			if (e == d or not P.active[e]) continue;
+			combos += 2;
+			const int f = 3 - d - e;
+			largest = max(largest, P.L.n[e] * P.L.n[f]);
+		}
+	}
+	if (combos == 0) return PAMHD_OK;
+	const dim3 grid(min(1024, (largest + 255) / 256), combos);
+	switch (solver) {
+	case PAMHD_RUSANOV: boundary_speed_kernel<PAMHD_RUSANOV><<<grid, 256, 0, stream>>>(P); break;
+	case PAMHD_HLL_ATHENA: boundary_speed_kernel<PAMHD_HLL_ATHENA><<<grid, 256, 0, stream>>>(P); break;
+	case PAMHD_HLLD_ATHENA: boundary_speed_kernel<PAMHD_HLLD_ATHENA><<<grid, 256, 0, stream>>>(P); break;
+	case PAMHD_ROE_ATHENA: boundary_speed_kernel<PAMHD_ROE_ATHENA><<<grid, 256, 0, stream>>>(P); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_scatter(const double* packed, double* var_base, const Layout& L, cudaStream_t stream)
+{
+	scatter_kernel<<<1184, 256, 0, stream>>>(packed, var_base, L);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_gather(const double* var_base, double* packed, const Layout& L, cudaStream_t stream)
+{
+	gather_kernel<<<1184, 256, 0, stream>>>(var_base, packed, L);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_fill_ghosts_values(const Step_Params& P, double* state, const double lo[3][8], const double hi[3][8],
+                              cudaStream_t stream)
+{
+	Ghost_Values V;
+	for (int d = 0; d < 3; d++) {
+		for (int v = 0; v < 8; v++) {
+			V.lo[d][v] = lo[d][v];
+			V.hi[d][v] = hi[d][v];
+		}
+	}
+	fill_ghosts_kernel<<<296, 256, 0, stream>>>(P, state, V);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_face_flux(const int solver, const long long n, const double* neg, const double* pos, const double* bg,
+                     const Gas& gas, double* flux, double* speed, uint32_t* flags, cudaStream_t stream)
+{
+	const int blocks = int(min(4096LL, (n + 127) / 128));
+	if (blocks == 0) return PAMHD_OK;
+	switch (solver) {
+	case PAMHD_RUSANOV: face_flux_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(n, neg, pos, bg, gas, flux, speed, flags); break;
+	case PAMHD_HLL_ATHENA: face_flux_kernel<PAMHD_HLL_ATHENA><<<blocks, 128, 0, stream>>>(n, neg, pos, bg, gas, flux, speed, flags); break;
+	case PAMHD_HLLD_ATHENA: face_flux_kernel<PAMHD_HLLD_ATHENA><<<blocks, 128, 0, stream>>>(n, neg, pos, bg, gas, flux, speed, flags); break;
+	case PAMHD_ROE_ATHENA: face_flux_kernel<PAMHD_ROE_ATHENA><<<blocks, 128, 0, stream>>>(n, neg, pos, bg, gas, flux, speed, flags); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_totals(const double* state, const Layout& L, const double /*volume*/, double* partial, const int nblocks,
+                  cudaStream_t stream)
+{
+	totals_kernel<<<nblocks, 256, 0, stream>>>(state, L, partial);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+} // namespace pamhd_b200

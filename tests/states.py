@@ -140,14 +140,11 @@ def smooth_3d(shape, rng, gamma=GAMMA_53, amp=0.1):
 
 def blast_wave(n, seed=20261203, gamma=GAMMA_53, amp=0.01, kmax=8):
     """Magnetised blast wave on [-0.5, 0.5]^3 with n^3 cells: rho 1, p 0.1 (10 inside r < 0.1),
-    B0 = (1, 1, 0)/sqrt(2) plus a divergence-free perturbation dB = curl A built from random-phase
+    B0 = (1, 1, 0)/sqrt(2) plus a divergence-free perturbation dB = curl A built from 48 random-phase
     modes with integer wavenumbers |k| in [1, kmax] (2 pi units), scaled so rms|dB| = amp |B0|.
-    Returns (8, n, n, n) float64."""
+    The modes are summed by one inverse FFT per component.  Returns (8, n, n, n) float64."""
     rng = np.random.default_rng(seed)
     c = (np.arange(n) + 0.5) / n - 0.5
-    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
-    B0 = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
-    dB = np.zeros((3, n, n, n))
     modes = []
     for kx in range(-kmax, kmax + 1):
         for ky in range(-kmax, kmax + 1):
@@ -156,26 +153,32 @@ def blast_wave(n, seed=20261203, gamma=GAMMA_53, amp=0.01, kmax=8):
                 if 1 <= k2 <= kmax * kmax and (kz > 0 or ky > 0 or (ky == 0 and kx > 0)):
                     modes.append((kx, ky, kz))
     sel = rng.choice(len(modes), size=min(48, len(modes)), replace=False)
+    # dB(x) = sum_m -(k x a) sin(k.x + ph), x = cell centres: written as Im of an inverse DFT over
+    # the cell index, with the centre offset folded into each mode's phase
+    spec = np.zeros((3, n, n, n), dtype=np.complex128)  # indexed [component, kz, ky, kx]
     for m in sel:
-        k = 2 * np.pi * np.array(modes[m], float)
+        mv = np.array(modes[m], float)
+        k = 2 * np.pi * mv
         a = rng.normal(size=3)
         a -= k * (a @ k) / (k @ k)  # transverse amplitude
         ph = rng.uniform(0, 2 * np.pi)
-        arg = k[0] * X + k[1] * Y + k[2] * Z + ph
-        # A = a cos(k.x + ph)  ->  curl A = -sin(k.x + ph) (k x a)
+        ph_cell = ph + 2 * np.pi * (mv @ np.full(3, 0.5 / n - 0.5))
         kxa = np.cross(k, a)
-        s = np.sin(arg)
+        idx = (int(modes[m][2]) % n, int(modes[m][1]) % n, int(modes[m][0]) % n)
         for d in range(3):
-            dB[d] -= kxa[d] * s
+            spec[(d,) + idx] += -kxa[d] * np.exp(1j * ph_cell)
+    dB = np.fft.ifftn(spec, axes=(1, 2, 3)).imag * float(n) ** 3
+    del spec
     rms = np.sqrt((dB ** 2).sum(0).mean())
+    B0 = np.array([1.0, 1.0, 0.0]) / np.sqrt(2.0)
     dB *= amp * np.linalg.norm(B0) / rms
     B = B0[:, None, None, None] + dB
+    del dB
     rho = np.ones((n, n, n))
-    r = np.sqrt(X ** 2 + Y ** 2 + Z ** 2)
-    p = np.where(r < 0.1, 10.0, 0.1)
-    v = np.zeros((3, n, n, n))
+    r2 = c[:, None, None] ** 2 + c[None, :, None] ** 2 + c[None, None, :] ** 2
+    p = np.where(r2 < 0.01, 10.0, 0.1)
     U = np.zeros((8, n, n, n))
     U[0] = rho
-    U[4] = energy(rho, v, p, B, gamma)
+    U[4] = p / (gamma - 1) + 0.5 * (B ** 2).sum(axis=0)
     U[5:8] = B
     return U

@@ -1,0 +1,78 @@
+"""The C-ABI library loads and exports what include/*.h declares (CPU only, no GPU calls
+beyond argument validation, which happens before any CUDA call)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+import pamhd_b200 as pg
+from oracle import pyoracle as po
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names.update(re.findall(r"\b(pamhd_gpu_\w+)\s*\(", text))
+    return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from pamhd_b200 import build
+    build.build()
+    return pg.lib()
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "pamhd_gpu_step" in names and "pamhd_gpu_face_flux" in names
+    assert len(names) >= 15
+
+
+@pytest.mark.parametrize("name", declared_symbols())
+def test_library_exports(lib, name):
+    assert hasattr(lib, name), name
+
+
+def test_abi_version_and_errstr(lib):
+    assert lib.pamhd_gpu_abi_version() == 1
+    assert lib.pamhd_gpu_errstr(pg.ERR_PHYSICS).decode().startswith("a face met")
+
+
+def test_cfg_layout_matches_oracle():
+    assert ctypes.sizeof(pg._Cfg) == ctypes.sizeof(po.Cfg)
+    for (a, ta), (b, tb) in zip(pg._Cfg._fields_, po.Cfg._fields_):
+        assert a == b and ctypes.sizeof(ta) == ctypes.sizeof(tb)
+        assert getattr(pg._Cfg, a).offset == getattr(po.Cfg, b).offset
+
+
+@pytest.mark.parametrize("change", [
+    dict(solver=1),                       # rusanov_staggered aborts in the reference dispatcher
+    dict(solver=9),
+    dict(n=(1, 8, 8)),                    # x must be active
+    dict(n=(8, 1, 8)),                    # active dimensions are x, x-y or x-y-z
+    dict(cell_length=(0.0, 1.0, 1.0)),
+    dict(adiabatic_index=1.0),
+    dict(vacuum_permeability=0.0),
+    dict(time_step_factor=0.0),
+    dict(bc_lo=(0, 0, 0), bc_hi=(1, 0, 0)),  # periodic on one side only
+])
+def test_create_rejects_invalid_config(lib, change):
+    kw = dict(n=(8, 8, 8), solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1))
+    kw.update(change)
+    cfg = pg.Config(**kw).to_c()
+    h = ctypes.c_void_p()
+    assert lib.pamhd_gpu_create(ctypes.byref(cfg), ctypes.byref(h)) == pg.ERR_ARGUMENT
+    assert not h.value
+
+
+def test_null_arguments_rejected(lib):
+    assert lib.pamhd_gpu_create(None, None) == pg.ERR_ARGUMENT
+    assert lib.pamhd_gpu_step(None, 0.0, None) == pg.ERR_ARGUMENT
+    assert lib.pamhd_gpu_destroy(None) == pg.OK

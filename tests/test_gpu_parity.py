@@ -1,0 +1,242 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerance: the GPU computes in FP64 with FMA contraction and reciprocals,
+the oracle in the reference's exact operation order, so results agree to
+round-off.  Per step the bar is a relative state error <= 1e-12: for every
+variable, |gpu - oracle| <= 1e-12 * max(|oracle| over that variable's
+field) per cell (a field-normwise relative error; momentum and field
+components pass through zero, where a cellwise ratio is meaningless).
+Face fluxes use the same bar per face: |gpu - oracle| <= 1e-12 * max over
+the face's eight flux components.
+"""
+import numpy as np
+import pytest
+
+import pamhd_b200 as pg
+from oracle import pyoracle as po
+import states
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-12
+
+
+def field_err(a, b):
+    """max over variables of max|a - b| / max|b| (b = oracle)."""
+    a = a.reshape(8, -1)
+    b = b.reshape(8, -1)
+    scale = np.abs(b).max(axis=1)
+    scale[scale == 0] = 1.0
+    return float((np.abs(a - b).max(axis=1) / scale).max())
+
+
+def pair(port, n, solver, lengths, gamma, mu0, cfl, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0),
+         value_lo=None, value_hi=None):
+    cfg = pg.Config(n=n, solver=solver, cell_length=lengths, adiabatic_index=gamma, vacuum_permeability=mu0,
+                    time_step_factor=cfl, bc_lo=bc_lo, bc_hi=bc_hi,
+                    value_lo=value_lo or [None] * 3, value_hi=value_hi or [None] * 3)
+    ocfg = po.make_cfg(n, solver, lengths, gamma, mu0, cfl, bc_lo, bc_hi, value_lo, value_hi)
+    return pg.Context(cfg), port.grid(ocfg, threads=8)
+
+
+# ---------------------------------------------------------------- solver level
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_face_flux_matches_oracle(port, solver):
+    rng = np.random.default_rng(11)
+    a, b = states.nearby_face_states(20000, rng)
+    c = states.random_face_states(20000, rng)
+    d = states.random_face_states(20000, rng)
+    e, f = states.edge_case_face_states()
+    neg = np.vstack([a, c, e])
+    pos = np.vstack([b, d, f])
+    sid = po.SOLVERS[solver]
+    for mu0, bg in ((1.0, None), (1.0, rng.normal(0, 0.3, (neg.shape[0], 3))), (4e-7 * np.pi, None)):
+        scale = np.ones(8)
+        if mu0 != 1.0:
+            scale[5:8] = np.sqrt(mu0)
+        n_, p_ = neg * scale, pos * scale
+        fo, so, go = port.face_flux(sid, n_, p_, bg, 5 / 3, mu0)
+        fg, sg, gg = pg.face_flux(sid, n_, p_, bg, 5 / 3, mu0)
+        # every face the reference rejects is rejected with the same class of error
+        assert np.array_equal(gg != 0, go != 0)
+        assert np.array_equal(gg[go != 0], go[go != 0])
+        ok = go == 0
+        row = np.abs(fo[ok]).max(axis=1, keepdims=True)
+        row[row == 0] = 1.0
+        assert (np.abs(fg[ok] - fo[ok]) / row).max() <= STEP_TOL
+        assert (np.abs(sg[ok] - so[ok]) / np.maximum(so[ok], 1e-300)).max() <= STEP_TOL
+
+
+# ---------------------------------------------------------------- one step from identical inputs
+
+CASES = {
+    "periodic3d": dict(n=(12, 10, 9), lengths=(1 / 12, 1 / 10, 1 / 9), gamma=5 / 3, mu0=1.0, cfl=0.4),
+    "periodic3d_wide": dict(n=(70, 19, 11), lengths=(0.01, 0.02, 0.03), gamma=5 / 3, mu0=1.0, cfl=0.4),
+    "orszag_tang64": dict(n=(64, 64, 1), lengths=(1 / 64, 1 / 64, 1.0), gamma=5 / 3, mu0=1.0, cfl=0.4),
+    "briowu200": dict(n=(200, 1, 1), lengths=(1 / 200, 1.0, 1.0), gamma=2.0, mu0=1.0, cfl=0.5,
+                      bc_lo=(1, 0, 0), bc_hi=(1, 0, 0)),
+}
+
+
+def initial_state(key, rng):
+    c = CASES[key]
+    nx, ny, nz = c["n"]
+    if key.startswith("orszag"):
+        return states.orszag_tang(nx)
+    if key.startswith("briowu"):
+        return states.brio_wu(nx)
+    return states.smooth_3d((nz, ny, nx), rng, amp=0.15)
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+@pytest.mark.parametrize("key", list(CASES))
+def test_one_step_matches_oracle(port, key, solver):
+    rng = np.random.default_rng(21)
+    U0 = initial_state(key, rng)
+    c = dict(CASES[key])
+    gpu, ora = pair(port, c.pop("n"), po.SOLVERS[solver], c.pop("lengths"), c.pop("gamma"), c.pop("mu0"),
+                    c.pop("cfl"), **c)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    # priming step: dt = 0, state unchanged, speeds recorded (tests/mhd/test.cpp:462)
+    assert gpu.step(1.0) == 0.0
+    assert ora.step(1.0)[0] == 0.0
+    np.testing.assert_array_equal(gpu.get_state(), U0)
+    # one real step from identical inputs
+    dg = gpu.step(1.0)
+    do, flag, _, _ = ora.step(1.0)
+    assert flag == 0
+    assert abs(dg - do) <= STEP_TOL * do
+    assert field_err(gpu.get_state(), ora.get_state()) <= STEP_TOL
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_bounded_grid_matches_oracle(port, solver):
+    """COPY and VALUE sides plus a periodic one: ghost refresh and the boundary-layer speeds."""
+    rng = np.random.default_rng(5)
+    U0 = states.smooth_3d((7, 9, 11), rng, amp=0.1)
+    inflow = np.array([1.2, 0.3 * 1.2, 0.2 * 1.2, 0.0,
+                       states.energy(1.2, np.array([[0.3], [0.2], [0.0]]), 0.7,
+                                     np.array([[0.4], [0.1], [-0.2]]), 5 / 3)[0], 0.4, 0.1, -0.2])
+    gpu, ora = pair(port, (11, 9, 7), po.SOLVERS[solver], (0.09, 0.11, 0.13), 5 / 3, 1.0, 0.4,
+                    bc_lo=(po.BC_VALUE, po.BC_COPY, po.BC_PERIODIC), bc_hi=(po.BC_COPY, po.BC_COPY, po.BC_PERIODIC),
+                    value_lo=[inflow, None, None])
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    for step in range(6):
+        dg = gpu.step(1.0)
+        do, flag, _, _ = ora.step(1.0)
+        assert flag == 0
+        assert abs(dg - do) <= 1e-12 * max(do, 1e-300) or dg == do == 0.0
+        assert field_err(gpu.get_state(), ora.get_state()) <= STEP_TOL * (1 + step)
+
+
+# ---------------------------------------------------------------- trajectories
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena"])
+def test_orszag_tang_trajectory(port, solver):
+    """50 steps of Orszag-Tang 64^2: dt history and state stay within round-off growth."""
+    U0 = states.orszag_tang(64)
+    c = dict(CASES["orszag_tang64"])
+    gpu, ora = pair(port, c.pop("n"), po.SOLVERS[solver], c.pop("lengths"), c.pop("gamma"), c.pop("mu0"),
+                    c.pop("cfl"))
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    t_o, dts_o = ora.run(0.0, 10.0, 50)
+    gpu.steps(50, 10.0)
+    gpu.sync()
+    t_g, n_g, _ = gpu.time()
+    dts_g = gpu.dt_history(50)
+    assert n_g == 50
+    np.testing.assert_allclose(dts_g, dts_o, rtol=1e-10, atol=0)
+    assert abs(t_g - t_o) <= 1e-10 * t_o
+    assert field_err(gpu.get_state(), ora.get_state()) <= 1e-9
+
+
+def test_brio_wu_to_t_end(port):
+    """Brio-Wu, 1000 cells, gamma 2, HLLD, CFL 0.5, copy boundaries, to t = 0.1."""
+    U0 = states.brio_wu(1000)
+    gpu, ora = pair(port, (1000, 1, 1), po.HLLD, (1e-3, 1.0, 1.0), 2.0, 1.0, 0.5,
+                    bc_lo=(po.BC_COPY, 0, 0), bc_hi=(po.BC_COPY, 0, 0))
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    t_o, dts_o = ora.run(0.0, 0.1, 100000)
+    gpu.steps(len(dts_o) + 5, 0.1)
+    t_g, n_g, _ = gpu.time()
+    assert t_o == pytest.approx(0.1, abs=0) or abs(t_o - 0.1) < 1e-15
+    assert abs(t_g - t_o) <= 1e-13
+    dts_g = gpu.dt_history(n_g)
+    np.testing.assert_allclose(dts_g[: len(dts_o)], dts_o, rtol=1e-9)
+    assert field_err(gpu.get_state(), ora.get_state()) <= 1e-8
+
+
+# ---------------------------------------------------------------- properties at any size
+
+def test_graph_steps_equal_single_steps():
+    rng = np.random.default_rng(8)
+    U0 = states.smooth_3d((20, 24, 40), rng)
+    cfg = pg.Config(n=(40, 24, 20), solver=pg.HLLD, cell_length=(0.025, 0.04, 0.05), time_step_factor=0.4)
+    a, b = pg.Context(cfg), pg.Context(cfg)
+    a.set_state(U0)
+    b.set_state(U0)
+    for _ in range(14):
+        a.step(1e9)
+    b.steps(14, 1e9)
+    b.sync()
+    np.testing.assert_array_equal(a.get_state(), b.get_state())
+    np.testing.assert_array_equal(a.dt_history(14), b.dt_history(14))
+
+
+def test_translation_invariance_bitwise():
+    """Shifting a periodic initial state by whole cells shifts the solution bit for bit:
+    every face is solved by the same arithmetic wherever it sits in the tiling."""
+    rng = np.random.default_rng(9)
+    U0 = states.smooth_3d((16, 20, 72), rng)
+    cfg = pg.Config(n=(72, 20, 16), solver=pg.HLLD, cell_length=(0.02, 0.05, 0.06), time_step_factor=0.4)
+    a, b = pg.Context(cfg), pg.Context(cfg)
+    shift = (5, 7, 13)  # z, y, x
+    a.set_state(U0)
+    b.set_state(np.roll(U0, shift, axis=(1, 2, 3)))
+    a.steps(7, 1e9)
+    b.steps(7, 1e9)
+    np.testing.assert_array_equal(np.roll(a.get_state(), shift, axis=(1, 2, 3)), b.get_state())
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_conservation_on_periodic_grid(solver):
+    rng = np.random.default_rng(10)
+    U0 = states.smooth_3d((24, 32, 40), rng)
+    cfg = pg.Config(n=(40, 32, 24), solver=po.SOLVERS[solver], cell_length=(0.025, 0.03, 0.04),
+                    time_step_factor=0.4)
+    g = pg.Context(cfg)
+    g.set_state(U0)
+    t0 = g.totals()
+    g.steps(20, 1e9)
+    t1 = g.totals()
+    absum = np.abs(U0).reshape(8, -1).sum(axis=1) * 0.025 * 0.03 * 0.04
+    assert np.all(np.abs(t1 - t0) <= 1e-13 * absum)
+
+
+def test_invalid_state_reported_like_oracle(port):
+    rng = np.random.default_rng(5)
+    U0 = states.smooth_3d((6, 5, 40), rng)
+    U0[4, 3, 2, 17] = 0.0  # negative pressure in cell x=17, y=2, z=3
+    gpu, ora = pair(port, (40, 5, 6), po.HLLD, (0.025, 0.2, 0.16), 5 / 3, 1.0, 0.4)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    _, flag, cell, d = ora.step(0.0)
+    with pytest.raises(pg.PhysicsError) as e:
+        gpu.step(0.0)
+    assert e.value.flags == flag == pg.FLAG_PRESSURE
+    assert e.value.cell == cell and e.value.direction == d
+
+
+def test_time_capped_at_t_end():
+    U0 = states.orszag_tang(32)
+    cfg = pg.Config(n=(32, 32, 1), solver=pg.HLL, cell_length=(1 / 32, 1 / 32, 1.0), time_step_factor=0.4)
+    g = pg.Context(cfg)
+    g.set_state(U0)
+    g.steps(400, 0.05)
+    t, n, _ = g.time()
+    assert t == 0.05 and n == 400
