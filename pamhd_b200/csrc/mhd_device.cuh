@@ -221,7 +221,7 @@ __device__ __forceinline__ double flux_rusanov(const Side& L, const Side& R, con
 	for (int v = 0; v < 8; v++) {
 		F[v] = 0.5 * (FL[v] + FR[v]) - (UR[v] - UL[v]) * h;
 	}
-	if (not is_finite(F[0]) or not is_finite(s)) flag |= PAMHD_FLAG_FLUX;
+	if (flag == 0 and (not is_finite(F[0]) or not is_finite(s))) flag = PAMHD_FLAG_FLUX;
 	return s;
 }
 

@@ -308,6 +308,8 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 	const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
 	const int gx = gx0 + tx, gy = gy0 + ty;
 	const bool own = gx < nx and gy < ny;
+	// the +x / +y ghost of a partial tile lies inside the tile's own columns / rows
+	const bool stage = gx <= nx and (TY == 1 ? gy == 0 : gy <= ny);
 	const int kb = blockIdx.z * P.kchunk;
 	const int ke = min(P.L.n[2], kb + P.kchunk);
 	const int kfirst = zact ? kb - 1 : kb;
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 		const bool inner = k >= kb and k < ke;
 
 		// (a) stage the plane: own cells, and the halo for planes with x / y faces
-		if (own) load_record<true, YACT, true>(P, rec, bad, T::CELLS, ri, gx, gy, k);
+		if (stage) load_record<true, YACT, true>(P, rec, bad, T::CELLS, ri, gx, gy, k);
 		if (inner) {
 			if (tid < 2 * TY) {
 				const int row = tid % TY;

@@ -240,3 +240,27 @@ def test_time_capped_at_t_end():
     g.steps(400, 0.05)
     t, n, _ = g.time()
     assert t == 0.05 and n == 400
+
+
+def test_blast_positivity_failure_matches_oracle(port):
+    """The 64^3 magnetised blast loses positivity in the reference scheme (first-order HLLD, cell-
+    centred field): the GPU must stop at the same step, on the same face, with the same error."""
+    n = 64
+    U0 = states.blast_wave(n)
+    gpu, ora = pair(port, (n, n, n), po.HLLD, (1 / n,) * 3, 5 / 3, 1.0, 0.4)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    fail_o = fail_g = None
+    for step in range(120):
+        do, flag, cell, d = ora.step(1e30)
+        if flag:
+            fail_o = (step, flag, cell, d)
+            break
+        dg = gpu.step(1e30)
+        assert abs(dg - do) <= 1e-10 * max(do, 1e-300) or dg == do == 0.0
+    assert fail_o is not None
+    try:
+        gpu.step(1e30)
+    except pg.PhysicsError as e:
+        fail_g = (fail_o[0], e.flags, e.cell, e.direction)
+    assert fail_g == fail_o
