@@ -131,7 +131,7 @@ void set_params(pamhd_ctx& x)
 	P.dt_hist = x.dt_hist;
 	P.hist_len = x.hist_len;
 	// z planes per block: enough blocks for several waves on 148 SMs, few redundant z faces
-	const int ty = P.active[1] ? 8 : 1;
+	const int ty = P.active[1] ? step_tile_rows() : 1;
 	const long long tiles = (long long)((c.n[0] + 31) / 32) * ((c.n[1] + ty - 1) / ty);
 	long long chunks = (2368 + tiles - 1) / tiles;
 	chunks = std::max(1LL, std::min(chunks, (long long)std::max(1, c.n[2] / 16)));

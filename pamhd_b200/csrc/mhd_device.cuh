@@ -67,32 +67,56 @@ struct Derived {
 	uint32_t bad;
 };
 
+/*
+Reciprocal of a non-zero normal double by Newton-Raphson iteration
+(r <- r + r (1 - x r), quadratic convergence) from the hardware estimate of
+PTX rcp.approx.ftz.f64; two iterations bring the estimate's relative error
+below 2^-52, so the result is within one unit in the last place of 1/x.
+Used where the operand is a normal, non-zero number by construction.
+*/
+__device__ __forceinline__ double recip(const double x)
+{
+	double r;
+	asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+	double e = __fma_rn(-x, r, 1.0);
+	r = __fma_rn(r, e, r);
+	e = __fma_rn(-x, r, 1.0);
+	return __fma_rn(r, e, r);
+}
+
+/*
+Every operation below is an explicitly rounded intrinsic, so that every
+inlined copy of this function computes the same bits for the same cell
+(the halo of one tile is the interior of the next).
+*/
 template <bool NEED_X, bool NEED_Y, bool NEED_Z>
 __device__ __forceinline__ Derived derive(
 	const double rho, const double mx, const double my, const double mz,
 	const double E, const double bx, const double by, const double bz, const Gas& g
 ) {
 	Derived d;
-	d.rinv = 1.0 / rho;
-	d.vx = mx * d.rinv;
-	d.vy = my * d.rinv;
-	d.vz = mz * d.rinv;
-	const double b2 = bx * bx + by * by + bz * bz;
-	const double kinetic = 0.5 * d.rinv * (mx * mx + my * my + mz * mz);
-	d.p = (E - kinetic - 0.5 * g.inv_mu0 * b2) * (g.gamma - 1.0);
+	d.rinv = recip(rho);
+	d.vx = __dmul_rn(mx, d.rinv);
+	d.vy = __dmul_rn(my, d.rinv);
+	d.vz = __dmul_rn(mz, d.rinv);
+	const double b2 = __fma_rn(bz, bz, __fma_rn(by, by, __dmul_rn(bx, bx)));
+	const double m2 = __fma_rn(mz, mz, __fma_rn(my, my, __dmul_rn(mx, mx)));
+	const double kinetic = __dmul_rn(__dmul_rn(0.5, d.rinv), m2);
+	const double magnetic = __dmul_rn(__dmul_rn(0.5, g.inv_mu0), b2);
+	d.p = __dmul_rn(__dsub_rn(__dsub_rn(E, kinetic), magnetic), g.gamma - 1.0);
 	d.bad = 0;
 	if (not (rho > 0.0 and is_normal(rho))) {
 		d.bad = PAMHD_FLAG_DENSITY;
 	} else if (not (d.p > 0.0 and is_normal(d.p))) {
 		d.bad = PAMHD_FLAG_PRESSURE;
 	}
-	const double cs2 = g.gamma * d.p * d.rinv;
+	const double cs2 = __dmul_rn(__dmul_rn(g.gamma, d.p), d.rinv);
 	if (b2 > 0.0) {
-		const double va2 = b2 * g.inv_mu0 * d.rinv;
-		const double sum2 = cs2 + va2;
-		const double inv_b2 = 1.0 / b2;
-		const double prod = 2.0 * cs2 * va2;
-		const double base = cs2 * cs2 + va2 * va2;
+		const double va2 = __dmul_rn(__dmul_rn(b2, g.inv_mu0), d.rinv);
+		const double sum2 = __dadd_rn(cs2, va2);
+		const double inv_b2 = recip(b2);
+		const double prod = __dmul_rn(__dmul_rn(2.0, cs2), va2);
+		const double base = __fma_rn(va2, va2, __dmul_rn(cs2, cs2));
 		const double comp[3] = {bx, by, bz};
 		const bool need[3] = {NEED_X, NEED_Y, NEED_Z};
 		bool wave_ok = is_normal(sum2) and is_finite(b2);
@@ -102,14 +126,14 @@ __device__ __forceinline__ Derived derive(
 				d.cf[a] = 0.0;
 				continue;
 			}
-			const double cos2 = comp[a] * comp[a] * inv_b2;
-			const double to_sqrt = base + prod * (1.0 - 2.0 * cos2);
+			const double cos2 = __dmul_rn(__dmul_rn(comp[a], comp[a]), inv_b2);
+			const double to_sqrt = __fma_rn(prod, __fma_rn(-2.0, cos2, 1.0), base);
 			wave_ok = wave_ok and to_sqrt > 0.0 and is_normal(to_sqrt);
-			d.cf[a] = sqrt(0.5 * (sum2 + sqrt(fmax(to_sqrt, 0.0))));
+			d.cf[a] = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(sum2, __dsqrt_rn(fmax(to_sqrt, 0.0)))));
 		}
 		if (d.bad == 0 and not wave_ok) d.bad = PAMHD_FLAG_WAVE_SPEED;
 	} else {
-		const double cs = sqrt(fmax(cs2, 0.0));
+		const double cs = __dsqrt_rn(fmax(cs2, 0.0));
 		d.cf[0] = d.cf[1] = d.cf[2] = cs;
 		if (d.bad == 0 and not is_finite(b2)) d.bad = PAMHD_FLAG_WAVE_SPEED;
 	}
@@ -256,7 +280,7 @@ __device__ __forceinline__ double flux_hll(const Side& L, const Side& R, const G
 	}
 	const double UL[8] = {L.rho, L.m0, L.m1, L.m2, L.E, L.b0, L.b1, L.b2};
 	const double UR[8] = {R.rho, R.m0, R.m1, R.m2, R.E, R.b0, R.b1, R.b2};
-	const double w = 0.5 * (bp + bm) / width;
+	const double w = 0.5 * (bp + bm) * recip(width);
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
 		const double a = (v == 5) ? 0.0 : FL[v] - bm * UL[v];
@@ -290,61 +314,65 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	}
 
 	const double bx = 0.5 * (L.b0 + R.b0);
-	const double bx2 = bx * bx;
-	const double bx2_mu = bx2 * g.inv_mu0;
-	const double sdL = s_neg - L.v0, sdR = s_pos - R.v0;
+	const double bx2_mu = bx * bx * g.inv_mu0;
+	const double sdL = s_neg - L.v0, sdR = s_pos - R.v0;       // < 0 and > 0 here
 	const double ptL = L.p + pbL, ptR = R.p + pbR;
-	// eqn 38
-	const double s_mid = (sdR * R.m0 - sdL * L.m0 - ptR + ptL) / (sdR * R.rho - sdL * L.rho);
-	const double smL = s_neg - s_mid, smR = s_pos - s_mid;
-	const double ismL = 1.0 / smL, ismR = 1.0 / smR;
+	// eqn 38; the denominator is sdR rho_R - sdL rho_L > 0
+	const double s_mid = (sdR * R.m0 - sdL * L.m0 - ptR + ptL) * recip(sdR * R.rho - sdL * L.rho);
+	const double smL = s_neg - s_mid, smR = s_pos - s_mid;     // < 0 and > 0 for physical states
+	const double ismL = recip(smL), ismR = recip(smR);
 	// eqn 43
 	const double rsL = L.rho * sdL * ismL, rsR = R.rho * sdR * ismR;
 	const double sqL = sqrt(rsL), sqR = sqrt(rsR);
-	const double isqL = 1.0 / sqL, isqR = 1.0 / sqR;
 	// eqn 51
 	const double abx = fabs(bx) * g.inv_sqrt_mu0;
-	const double ssL = s_mid - abx * isqL, ssR = s_mid + abx * isqR;
+	const double ssL = s_mid - abx * recip(sqL), ssR = s_mid + abx * recip(sqR);
 	const double ptst = ptL + L.rho * sdL * (s_mid - L.v0);
 	const double thr = DBL_EPS * ptst;
 
-	// star states, eqns 44-48
-	double uL[8], uR[8], vbL, vbR;
+	/*
+	Star states, eqns 44-48.  The star velocity is (v - B t1) (non-degenerate)
+	or v (degenerate): computed directly instead of dividing the star
+	momentum by the star density.
+	*/
+	double uL[8], uR[8], wL1, wL2, wR1, wR2, vbL, vbR;
 	{
 		const double tmp = L.rho * sdL * smL - bx2_mu;
-		double m1, m2, b1, b2;
-		if (fabs(tmp) < thr) {
-			m1 = rsL * L.v1; m2 = rsL * L.v2; b1 = L.b1; b2 = L.b2;
-		} else {
-			const double it = 1.0 / tmp;
+		double b1 = L.b1, b2 = L.b2;
+		wL1 = L.v1;
+		wL2 = L.v2;
+		if (not (fabs(tmp) < thr)) {
+			const double it = recip(tmp);
 			const double t1 = bx * (s_mid - L.v0) * g.inv_mu0 * it;
 			const double t2 = (L.rho * sdL * sdL - bx2_mu) * it;
-			m1 = rsL * (L.v1 - L.b1 * t1); m2 = rsL * (L.v2 - L.b2 * t1);
-			b1 = L.b1 * t2; b2 = L.b2 * t2;
+			wL1 = L.v1 - L.b1 * t1;
+			wL2 = L.v2 - L.b2 * t1;
+			b1 = L.b1 * t2;
+			b2 = L.b2 * t2;
 		}
-		const double m0 = rsL * s_mid;
-		vbL = (m0 * bx + m1 * b1 + m2 * b2) / rsL;
+		vbL = s_mid * bx + wL1 * b1 + wL2 * b2;
 		const double vb = L.v0 * L.b0 + L.v1 * L.b1 + L.v2 * L.b2;
-		uL[0] = rsL; uL[1] = m0; uL[2] = m1; uL[3] = m2;
+		uL[0] = rsL; uL[1] = rsL * s_mid; uL[2] = rsL * wL1; uL[3] = rsL * wL2;
 		uL[4] = (sdL * L.E - ptL * L.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vbL)) * ismL;
 		uL[5] = bx; uL[6] = b1; uL[7] = b2;
 	}
 	{
 		const double tmp = R.rho * sdR * smR - bx2_mu;
-		double m1, m2, b1, b2;
-		if (fabs(tmp) < thr) {
-			m1 = rsR * R.v1; m2 = rsR * R.v2; b1 = R.b1; b2 = R.b2;
-		} else {
-			const double it = 1.0 / tmp;
+		double b1 = R.b1, b2 = R.b2;
+		wR1 = R.v1;
+		wR2 = R.v2;
+		if (not (fabs(tmp) < thr)) {
+			const double it = recip(tmp);
 			const double t1 = bx * (s_mid - R.v0) * g.inv_mu0 * it;
 			const double t2 = (R.rho * sdR * sdR - bx2_mu) * it;
-			m1 = rsR * (R.v1 - R.b1 * t1); m2 = rsR * (R.v2 - R.b2 * t1);
-			b1 = R.b1 * t2; b2 = R.b2 * t2;
+			wR1 = R.v1 - R.b1 * t1;
+			wR2 = R.v2 - R.b2 * t1;
+			b1 = R.b1 * t2;
+			b2 = R.b2 * t2;
 		}
-		const double m0 = rsR * s_mid;
-		vbR = (m0 * bx + m1 * b1 + m2 * b2) / rsR;
+		vbR = s_mid * bx + wR1 * b1 + wR2 * b2;
 		const double vb = R.v0 * R.b0 + R.v1 * R.b1 + R.v2 * R.b2;
-		uR[0] = rsR; uR[1] = m0; uR[2] = m1; uR[3] = m2;
+		uR[0] = rsR; uR[1] = rsR * s_mid; uR[2] = rsR * wR1; uR[3] = rsR * wR2;
 		uR[4] = (sdR * R.E - ptR * R.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vbR)) * ismR;
 		uR[5] = bx; uR[6] = b1; uR[7] = b2;
 	}
@@ -352,6 +380,7 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	const double UL[8] = {L.rho, L.m0, L.m1, L.m2, L.E, L.b0, L.b1, L.b2};
 	const double UR[8] = {R.rho, R.m0, R.m1, R.m2, R.E, R.b0, R.b1, R.b2};
 
+	// region order of hlld_athena.hpp:475-552: S*_L >= 0, S_M >= 0, S*_R > 0, else
 	if (ssL >= 0.0) {
 		physical_flux(L, pbL, g, F);
 		#pragma unroll
@@ -359,7 +388,6 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 		F[5] = 0.0;
 		return fmax(fabs(s_neg), fabs(s_pos));
 	}
-	// region order of hlld_athena.hpp:475-552: S*_L >= 0, S_M >= 0, S*_R > 0, else
 	const bool left = s_mid >= 0.0;
 	if (not left and not (ssR > 0.0)) {
 		physical_flux(R, pbR, g, F);
@@ -372,20 +400,18 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	// double-star states, eqns 59-63 (identical to the star states when Bx ~ 0)
 	double u2[8];
 	const double* us = left ? uL : uR;
-	if (0.5 * bx2 < thr) {
+	if (0.5 * bx * bx < thr) {
 		#pragma unroll
 		for (int v = 0; v < 8; v++) u2[v] = us[v];
 	} else {
-		const double inv_sum = 1.0 / (sqL + sqR);
+		const double inv_sum = recip(sqL + sqR);
 		const double sgn = (bx > 0.0) ? 1.0 : -1.0;
-		const double irL = 1.0 / rsL, irR = 1.0 / rsR;
-		const double vL1 = uL[2] * irL, vL2 = uL[3] * irL, vR1 = uR[2] * irR, vR2 = uR[3] * irR;
 		const double cv = sgn * g.inv_sqrt_mu0;
-		const double v1 = inv_sum * ((sqL * vL1 + sqR * vR1) + cv * (uR[6] - uL[6]));
-		const double v2 = inv_sum * ((sqL * vL2 + sqR * vR2) + cv * (uR[7] - uL[7]));
+		const double v1 = inv_sum * ((sqL * wL1 + sqR * wR1) + cv * (uR[6] - uL[6]));
+		const double v2 = inv_sum * ((sqL * wL2 + sqR * wR2) + cv * (uR[7] - uL[7]));
 		const double wb = sgn * sqL * sqR * g.sqrt_mu0;
-		const double b1 = inv_sum * ((sqL * uR[6] + sqR * uL[6]) + wb * (vR1 - vL1));
-		const double b2 = inv_sum * ((sqL * uR[7] + sqR * uL[7]) + wb * (vR2 - vL2));
+		const double b1 = inv_sum * ((sqL * uR[6] + sqR * uL[6]) + wb * (wR1 - wL1));
+		const double b2 = inv_sum * ((sqL * uR[7] + sqR * uL[7]) + wb * (wR2 - wL2));
 		const double vb2 = s_mid * bx + v1 * b1 + v2 * b2;
 		const double rs = us[0];
 		u2[0] = rs;

@@ -98,6 +98,7 @@ int launch_face_flux(int solver, long long n, const double* neg, const double* p
 int launch_totals(const double* state, const Layout& L, double volume, double* partial, int nblocks,
                   cudaStream_t stream);
 int step_smem_bytes(int ty);
+int step_tile_rows();
 
 } // namespace pamhd_b200
 

@@ -1,7 +1,7 @@
 /*
 Kernels of the fused finite-volume MHD step (sm_100a, FP64 CUDA cores).
 
-step_kernel<SOLVER, TY> - one launch = one whole step (the reference's
+step_kernel<SOLVER, TY, MINB> - one launch = one whole step (the reference's
   get_all_fluxes + update_mhd_state + minimize_timestep, mhd/solve.hpp:
   1702-1811, :1518-1614, :1933-2014, in their cell-centred form):
   * a block owns a 32 x TY column tile and marches along z through a chunk
@@ -31,6 +31,14 @@ and one z plane per chunk are solved twice.
 namespace pamhd_b200 {
 
 constexpr int TX = 32;
+#ifndef PAMHD_TY
+#define PAMHD_TY 4
+#endif
+#ifndef PAMHD_MINB
+#define PAMHD_MINB 3
+#endif
+constexpr int TY_3D = PAMHD_TY;     // tile rows of 2-D and 3-D grids
+constexpr int MINB = PAMHD_MINB;    // resident blocks per SM asked of the register allocator
 constexpr int NV = 13;  // record: rho, mom xyz, E, B xyz, 1/rho, p, cf x, cf y, cf z
 enum { R_RINV = 8, R_P = 9, R_CF = 10 };
 
@@ -47,7 +55,12 @@ template <int TY> struct Tile {
 
 int step_smem_bytes(const int ty)
 {
-	return ty == 1 ? int(Tile<1>::BYTES) : int(Tile<8>::BYTES);
+	return ty == 1 ? int(Tile<1>::BYTES) : int(Tile<TY_3D>::BYTES);
+}
+
+int step_tile_rows()
+{
+	return TY_3D;
 }
 
 // ------------------------------------------------------------------ helpers
@@ -242,6 +255,7 @@ __device__ __forceinline__ void load_record(const Step_Params& P, double* rec, u
 	bad[ri] = d.bad;
 }
 
+// one cell of a record slot seen from a face normal to axis A (rotation by index permutation)
 template <int A>
 __device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, const int cells, const int ri)
 {
@@ -260,35 +274,42 @@ __device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, 
 	return s;
 }
 
-// solve one face, fold its speed into the running max, store dt * F in the xyz frame
-template <int SOLVER, int A>
-__device__ __forceinline__ void face(const Step_Params& P, const Side& L, const Side& R, const double dt,
-                                     double* dst, const int stride, double smax[3], bool& zero,
-                                     const int i, const int j, const int k)
+/*
+Solves one face normal to axis A, folds its speed into the running max and
+stores dt * F in the xyz frame.  Each kernel inlines this once per axis, so
+a face is computed by the same instructions wherever it lies in the tiling.
+*/
+template <int SOLVER, int CELLS, int A>
+__device__ __forceinline__ void solve_axis(const Step_Params& P, const double* rec_l, const uint32_t* bad_l,
+                                           const int ri_l, const double* rec_r, const uint32_t* bad_r,
+                                           const int ri_r, const double dt, double d[8],
+                                           double& smax, bool& zero, const int i, const int j, const int k)
 {
+	const Side L = side_at<A>(rec_l, bad_l, CELLS, ri_l);
+	const Side R = side_at<A>(rec_r, bad_r, CELLS, ri_r);
 	double F[8];
 	uint32_t flag = 0;
 	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
 	if (flag != 0) record_failure(P, flag, i, j, k, A + 1);
-	smax[A] = fmax(smax[A], s);
+	smax = fmax(smax, s);
 	zero = zero or not (s > 0.0);
 	double m0, m1, m2, b0, b1, b2;
 	unrotate<A>(F[1], F[2], F[3], m0, m1, m2);
 	unrotate<A>(F[5], F[6], F[7], b0, b1, b2);
-	dst[0 * stride] = dt * F[0];
-	dst[1 * stride] = dt * m0;
-	dst[2 * stride] = dt * m1;
-	dst[3 * stride] = dt * m2;
-	dst[4 * stride] = dt * F[4];
-	dst[5 * stride] = dt * b0;
-	dst[6 * stride] = dt * b1;
-	dst[7 * stride] = dt * b2;
+	d[0] = dt * F[0];
+	d[1] = dt * m0;
+	d[2] = dt * m1;
+	d[3] = dt * m2;
+	d[4] = dt * F[4];
+	d[5] = dt * b0;
+	d[6] = dt * b1;
+	d[7] = dt * b2;
 }
 
 // ------------------------------------------------------------------ the step
 
-template <int SOLVER, int TY>
-__global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
+template <int SOLVER, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P)
 {
 	using T = Tile<TY>;
 	extern __shared__ __align__(16) double smem[];
@@ -304,7 +325,14 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 	constexpr bool YACT = TY > 1;
 	const bool zact = P.active[2] != 0;
 	const int nx = P.L.n[0], ny = P.L.n[1];
-	const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+	const int tx = threadIdx.x, ty = threadIdx.y;
+	const int warp = ty, lane = tx;  // TX = 32: one warp per tile row
+	// warps given the halo columns and the tile's extra +x / +y faces (kept apart from the
+	// warps loading the halo rows, so that no warp does more than one extra pass per phase)
+	static_assert(TY == 1 or TY >= 4, "tile rows: 1 or at least 4");
+	constexpr int XHALO_WARP = TY >= 4 ? 2 : 0;
+	constexpr int XFACE_WARP = TY >= 4 ? TY - 2 : 0;
+	constexpr int YFACE_WARP = TY >= 4 ? TY - 1 : 0;
 	const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
 	const int gx = gx0 + tx, gy = gy0 + ty;
 	const bool own = gx < nx and gy < ny;
@@ -316,7 +344,7 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
 
-	double smax[3] = {0.0, 0.0, 0.0};
+	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	bool zero = false;
 	double Up[8], Fzm[8];
 	#pragma unroll
@@ -332,66 +360,67 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 
 		// (a) stage the plane: own cells, and the halo for planes with x / y faces
 		if (stage) load_record<true, YACT, true>(P, rec, bad, T::CELLS, ri, gx, gy, k);
+		// halo, spread over warps: the rows below / above the tile on warps 0 and 1, the columns
+		// left / right of it on warp 2 (warp 0 when y is inactive)
 		if (inner) {
-			if (tid < 2 * TY) {
-				const int row = tid % TY;
-				const bool right = tid >= TY;
+			if (YACT and warp < 2) {
+				const bool top = warp == 1;
+				const int hy = top ? gy0 + TY : gy0 - 1;
+				if (gx0 + lane < nx and hy <= ny) {
+					const int hri = (top ? TY + 1 : 0) * T::W + lane + 1;
+					load_record<false, true, false>(P, rec, bad, T::CELLS, hri, gx0 + lane, hy, k);
+				}
+			} else if (warp == XHALO_WARP and lane < 2 * TY) {
+				const int row = lane % TY;
+				const bool right = lane >= TY;
 				const int hx = right ? gx0 + TX : gx0 - 1;
 				if (gy0 + row < ny and hx <= nx) {
 					const int hri = (row + T::JO) * T::W + (right ? TX + 1 : 0);
 					load_record<true, false, false>(P, rec, bad, T::CELLS, hri, hx, gy0 + row, k);
 				}
-			} else if (YACT and tid < 2 * TY + 2 * TX) {
-				const int col = (tid - 2 * TY) % TX;
-				const bool top = tid >= 2 * TY + TX;
-				const int hy = top ? gy0 + TY : gy0 - 1;
-				if (gx0 + col < nx and hy <= ny) {
-					const int hri = (top ? TY + 1 : 0) * T::W + col + 1;
-					load_record<false, true, false>(P, rec, bad, T::CELLS, hri, gx0 + col, hy, k);
-				}
 			}
 		}
 		__syncthreads();
 
-		// (b) faces
-		double Fz[8];
+		// (b) faces: every thread its -x, -y and -z face; the tile's last column and row also need
+		// their +x / +y faces, taken by the first TY + TX threads in a second pass of the same loop
 		if (inner) {
-			if (gx0 + tx <= nx and gy < ny) {
-				const Side L = side_at<0>(rec, bad, T::CELLS, ri - 1);
-				const Side R = side_at<0>(rec, bad, T::CELLS, ri);
-				face<SOLVER, 0>(P, L, R, dt, fx + ty * (TX + 1) + tx, T::FXN, smax, zero, gx - 1, gy, k);
-			}
-			if (YACT and gy0 + ty <= ny and gx < nx) {
-				const Side L = side_at<1>(rec, bad, T::CELLS, ri - T::W);
-				const Side R = side_at<1>(rec, bad, T::CELLS, ri);
-				face<SOLVER, 1>(P, L, R, dt, fy + ty * TX + tx, T::FYN, smax, zero, gx, gy - 1, k);
-			}
-			if (tid < TY) {
-				// the +x face of the tile's last column
-				const int row = tid;
-				if (gx0 + TX <= nx and gy0 + row < ny) {
-					const int r2 = (row + T::JO) * T::W + TX;
-					const Side L = side_at<0>(rec, bad, T::CELLS, r2);
-					const Side R = side_at<0>(rec, bad, T::CELLS, r2 + 1);
-					face<SOLVER, 0>(P, L, R, dt, fx + row * (TX + 1) + TX, T::FXN, smax, zero,
-					                gx0 + TX - 1, gy0 + row, k);
+			#pragma unroll 1
+			for (int pass = 0; pass < 2; pass++) {
+				const bool extra = pass == 1;
+				if (extra and warp != XFACE_WARP) break;
+				const int row = extra ? lane : ty;
+				const int col = extra ? TX : tx;
+				if ((extra ? lane < TY : true) and gx0 + col <= nx and gy0 + row < ny) {
+					const int r = (row + T::JO) * T::W + col;
+					double F[8];
+					solve_axis<SOLVER, T::CELLS, 0>(P, rec, bad, r, rec, bad, r + 1, dt, F, s0, zero,
+					                                gx0 + col - 1, gy0 + row, k);
+					#pragma unroll
+					for (int v = 0; v < 8; v++) fx[v * T::FXN + row * (TX + 1) + col] = F[v];
 				}
-			} else if (YACT and tid < TY + TX) {
-				// the +y face of the tile's last row
-				const int col = tid - TY;
-				if (gy0 + TY <= ny and gx0 + col < nx) {
-					const int r2 = TY * T::W + col + 1;
-					const Side L = side_at<1>(rec, bad, T::CELLS, r2);
-					const Side R = side_at<1>(rec, bad, T::CELLS, r2 + T::W);
-					face<SOLVER, 1>(P, L, R, dt, fy + TY * TX + col, T::FYN, smax, zero,
-					                gx0 + col, gy0 + TY - 1, k);
+			}
+			if (YACT) {
+				#pragma unroll 1
+				for (int pass = 0; pass < 2; pass++) {
+					const bool extra = pass == 1;
+					if (extra and warp != YFACE_WARP) break;
+					const int row = extra ? TY : ty;
+					const int col = tx;
+					if (gy0 + row <= ny and gx0 + col < nx) {
+						const int r = row * T::W + col + 1;
+						double F[8];
+						solve_axis<SOLVER, T::CELLS, 1>(P, rec, bad, r, rec, bad, r + T::W, dt, F, s1, zero,
+						                                gx0 + col, gy0 + row - 1, k);
+						#pragma unroll
+						for (int v = 0; v < 8; v++) fy[v * T::FYN + row * TX + col] = F[v];
+					}
 				}
 			}
 		}
+		double Fz[8];
 		if (zact and k > kfirst and own) {
-			const Side L = side_at<2>(prev, prev_bad, T::CELLS, ri);
-			const Side R = side_at<2>(rec, bad, T::CELLS, ri);
-			face<SOLVER, 2>(P, L, R, dt, Fz, 1, smax, zero, gx, gy, k - 1);
+			solve_axis<SOLVER, T::CELLS, 2>(P, prev, prev_bad, ri, rec, bad, ri, dt, Fz, s2, zero, gx, gy, k - 1);
 		}
 		__syncthreads();
 
@@ -425,6 +454,7 @@ __global__ void __launch_bounds__(TX * TY) step_kernel(const Step_Params P)
 			}
 		}
 	}
+	double smax[3] = {s0, s1, s2};
 	flush_speeds(P, smax, zero);
 }
 
@@ -676,7 +706,7 @@ __global__ void totals_kernel(const double* __restrict__ state, const Layout L, 
 template <int SOLVER, int TY>
 static int prepare_t()
 {
-	const cudaError_t e = cudaFuncSetAttribute(step_kernel<SOLVER, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	const cudaError_t e = cudaFuncSetAttribute(step_kernel<SOLVER, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                                           int(Tile<TY>::BYTES));
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
@@ -684,10 +714,10 @@ static int prepare_t()
 int prepare_step_kernels(const int solver, const bool y)
 {
 	switch (solver) {
-	case PAMHD_RUSANOV: return y ? prepare_t<PAMHD_RUSANOV, 8>() : prepare_t<PAMHD_RUSANOV, 1>();
-	case PAMHD_HLL_ATHENA: return y ? prepare_t<PAMHD_HLL_ATHENA, 8>() : prepare_t<PAMHD_HLL_ATHENA, 1>();
-	case PAMHD_HLLD_ATHENA: return y ? prepare_t<PAMHD_HLLD_ATHENA, 8>() : prepare_t<PAMHD_HLLD_ATHENA, 1>();
-	case PAMHD_ROE_ATHENA: return y ? prepare_t<PAMHD_ROE_ATHENA, 8>() : prepare_t<PAMHD_ROE_ATHENA, 1>();
+	case PAMHD_RUSANOV: return y ? prepare_t<PAMHD_RUSANOV, TY_3D>() : prepare_t<PAMHD_RUSANOV, 1>();
+	case PAMHD_HLL_ATHENA: return y ? prepare_t<PAMHD_HLL_ATHENA, TY_3D>() : prepare_t<PAMHD_HLL_ATHENA, 1>();
+	case PAMHD_HLLD_ATHENA: return y ? prepare_t<PAMHD_HLLD_ATHENA, TY_3D>() : prepare_t<PAMHD_HLLD_ATHENA, 1>();
+	case PAMHD_ROE_ATHENA: return y ? prepare_t<PAMHD_ROE_ATHENA, TY_3D>() : prepare_t<PAMHD_ROE_ATHENA, 1>();
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 }
@@ -699,7 +729,7 @@ static int launch_step_t(const Step_Params& P, cudaStream_t stream)
 	const dim3 block(TX, TY);
 	const dim3 grid((P.L.n[0] + TX - 1) / TX, (P.L.n[1] + TY - 1) / TY,
 	                (P.L.n[2] + P.kchunk - 1) / P.kchunk);
-	step_kernel<SOLVER, TY><<<grid, block, smem, stream>>>(P);
+	step_kernel<SOLVER, TY, MINB><<<grid, block, smem, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -707,10 +737,10 @@ int launch_step(const Step_Params& P, const int solver, cudaStream_t stream)
 {
 	const bool y = P.active[1] != 0;
 	switch (solver) {
-	case PAMHD_RUSANOV: return y ? launch_step_t<PAMHD_RUSANOV, 8>(P, stream) : launch_step_t<PAMHD_RUSANOV, 1>(P, stream);
-	case PAMHD_HLL_ATHENA: return y ? launch_step_t<PAMHD_HLL_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_HLL_ATHENA, 1>(P, stream);
-	case PAMHD_HLLD_ATHENA: return y ? launch_step_t<PAMHD_HLLD_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_HLLD_ATHENA, 1>(P, stream);
-	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, 8>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
+	case PAMHD_RUSANOV: return y ? launch_step_t<PAMHD_RUSANOV, TY_3D>(P, stream) : launch_step_t<PAMHD_RUSANOV, 1>(P, stream);
+	case PAMHD_HLL_ATHENA: return y ? launch_step_t<PAMHD_HLL_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_HLL_ATHENA, 1>(P, stream);
+	case PAMHD_HLLD_ATHENA: return y ? launch_step_t<PAMHD_HLLD_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_HLLD_ATHENA, 1>(P, stream);
+	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 }
