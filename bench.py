@@ -52,6 +52,7 @@ def args_():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--n", type=int, default=256, help="cells per dimension")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true")
     return p.parse_args()
 
 
@@ -191,6 +192,67 @@ def cpu_baseline(U_full, n):
         "kind": kind,
         "sample": f"{steps} HLLD steps on a {n}x{n}x{planes} periodic slab of the blast initial state "
                   f"({el:.1f} s wall on {threads} threads, std::thread over cells)",
+    }
+
+
+def batched_section(local, steps=500):
+    """Batched ensemble (64 uneven SI solar-wind boxes, HLL, 500 steps) in one batch against the same
+    boxes run one after another, each in its own context (sequential per-box launches)."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+
+    boxes = states.solar_wind_ensemble()
+    cfgs = [pg.Config(n=(b["n"],) * 3, solver=pg.HLL, cell_length=(states.EARTH_RADIUS_CELL,) * 3,
+                      adiabatic_index=5 / 3, vacuum_permeability=states.MU0_SI, time_step_factor=0.5,
+                      bc_lo=(pg.BC_VALUE, pg.BC_COPY, pg.BC_COPY), bc_hi=(pg.BC_COPY,) * 3,
+                      value_lo=[b["inflow"], None, None], device=local) for b in boxes]
+    cells = sum(b["n"] ** 3 for b in boxes)
+    dev = torch.device("cuda", local)
+
+    batch = pg.Batch(cfgs, device=local)
+    for i, b in enumerate(boxes):
+        batch.set_state(i, states.ensemble_state(b))
+    planes, grid = batch.tune(3)
+    st = torch.cuda.ExternalStream(batch.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    batch.steps(steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    batch.sync()
+    batched_ms = e0.elapsed_time(e1)
+    batch.close()
+
+    plain_ms = 0.0
+    for cfg, b in zip(cfgs, boxes):
+        ctx = pg.Context(cfg)
+        ctx.set_state(states.ensemble_state(b))
+        cs = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        p0.record(cs)
+        ctx.steps(steps, 1e300)
+        p1.record(cs)
+        torch.cuda.synchronize()
+        ctx.sync()
+        plain_ms += p0.elapsed_time(p1)
+        ctx.close()
+    batched = cells * steps / (batched_ms / 1e3)
+    plain = cells * steps / (plain_ms / 1e3)
+    return {
+        "workload": f"{len(boxes)} independent SI solar-wind boxes, edges from {{32,48,64,96,128}} "
+                    f"({cells} cells), HLL, inflow -x, copy elsewhere, per-box CFL 0.5 timestep, {steps} steps",
+        "value": batched,
+        "unit": UNIT,
+        "ms": batched_ms,
+        "plain_sequential": plain,
+        "plain_ms": plain_ms,
+        "batched_over_plain": batched / plain,
+        "tuned": {"planes_per_item": planes, "grid": grid},
+        "what": "batched: one launch per step for all boxes, graph-replayed; plain: each box in its own "
+                "context, one box after another (the same kernels); device time by CUDA events",
     }
 
 
@@ -397,6 +459,8 @@ def run_b200(a):
         "gpu_launches": a.steps,
         "clocks": clocks.summary(),
     }
+    if not a.no_batched:
+        line["batched"] = batched_section(local)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)

@@ -220,6 +220,44 @@ int pamhd_gpu_face_flux(
 	double adiabatic_index, double vacuum_permeability,
 	double* flux, double* speed, uint32_t* flags);
 
+/*
+Batched ensemble: independent uniform boxes of uneven sizes (each its own
+pamhd_cfg: cells, cell size, boundary kinds and values) advanced together,
+one kernel launch per step for the whole ensemble, each box with its own
+CFL timestep and clock.  The reference advances one grid per program
+(tests/mhd/test.cpp, tests/mhd/solar_wind_box.cpp); an ensemble there is
+one run per box, which pamhd_gpu_create / pamhd_gpu_steps reproduce box
+by box.  All boxes use the same solver and the same active dimensions.
+*/
+typedef struct pamhd_batch pamhd_batch;
+
+int pamhd_gpu_batch_create(int32_t device, int32_t nboxes, const pamhd_cfg* cfgs, pamhd_batch** batch);
+int pamhd_gpu_batch_destroy(pamhd_batch* batch);
+
+/*
+Copies the interior state of one box in from host arrays and fills its
+ghosts.  Any set_state restarts the whole ensemble's step count: the next
+step is a dt = 0 priming step for every box.
+*/
+int pamhd_gpu_batch_set_state(pamhd_batch* batch, int32_t box, const double* const soa[8]);
+int pamhd_gpu_batch_get_state(pamhd_batch* batch, int32_t box, double* const soa[8]);
+
+/* nsteps steps of every box, each capped so that its time does not pass t_end; no host sync. */
+int pamhd_gpu_batch_steps(pamhd_batch* batch, int32_t nsteps, double t_end);
+
+/*
+Autotuner: times trial_steps steps of the loaded ensemble for each
+candidate number of z planes per work item and resident grid size, keeps
+the fastest and restores the state it started from.
+*/
+int pamhd_gpu_batch_tune(pamhd_batch* batch, int32_t trial_steps, int32_t* planes, int32_t* grid);
+
+int pamhd_gpu_batch_sync(pamhd_batch* batch);
+int pamhd_gpu_batch_get_stream(pamhd_batch* batch, void** stream);
+int pamhd_gpu_batch_time(pamhd_batch* batch, int32_t box, double* time, int64_t* steps, double* last_dt);
+int pamhd_gpu_batch_dt_history(pamhd_batch* batch, int32_t box, double* dt, int32_t count, int32_t* written);
+int pamhd_gpu_batch_status(pamhd_batch* batch, int32_t box, uint32_t* flags, int32_t cell[3], int32_t* dir);
+
 #ifdef __cplusplus
 }
 #endif

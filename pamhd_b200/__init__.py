@@ -133,6 +133,19 @@ def lib() -> ctypes.CDLL:
     L.pamhd_gpu_totals.argtypes = [ctypes.c_void_p, _DP]
     L.pamhd_gpu_face_flux.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _DP, _DP, _DP, _D, _D,
                                       _DP, _DP, _P(ctypes.c_uint32)]
+    V = ctypes.c_void_p
+    L.pamhd_gpu_batch_create.argtypes = [ctypes.c_int32, ctypes.c_int32, _P(_Cfg), _P(V)]
+    L.pamhd_gpu_batch_destroy.argtypes = [V]
+    L.pamhd_gpu_batch_set_state.argtypes = [V, ctypes.c_int32, V]
+    L.pamhd_gpu_batch_get_state.argtypes = [V, ctypes.c_int32, V]
+    L.pamhd_gpu_batch_steps.argtypes = [V, ctypes.c_int32, _D]
+    L.pamhd_gpu_batch_tune.argtypes = [V, ctypes.c_int32, _P(ctypes.c_int32), _P(ctypes.c_int32)]
+    L.pamhd_gpu_batch_sync.argtypes = [V]
+    L.pamhd_gpu_batch_get_stream.argtypes = [V, _P(V)]
+    L.pamhd_gpu_batch_time.argtypes = [V, ctypes.c_int32, _DP, _P(ctypes.c_int64), _DP]
+    L.pamhd_gpu_batch_dt_history.argtypes = [V, ctypes.c_int32, _DP, ctypes.c_int32, _P(ctypes.c_int32)]
+    L.pamhd_gpu_batch_status.argtypes = [V, ctypes.c_int32, _P(ctypes.c_uint32), _P(ctypes.c_int32),
+                                         _P(ctypes.c_int32)]
     if L.pamhd_gpu_abi_version() != 1:
         raise ImportError("libpamhd_gpu.so ABI version mismatch")
     _lib = L
@@ -272,3 +285,88 @@ def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
     if rc not in (OK, ERR_PHYSICS):
         raise PamhdError(rc, "pamhd_gpu_face_flux")
     return flux, speed, flags
+
+
+class Batch:
+    """A pamhd_batch: independent boxes advanced together, each with its own timestep."""
+
+    def __init__(self, cfgs, device: int = 0):
+        self.L = lib()
+        self.cfgs = list(cfgs)
+        self.shapes = [(int(c.n[2]), int(c.n[1]), int(c.n[0])) for c in self.cfgs]
+        arr = (_Cfg * len(self.cfgs))(*[c.to_c() for c in self.cfgs])
+        self._arr = arr
+        h = ctypes.c_void_p()
+        rc = self.L.pamhd_gpu_batch_create(device, len(self.cfgs), arr, ctypes.byref(h))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pamhd_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc, what, box=None):
+        if rc == ERR_PHYSICS:
+            boxes = range(len(self.cfgs)) if box is None else [box]
+            for b in boxes:
+                flags, cell, d = self.status(b)
+                if flags:
+                    raise PhysicsError(rc, f"{what} (box {b})", flags, cell, d)
+            raise PhysicsError(rc, what)
+        if rc != OK:
+            raise PamhdError(rc, what)
+
+    def set_state(self, box: int, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shapes[box])
+        self._check(self.L.pamhd_gpu_batch_set_state(self.h, box, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_batch_set_state")
+
+    def get_state(self, box: int) -> np.ndarray:
+        U = np.empty((8,) + self.shapes[box])
+        self._check(self.L.pamhd_gpu_batch_get_state(self.h, box, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_batch_get_state")
+        return U
+
+    def steps(self, n: int, t_end: float = 1e300):
+        self._check(self.L.pamhd_gpu_batch_steps(self.h, int(n), float(t_end)), "pamhd_gpu_batch_steps")
+
+    def tune(self, trial_steps: int = 3):
+        planes, grid = ctypes.c_int32(0), ctypes.c_int32(0)
+        self._check(self.L.pamhd_gpu_batch_tune(self.h, trial_steps, ctypes.byref(planes), ctypes.byref(grid)),
+                    "pamhd_gpu_batch_tune")
+        return planes.value, grid.value
+
+    def sync(self):
+        self._check(self.L.pamhd_gpu_batch_sync(self.h), "pamhd_gpu_batch_sync")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.pamhd_gpu_batch_get_stream(self.h, ctypes.byref(s)), "pamhd_gpu_batch_get_stream")
+        return int(s.value or 0)
+
+    def time(self, box: int):
+        t, n, dt = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_batch_time(self.h, box, ctypes.byref(t), ctypes.byref(n), ctypes.byref(dt)),
+                    "pamhd_gpu_batch_time")
+        return t.value, n.value, dt.value
+
+    def dt_history(self, box: int, count: int) -> np.ndarray:
+        out = np.zeros(count)
+        w = ctypes.c_int32(0)
+        self._check(self.L.pamhd_gpu_batch_dt_history(self.h, box, out.ctypes.data_as(_DP), count, ctypes.byref(w)),
+                    "pamhd_gpu_batch_dt_history")
+        return out[: w.value]
+
+    def status(self, box: int):
+        f = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.L.pamhd_gpu_batch_status(self.h, box, ctypes.byref(f), cell, ctypes.byref(d))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_batch_status")
+        return f.value, tuple(cell), d.value

@@ -17,6 +17,7 @@ six consecutive steps are captured once into a CUDA graph and replayed.
 #include <string>
 #include <vector>
 
+#include "grid_setup.cuh"
 #include "step.cuh"
 
 using namespace pamhd_b200;
@@ -55,87 +56,16 @@ int check(const cudaError_t e)
 
 #define PAMHD_TRY(expr) do { const int rc_ = (expr); if (rc_ != PAMHD_OK) return rc_; } while (0)
 
-int validate(const pamhd_cfg& c)
-{
-	if (c.reserved != 0) return PAMHD_ERR_ARGUMENT;
-	if (c.solver != PAMHD_RUSANOV and c.solver != PAMHD_HLL_ATHENA and c.solver != PAMHD_HLLD_ATHENA
-		and c.solver != PAMHD_ROE_ATHENA) {
-		return PAMHD_ERR_ARGUMENT;
-	}
-	for (int d = 0; d < 3; d++) {
-		if (c.n[d] < 1) return PAMHD_ERR_ARGUMENT;
-		if (not (c.cell_length[d] > 0.0) or not std::isfinite(c.cell_length[d])) return PAMHD_ERR_ARGUMENT;
-		for (const int b: {c.bc_lo[d], c.bc_hi[d]}) {
-			if (b != PAMHD_BC_PERIODIC and b != PAMHD_BC_COPY and b != PAMHD_BC_VALUE) return PAMHD_ERR_ARGUMENT;
-		}
-		if (c.n[d] > 1 and ((c.bc_lo[d] == PAMHD_BC_PERIODIC) != (c.bc_hi[d] == PAMHD_BC_PERIODIC))) {
-			return PAMHD_ERR_ARGUMENT;
-		}
-	}
-	// active dimensions must be x, x-y or x-y-z
-	if (c.n[0] < 2) return PAMHD_ERR_ARGUMENT;
-	if (c.n[1] < 2 and c.n[2] > 1) return PAMHD_ERR_ARGUMENT;
-	if (not (c.adiabatic_index > 1.0) or not (c.vacuum_permeability > 0.0) or not (c.time_step_factor > 0.0)) {
-		return PAMHD_ERR_ARGUMENT;
-	}
-	return PAMHD_OK;
-}
-
-Layout make_layout(const pamhd_cfg& c)
-{
-	Layout L;
-	for (int d = 0; d < 3; d++) {
-		L.n[d] = c.n[d];
-		L.g[d] = c.n[d] > 1 ? 1 : 0;
-	}
-	L.xoff = 4;  // ghost column at 3: interior rows start 32-byte aligned
-	L.pitch = ((L.xoff + L.n[0] + 1) + 3) / 4 * 4;
-	L.rows = L.n[1] + 2 * L.g[1];
-	L.planes = L.n[2] + 2 * L.g[2];
-	L.plane = (long long)L.pitch * L.rows;
-	L.var = (L.plane * L.planes + 31) / 32 * 32;
-	return L;
-}
-
 void set_params(pamhd_ctx& x)
 {
-	const pamhd_cfg& c = x.cfg;
+	x.needs_boundary_speeds = grid_params(x.cfg, x.L, x.base);
 	Step_Params& P = x.base;
-	std::memset(&P, 0, sizeof P);
-	P.L = x.L;
-	P.gas.gamma = c.adiabatic_index;
-	P.gas.mu0 = c.vacuum_permeability;
-	P.gas.inv_mu0 = 1.0 / c.vacuum_permeability;
-	P.gas.sqrt_mu0 = std::sqrt(c.vacuum_permeability);
-	P.gas.inv_sqrt_mu0 = 1.0 / std::sqrt(c.vacuum_permeability);
-	P.cfl = c.time_step_factor;
-	x.needs_boundary_speeds = false;
-	int active_count = 0;
-	for (int d = 0; d < 3; d++) {
-		P.len[d] = c.cell_length[d];
-		P.inv_len[d] = 1.0 / c.cell_length[d];
-		P.active[d] = c.n[d] > 1;
-		P.periodic[d] = P.active[d] and c.bc_lo[d] == PAMHD_BC_PERIODIC;
-		P.bc_lo[d] = c.bc_lo[d];
-		P.bc_hi[d] = c.bc_hi[d];
-		P.ext[d] = (P.active[d] and not P.periodic[d]) ? 1 : 0;
-		active_count += P.active[d];
-	}
-	for (int d = 0; d < 3; d++) {
-		if (P.active[d] and not P.periodic[d] and active_count > 1) x.needs_boundary_speeds = true;
-	}
 	P.red = x.red;
 	P.clock = x.clock;
 	P.status = x.status;
 	P.control = x.control;
 	P.dt_hist = x.dt_hist;
 	P.hist_len = x.hist_len;
-	// z planes per block: enough blocks for several waves on 148 SMs, few redundant z faces
-	const int ty = P.active[1] ? step_tile_rows() : 1;
-	const long long tiles = (long long)((c.n[0] + 31) / 32) * ((c.n[1] + ty - 1) / ty);
-	long long chunks = (2368 + tiles - 1) / tiles;
-	chunks = std::max(1LL, std::min(chunks, (long long)std::max(1, c.n[2] / 16)));
-	P.kchunk = int((c.n[2] + chunks - 1) / chunks);
 }
 
 Step_Params params_for(const pamhd_ctx& x, const long long step, const int cur)

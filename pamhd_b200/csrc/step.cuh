@@ -99,6 +99,12 @@ int launch_totals(const double* state, const Layout& L, double volume, double* p
                   cudaStream_t stream);
 int step_smem_bytes(int ty);
 int step_tile_rows();
+int prepare_batch_kernels(int solver, bool y_active);
+int batch_blocks_per_sm(int solver, bool y_active, int* blocks);
+int launch_batch_step(const Step_Params* boxes, const int4* items, int nitems, int phase, int grid, int solver,
+                      bool y_active, cudaStream_t stream);
+int launch_batch_boundary_speeds(const Step_Params* boxes, int nboxes, int largest, int phase, int solver,
+                                 cudaStream_t stream);
 
 } // namespace pamhd_b200
 

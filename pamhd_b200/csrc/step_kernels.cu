@@ -308,19 +308,22 @@ __device__ __forceinline__ void solve_axis(const Step_Params& P, const double* r
 
 // ------------------------------------------------------------------ the step
 
-template <int SOLVER, int TY, int MINB>
-__global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P)
+/*
+One work item of a step: the tile (bx, by) of 32 x TY columns over the z
+chunk bz, marched plane by plane; the face speeds are folded into
+s0, s1, s2 and zero (flushed by the caller).  Shared by the single-grid
+and the batched kernels, so that both compute the same bits.
+*/
+template <int SOLVER, int TY>
+__device__ __forceinline__ void tile_step(const Step_Params& P, double* const smem, const double dt,
+                                          const int bx, const int by, const int bz,
+                                          double& s0, double& s1, double& s2, bool& zero)
 {
 	using T = Tile<TY>;
-	extern __shared__ __align__(16) double smem[];
-	__shared__ double s_dt;
 	double* const rec_base = smem;
 	double* const fx = smem + 2 * T::REC;        // [8][TY][TX + 1]
 	double* const fy = fx + 8 * T::FXN;          // [8][TY + 1][TX]
 	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(fy + 8 * T::FYN);
-
-	const bool first_block = blockIdx.x == 0 and blockIdx.y == 0 and blockIdx.z == 0;
-	const double dt = begin_step(P, &s_dt, first_block);
 
 	constexpr bool YACT = TY > 1;
 	const bool zact = P.active[2] != 0;
@@ -333,19 +336,17 @@ __global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P
 	constexpr int XHALO_WARP = TY >= 4 ? 2 : 0;
 	constexpr int XFACE_WARP = TY >= 4 ? TY - 2 : 0;
 	constexpr int YFACE_WARP = TY >= 4 ? TY - 1 : 0;
-	const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
+	const int gx0 = bx * TX, gy0 = by * TY;
 	const int gx = gx0 + tx, gy = gy0 + ty;
 	const bool own = gx < nx and gy < ny;
 	// the +x / +y ghost of a partial tile lies inside the tile's own columns / rows
 	const bool stage = gx <= nx and (TY == 1 ? gy == 0 : gy <= ny);
-	const int kb = blockIdx.z * P.kchunk;
+	const int kb = bz * P.kchunk;
 	const int ke = min(P.L.n[2], kb + P.kchunk);
 	const int kfirst = zact ? kb - 1 : kb;
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
 
-	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-	bool zero = false;
 	double Up[8], Fzm[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) Up[v] = Fzm[v] = 0.0;
@@ -454,8 +455,55 @@ __global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P
 			}
 		}
 	}
+}
+
+template <int SOLVER, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P)
+{
+	extern __shared__ __align__(16) double smem[];
+	__shared__ double s_dt;
+	const bool first_block = blockIdx.x == 0 and blockIdx.y == 0 and blockIdx.z == 0;
+	const double dt = begin_step(P, &s_dt, first_block);
+	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+	bool zero = false;
+	tile_step<SOLVER, TY>(P, smem, dt, blockIdx.x, blockIdx.y, blockIdx.z, s0, s1, s2, zero);
 	double smax[3] = {s0, s1, s2};
 	flush_speeds(P, smax, zero);
+}
+
+/*
+The batched step: every box of an ensemble advances one step in one launch.
+Blocks walk the work-item table (box, tile x, tile y, z chunk) with a grid
+stride; each box has its own parameters (state buffers, layout, boundary
+kinds, reduction ring, clock, status), so each advances with its own dt.
+The block holding a box's first item advances that box's clock.
+*/
+template <int SOLVER, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) batch_step_kernel(const Step_Params* __restrict__ boxes,
+                                                                  const int4* __restrict__ items,
+                                                                  const int nitems, const int phase)
+{
+	extern __shared__ __align__(16) double smem[];
+	__shared__ Step_Params sp;
+	__shared__ double s_dt;
+	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+	for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+		const int4 w = items[item];
+		__syncthreads();  // the previous item is done with sp
+		if (tid == 0) {
+			sp = boxes[w.x];
+			sp.phase = phase;
+		}
+		__syncthreads();
+		const bool first = w.y == 0 and w.z == 0 and w.w == 0;
+		const double dt = begin_step(sp, &s_dt, first);
+		const int tiles_x = (sp.L.n[0] + TX - 1) / TX;
+		double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+		bool zero = false;
+		tile_step<SOLVER, TY>(sp, smem, dt, w.y % tiles_x, w.y / tiles_x, w.z, s0, s1, s2, zero);
+		double smax[3] = {s0, s1, s2};
+		flush_speeds(sp, smax, zero);
+	}
 }
 
 /*
@@ -466,10 +514,8 @@ enter the timestep (:1965-2005); their fluxes change nothing.
 blockIdx.y enumerates (ghost dimension d, side, tangential axis e).
 */
 template <int SOLVER>
-__global__ void boundary_speed_kernel(const Step_Params P)
+__device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 {
-	__shared__ double s_dt;
-	(void)s_dt;
 	int combos[12][3];
 	int nc = 0;
 	for (int d = 0; d < 3; d++) {
@@ -531,6 +577,25 @@ __global__ void boundary_speed_kernel(const Step_Params P)
 		}
 	}
 	flush_speeds(P, smax, zero);
+}
+
+template <int SOLVER>
+__global__ void boundary_speed_kernel(const Step_Params P)
+{
+	boundary_speeds<SOLVER>(P);
+}
+
+// the same for every box of a batch: blockIdx.z is the box
+template <int SOLVER>
+__global__ void batch_boundary_speed_kernel(const Step_Params* __restrict__ boxes, const int phase)
+{
+	__shared__ Step_Params sp;
+	if (threadIdx.x == 0) {
+		sp = boxes[blockIdx.z];
+		sp.phase = phase;
+	}
+	__syncthreads();
+	boundary_speeds<SOLVER>(sp);
 }
 
 // ------------------------------------------------------------------ layout and ghosts
@@ -743,6 +808,81 @@ int launch_step(const Step_Params& P, const int solver, cudaStream_t stream)
 	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
 	default: return PAMHD_ERR_ARGUMENT;
 	}
+}
+
+template <int SOLVER, int TY>
+static int prepare_batch_t()
+{
+	const cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<SOLVER, TY, MINB>,
+	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tile<TY>::BYTES));
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int prepare_batch_kernels(const int solver, const bool y)
+{
+	switch (solver) {
+	case PAMHD_RUSANOV: return y ? prepare_batch_t<PAMHD_RUSANOV, TY_3D>() : prepare_batch_t<PAMHD_RUSANOV, 1>();
+	case PAMHD_HLL_ATHENA: return y ? prepare_batch_t<PAMHD_HLL_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_HLL_ATHENA, 1>();
+	case PAMHD_HLLD_ATHENA: return y ? prepare_batch_t<PAMHD_HLLD_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_HLLD_ATHENA, 1>();
+	case PAMHD_ROE_ATHENA: return y ? prepare_batch_t<PAMHD_ROE_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_ROE_ATHENA, 1>();
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+int batch_blocks_per_sm(const int solver, const bool y, int* blocks)
+{
+	cudaError_t e = cudaErrorInvalidValue;
+	#define PAMHD_OCC(S) \
+		e = y ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<S, TY_3D, MINB>, \
+		                                                    TX * TY_3D, Tile<TY_3D>::BYTES) \
+		      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<S, 1, MINB>, TX, Tile<1>::BYTES)
+	switch (solver) {
+	case PAMHD_RUSANOV: PAMHD_OCC(PAMHD_RUSANOV); break;
+	case PAMHD_HLL_ATHENA: PAMHD_OCC(PAMHD_HLL_ATHENA); break;
+	case PAMHD_HLLD_ATHENA: PAMHD_OCC(PAMHD_HLLD_ATHENA); break;
+	case PAMHD_ROE_ATHENA: PAMHD_OCC(PAMHD_ROE_ATHENA); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	#undef PAMHD_OCC
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+template <int SOLVER, int TY>
+static void launch_batch_t(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
+                           const int grid, cudaStream_t stream)
+{
+	batch_step_kernel<SOLVER, TY, MINB><<<grid, dim3(TX, TY), Tile<TY>::BYTES, stream>>>(boxes, items, nitems, phase);
+}
+
+int launch_batch_step(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
+                      const int grid, const int solver, const bool y, cudaStream_t stream)
+{
+	switch (solver) {
+	case PAMHD_RUSANOV: y ? launch_batch_t<PAMHD_RUSANOV, TY_3D>(boxes, items, nitems, phase, grid, stream)
+	                      : launch_batch_t<PAMHD_RUSANOV, 1>(boxes, items, nitems, phase, grid, stream); break;
+	case PAMHD_HLL_ATHENA: y ? launch_batch_t<PAMHD_HLL_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
+	                         : launch_batch_t<PAMHD_HLL_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
+	case PAMHD_HLLD_ATHENA: y ? launch_batch_t<PAMHD_HLLD_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
+	                          : launch_batch_t<PAMHD_HLLD_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
+	case PAMHD_ROE_ATHENA: y ? launch_batch_t<PAMHD_ROE_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
+	                         : launch_batch_t<PAMHD_ROE_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_batch_boundary_speeds(const Step_Params* boxes, const int nboxes, const int largest, const int phase,
+                                 const int solver, cudaStream_t stream)
+{
+	const dim3 grid(min(1024, (largest + 255) / 256), 12, nboxes);
+	switch (solver) {
+	case PAMHD_RUSANOV: batch_boundary_speed_kernel<PAMHD_RUSANOV><<<grid, 256, 0, stream>>>(boxes, phase); break;
+	case PAMHD_HLL_ATHENA: batch_boundary_speed_kernel<PAMHD_HLL_ATHENA><<<grid, 256, 0, stream>>>(boxes, phase); break;
+	case PAMHD_HLLD_ATHENA: batch_boundary_speed_kernel<PAMHD_HLLD_ATHENA><<<grid, 256, 0, stream>>>(boxes, phase); break;
+	case PAMHD_ROE_ATHENA: batch_boundary_speed_kernel<PAMHD_ROE_ATHENA><<<grid, 256, 0, stream>>>(boxes, phase); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
 int launch_boundary_speeds(const Step_Params& P, const int solver, cudaStream_t stream)

@@ -182,3 +182,45 @@ def blast_wave(n, seed=20261203, gamma=GAMMA_53, amp=0.01, kmax=8):
     U[4] = p / (gamma - 1) + 0.5 * (B ** 2).sum(axis=0)
     U[5:8] = B
     return U
+
+
+PROTON_MASS = 1.672621777e-27   # simulation_options.hpp:61
+MU0_SI = 4e-7 * np.pi            # simulation_options.hpp:60
+K_BOLTZMANN = 1.380649e-23
+EARTH_RADIUS_CELL = 6.371e5      # cell size of the reference's solar-wind box configs (m)
+
+
+def solar_wind_ensemble(nboxes=64, seed=20261204, sizes=(32, 48, 64, 96, 128), gamma=GAMMA_53):
+    """The batched-ensemble configuration: `nboxes` independent cubes with edge drawn uniformly
+    from `sizes`, SI units, each with its own seeded solar wind entering through the -x face:
+    n ~ U[1, 20] cm^-3, |v_x| ~ U[300, 800] km/s pointing into the box (+x), |B| ~ U[1, 20] nT
+    with an isotropic random direction, T log-uniform on [1e4, 1e6] K, p = n k_B T.  The interior
+    starts at rest with a quarter of the wind density, the wind temperature and field.
+    Returns a list of dicts: n (edge), inflow (8 conservative values), interior (8 conservative
+    values of the uniform initial state; ensemble_state() expands it to (8, n, n, n))."""
+    rng = np.random.default_rng(seed)
+    boxes = []
+    for _ in range(nboxes):
+        n = int(rng.choice(sizes))
+        dens = rng.uniform(1.0, 20.0) * 1e6
+        speed = rng.uniform(300.0, 800.0) * 1e3
+        bmag = rng.uniform(1.0, 20.0) * 1e-9
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        T = 10 ** rng.uniform(4.0, 6.0)
+        rho = dens * PROTON_MASS
+        v = np.array([speed, 0.0, 0.0])
+        B = bmag * d
+        p = dens * K_BOLTZMANN * T
+        inflow = np.array([rho, *(rho * v), energy(rho, v[:, None], p, B[:, None], gamma, MU0_SI)[0], *B])
+        rho0 = 0.25 * rho
+        p0 = 0.25 * dens * K_BOLTZMANN * T
+        interior = np.array([rho0, 0.0, 0.0, 0.0,
+                             energy(rho0, np.zeros((3, 1)), p0, B[:, None], gamma, MU0_SI)[0], *B])
+        boxes.append({"n": n, "inflow": inflow, "interior": interior})
+    return boxes
+
+
+def ensemble_state(box):
+    n = box["n"]
+    return np.broadcast_to(box["interior"][:, None, None, None], (8, n, n, n)).copy()

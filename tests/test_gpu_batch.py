@@ -1,0 +1,120 @@
+"""The batched ensemble (pamhd_gpu_batch_*) through the C ABI.
+
+A batch runs the same tile code as a single-grid context, so every box of a
+batch must match, bit for bit, the same box run alone; one box is also held
+to the CPU oracle at the step tolerance of test_gpu_parity.py (1e-12,
+field-normwise)."""
+import numpy as np
+import pytest
+
+import pamhd_b200 as pg
+from oracle import pyoracle as po
+import states
+
+pytestmark = pytest.mark.gpu
+
+
+def wind_cfg(n, inflow, solver=pg.HLL, shape=None):
+    shape = shape or (n, n, n)
+    return pg.Config(n=shape, solver=solver, cell_length=(states.EARTH_RADIUS_CELL,) * 3,
+                     adiabatic_index=5 / 3, vacuum_permeability=states.MU0_SI, time_step_factor=0.5,
+                     bc_lo=(pg.BC_VALUE, pg.BC_COPY, pg.BC_COPY), bc_hi=(pg.BC_COPY,) * 3,
+                     value_lo=[inflow, None, None])
+
+
+def small_ensemble():
+    boxes = states.solar_wind_ensemble(nboxes=5, sizes=(12, 17, 24, 33))
+    cfgs, U0s = [], []
+    for i, b in enumerate(boxes):
+        n = b["n"]
+        shape = (n, n + i, max(2, n - 2 * i))  # uneven boxes, not cubes
+        cfgs.append(wind_cfg(n, b["inflow"], shape=shape))
+        U = np.broadcast_to(b["interior"][:, None, None, None], (8, shape[2], shape[1], shape[0])).copy()
+        rng = np.random.default_rng(i)
+        U[0] *= 1 + 0.05 * rng.random(U[0].shape)  # some structure
+        U0s.append(U)
+    return cfgs, U0s
+
+
+def test_batch_equals_single_contexts_bitwise():
+    cfgs, U0s = small_ensemble()
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.steps(14)
+    batch.sync()
+    for i, (cfg, U) in enumerate(zip(cfgs, U0s)):
+        ctx = pg.Context(cfg)
+        ctx.set_state(U)
+        ctx.steps(14, 1e300)
+        ctx.sync()
+        np.testing.assert_array_equal(batch.get_state(i), ctx.get_state())
+        np.testing.assert_array_equal(batch.dt_history(i, 14), ctx.dt_history(14))
+        assert batch.time(i) == ctx.time()
+
+
+def test_boxes_take_their_own_timesteps():
+    cfgs, U0s = small_ensemble()
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.steps(5)
+    dts = [batch.time(i)[2] for i in range(len(cfgs))]
+    assert len(set(dts)) == len(dts) and min(dts) > 0
+
+
+def test_batch_box_matches_oracle(port):
+    b = states.solar_wind_ensemble(nboxes=1, sizes=(20,))[0]
+    n = b["n"]
+    U = states.ensemble_state(b)
+    U[0] *= 1 + 0.1 * np.random.default_rng(3).random(U[0].shape)
+    cfg = wind_cfg(n, b["inflow"])
+    batch = pg.Batch([cfg, wind_cfg(12, b["inflow"])])
+    batch.set_state(0, U)
+    batch.set_state(1, states.ensemble_state({"n": 12, "interior": b["interior"]}))
+    ora = port.grid(po.make_cfg((n, n, n), po.HLL, (states.EARTH_RADIUS_CELL,) * 3, 5 / 3, states.MU0_SI, 0.5,
+                                bc_lo=(po.BC_VALUE, po.BC_COPY, po.BC_COPY), bc_hi=(po.BC_COPY,) * 3,
+                                value_lo=[b["inflow"], None, None]), threads=8)
+    ora.set_state(U)
+    for step in range(4):
+        batch.steps(1)
+        do, flag, _, _ = ora.step(1e300)
+        assert flag == 0
+        dg = batch.time(0)[2]
+        assert abs(dg - do) <= 1e-12 * max(do, 1e-300) or dg == do == 0.0
+        a = batch.get_state(0).reshape(8, -1)
+        o = ora.get_state().reshape(8, -1)
+        scale = np.abs(o).max(axis=1)
+        scale[scale == 0] = 1.0
+        assert (np.abs(a - o).max(axis=1) / scale).max() <= 1e-12 * (1 + step)
+
+
+def test_tuner_restores_state():
+    cfgs, U0s = small_ensemble()
+    tuned, plain = pg.Batch(cfgs), pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        tuned.set_state(i, U)
+        plain.set_state(i, U)
+    planes, grid = tuned.tune(2)
+    assert planes in (8, 16, 32, 64) and grid >= 1
+    for i, U in enumerate(U0s):
+        np.testing.assert_array_equal(tuned.get_state(i), U)
+    tuned.steps(9)
+    plain.steps(9)
+    for i in range(len(cfgs)):
+        np.testing.assert_array_equal(tuned.get_state(i), plain.get_state(i))
+
+
+def test_batch_reports_failing_box():
+    cfgs, U0s = small_ensemble()
+    U0s[2] = U0s[2].copy()
+    U0s[2][4, 1, 2, 3] = 0.0  # negative pressure in box 2
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.steps(1)
+    with pytest.raises(pg.PhysicsError) as e:
+        batch.sync()
+    assert "box 2" in str(e.value) and e.value.flags == pg.FLAG_PRESSURE
+    for i in (0, 1, 3, 4):
+        assert batch.status(i)[0] == 0
