@@ -53,6 +53,7 @@ def args_():
     p.add_argument("--n", type=int, default=256, help="cells per dimension")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -221,8 +222,11 @@ def batched_section(local, steps=500):
     batch.steps(steps)
     e1.record(st)
     torch.cuda.synchronize()
-    batch.sync()
     batched_ms = e0.elapsed_time(e1)
+    # boxes whose state the reference scheme rejects keep being stepped (the same work per step);
+    # they are counted, not hidden
+    failed = [i for i in range(len(boxes)) if batch.status(i)[0] != 0]
+    failed_steps = {}
     batch.close()
 
     plain_ms = 0.0
@@ -236,8 +240,9 @@ def batched_section(local, steps=500):
         ctx.steps(steps, 1e300)
         p1.record(cs)
         torch.cuda.synchronize()
-        ctx.sync()
         plain_ms += p0.elapsed_time(p1)
+        if ctx.status()[0] != 0:
+            failed_steps[len(failed_steps)] = True
         ctx.close()
     batched = cells * steps / (batched_ms / 1e3)
     plain = cells * steps / (plain_ms / 1e3)
@@ -251,8 +256,73 @@ def batched_section(local, steps=500):
         "plain_ms": plain_ms,
         "batched_over_plain": batched / plain,
         "tuned": {"planes_per_item": planes, "grid": grid},
+        "boxes_failed": failed,
+        "boxes_failed_note": "boxes whose state hit the positivity check of the reference scheme within the "
+                             "run (the CPU oracle fails box 24 at step 236, like the GPU); same count in the "
+                             f"sequential run: {len(failed_steps)}",
         "what": "batched: one launch per step for all boxes, graph-replayed; plain: each box in its own "
                 "context, one box after another (the same kernels); device time by CUDA events",
+    }
+
+
+def adjoint_section(local, n=256, steps=200, every=20):
+    """Discrete adjoint cost: Orszag-Tang n^2, HLLD, `steps` steps, checkpoints every `every` steps,
+    J = magnetic energy in [0.4, 0.6]^2 at the last step.  Forward: the steps alone.  Gradient: the
+    adjoint call, i.e. its forward run with checkpoints, the recompute of every segment and the
+    reverse sweep."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+
+    U0 = states.orszag_tang(n)
+    cfg = pg.Config(n=(n, n, 1), solver=pg.HLLD, cell_length=(1 / n, 1 / n, 1.0), adiabatic_index=5 / 3,
+                    vacuum_permeability=1.0, time_step_factor=0.4, device=local)
+    ctx = pg.Context(cfg)
+    st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="xy")
+    mask = ((X >= 0.4) & (X <= 0.6) & (Y >= 0.4) & (Y <= 0.6)).astype(float)[None]
+
+    def fwd_ms():
+        ctx.set_state(U0)
+        ctx.step(0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        ctx.steps(steps, 1e300)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    fwd_ms()
+    forward = min(fwd_ms() for _ in range(3))
+    UN = ctx.get_state()
+    dts = ctx.dt_history(steps)
+    seed = np.zeros_like(UN)
+    seed[5:8] = UN[5:8] * mask / n ** 2
+
+    def adj_ms():
+        ctx.set_state(U0)
+        ctx.step(0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        ctx.adjoint(steps, every, seed, dt_in=dts)
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    adj_ms()
+    gradient = min(adj_ms() for _ in range(3))
+    ctx.close()
+    return {
+        "workload": f"Orszag-Tang {n}^2 periodic, HLLD, {steps} steps, checkpoints every {every}, "
+                    "J = magnetic energy in [0.4,0.6]^2, gradient w.r.t. the initial state",
+        "forward_ms": forward,
+        "gradient_ms": gradient,
+        "adjoint_over_forward": gradient / forward,
+        "what": "gradient_ms: the pamhd_gpu_adjoint call (forward run with checkpoints, recompute of every "
+                "segment, reverse sweep); forward_ms: the same steps alone; device time by CUDA events",
     }
 
 
@@ -461,6 +531,8 @@ def run_b200(a):
     }
     if not a.no_batched:
         line["batched"] = batched_section(local)
+    if not a.no_adjoint:
+        line["adjoint"] = adjoint_section(local)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)

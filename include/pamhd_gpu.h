@@ -221,6 +221,29 @@ int pamhd_gpu_face_flux(
 	double* flux, double* speed, uint32_t* flags);
 
 /*
+nsteps steps with the given dt each (host array), instead of the CFL rule:
+the forward map the adjoint linearises, for perturbed runs on a frozen dt
+schedule.  No reference counterpart (the reference always takes the CFL
+dt, mhd/solve.hpp:1870-1877).
+*/
+int pamhd_gpu_steps_dt(pamhd_ctx* ctx, int32_t nsteps, const double* dt);
+
+/*
+Discrete adjoint of nsteps steps from the context's current state U_0:
+runs the forward steps (CFL rule, or the dt_in schedule when not NULL),
+storing the state every `every` steps, leaves the context at U_N, then
+computes grad = (dU_N/dU_0)^T seed by a reverse sweep that recomputes each
+segment from its checkpoint, on the forward run's dt schedule held fixed.
+seed and grad: eight host arrays each (the layout of set_state).
+grad_value (NULL or 48 doubles): the gradient with respect to the state
+of each VALUE side, [dimension][lo, hi][8].  dt_out (NULL or nsteps
+doubles) receives the schedule.  Solvers: Rusanov, HLL, HLLD.  No
+reference counterpart: the reference has no derivatives.
+*/
+int pamhd_gpu_adjoint(pamhd_ctx* ctx, int32_t nsteps, int32_t every, const double* const seed[8],
+                      double* const grad[8], double* grad_value, const double* dt_in, double* dt_out);
+
+/*
 Batched ensemble: independent uniform boxes of uneven sizes (each its own
 pamhd_cfg: cells, cell size, boundary kinds and values) advanced together,
 one kernel launch per step for the whole ensemble, each box with its own

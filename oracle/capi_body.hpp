@@ -143,6 +143,22 @@ int ORACLE_API(grid_step)(void* grid, double max_dt, double* dt_taken,
 	return PAMHD_OK;
 }
 
+// one step with a prescribed dt (see Mode_C_Grid::step_with)
+int ORACLE_API(grid_step_dt)(void* grid, double dt, uint32_t* flag)
+{
+	Grid& g = *static_cast<Grid*>(grid);
+	*flag = 0;
+	try {
+		g.step_with(dt);
+	} catch (const oracle::Domain_Error& e) {
+		*flag = e.flag;
+		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
 // runs steps until t reaches t_end or max_steps steps were taken; returns steps taken or -1
 int64_t ORACLE_API(grid_run)(void* grid, double t_start, double t_end, int64_t max_steps,
                              double* t_reached, double* dt_history)

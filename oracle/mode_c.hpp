@@ -288,7 +288,16 @@ public:
 	// one step; returns dt taken; throws Domain_Error at the first failing face
 	double step(const double max_dt)
 	{
-		const double dt = timestep(max_dt);
+		return step_with(timestep(max_dt));
+	}
+
+	/*
+	One step with a given dt instead of the CFL rule (a frozen dt schedule, for
+	the perturbed runs that check the GPU adjoint); the face speeds are still
+	recorded as in step().
+	*/
+	double step_with(const double dt)
+	{
 		failure = Failure();
 		std::mutex fail_lock;
 		parallel(U.size(), [&](size_t a, size_t b) {

@@ -121,6 +121,8 @@ class Oracle:
         self._step = getattr(L, p + "grid_step")
         self._step.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                _P(ctypes.c_int32)]
+        self._step_dt = getattr(L, p + "grid_step_dt")
+        self._step_dt.argtypes = [ctypes.c_void_p, _D, _P(ctypes.c_uint32)]
         self._run = getattr(L, p + "grid_run")
         self._run.restype = ctypes.c_int64
         self._run.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int64, _DP, _DP]
@@ -204,6 +206,14 @@ class OracleGrid:
         if rc not in (0, 3):
             raise ValueError(self.o.last_error())
         return dt.value, flag.value, tuple(cell), d.value
+
+    def step_dt(self, dt):
+        """One step with a prescribed dt; returns the failure flag (0 when fine)."""
+        flag = ctypes.c_uint32(0)
+        rc = self.o._step_dt(self.h, dt, ctypes.byref(flag))
+        if rc not in (0, 3):
+            raise ValueError(self.o.last_error())
+        return flag.value
 
     def run(self, t_start, t_end, max_steps):
         hist = np.zeros(max_steps)

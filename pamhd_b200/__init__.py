@@ -134,6 +134,8 @@ def lib() -> ctypes.CDLL:
     L.pamhd_gpu_face_flux.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _DP, _DP, _DP, _D, _D,
                                       _DP, _DP, _P(ctypes.c_uint32)]
     V = ctypes.c_void_p
+    L.pamhd_gpu_steps_dt.argtypes = [V, ctypes.c_int32, _DP]
+    L.pamhd_gpu_adjoint.argtypes = [V, ctypes.c_int32, ctypes.c_int32, V, V, _DP, _DP, _DP]
     L.pamhd_gpu_batch_create.argtypes = [ctypes.c_int32, ctypes.c_int32, _P(_Cfg), _P(V)]
     L.pamhd_gpu_batch_destroy.argtypes = [V]
     L.pamhd_gpu_batch_set_state.argtypes = [V, ctypes.c_int32, V]
@@ -236,6 +238,30 @@ class Context:
 
     def sync(self):
         self._check(self.L.pamhd_gpu_sync(self.h), "pamhd_gpu_sync")
+
+    def steps_dt(self, dts):
+        """Steps with the given dt each (a frozen schedule) instead of the CFL rule."""
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        self._check(self.L.pamhd_gpu_steps_dt(self.h, len(dts), dts.ctypes.data_as(_DP)), "pamhd_gpu_steps_dt")
+
+    def adjoint(self, nsteps: int, every: int, seed: np.ndarray, dt_in=None):
+        """Runs nsteps steps (checkpoint every `every`) and returns (grad, grad_value, dts):
+        grad = (dU_N/dU_0)^T seed, grad_value = gradient with respect to the VALUE side states
+        (3, 2, 8), dts = the dt schedule used."""
+        seed = np.ascontiguousarray(seed, dtype=np.float64).reshape((8,) + self.shape)
+        grad = np.zeros((8,) + self.shape)
+        gv = np.zeros(48)
+        dts = np.zeros(nsteps)
+        din = None
+        if dt_in is not None:
+            dt_in = np.ascontiguousarray(dt_in, dtype=np.float64)
+            din = dt_in.ctypes.data_as(_DP)
+        rc = self.L.pamhd_gpu_adjoint(self.h, int(nsteps), int(every),
+                                      _pointers([seed[k].ctypes.data for k in range(8)]),
+                                      _pointers([grad[k].ctypes.data for k in range(8)]),
+                                      gv.ctypes.data_as(_DP), din, dts.ctypes.data_as(_DP))
+        self._check(rc, "pamhd_gpu_adjoint")
+        return grad, gv.reshape(3, 2, 8), dts
 
     def time(self):
         t, n, dt = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_double(0)

@@ -17,33 +17,9 @@ six consecutive steps are captured once into a CUDA graph and replayed.
 #include <string>
 #include <vector>
 
-#include "grid_setup.cuh"
-#include "step.cuh"
+#include "context.cuh"
 
 using namespace pamhd_b200;
-
-struct pamhd_ctx {
-	pamhd_cfg cfg;
-	int device = 0;
-	cudaStream_t stream = nullptr;
-	Layout L;
-	Step_Params base;
-	double* state[2] = {nullptr, nullptr};
-	int cur = 0;
-	Speed_Max* red = nullptr;
-	Clock* clock = nullptr;
-	Status* status = nullptr;
-	Control* control = nullptr;
-	double* dt_hist = nullptr;
-	int hist_len = 1 << 16;
-	long long steps = 0;
-	double* staging = nullptr;
-	double* partial = nullptr;
-	int partial_blocks = 296;
-	bool needs_boundary_speeds = false;
-	cudaGraphExec_t graph = nullptr;
-	bool loaded = false;
-};
 
 namespace {
 
@@ -86,6 +62,15 @@ int issue_step(pamhd_ctx& x)
 	x.steps++;
 	return PAMHD_OK;
 }
+
+} // namespace
+
+int pamhd_b200::context_issue_step(pamhd_ctx& x)
+{
+	return issue_step(x);
+}
+
+namespace {
 
 int reset_run_state(pamhd_ctx& x)
 {

@@ -1,0 +1,43 @@
+/*
+The single-grid context behind pamhd_ctx (include/pamhd_gpu.h), shared by
+the entry points of context.cu and the adjoint driver of adjoint.cu.
+*/
+#ifndef PAMHD_B200_CONTEXT_CUH
+#define PAMHD_B200_CONTEXT_CUH
+
+#include <cuda_runtime.h>
+
+#include "grid_setup.cuh"
+#include "step.cuh"
+
+using namespace pamhd_b200;
+
+struct pamhd_ctx {
+	pamhd_cfg cfg;
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	Layout L;
+	Step_Params base;
+	double* state[2] = {nullptr, nullptr};
+	int cur = 0;
+	Speed_Max* red = nullptr;
+	Clock* clock = nullptr;
+	Status* status = nullptr;
+	Control* control = nullptr;
+	double* dt_hist = nullptr;
+	int hist_len = 1 << 16;
+	long long steps = 0;
+	double* staging = nullptr;
+	double* partial = nullptr;
+	int partial_blocks = 296;
+	bool needs_boundary_speeds = false;
+	cudaGraphExec_t graph = nullptr;
+	bool loaded = false;
+};
+
+namespace pamhd_b200 {
+// the next step of a context (launch only; advances the step counter and parity)
+int context_issue_step(pamhd_ctx& x);
+}
+
+#endif

@@ -72,6 +72,7 @@ inline bool grid_params(const pamhd_cfg& c, const Layout& L, Step_Params& P, con
 	P.gas.sqrt_mu0 = std::sqrt(c.vacuum_permeability);
 	P.gas.inv_sqrt_mu0 = 1.0 / std::sqrt(c.vacuum_permeability);
 	P.cfl = c.time_step_factor;
+	P.forced_dt = -1.0;
 	bool needs_boundary_speeds = false;
 	int active_count = 0;
 	for (int d = 0; d < 3; d++) {

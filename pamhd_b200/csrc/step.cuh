@@ -83,6 +83,7 @@ struct Step_Params {
 	int hist_len;
 	int phase;           // step index mod 3
 	int kchunk;          // z planes per block
+	double forced_dt;    // >= 0: the step's dt (a prescribed schedule); < 0: the CFL rule
 };
 
 // launchers (step_kernels.cu)

@@ -81,6 +81,7 @@ face speed was <= 0; replaced by the cap when cap <= that minimum
 */
 __device__ __forceinline__ double step_dt(const Step_Params& P)
 {
+	if (P.forced_dt >= 0.0) return P.forced_dt;
 	const Speed_Max& r = P.red[P.phase];
 	bool zero = r.zero != 0;
 	double smallest = 1.7976931348623157e308;
