@@ -207,6 +207,28 @@ __host__ __device__ __forceinline__ void phys_reverse(const Side_Fwd& s, const G
 	a.v2 += -s.b0 * aF[7];
 }
 
+/*
+Kinks.  At a tie of max(a, b) / min(a, b) (equal to within round-off:
+symmetric data give exact-arithmetic ties that rounding breaks by an ulp),
+or at |x| with x = 0, the flux has no derivative; the adjoint then uses the average of the one-sided
+derivatives (half to each argument, 0 for |0|), which is what a central
+difference across the kink measures.  Ties are common, not exceptional, in
+symmetric data such as the Orszag-Tang vortex.
+*/
+__host__ __device__ __forceinline__ void max_rev(const double a, const double b, const double g, double& ga, double& gb)
+{
+	// arguments equal to within round-off are ties of the exact-arithmetic flux
+	const double tie = 1e-12 * fmax(fabs(a), fabs(b));
+	if (a > b + tie) ga += g;
+	else if (b > a + tie) gb += g;
+	else { ga += 0.5 * g; gb += 0.5 * g; }
+}
+
+__host__ __device__ __forceinline__ double abs_rev(const double x, const double g)
+{
+	return x > 0.0 ? g : (x < 0.0 ? -g : 0.0);
+}
+
 __host__ __device__ __forceinline__ void state_of(const Side_Fwd& s, double* U)
 {
 	U[0] = s.rho; U[1] = s.m0; U[2] = s.m1; U[3] = s.m2; U[4] = s.E; U[5] = s.b0; U[6] = s.b1; U[7] = s.b2;
@@ -253,10 +275,11 @@ __host__ __device__ __forceinline__ void rusanov_vjp(const double* UL, const dou
 	phys_reverse(L, g, aFh, AL);
 	phys_reverse(R, g, aFh, AR);
 	// s = max(|vL0|, |vR0|) + max(cfL, cfR)
-	if (aL >= aR) AL.v0 += (L.v0 >= 0.0 ? 1.0 : -1.0) * a_s;
-	else AR.v0 += (R.v0 >= 0.0 ? 1.0 : -1.0) * a_s;
-	if (L.cf >= R.cf) AL.cf += a_s;
-	else AR.cf += a_s;
+	double a_aL = 0.0, a_aR = 0.0;
+	max_rev(aL, aR, a_s, a_aL, a_aR);
+	AL.v0 += abs_rev(L.v0, a_aL);
+	AR.v0 += abs_rev(R.v0, a_aR);
+	max_rev(L.cf, R.cf, a_s, AL.cf, AR.cf);
 	side_reverse(L, AL, g, gL);
 	side_reverse(R, AR, g, gR);
 }
@@ -324,18 +347,13 @@ __host__ __device__ __forceinline__ void hll_vjp(const double* UL, const double*
 	add_state(AR, dUR);
 	phys_reverse(L, g, aa, AL);
 	phys_reverse(R, g, ab, AR);
-	const double a_sneg = bm_on ? a_bm : 0.0;
-	const double a_spos = bp_on ? a_bp : 0.0;
-	if (order) {
-		AL.v0 += a_sneg;
-		AR.v0 += a_spos;
-	} else {
-		AR.v0 += a_sneg;
-		AL.v0 += a_spos;
-	}
-	const double a_fast = -a_sneg + a_spos;
-	if (left_fast) AL.cf += a_fast;
-	else AR.cf += a_fast;
+	// bm = min(s_neg, 0), bp = max(s_pos, 0)
+	const double a_sneg = s_neg < 0.0 ? a_bm : (s_neg == 0.0 ? 0.5 * a_bm : 0.0);
+	const double a_spos = s_pos > 0.0 ? a_bp : (s_pos == 0.0 ? 0.5 * a_bp : 0.0);
+	// s_neg = min(vL0, vR0) - fast, s_pos = max(vL0, vR0) + fast
+	max_rev(L.v0, R.v0, a_spos, AL.v0, AR.v0);
+	max_rev(R.v0, L.v0, a_sneg, AL.v0, AR.v0);
+	max_rev(L.cf, R.cf, -a_sneg + a_spos, AL.cf, AR.cf);
 	side_reverse(L, AL, g, gL);
 	side_reverse(R, AR, g, gR);
 }
@@ -653,7 +671,7 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 	const double a_abx = -a_ssL / sqL + a_ssR / sqR;
 	a_sqL += abx / (sqL * sqL) * a_ssL;
 	a_sqR += -abx / (sqR * sqR) * a_ssR;
-	a_bx += (bx >= 0.0 ? 1.0 : -1.0) * g.inv_sqrt_mu0 * a_abx;
+	a_bx += abs_rev(bx, g.inv_sqrt_mu0 * a_abx);
 	// sq = sqrt(rs)
 	a_rsL += 0.5 / sqL * a_sqL;
 	a_rsR += 0.5 / sqR * a_sqR;
@@ -691,10 +709,10 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 	// bx = (bL0 + bR0) / 2
 	AL.b0 += 0.5 * a_bx;
 	AR.b0 += 0.5 * a_bx;
-	// s_neg, s_pos
-	if (order) { AL.v0 += a_sneg; AR.v0 += a_spos; } else { AR.v0 += a_sneg; AL.v0 += a_spos; }
-	const double a_fast = -a_sneg + a_spos;
-	if (left_fast) AL.cf += a_fast; else AR.cf += a_fast;
+	// s_neg = min(vL0, vR0) - fast, s_pos = max(vL0, vR0) + fast, fast = max(cfL, cfR)
+	max_rev(L.v0, R.v0, a_spos, AL.v0, AR.v0);
+	max_rev(R.v0, L.v0, a_sneg, AL.v0, AR.v0);
+	max_rev(L.cf, R.cf, -a_sneg + a_spos, AL.cf, AR.cf);
 	side_reverse(L, AL, g, gL);
 	side_reverse(R, AR, g, gR);
 }
