@@ -41,7 +41,9 @@ enum {
 	PAMHD_ERR_PHYSICS = 3,   /* a solver met a state the reference throws on
 	                            (see pamhd_gpu_status for which and where) */
 	PAMHD_ERR_STATE = 4,     /* call made in the wrong order */
-	PAMHD_ERR_TIMEOUT = 5    /* a bounded device-side wait gave up */
+	PAMHD_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+	PAMHD_ERR_TOO_LARGE = 6  /* request larger than the fixed scratch of a
+	                            no-alloc entry point (split it) */
 };
 
 /*
@@ -215,6 +217,33 @@ means zero), speed n, flags n (0 or PAMHD_FLAG_* of the first check that
 failed).  Runs on `device`; returns PAMHD_ERR_PHYSICS if any face failed.
 */
 int pamhd_gpu_face_flux(
+	int32_t device, int32_t solver, int64_t n,
+	const double* neg, const double* pos, const double* bg,
+	double adiabatic_index, double vacuum_permeability,
+	double* flux, double* speed, uint32_t* flags);
+
+/* Most faces one pamhd_gpu_face_flux_noalloc call takes. */
+#define PAMHD_NOALLOC_MAX_FACES 16384
+
+/*
+pamhd_gpu_face_flux without device memory allocation.  No reference
+counterpart: the reference evaluates its solvers on the host.  Same
+arguments, results and return codes as pamhd_gpu_face_flux, for callers
+that cannot allocate device memory once set up (device memory reserved by
+another allocator, or a loop that cannot take the device-wide
+synchronisation of cudaMalloc / cudaFree).  Faces are staged through a
+fixed 3.56 MiB scratch area of this library's device code instead of
+per-call buffers, so:
+  - n > PAMHD_NOALLOC_MAX_FACES is rejected with PAMHD_ERR_TOO_LARGE
+    before any CUDA call: split the faces into calls of at most that many;
+  - all calls on one device share the scratch, so calls that overlap in
+    time (from several host threads) race: serialise them;
+  - the first call on a device does the set-up (loads this scratch, which
+    the CUDA driver places when it loads the library's device code, and
+    looks up its address): make it before any stream capture.
+Runs on the legacy default stream of `device`, synchronously.
+*/
+int pamhd_gpu_face_flux_noalloc(
 	int32_t device, int32_t solver, int64_t n,
 	const double* neg, const double* pos, const double* bg,
 	double adiabatic_index, double vacuum_permeability,

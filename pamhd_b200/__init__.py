@@ -29,6 +29,8 @@ SOLVERS = {"rusanov": RUSANOV, "hll_athena": HLL, "hlld_athena": HLLD, "roe_athe
 BC_PERIODIC, BC_COPY, BC_VALUE = 0, 1, 2
 
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_PHYSICS, ERR_STATE, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
+ERR_TOO_LARGE = 6
+NOALLOC_MAX_FACES = 16384
 FLAG_DENSITY, FLAG_PRESSURE, FLAG_WAVE_SPEED, FLAG_FLUX = 1, 2, 4, 8
 FLAG_ROE_DENSITY, FLAG_ROE_PRESSURE, FLAG_NEW_STATE, FLAG_TIMEOUT = 16, 32, 64, 128
 
@@ -310,6 +312,31 @@ def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
                                flags.ctypes.data_as(_P(ctypes.c_uint32)))
     if rc not in (OK, ERR_PHYSICS):
         raise PamhdError(rc, "pamhd_gpu_face_flux")
+    return flux, speed, flags
+
+
+def face_flux_noalloc(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
+    """face_flux through pamhd_gpu_face_flux_noalloc: no device allocation, at most
+    NOALLOC_MAX_FACES faces per call (PamhdError with ERR_TOO_LARGE beyond that); calls on one
+    device share one scratch area, so concurrent calls from several threads race."""
+    L = lib()
+    fn = L.pamhd_gpu_face_flux_noalloc
+    fn.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _DP, _DP, _DP, _D, _D, _DP, _DP,
+                   _P(ctypes.c_uint32)]
+    neg = np.ascontiguousarray(neg, dtype=np.float64)
+    pos = np.ascontiguousarray(pos, dtype=np.float64)
+    n = neg.shape[0]
+    flux = np.zeros((n, 8))
+    speed = np.zeros(n)
+    flags = np.zeros(n, dtype=np.uint32)
+    bgp = None
+    if bg is not None:
+        bg = np.ascontiguousarray(bg, dtype=np.float64)
+        bgp = bg.ctypes.data_as(_DP)
+    rc = fn(device, solver, n, neg.ctypes.data_as(_DP), pos.ctypes.data_as(_DP), bgp, gamma, mu0,
+            flux.ctypes.data_as(_DP), speed.ctypes.data_as(_DP), flags.ctypes.data_as(_P(ctypes.c_uint32)))
+    if rc not in (OK, ERR_PHYSICS):
+        raise PamhdError(rc, "pamhd_gpu_face_flux_noalloc")
     return flux, speed, flags
 
 

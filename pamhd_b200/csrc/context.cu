@@ -148,6 +148,7 @@ const char* pamhd_gpu_errstr(const int code)
 	case PAMHD_ERR_PHYSICS: return "a face met an invalid state (see pamhd_gpu_status)";
 	case PAMHD_ERR_STATE: return "call made in the wrong order";
 	case PAMHD_ERR_TIMEOUT: return "a bounded device wait expired";
+	case PAMHD_ERR_TOO_LARGE: return "request larger than the fixed scratch of a no-alloc entry point; split it";
 	default: return "unknown error";
 	}
 }
