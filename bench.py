@@ -186,6 +186,8 @@ def cpu_baseline(U_full, n):
     # aim at ~10 s of wall time (not more than 8 steps)
     steps = int(max(1, min(8, 10.0 / max(el, 1e-3))))
     rate, kind, el = cpu_sample_run(U_full, n, planes, steps, threads)
+    # one core: the reference's own model is one MPI rank per core
+    rate1, _, el1 = cpu_sample_run(U_full, n, 4, 2, 1)
     return {
         "value": rate,
         "unit": UNIT,
@@ -193,7 +195,21 @@ def cpu_baseline(U_full, n):
         "kind": kind,
         "sample": f"{steps} HLLD steps on a {n}x{n}x{planes} periodic slab of the blast initial state "
                   f"({el:.1f} s wall on {threads} threads, std::thread over cells)",
+        "one_core": {"value": rate1, "unit": UNIT,
+                     "sample": f"2 HLLD steps on a {n}x{n}x4 periodic slab, 1 thread ({el1:.1f} s wall)"},
+        "cpu": cpu_model(),
     }
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def batched_section(local, steps=500):
@@ -316,6 +332,40 @@ def adjoint_section(local, n=256, steps=200, every=20):
 
     adj_ms()
     gradient = min(adj_ms() for _ in range(3))
+
+    # gradient check: 16 seeded Gaussian directions in (rho, v) at fixed p and B, central
+    # differences at h = 1e-6 of the field rms and h/2 on the frozen dt schedule, Richardson-combined
+    ctx.set_state(U0)
+    ctx.step(0.0)
+    grad, _, _ = ctx.adjoint(steps, every, seed, dt_in=dts)
+    rho0, v0 = U0[0], U0[1:4] / U0[0]
+    p0 = (5 / 3 - 1) * (U0[4] - 0.5 * (U0[1:4] ** 2).sum(0) / U0[0] - 0.5 * (U0[5:8] ** 2).sum(0))
+    g_rho = grad[0] + (grad[1:4] * v0).sum(0) + grad[4] * 0.5 * (v0 ** 2).sum(0)
+    g_v = grad[1:4] * rho0 + grad[4] * rho0 * v0
+    rms_rho, rms_v = np.sqrt((rho0 ** 2).mean()), np.sqrt((v0[:2] ** 2).mean())
+
+    def J_of(rho, v):
+        U = U0.copy()
+        U[0] = rho
+        U[1:4] = rho * v
+        U[4] = p0 / (5 / 3 - 1) + 0.5 * rho * (v ** 2).sum(0) + 0.5 * (U0[5:8] ** 2).sum(0)
+        ctx.set_state(U)
+        ctx.step(0.0)
+        ctx.steps_dt(dts)
+        return float((0.5 * (ctx.get_state()[5:8] ** 2).sum(0) * mask).sum() / n ** 2)
+
+    rng = np.random.default_rng(20261205)
+    ads, fds = [], []
+    for _ in range(16):
+        d_rho = rng.normal(size=rho0.shape)
+        d_v = rng.normal(size=v0.shape)
+        d_v[2] = 0.0
+        h_rho, h_v = 1e-6 * rms_rho, 1e-6 * rms_v
+        D = [(J_of(rho0 + f * h_rho * d_rho, v0 + f * h_v * d_v) - J_of(rho0 - f * h_rho * d_rho, v0 - f * h_v * d_v))
+             / (2 * f) for f in (1.0, 0.5)]
+        fds.append((4 * D[1] - D[0]) / 3)
+        ads.append(float((g_rho * d_rho).sum() * h_rho + (g_v * d_v).sum() * h_v))
+    ads, fds = np.array(ads), np.array(fds)
     ctx.close()
     return {
         "workload": f"Orszag-Tang {n}^2 periodic, HLLD, CFL 0.25, {steps} steps, checkpoints every {every}, "
@@ -323,6 +373,9 @@ def adjoint_section(local, n=256, steps=200, every=20):
         "forward_ms": forward,
         "gradient_ms": gradient,
         "adjoint_over_forward": gradient / forward,
+        "fd_check": {"directions": 16, "h": "1e-6 of the field rms, Richardson with h/2",
+                     "max_err_over_max_fd": float(np.abs(ads - fds).max() / np.abs(fds).max()),
+                     "bar": 1e-6},
         "what": "gradient_ms: the pamhd_gpu_adjoint call (forward run with checkpoints, recompute of every "
                 "segment, reverse sweep); forward_ms: the same steps alone; device time by CUDA events",
     }

@@ -266,8 +266,12 @@ segment from its checkpoint, on the forward run's dt schedule held fixed.
 seed and grad: eight host arrays each (the layout of set_state).
 grad_value (NULL or 48 doubles): the gradient with respect to the state
 of each VALUE side, [dimension][lo, hi][8].  dt_out (NULL or nsteps
-doubles) receives the schedule.  Solvers: Rusanov, HLL, HLLD.  No
-reference counterpart: the reference has no derivatives.
+doubles) receives the schedule.  Solvers: Rusanov, HLL, HLLD.  The
+device memory (ceil(nsteps/every) checkpoints, two buffers of every - 1
+recompute states, cotangents) stays with the context after the first call
+and is reused by later calls; it grows when a call needs more and is freed
+by pamhd_gpu_destroy.  No reference counterpart: the reference has no
+derivatives.
 */
 int pamhd_gpu_adjoint(pamhd_ctx* ctx, int32_t nsteps, int32_t every, const double* const seed[8],
                       double* const grad[8], double* grad_value, const double* dt_in, double* dt_out);

@@ -12,19 +12,25 @@ linearisation).  With lambda = dJ/dU_{n+1}, one reverse step is
              a ghost's g going to the cell it is made from (periodic image,
              COPY source) or, for VALUE sides, to the inflow-state gradient.
 
-Kernels: face_vjp_kernel (one thread per face of one axis, writes g_L and
-g_R of every face), gather_kernel (one thread per cell, sums its faces in
-a fixed order: deterministic), value_side_kernel (sums the ghost gradients
-of VALUE sides, one block per side, fixed order).
+Kernels: faces_vjp_kernel (one launch for every active axis: one thread
+per cell, extended by the low ghost layer, computes the faces whose lower
+cell it is and writes g_L and g_R as 16 arrays per axis, x fastest, so that
+reads and writes are coalesced), gather_kernel (one thread per cell, sums
+its faces in a fixed order: deterministic), value_side_kernel (sums the
+ghost gradients of VALUE sides, one block per side, fixed order; launched
+only when the grid has a VALUE side).
 
 Driver (pamhd_gpu_adjoint): the forward run stores the state every K
-steps; the reverse sweep recomputes each segment of K states from its
-checkpoint (same kernels, so the same bits) and steps lambda back through
-it.  Memory: ceil(N/K) + K - 1 state copies.
+steps and keeps every state of the last segment; the reverse sweep steps
+lambda back through each segment while the segment before it is
+recomputed from its checkpoint on a second stream (same kernels, so the
+same bits), into the other of two segment buffers.  Memory: ceil(N/K)
+checkpoints + 2 (K - 1) state copies, kept by the context between calls.
 */
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <new>
 #include <vector>
 
 #include "adjoint_face.cuh"
@@ -43,7 +49,8 @@ struct Adj_Params {
 	const double* U;      // state at step n, ghosts valid
 	const double* lam;    // dJ/dU_{n+1}, padded layout, ghosts zero
 	double* lam_out;      // dJ/dU_n
-	double* G[3];         // per axis: 16 values per face (g_L, g_R)
+	double* G[3];         // per axis: 16 arrays of nf[d] doubles, g_L then g_R in the state's variable order
+	long long nf[3];      // faces per axis
 	Layout L;
 	Gas_Adj gas;
 	double dt;
@@ -60,54 +67,122 @@ __host__ __device__ inline long long faces_of(const Layout& L, const int d)
 	return (long long)(L.n[d] + 1) * L.n[e] * L.n[f];
 }
 
-// face of axis d whose lower cell has coordinate l along d
-__device__ inline long long face_index(const Layout& L, const int d, const int l, const int ce, const int cf)
+/*
+Index of the face of axis D whose lower cell is (c0, c1, c2): c_D runs over
+-1 .. n_D - 1, the other coordinates over the interior; x fastest, so that
+the faces of consecutive threads are consecutive in memory.
+*/
+template <int D>
+__device__ __forceinline__ long long face_at(const Layout& L, const int c0, const int c1, const int c2)
 {
-	const int e = (d + 1) % 3;
-	return (long long)(l + 1) + (long long)(L.n[d] + 1) * (ce + (long long)L.n[e] * cf);
+	constexpr int s0 = D == 0, s1 = D == 1, s2 = D == 2;
+	const long long N0 = L.n[0] + s0, N1 = L.n[1] + s1;
+	return (c0 + s0) + N0 * ((c1 + s1) + N1 * (long long)(c2 + s2));
 }
 
-template <int SOLVER>
-__global__ void face_vjp_kernel(const Adj_Params A, const int d)
+/*
+g_L and g_R of the axis-D face whose lower cell is c (state UL and cotangent
+LL of that cell already loaded, in the state's variable order).
+*/
+template <int SOLVER, int D>
+__device__ __forceinline__ void face_vjp_at(const Adj_Params& A, const int* c, const double* UL, const double* LL)
 {
-	const int e = (d + 1) % 3, f = (d + 2) % 3;
-	const long long count = faces_of(A.L, d);
-	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
-	     t += (long long)gridDim.x * blockDim.x) {
-		const int l = int(t % (A.L.n[d] + 1)) - 1;
-		const long long rest = t / (A.L.n[d] + 1);
-		int c[3];
-		c[d] = l;
-		c[e] = int(rest % A.L.n[e]);
-		c[f] = int(rest / A.L.n[e]);
-		const long long oL = A.L.offset(c[0], c[1], c[2]);
-		c[d] = l + 1;
-		const long long oR = A.L.offset(c[0], c[1], c[2]);
-		const int a0 = d, a1 = e, a2 = f;
-		double UL[8], UR[8], phi[8];
-		const double scale = A.dt * A.inv_len[d];
-		const int perm[8] = {0, 1 + a0, 1 + a1, 1 + a2, 4, 5 + a0, 5 + a1, 5 + a2};
-		const bool in_l = l >= 0, in_r = l + 1 <= A.L.n[d] - 1;
-		#pragma unroll
-		for (int v = 0; v < 8; v++) {
-			const long long vo = perm[v] * A.L.var;
-			UL[v] = A.U[vo + oL];
-			UR[v] = A.U[vo + oR];
-			const double lr = in_r ? A.lam[vo + oR] : 0.0;
-			const double ll = in_l ? A.lam[vo + oL] : 0.0;
-			phi[v] = scale * (lr - ll);
-		}
-		double gL[8], gR[8];
-		pamhd_b200::adjoint::face_vjp<SOLVER>(UL, UR, A.gas, phi, gL, gR);
-		double* out = A.G[d] + 16 * t;
-		#pragma unroll
-		for (int v = 0; v < 8; v++) {
-			out[perm[v]] = gL[v];
-			out[8 + perm[v]] = gR[v];
-		}
+	constexpr int E = (D + 1) % 3, F = (D + 2) % 3;
+	constexpr int perm[8] = {0, 1 + D, 1 + E, 1 + F, 4, 5 + D, 5 + E, 5 + F};
+	int r[3] = {c[0], c[1], c[2]};
+	r[D] += 1;
+	const long long oR = A.L.offset(r[0], r[1], r[2]);
+	const bool lam_r = r[D] <= A.L.n[D] - 1;
+	const double scale = A.dt * A.inv_len[D];
+	double uL[8], uR[8], phi[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) {
+		uL[v] = UL[perm[v]];
+		uR[v] = A.U[perm[v] * A.L.var + oR];
+		const double lr = lam_r ? A.lam[perm[v] * A.L.var + oR] : 0.0;
+		phi[v] = scale * (lr - LL[perm[v]]);
+	}
+	double gL[8], gR[8];
+	pamhd_b200::adjoint::face_vjp<SOLVER>(uL, uR, A.gas, phi, gL, gR);
+	const long long idx = face_at<D>(A.L, c[0], c[1], c[2]);
+	double* G = A.G[D];
+	const long long nf = A.nf[D];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) {
+		G[perm[v] * nf + idx] = gL[v];
+		G[(8 + perm[v]) * nf + idx] = gR[v];
 	}
 }
 
+/*
+Cotangents of every face of every active axis in one launch: one thread per
+cell of the interior extended by the ghost layer on the low side of each
+active axis; the thread computes the faces whose lower cell is its cell
+(a ghost-layer thread only the face into the interior).
+*/
+template <int SOLVER>
+__global__ void faces_vjp_kernel(const Adj_Params A)
+{
+	const int a0 = A.active[0], a1 = A.active[1], a2 = A.active[2];
+	const int E0 = A.L.n[0] + a0, E1 = A.L.n[1] + a1, E2 = A.L.n[2] + a2;
+	const long long count = (long long)E0 * E1 * E2;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
+	     t += (long long)gridDim.x * blockDim.x) {
+		int c[3];
+		c[0] = int(t % E0) - a0;
+		c[1] = int((t / E0) % E1) - a1;
+		c[2] = int(t / ((long long)E0 * E1)) - a2;
+		const int ghosts = (c[0] < 0) + (c[1] < 0) + (c[2] < 0);
+		if (ghosts > 1) continue;
+		const long long oL = A.L.offset(c[0], c[1], c[2]);
+		double UL[8], LL[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) {
+			UL[v] = A.U[v * A.L.var + oL];
+			LL[v] = ghosts == 0 ? A.lam[v * A.L.var + oL] : 0.0;
+		}
+		if (a0 and (ghosts == 0 or c[0] < 0)) face_vjp_at<SOLVER, 0>(A, c, UL, LL);
+		if (a1 and (ghosts == 0 or c[1] < 0)) face_vjp_at<SOLVER, 1>(A, c, UL, LL);
+		if (a2 and (ghosts == 0 or c[2] < 0)) face_vjp_at<SOLVER, 2>(A, c, UL, LL);
+	}
+}
+
+// adds to acc the cotangents that axis D's faces give the interior cell c, ghosts included
+template <int D>
+__device__ __forceinline__ void gather_axis(const Adj_Params& A, const int* c, double* acc)
+{
+	const double* G = A.G[D];
+	const long long nf = A.nf[D];
+	const int nd = A.L.n[D];
+	int m[3] = {c[0], c[1], c[2]};
+	m[D] -= 1;
+	// the cell is the right side of its -D face and the left side of its +D face
+	const long long i_minus = face_at<D>(A.L, m[0], m[1], m[2]);
+	const long long i_plus = face_at<D>(A.L, c[0], c[1], c[2]);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) acc[v] += G[(8 + v) * nf + i_minus] + G[v * nf + i_plus];
+	// ghosts made from this cell: a periodic image, or a COPY ghost (equal to its source cell in
+	// exact arithmetic: identity Jacobian)
+	const bool first = c[D] == 0, last = c[D] == nd - 1;
+	const bool from_lo = A.periodic[D] ? last : (first and A.bc_lo[D] == PAMHD_BC_COPY);
+	const bool from_hi = A.periodic[D] ? first : (last and A.bc_hi[D] == PAMHD_BC_COPY);
+	if (from_lo) {   // the ghost at -1 is this cell: left side of the face with lower cell -1
+		int g[3] = {c[0], c[1], c[2]};
+		g[D] = -1;
+		const long long i = face_at<D>(A.L, g[0], g[1], g[2]);
+		#pragma unroll
+		for (int v = 0; v < 8; v++) acc[v] += G[v * nf + i];
+	}
+	if (from_hi) {   // the ghost at n is this cell: right side of the face with lower cell n - 1
+		int g[3] = {c[0], c[1], c[2]};
+		g[D] = nd - 1;
+		const long long i = face_at<D>(A.L, g[0], g[1], g[2]);
+		#pragma unroll
+		for (int v = 0; v < 8; v++) acc[v] += G[(8 + v) * nf + i];
+	}
+}
+
+// lambda_n = lambda_{n+1} + the cotangents of each interior cell's faces, summed in a fixed order
 __global__ void gather_kernel(const Adj_Params A)
 {
 	const long long n = (long long)A.L.n[0] * A.L.n[1] * A.L.n[2];
@@ -120,45 +195,28 @@ __global__ void gather_kernel(const Adj_Params A)
 		double acc[8];
 		#pragma unroll
 		for (int v = 0; v < 8; v++) acc[v] = A.lam[v * A.L.var + o];
-		for (int d = 0; d < 3; d++) {
-			if (not A.active[d]) continue;
-			const int e = (d + 1) % 3, f = (d + 2) % 3;
-			const int nd = A.L.n[d];
-			const double* G = A.G[d];
-			// the cell is the right side of its -d face and the left side of its +d face
-			const double* minus = G + 16 * face_index(A.L, d, c[d] - 1, c[e], c[f]);
-			const double* plus = G + 16 * face_index(A.L, d, c[d], c[e], c[f]);
-			#pragma unroll
-			for (int v = 0; v < 8; v++) acc[v] += minus[8 + v] + plus[v];
-			// ghosts made from this cell
-			const bool first = c[d] == 0, last = c[d] == nd - 1;
-			if (A.periodic[d]) {
-				if (last) {   // ghost -1 is this cell
-					const double* g = G + 16 * face_index(A.L, d, -1, c[e], c[f]);
-					for (int v = 0; v < 8; v++) acc[v] += g[v];
-				}
-				if (first) {  // ghost n is this cell
-					const double* g = G + 16 * face_index(A.L, d, nd - 1, c[e], c[f]);
-					for (int v = 0; v < 8; v++) acc[v] += g[8 + v];
-				}
-			} else {
-				// a COPY ghost equals its source cell in exact arithmetic: identity Jacobian
-				if (first and A.bc_lo[d] == PAMHD_BC_COPY) {
-					const double* g = G + 16 * face_index(A.L, d, -1, c[e], c[f]);
-					for (int v = 0; v < 8; v++) acc[v] += g[v];
-				}
-				if (last and A.bc_hi[d] == PAMHD_BC_COPY) {
-					const double* g = G + 16 * face_index(A.L, d, nd - 1, c[e], c[f]);
-					for (int v = 0; v < 8; v++) acc[v] += g[8 + v];
-				}
-			}
-		}
+		if (A.active[0]) gather_axis<0>(A, c, acc);
+		if (A.active[1]) gather_axis<1>(A, c, acc);
+		if (A.active[2]) gather_axis<2>(A, c, acc);
 		#pragma unroll
 		for (int v = 0; v < 8; v++) A.lam_out[v * A.L.var + o] = acc[v];
 	}
 }
 
-// block (d, side): adds the gradients of the VALUE ghosts of that side into acc[d][side][8]
+template <int D>
+__device__ __forceinline__ const double* value_ghost_cotangent(const Adj_Params& A, const int side, const int ce,
+                                                               const int cf, long long& stride)
+{
+	constexpr int E = (D + 1) % 3, F = (D + 2) % 3;
+	int c[3];
+	c[D] = side ? A.L.n[D] - 1 : -1;
+	c[E] = ce;
+	c[F] = cf;
+	stride = A.nf[D];
+	return A.G[D] + (side ? 8 * stride : 0) + face_at<D>(A.L, c[0], c[1], c[2]);
+}
+
+// block (d, side): adds the cotangents of the VALUE ghosts of that side into acc[d][side][8]
 __global__ void value_side_kernel(const Adj_Params A, double* acc)
 {
 	__shared__ double red[8][256];
@@ -170,8 +228,11 @@ __global__ void value_side_kernel(const Adj_Params A, double* acc)
 		const long long m = (long long)A.L.n[e] * A.L.n[(d + 2) % 3];
 		for (long long t = threadIdx.x; t < m; t += blockDim.x) {
 			const int ce = int(t % A.L.n[e]), cf = int(t / A.L.n[e]);
-			const double* g = A.G[d] + 16 * face_index(A.L, d, side ? A.L.n[d] - 1 : -1, ce, cf) + (side ? 8 : 0);
-			for (int v = 0; v < 8; v++) s[v] += g[v];
+			long long stride = 0;
+			const double* g = d == 0 ? value_ghost_cotangent<0>(A, side, ce, cf, stride)
+			                : d == 1 ? value_ghost_cotangent<1>(A, side, ce, cf, stride)
+			                         : value_ghost_cotangent<2>(A, side, ce, cf, stride);
+			for (int v = 0; v < 8; v++) s[v] += g[v * stride];
 		}
 	}
 	for (int v = 0; v < 8; v++) red[v][threadIdx.x] = s[v];
@@ -196,16 +257,14 @@ int check(const cudaError_t e)
 
 int launch_vjp(const Adj_Params& A, const int solver, cudaStream_t stream)
 {
-	for (int d = 0; d < 3; d++) {
-		if (not A.active[d]) continue;
-		const long long count = faces_of(A.L, d);
-		const int blocks = int(std::min<long long>(4096, (count + 127) / 128));
-		switch (solver) {
-		case PAMHD_RUSANOV: face_vjp_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(A, d); break;
-		case PAMHD_HLL_ATHENA: face_vjp_kernel<PAMHD_HLL_ATHENA><<<blocks, 128, 0, stream>>>(A, d); break;
-		case PAMHD_HLLD_ATHENA: face_vjp_kernel<PAMHD_HLLD_ATHENA><<<blocks, 128, 0, stream>>>(A, d); break;
-		default: return PAMHD_ERR_ARGUMENT;
-		}
+	const long long count = (long long)(A.L.n[0] + A.active[0]) * (A.L.n[1] + A.active[1])
+	                        * (A.L.n[2] + A.active[2]);
+	const int blocks = int(std::min<long long>(65535, (count + 127) / 128));
+	switch (solver) {
+	case PAMHD_RUSANOV: faces_vjp_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(A); break;
+	case PAMHD_HLL_ATHENA: faces_vjp_kernel<PAMHD_HLL_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
+	case PAMHD_HLLD_ATHENA: faces_vjp_kernel<PAMHD_HLLD_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
+	default: return PAMHD_ERR_ARGUMENT;
 	}
 	return check(cudaGetLastError());
 }
@@ -227,9 +286,66 @@ int forward_step(pamhd_ctx& x, const double dt)
 
 struct Device_Buffer {
 	double* p = nullptr;
+	size_t len = 0;
 	~Device_Buffer() { cudaFree(p); }
-	int alloc(const size_t n) { return check(cudaMalloc(&p, n * sizeof(double))); }
+	// grows to at least n doubles (contents not kept)
+	int reserve(const size_t n)
+	{
+		if (n <= len) return PAMHD_OK;
+		cudaFree(p);
+		p = nullptr;
+		len = 0;
+		PAMHD_TRY(check(cudaMalloc(&p, n * sizeof(double))));
+		len = n;
+		return PAMHD_OK;
+	}
 };
+
+} // namespace
+
+/*
+Device memory of the adjoint, kept by the context between calls so that
+repeated gradients do not allocate: checkpoints, two buffers of recompute
+states, the two cotangent copies, per-axis face cotangents, VALUE-side sums
+and the reduction ring of the recompute steps.  Grows when a call needs
+more.  The recompute of a segment runs on its own stream, overlapping the
+reverse sweep of the segment after it.
+*/
+struct Adjoint_Work {
+	Device_Buffer ck, seg[2], lam[2], G[3], acc, scratch;
+	int seg_ready[2] = {0, 0};  // recompute states whose VALUE ghosts are filled
+	cudaStream_t side = nullptr;
+	cudaEvent_t forward_done = nullptr, recomputed[2] = {nullptr, nullptr}, swept[2] = {nullptr, nullptr};
+
+	int init(const int device)
+	{
+		if (side != nullptr) return PAMHD_OK;
+		PAMHD_TRY(check(cudaSetDevice(device)));
+		PAMHD_TRY(check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)));
+		for (cudaEvent_t* e: {&forward_done, &recomputed[0], &recomputed[1], &swept[0], &swept[1]}) {
+			PAMHD_TRY(check(cudaEventCreateWithFlags(e, cudaEventDisableTiming)));
+		}
+		return PAMHD_OK;
+	}
+	~Adjoint_Work()
+	{
+		if (side != nullptr) cudaStreamSynchronize(side);
+		for (cudaEvent_t e: {forward_done, recomputed[0], recomputed[1], swept[0], swept[1]}) {
+			if (e != nullptr) cudaEventDestroy(e);
+		}
+		if (side != nullptr) cudaStreamDestroy(side);
+	}
+};
+
+namespace pamhd_b200 {
+void release_adjoint(pamhd_ctx& x)
+{
+	delete x.adjoint;
+	x.adjoint = nullptr;
+}
+}
+
+namespace {
 
 } // namespace
 
@@ -261,25 +377,79 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 	const Layout& L = x->L;
 	const size_t state_len = size_t(8) * L.var;
 	const int nck = (nsteps + every - 1) / every;
+	const int seg_len = std::min(every, nsteps);
+	if (nsteps > x->hist_len) return PAMHD_ERR_ARGUMENT;
+	if (x->adjoint == nullptr) {
+		x->adjoint = new (std::nothrow) Adjoint_Work;
+		if (x->adjoint == nullptr) return PAMHD_ERR_ARGUMENT;
+	}
+	Adjoint_Work& W = *x->adjoint;
+	PAMHD_TRY(W.init(x->device));
+	const size_t scratch_bytes = 3 * sizeof(Speed_Max) + 3 * sizeof(Clock) + sizeof(Status);
+	PAMHD_TRY(W.ck.reserve(state_len * size_t(nck)));
+	for (int b = 0; b < 2; b++) {
+		if (seg_len > 1 and W.seg[b].len < state_len * size_t(seg_len - 1)) {
+			PAMHD_TRY(W.seg[b].reserve(state_len * size_t(seg_len - 1)));
+			W.seg_ready[b] = 0;
+		}
+	}
+	PAMHD_TRY(W.lam[0].reserve(state_len));
+	PAMHD_TRY(W.lam[1].reserve(state_len));
+	PAMHD_TRY(W.acc.reserve(48));
+	PAMHD_TRY(W.scratch.reserve((scratch_bytes + 7) / 8));
+	Adj_Params A;
+	A.L = L;
+	A.gas.gamma = x->base.gas.gamma;
+	A.gas.inv_mu0 = x->base.gas.inv_mu0;
+	A.gas.sqrt_mu0 = x->base.gas.sqrt_mu0;
+	A.gas.inv_sqrt_mu0 = x->base.gas.inv_sqrt_mu0;
+	bool any_value = false;
+	for (int d = 0; d < 3; d++) {
+		A.inv_len[d] = x->base.inv_len[d];
+		A.active[d] = x->base.active[d];
+		A.periodic[d] = x->base.periodic[d];
+		A.bc_lo[d] = x->base.bc_lo[d];
+		A.bc_hi[d] = x->base.bc_hi[d];
+		A.G[d] = nullptr;
+		A.nf[d] = 0;
+		if (A.active[d]) {
+			A.nf[d] = faces_of(L, d);
+			PAMHD_TRY(W.G[d].reserve(16 * size_t(A.nf[d])));
+			A.G[d] = W.G[d].p;
+			if (not A.periodic[d] and (A.bc_lo[d] == PAMHD_BC_VALUE or A.bc_hi[d] == PAMHD_BC_VALUE)) any_value = true;
+		}
+	}
 
 	// ---- forward run with checkpoints
-	std::vector<Device_Buffer> ck(nck);
-	for (auto& b: ck) PAMHD_TRY(b.alloc(state_len));
 	{
 		Control c;
 		c.max_dt = -1.0;
 		c.t_end = 1.0e300;
 		PAMHD_TRY(check(cudaMemcpyAsync(x->control, &c, sizeof c, cudaMemcpyHostToDevice, x->stream)));
-		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	}
+	// VALUE ghosts are constant and the step kernel never writes them: fill each recompute state once
+	for (int b = 0; b < 2; b++) {
+		for (int i = W.seg_ready[b]; i < seg_len - 1; i++) {
+			PAMHD_TRY(launch_fill_ghosts_values(x->base, W.seg[b].p + state_len * size_t(i), x->cfg.value_lo,
+			                                    x->cfg.value_hi, x->stream));
+		}
+		W.seg_ready[b] = std::max(W.seg_ready[b], seg_len - 1);
 	}
 	std::vector<double> dts(nsteps);
+	const int last = nck - 1, last_start = last * every;
 	for (int n = 0; n < nsteps; n++) {
 		if (n % every == 0) {
-			PAMHD_TRY(check(cudaMemcpyAsync(ck[n / every].p, x->state[x->cur], state_len * sizeof(double),
-			                                cudaMemcpyDeviceToDevice, x->stream)));
+			PAMHD_TRY(check(cudaMemcpyAsync(W.ck.p + state_len * size_t(n / every), x->state[x->cur],
+			                                state_len * sizeof(double), cudaMemcpyDeviceToDevice, x->stream)));
 		}
 		PAMHD_TRY(forward_step(*x, dt_in != nullptr ? dt_in[n] : -1.0));
+		// the states of the last segment are kept as they are made instead of being recomputed
+		if (n >= last_start and n + 1 < nsteps) {
+			PAMHD_TRY(check(cudaMemcpyAsync(W.seg[last & 1].p + state_len * size_t(n - last_start), x->state[x->cur],
+			                                state_len * sizeof(double), cudaMemcpyDeviceToDevice, x->stream)));
+		}
 	}
+	PAMHD_TRY(check(cudaEventRecord(W.forward_done, x->stream)));
 	{
 		std::vector<double> hist(x->hist_len);
 		PAMHD_TRY(check(cudaMemcpyAsync(hist.data(), x->dt_hist, x->hist_len * sizeof(double),
@@ -288,94 +458,72 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 		PAMHD_TRY(check(cudaMemcpyAsync(&s, x->status, sizeof s, cudaMemcpyDeviceToHost, x->stream)));
 		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
 		if (s.flags != 0) return PAMHD_ERR_PHYSICS;
-		if (nsteps > x->hist_len) return PAMHD_ERR_ARGUMENT;
 		for (int n = 0; n < nsteps; n++) dts[n] = hist[(x->steps - nsteps + n) % x->hist_len];
 	}
 	if (dt_out != nullptr) std::copy(dts.begin(), dts.end(), dt_out);
 
 	// ---- reverse sweep
-	Device_Buffer lam[2], G[3], seg_store, acc, scratch;
-	PAMHD_TRY(lam[0].alloc(state_len));
-	PAMHD_TRY(lam[1].alloc(state_len));
-	Adj_Params A;
-	A.L = L;
-	A.gas.gamma = x->base.gas.gamma;
-	A.gas.inv_mu0 = x->base.gas.inv_mu0;
-	A.gas.sqrt_mu0 = x->base.gas.sqrt_mu0;
-	A.gas.inv_sqrt_mu0 = x->base.gas.inv_sqrt_mu0;
-	for (int d = 0; d < 3; d++) {
-		A.inv_len[d] = x->base.inv_len[d];
-		A.active[d] = x->base.active[d];
-		A.periodic[d] = x->base.periodic[d];
-		A.bc_lo[d] = x->base.bc_lo[d];
-		A.bc_hi[d] = x->base.bc_hi[d];
-		A.G[d] = nullptr;
-		if (A.active[d]) {
-			PAMHD_TRY(G[d].alloc(16 * size_t(faces_of(L, d))));
-			A.G[d] = G[d].p;
-		}
-	}
-	PAMHD_TRY(acc.alloc(6 * 8));
-	PAMHD_TRY(check(cudaMemsetAsync(acc.p, 0, 48 * sizeof(double), x->stream)));
-	PAMHD_TRY(check(cudaMemsetAsync(lam[0].p, 0, state_len * sizeof(double), x->stream)));
-	PAMHD_TRY(check(cudaMemsetAsync(lam[1].p, 0, state_len * sizeof(double), x->stream)));
+	PAMHD_TRY(check(cudaMemsetAsync(W.acc.p, 0, 48 * sizeof(double), x->stream)));
+	PAMHD_TRY(check(cudaMemsetAsync(W.lam[0].p, 0, state_len * sizeof(double), x->stream)));
+	PAMHD_TRY(check(cudaMemsetAsync(W.lam[1].p, 0, state_len * sizeof(double), x->stream)));
 	const size_t cells = size_t(L.n[0]) * L.n[1] * L.n[2];
 	for (int v = 0; v < 8; v++) {
 		PAMHD_TRY(check(cudaMemcpyAsync(x->staging, seed[v], cells * sizeof(double), cudaMemcpyHostToDevice,
 		                                x->stream)));
-		PAMHD_TRY(launch_scatter(x->staging, lam[0].p + v * L.var, L, x->stream));
+		PAMHD_TRY(launch_scatter(x->staging, W.lam[0].p + v * L.var, L, x->stream));
 	}
-	// recompute buffers: K - 1 states after each checkpoint, and a scratch ring for the recompute steps
-	const int seg_len = std::min(every, nsteps);
-	if (seg_len > 1) {
-		PAMHD_TRY(seg_store.alloc(state_len * size_t(seg_len - 1)));
-		// VALUE ghosts are constant: the step kernel never writes them
-		for (int i = 0; i < seg_len - 1; i++) {
-			PAMHD_TRY(launch_fill_ghosts_values(x->base, seg_store.p + state_len * size_t(i), x->cfg.value_lo,
-			                                    x->cfg.value_hi, x->stream));
-		}
-	}
-	const size_t scratch_bytes = 3 * sizeof(Speed_Max) + 3 * sizeof(Clock) + sizeof(Status);
-	PAMHD_TRY(scratch.alloc((scratch_bytes + 7) / 8));
-	PAMHD_TRY(check(cudaMemsetAsync(scratch.p, 0, scratch_bytes, x->stream)));
+	PAMHD_TRY(check(cudaStreamWaitEvent(W.side, W.forward_done, 0)));
+	PAMHD_TRY(check(cudaMemsetAsync(W.scratch.p, 0, scratch_bytes, W.side)));
 	Step_Params R = x->base;
-	R.red = reinterpret_cast<Speed_Max*>(scratch.p);
-	R.clock = reinterpret_cast<Clock*>(reinterpret_cast<char*>(scratch.p) + 3 * sizeof(Speed_Max));
-	R.status = reinterpret_cast<Status*>(reinterpret_cast<char*>(scratch.p) + 3 * sizeof(Speed_Max) + 3 * sizeof(Clock));
+	R.red = reinterpret_cast<Speed_Max*>(W.scratch.p);
+	R.clock = reinterpret_cast<Clock*>(reinterpret_cast<char*>(W.scratch.p) + 3 * sizeof(Speed_Max));
+	R.status = reinterpret_cast<Status*>(reinterpret_cast<char*>(W.scratch.p) + 3 * sizeof(Speed_Max)
+	                                     + 3 * sizeof(Clock));
 	R.dt_hist = nullptr;
 	R.phase = 0;
+	// state i of segment s: its checkpoint (i = 0) or entry i - 1 of segment buffer s & 1
+	auto state_of = [&](const int s, const int i) -> const double* {
+		return i == 0 ? W.ck.p + state_len * size_t(s) : W.seg[s & 1].p + state_len * size_t(i - 1);
+	};
+	// segment s recomputed on the side stream, once the sweep two segments later freed its buffer
+	auto recompute = [&](const int s) -> int {
+		const int start = s * every, end = std::min(nsteps, start + every);
+		PAMHD_TRY(check(cudaStreamWaitEvent(W.side, W.swept[s & 1], 0)));
+		for (int i = 1; i < end - start; i++) {
+			R.in = state_of(s, i - 1);
+			R.out = const_cast<double*>(state_of(s, i));
+			R.forced_dt = dts[start + i - 1];
+			PAMHD_TRY(launch_step(R, x->cfg.solver, W.side));
+		}
+		return check(cudaEventRecord(W.recomputed[s & 1], W.side));
+	};
 	int li = 0;
 	for (int s = nck - 1; s >= 0; s--) {
 		const int start = s * every, end = std::min(nsteps, start + every);
+		if (s >= 1) PAMHD_TRY(recompute(s - 1));
+		if (s != last) PAMHD_TRY(check(cudaStreamWaitEvent(x->stream, W.recomputed[s & 1], 0)));
 		std::vector<const double*> states(end - start);
-		states[0] = ck[s].p;
-		for (int i = 1; i < end - start; i++) {
-			double* dst = seg_store.p + state_len * size_t(i - 1);
-			R.in = states[i - 1];
-			R.out = dst;
-			R.forced_dt = dts[start + i - 1];
-			PAMHD_TRY(launch_step(R, x->cfg.solver, x->stream));
-			states[i] = dst;
-		}
+		for (int i = 0; i < end - start; i++) states[i] = state_of(s, i);
 		for (int n = end - 1; n >= start; n--) {
 			A.U = states[n - start];
 			A.dt = dts[n];
-			A.lam = lam[li].p;
-			A.lam_out = lam[li ^ 1].p;
+			A.lam = W.lam[li].p;
+			A.lam_out = W.lam[li ^ 1].p;
 			PAMHD_TRY(launch_vjp(A, x->cfg.solver, x->stream));
-			gather_kernel<<<int(std::min<size_t>(4096, (cells + 255) / 256)), 256, 0, x->stream>>>(A);
-			value_side_kernel<<<6, 256, 0, x->stream>>>(A, acc.p);
+			gather_kernel<<<int(std::min<size_t>(65535, (cells + 255) / 256)), 256, 0, x->stream>>>(A);
+			if (any_value) value_side_kernel<<<6, 256, 0, x->stream>>>(A, W.acc.p);
 			PAMHD_TRY(check(cudaGetLastError()));
 			li ^= 1;
 		}
+		PAMHD_TRY(check(cudaEventRecord(W.swept[s & 1], x->stream)));
 	}
 	for (int v = 0; v < 8; v++) {
-		PAMHD_TRY(launch_gather(lam[li].p + v * L.var, x->staging, L, x->stream));
+		PAMHD_TRY(launch_gather(W.lam[li].p + v * L.var, x->staging, L, x->stream));
 		PAMHD_TRY(check(cudaMemcpyAsync(grad[v], x->staging, cells * sizeof(double), cudaMemcpyDeviceToHost,
 		                                x->stream)));
 	}
 	if (grad_value != nullptr) {
-		PAMHD_TRY(check(cudaMemcpyAsync(grad_value, acc.p, 48 * sizeof(double), cudaMemcpyDeviceToHost,
+		PAMHD_TRY(check(cudaMemcpyAsync(grad_value, W.acc.p, 48 * sizeof(double), cudaMemcpyDeviceToHost,
 		                                x->stream)));
 	}
 	return check(cudaStreamSynchronize(x->stream));

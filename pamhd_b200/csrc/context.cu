@@ -202,6 +202,7 @@ int pamhd_gpu_destroy(pamhd_ctx* x)
 	cudaSetDevice(x->device);
 	if (x->stream != nullptr) cudaStreamSynchronize(x->stream);
 	if (x->graph != nullptr) cudaGraphExecDestroy(x->graph);
+	release_adjoint(*x);
 	cudaFree(x->state[0]);
 	cudaFree(x->state[1]);
 	cudaFree(x->red);

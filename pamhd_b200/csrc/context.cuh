@@ -12,6 +12,8 @@ the entry points of context.cu and the adjoint driver of adjoint.cu.
 
 using namespace pamhd_b200;
 
+struct Adjoint_Work;
+
 struct pamhd_ctx {
 	pamhd_cfg cfg;
 	int device = 0;
@@ -33,11 +35,14 @@ struct pamhd_ctx {
 	bool needs_boundary_speeds = false;
 	cudaGraphExec_t graph = nullptr;
 	bool loaded = false;
+	Adjoint_Work* adjoint = nullptr;  // adjoint workspace, kept between pamhd_gpu_adjoint calls
 };
 
 namespace pamhd_b200 {
 // the next step of a context (launch only; advances the step counter and parity)
 int context_issue_step(pamhd_ctx& x);
+// frees the adjoint workspace of a context (adjoint.cu)
+void release_adjoint(pamhd_ctx& x);
 }
 
 #endif
