@@ -71,7 +71,10 @@ mhd/solar_wind_box.hpp:227).
 enum {
 	PAMHD_BC_PERIODIC = 0,
 	PAMHD_BC_COPY = 1,
-	PAMHD_BC_VALUE = 2
+	PAMHD_BC_VALUE = 2,
+	PAMHD_BC_EXTERNAL = 3    /* z sides only: the ghost plane belongs to a neighbouring
+	                            slab and is written by the caller (halo exchange, see
+	                            pamhd_gpu_halo); the step never writes it */
 };
 
 /*
@@ -177,6 +180,32 @@ that callers can order their own work with it or time it with CUDA events.
 No reference counterpart (the reference has no device streams).
 */
 int pamhd_gpu_get_stream(pamhd_ctx* ctx, void** stream);
+
+/*
+Halo planes of a z slab, for the exchange between slabs of one grid split
+along z (one slab per GPU; the cut sides are PAMHD_BC_EXTERNAL).  The
+dccrg halo update the reference does between steps (mhd/solve.hpp:
+1767-1791) becomes: after each step, copy the interior boundary planes of
+each slab into its neighbours' ghost planes.
+side: 0 = low z, 1 = high z; ghost: 0 = the interior plane next to that
+side (to send), 1 = the ghost plane of that side (to receive).
+planes[v] receives the device address of variable v's plane in the
+current state, *count the plane's length in doubles (padded rows; a plane
+of one variable is contiguous).  The addresses alternate between two
+buffers from step to step: ask again after every step.
+*/
+int pamhd_gpu_halo(pamhd_ctx* ctx, int32_t side, int32_t ghost, double* planes[8], int64_t* count);
+
+/*
+Device address of the speed reduction the next step takes its dt from:
+four 64-bit words, the per-axis maxima of face speed / cell length as the
+bits of non-negative doubles (so an integer max over slabs is the max of
+the doubles) and a flag word (non-zero if any face speed was <= 0).  Slabs
+of one grid combine it by an element-wise max over all slabs before the
+next step, so that every slab takes the grid's dt
+(mhd/solve.hpp:1933-2014 takes the minimum over all cells of all ranks).
+*/
+int pamhd_gpu_speed_slot(pamhd_ctx* ctx, void** slot);
 
 /* Waits for the context's stream; returns PAMHD_ERR_PHYSICS if a face failed. */
 int pamhd_gpu_sync(pamhd_ctx* ctx);

@@ -26,7 +26,7 @@ LIB_PATH = os.path.join(PKG, "libpamhd_gpu.so")
 
 RUSANOV, RUSANOV_STAGGERED, HLL, HLLD, ROE = 0, 1, 2, 3, 4
 SOLVERS = {"rusanov": RUSANOV, "hll_athena": HLL, "hlld_athena": HLLD, "roe_athena": ROE}
-BC_PERIODIC, BC_COPY, BC_VALUE = 0, 1, 2
+BC_PERIODIC, BC_COPY, BC_VALUE, BC_EXTERNAL = 0, 1, 2, 3
 
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_PHYSICS, ERR_STATE, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
 ERR_TOO_LARGE = 6
@@ -231,6 +231,24 @@ class Context:
 
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
+
+    def halo(self, side: int, ghost: int):
+        """Device addresses of the eight variables' z plane (pamhd_gpu_halo) in the current state
+        and the plane length in doubles."""
+        fn = self.L.pamhd_gpu_halo
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, _P(ctypes.c_void_p), _P(ctypes.c_int64)]
+        planes = (ctypes.c_void_p * 8)()
+        count = ctypes.c_int64(0)
+        self._check(fn(self.h, side, ghost, planes, ctypes.byref(count)), "pamhd_gpu_halo")
+        return [int(p) for p in planes], int(count.value)
+
+    def speed_slot(self) -> int:
+        """Device address of the speed reduction the next step reads (pamhd_gpu_speed_slot)."""
+        fn = self.L.pamhd_gpu_speed_slot
+        fn.argtypes = [ctypes.c_void_p, _P(ctypes.c_void_p)]
+        p = ctypes.c_void_p()
+        self._check(fn(self.h, ctypes.byref(p)), "pamhd_gpu_speed_slot")
+        return int(p.value)
 
     def stream(self) -> int:
         """The cudaStream_t of the context, as an integer handle."""

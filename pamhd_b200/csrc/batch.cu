@@ -239,6 +239,7 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 	*out = nullptr;
 	for (int i = 0; i < nboxes; i++) {
 		PAMHD_TRY(validate(cfgs[i]));
+		if (cfgs[i].bc_lo[2] == PAMHD_BC_EXTERNAL or cfgs[i].bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
 		if (cfgs[i].solver != cfgs[0].solver) return PAMHD_ERR_ARGUMENT;
 		if ((cfgs[i].n[1] > 1) != (cfgs[0].n[1] > 1)) return PAMHD_ERR_ARGUMENT;
 	}

@@ -308,6 +308,27 @@ int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
 	return PAMHD_OK;
 }
 
+int pamhd_gpu_halo(pamhd_ctx* x, const int32_t side, const int32_t ghost, double* planes[8], int64_t* count)
+{
+	if (x == nullptr or planes == nullptr or count == nullptr) return PAMHD_ERR_ARGUMENT;
+	if ((side != 0 and side != 1) or (ghost != 0 and ghost != 1)) return PAMHD_ERR_ARGUMENT;
+	const Layout& L = x->L;
+	if (L.g[2] == 0) return PAMHD_ERR_ARGUMENT;  // no z ghosts: not a slab
+	const int k = side == 0 ? (ghost ? -1 : 0) : (ghost ? L.n[2] : L.n[2] - 1);
+	const long long first = (long long)(k + L.g[2]) * L.plane;
+	for (int v = 0; v < 8; v++) planes[v] = x->state[x->cur] + v * L.var + first;
+	*count = L.plane;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_speed_slot(pamhd_ctx* x, void** slot)
+{
+	if (x == nullptr or slot == nullptr) return PAMHD_ERR_ARGUMENT;
+	static_assert(sizeof(Speed_Max) == 32, "four 64-bit words");
+	*slot = static_cast<void*>(x->red + x->steps % 3);
+	return PAMHD_OK;
+}
+
 int pamhd_gpu_get_stream(pamhd_ctx* x, void** stream)
 {
 	if (x == nullptr or stream == nullptr) return PAMHD_ERR_ARGUMENT;

@@ -25,7 +25,11 @@ inline int validate(const pamhd_cfg& c)
 		if (c.n[d] < 1) return PAMHD_ERR_ARGUMENT;
 		if (not (c.cell_length[d] > 0.0) or not std::isfinite(c.cell_length[d])) return PAMHD_ERR_ARGUMENT;
 		for (const int b: {c.bc_lo[d], c.bc_hi[d]}) {
-			if (b != PAMHD_BC_PERIODIC and b != PAMHD_BC_COPY and b != PAMHD_BC_VALUE) return PAMHD_ERR_ARGUMENT;
+			if (b != PAMHD_BC_PERIODIC and b != PAMHD_BC_COPY and b != PAMHD_BC_VALUE and b != PAMHD_BC_EXTERNAL) {
+				return PAMHD_ERR_ARGUMENT;
+			}
+			// slab cuts: z only, and the slab needs z faces (two planes or more)
+			if (b == PAMHD_BC_EXTERNAL and (d != 2 or c.n[2] < 2)) return PAMHD_ERR_ARGUMENT;
 		}
 		if (c.n[d] > 1 and ((c.bc_lo[d] == PAMHD_BC_PERIODIC) != (c.bc_hi[d] == PAMHD_BC_PERIODIC))) {
 			return PAMHD_ERR_ARGUMENT;
@@ -86,7 +90,8 @@ inline bool grid_params(const pamhd_cfg& c, const Layout& L, Step_Params& P, con
 		active_count += P.active[d];
 	}
 	for (int d = 0; d < 3; d++) {
-		if (P.active[d] and not P.periodic[d] and active_count > 1) needs_boundary_speeds = true;
+		const bool own_side = c.bc_lo[d] != PAMHD_BC_EXTERNAL or c.bc_hi[d] != PAMHD_BC_EXTERNAL;
+		if (P.active[d] and not P.periodic[d] and own_side and active_count > 1) needs_boundary_speeds = true;
 	}
 	// z planes per block: enough blocks for several waves on 148 SMs, few redundant z faces
 	const int ty = P.active[1] ? step_tile_rows() : 1;

@@ -522,6 +522,8 @@ __device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 	for (int d = 0; d < 3; d++) {
 		if (not P.active[d] or P.periodic[d]) continue;
 		for (int side = 0; side < 2; side++) {
+			// the ghost layer of a slab cut is the neighbouring slab's interior: its faces are counted there
+			if ((side ? P.bc_hi[d] : P.bc_lo[d]) == PAMHD_BC_EXTERNAL) continue;
 			for (int e = 0; e < 3; e++) {
 				if (e == d or not P.active[e]) continue;
 				combos[nc][0] = d; combos[nc][1] = side; combos[nc][2] = e;
@@ -534,7 +536,9 @@ __device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 	if ((int)blockIdx.y < nc) {
 		const int d = combos[blockIdx.y][0], side = combos[blockIdx.y][1], e = combos[blockIdx.y][2];
 		const int f = 3 - d - e;
-		const int ne = P.periodic[e] ? P.L.n[e] : P.L.n[e] - 1;
+		// along a slab cut at the high side, the face into the ghost plane is this slab's
+		// (the one into the low ghost plane is the lower neighbour's)
+		const int ne = (P.periodic[e] or P.bc_hi[e] == PAMHD_BC_EXTERNAL) ? P.L.n[e] : P.L.n[e] - 1;
 		const int nf = P.L.n[f];
 		const long long count = (long long)ne * nf;
 		for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
@@ -542,7 +546,7 @@ __device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 			int a[3], b[3];
 			a[d] = b[d] = side ? P.L.n[d] : -1;
 			a[e] = int(t % ne);
-			b[e] = a[e] + 1 == P.L.n[e] ? 0 : a[e] + 1;
+			b[e] = (a[e] + 1 == P.L.n[e] and P.periodic[e]) ? 0 : a[e] + 1;
 			a[f] = b[f] = int(t / ne);
 			double UA[8], UB[8];
 			const long long oa = P.L.offset(a[0], a[1], a[2]), ob = P.L.offset(b[0], b[1], b[2]);
@@ -650,6 +654,7 @@ __global__ void fill_ghosts_kernel(const Step_Params P, double* state, const Gho
 			int s[3] = {c[0], c[1], c[2]};
 			double U[8];
 			const int kind = side ? P.bc_hi[d] : P.bc_lo[d];
+			if (kind == PAMHD_BC_EXTERNAL) continue;  // written by the halo exchange
 			if (P.periodic[d]) {
 				s[d] = side ? 0 : P.L.n[d] - 1;
 				const long long o = P.L.offset(s[0], s[1], s[2]);
