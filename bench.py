@@ -81,18 +81,38 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(n):
-    """dram bytes per launch of the step kernel from the committed ncu summary, scaled to n^3."""
+def ncu_count(n, key="step_kernel_hlld"):
+    """A per-launch count of the step kernel from the committed ncu summary (DRAM bytes, or FP64
+    flops for key step_kernel_hlld_fp64), scaled from the captured grid to n^3 cells."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     try:
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 3 and parts[0] == "step_kernel_hlld":
-                cells, dram = float(parts[1]), float(parts[2])
-                return dram * (n ** 3) / cells
+            if len(parts) >= 3 and parts[0] == key:
+                cells, value = float(parts[1]), float(parts[2])
+                return value * (n ** 3) / cells
     except OSError:
         pass
     return None
+
+
+def ncu_traffic(n):
+    return ncu_count(n, "step_kernel_hlld")
+
+
+def fp64_roof(n, kernel_ms, clocks):
+    """The second roof: FP64 flops of one step (ncu count per cell-update x cells) per second
+    against the chip's FP64 rate, 148 SMs x 64 FMA lanes x 2 flops at the median SM clock sampled
+    during the timed region (the max clock when no sample was taken)."""
+    flops = ncu_count(n, "step_kernel_hlld_fp64")
+    if flops is None:
+        return None
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = 148 * 64 * 2 * mhz * 1e6 / 1e12
+    achieved = flops / (kernel_ms / 1e3) / 1e12
+    return {"achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "flop_per_cell_update": flops / n ** 3,
+            "peak_source": f"148 SMs x 64 FP64 FMA/cycle x 2 at {mhz:.0f} MHz (nominal rate, measured clock)"}
 
 
 class ClockSampler:
@@ -579,6 +599,7 @@ def run_b200(a):
             "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
             "kernel_ms": kernel_ms,
+            "fp64": fp64_roof(n, kernel_ms, clocks.summary()),
         },
         "e2e": {
             "value": e2e,

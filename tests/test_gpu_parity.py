@@ -264,3 +264,69 @@ def test_blast_positivity_failure_matches_oracle(port):
     except pg.PhysicsError as e:
         fail_g = (fail_o[0], e.flags, e.cell, e.direction)
     assert fail_g == fail_o
+
+
+# ---------------------------------------------------------------- the configured workloads
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_brio_wu_configured_every_solver(port, solver):
+    """The shock-tube workload with each solver: 1000 cells on [0, 1], gamma 2, CFL 0.5, copy
+    boundaries, to t = 0.1; same step count, dt history within 1e-9, state within 1e-8."""
+    U0 = states.brio_wu(1000)
+    gpu, ora = pair(port, (1000, 1, 1), po.SOLVERS[solver], (1e-3, 1.0, 1.0), 2.0, 1.0, 0.5,
+                    bc_lo=(po.BC_COPY, 0, 0), bc_hi=(po.BC_COPY, 0, 0))
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    t_o, dts_o = ora.run(0.0, 0.1, 100000)
+    gpu.steps(len(dts_o) + 5, 0.1)
+    gpu.sync()
+    t_g, n_g, _ = gpu.time()
+    assert abs(t_g - t_o) <= 1e-13
+    dts_g = gpu.dt_history(n_g)
+    np.testing.assert_allclose(dts_g[: len(dts_o)], dts_o, rtol=1e-9)
+    assert np.all(dts_g[len(dts_o):] == 0.0)
+    assert field_err(gpu.get_state(), ora.get_state()) <= 1e-8
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_orszag_tang_512_configured(port, solver):
+    """The 2-D workload at its size: Orszag-Tang 512^2, periodic, gamma 5/3, CFL 0.4, up to 1000
+    steps with each solver.  Every 50 steps both are restarted from the GPU's state (a priming
+    step, then one step from identical inputs must agree to 1e-12, the per-step bar); in between
+    they run independently (dt within 1e-9).  The reference scheme loses positivity on this
+    problem near t = 0.104 for some solvers: the GPU must stop at the same step and face, with
+    the same error class, as the oracle, or both run all the steps."""
+    n = 512
+    U0 = states.orszag_tang(n)
+    gpu, ora = pair(port, (n, n, 1), po.SOLVERS[solver], (1 / n, 1 / n, 1.0), 5 / 3, 1.0, 0.4)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    fail_g = fail_o = None
+    for s in range(1001):
+        if s % 50 == 0 and s > 0:
+            U = gpu.get_state()
+            gpu.set_state(U)
+            ora.set_state(U)
+            assert gpu.step(1.0) == 0.0 and ora.step(1.0)[0] == 0.0
+            checked = True
+        else:
+            checked = False
+        try:
+            dg = gpu.step(1.0)
+        except pg.PhysicsError as e:
+            fail_g = (s, tuple(e.cell), e.direction, e.flags)
+        do, flag, cell, d = ora.step(1.0)
+        if flag:
+            fail_o = (s, tuple(cell), d, flag)
+        if fail_g or fail_o:
+            break
+        assert abs(dg - do) <= 1e-9 * max(do, 1e-300) or dg == do == 0.0
+        if checked:
+            assert abs(dg - do) <= STEP_TOL * do, s
+            assert field_err(gpu.get_state(), ora.get_state()) <= STEP_TOL, s
+    # the same step and first failing face; the GPU's flags (all failures of the step, OR-ed)
+    # include the oracle's (the first face's)
+    assert (fail_g is None) == (fail_o is None), (fail_g, fail_o)
+    if fail_g is not None:
+        assert fail_g[:3] == fail_o[:3], (fail_g, fail_o)
+        assert fail_g[3] & fail_o[3], (fail_g, fail_o)
