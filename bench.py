@@ -393,11 +393,15 @@ def adjoint_section(local, n=256, steps=200, every=20):
         "forward_ms": forward,
         "gradient_ms": gradient,
         "adjoint_over_forward": gradient / forward,
+        "reverse_step_over_forward_step": (gradient - forward) / forward,
         "fd_check": {"directions": 16, "h": "1e-6 of the field rms, Richardson with h/2",
                      "max_err_over_max_fd": float(np.abs(ads - fds).max() / np.abs(fds).max()),
                      "bar": 1e-6},
         "what": "gradient_ms: the pamhd_gpu_adjoint call (forward run with checkpoints, recompute of every "
-                "segment, reverse sweep); forward_ms: the same steps alone; device time by CUDA events",
+                "segment, reverse sweep); forward_ms: the same steps alone; device time by CUDA events; "
+                "adjoint_over_forward: the whole gradient against the forward run; "
+                "reverse_step_over_forward_step: (gradient - forward) / forward, the cost of one adjoint step "
+                "(recompute overlapped) against one forward step",
     }
 
 

@@ -224,3 +224,18 @@ def solar_wind_ensemble(nboxes=64, seed=20261204, sizes=(32, 48, 64, 96, 128), g
 def ensemble_state(box):
     n = box["n"]
     return np.broadcast_to(box["interior"][:, None, None, None], (8, n, n, n)).copy()
+
+
+def density_advection(n, gamma, vx, proton_mass=1.0):
+    """The reference's density-advection test (tests/mhd/config_files/hydrodynamic/
+    density_advection/1d/{+x,-x}/rusanov.json): n periodic cells on [0, 1], number density 1.01
+    where |x - 0.5| < 0.25 else 1, velocity (vx, 0, 0), pressure 1, no field; conservative state
+    as mhd/initialize.hpp builds it (rho = m_p n, mom = rho v, E = p / (gamma - 1) + rho v^2 / 2).
+    Returns (8, 1, 1, n)."""
+    x = (np.arange(n) + 0.5) / n
+    rho = np.where(np.abs(x - 0.5) < 0.25, 1.01, 1.0) * proton_mass
+    U = np.zeros((8, 1, 1, n))
+    U[0, 0, 0] = rho
+    U[1, 0, 0] = rho * vx
+    U[4, 0, 0] = 1.0 / (gamma - 1) + 0.5 * rho * vx * vx
+    return U

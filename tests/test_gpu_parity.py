@@ -330,3 +330,31 @@ def test_orszag_tang_512_configured(port, solver):
     if fail_g is not None:
         assert fail_g[:3] == fail_o[:3], (fail_g, fail_o)
         assert fail_g[3] & fail_o[3], (fail_g, fail_o)
+
+
+@pytest.mark.parametrize("case,vx", [("da_px", 1.0), ("da_mx", -1.0)])
+def test_reproduces_reference_program_output(case, vx):
+    """The reference program's own output (tests/mhd/reference/hydrodynamic/density_advection/1d/
+    {+x,-x}/rusanov/mhd_000000917.dc, via tests/golden/dc_goldens.npz): density advection, 200
+    periodic cells, Rusanov, CFL 0.5, t = 0 .. 1.  Same 917 steps and final time, state within
+    1e-12 of the reference's."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "dc_goldens.npz"))
+    gamma = float(g[case + "_gamma"])
+    n = int(g[case + "_cells"][0])
+    U0 = states.density_advection(n, gamma, vx, float(g[case + "_proton_mass"]))
+    cfg = pg.Config(n=(n, 1, 1), solver=pg.RUSANOV, cell_length=tuple(g[case + "_cell_length"]),
+                    adiabatic_index=gamma, vacuum_permeability=float(g[case + "_mu0"]), time_step_factor=0.5)
+    ctx = pg.Context(cfg)
+    ctx.set_state(U0)
+    t_end = float(g[case + "_time"])
+    ctx.steps(int(g[case + "_step"]) + 10, t_end)
+    ctx.sync()
+    t, steps, _ = ctx.time()
+    dts = ctx.dt_history(steps)
+    assert abs(t - t_end) <= 1e-14
+    assert int((dts > 0).sum()) == int(g[case + "_step"])
+    out = ctx.get_state().reshape(8, n)
+    ref = g[case + "_state"]
+    scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert (np.abs(out - ref).max(axis=1) / scale).max() <= STEP_TOL

@@ -7,7 +7,11 @@ reference's solvers and step.  These tests hold it to:
   - the live reference build (oracle/_ref) where the reference tree exists;
   - the reference's shipped goldens tests/mhd/mhd_{rusanov,hll_athena}.ref at
     the reference's own tolerance (tests/mhd/reference.cpp:637-640);
-  - rotation symmetry, the property mhd_diff.py --rotate checks.
+  - rotation symmetry, the property mhd_diff.py --rotate checks;
+  - the reference program's own output files (tests/mhd/reference/**/*.dc, extracted into
+    tests/golden/dc_goldens.npz by tests/golden/make_dc_golden.py with the reference's reader)
+    for the cases whose field is zero, where its staggered-field step reduces to the
+    cell-centred one: same step count, state within a few ulps after 917 steps.
 Bit-for-bit equality is required wherever both sides run the same
 arithmetic (the oracle is built with -ffp-contract=off, as the reference).
 """
@@ -208,3 +212,24 @@ def test_invalid_state_reports_first_failing_face(port):
     assert flag == 2  # PAMHD_FLAG_PRESSURE
     # first face in x-fastest cell order touching the bad cell: the +z face of (3, 1, 1)
     assert cell == (3, 1, 1) and d == 3
+
+
+@pytest.mark.parametrize("case,vx", [("da_px", 1.0), ("da_mx", -1.0)])
+def test_mode_c_reproduces_reference_program_output(port, case, vx):
+    """Density advection, 200 periodic cells, Rusanov, CFL 0.5, t = 0 .. 1: the reference
+    program wrote its state after 917 steps; the oracle's step (priming step, lagged CFL dt,
+    time cap, update) reproduces it."""
+    g = _load("dc_goldens.npz")
+    gamma = float(g[case + "_gamma"])
+    n = int(g[case + "_cells"][0])
+    U0 = states.density_advection(n, gamma, vx, float(g[case + "_proton_mass"]))
+    grid = port.grid(po.make_cfg((n, 1, 1), po.RUSANOV, tuple(g[case + "_cell_length"]), gamma,
+                                 float(g[case + "_mu0"]), 0.5))
+    grid.set_state(U0)
+    t, dts = grid.run(0.0, float(g[case + "_time"]), 100000)
+    assert t == float(g[case + "_time"])
+    assert int((dts > 0).sum()) == int(g[case + "_step"])   # plus the dt = 0 priming step
+    out = grid.get_state().reshape(8, n)
+    ref = g[case + "_state"]
+    scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
+    assert (np.abs(out - ref).max(axis=1) / scale).max() <= 1e-14
