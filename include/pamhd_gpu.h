@@ -42,8 +42,9 @@ enum {
 	                            (see pamhd_gpu_status for which and where) */
 	PAMHD_ERR_STATE = 4,     /* call made in the wrong order */
 	PAMHD_ERR_TIMEOUT = 5,   /* a bounded device-side wait gave up */
-	PAMHD_ERR_TOO_LARGE = 6  /* request larger than the fixed scratch of a
+	PAMHD_ERR_TOO_LARGE = 6, /* request larger than the fixed scratch of a
 	                            no-alloc entry point (split it) */
+	PAMHD_ERR_IO = 7         /* a file could not be opened, read or written */
 };
 
 /*
@@ -342,6 +343,40 @@ int pamhd_gpu_batch_get_stream(pamhd_batch* batch, void** stream);
 int pamhd_gpu_batch_time(pamhd_batch* batch, int32_t box, double* time, int64_t* steps, double* last_dt);
 int pamhd_gpu_batch_dt_history(pamhd_batch* batch, int32_t box, double* dt, int32_t count, int32_t* written);
 int pamhd_gpu_batch_status(pamhd_batch* batch, int32_t box, uint32_t* flags, int32_t cell[3], int32_t* dir);
+
+/*
+The reference's MHD output files (.dc, file version 4; written by
+mhd/save.hpp:75-375, read by the reference's tests/common.py and its tools
+such as tests/mhd/mhd_diff.py), for uniform grids: header, cell id list and
+the variable "mhd     " (mass density, momentum density, total energy
+density, magnetic field: 8 doubles per cell).  Host only: pair them with
+pamhd_gpu_get_state / pamhd_gpu_set_state.
+*/
+typedef struct pamhd_dc_info {
+	uint64_t step;               /* simulation step */
+	double time;                 /* simulation time */
+	double adiabatic_index;
+	double proton_mass;
+	double vacuum_permeability;
+	int32_t n[3];                /* level-0 cells */
+	int32_t periodic[3];
+	double start[3];             /* grid start coordinate */
+	double cell_length[3];
+	uint64_t cells;              /* n[0] * n[1] * n[2] (read only) */
+} pamhd_dc_info;
+
+/* Writes a .dc file: soa in the layout of pamhd_gpu_set_state (x fastest). */
+int pamhd_dc_write(const char* path, const pamhd_dc_info* info, const double* const soa[8]);
+
+/*
+Reads the header of a .dc file.  PAMHD_ERR_ARGUMENT for another file
+version or byte order, a refined (non-uniform) grid or a missing cell;
+PAMHD_ERR_IO when the file cannot be read.
+*/
+int pamhd_dc_read_info(const char* path, pamhd_dc_info* info);
+
+/* Reads the "mhd     " variable of a .dc file into eight arrays of info.cells doubles. */
+int pamhd_dc_read(const char* path, double* const soa[8]);
 
 #ifdef __cplusplus
 }

@@ -30,6 +30,7 @@ BC_PERIODIC, BC_COPY, BC_VALUE, BC_EXTERNAL = 0, 1, 2, 3
 
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_PHYSICS, ERR_STATE, ERR_TIMEOUT = 0, 1, 2, 3, 4, 5
 ERR_TOO_LARGE = 6
+ERR_IO = 7
 NOALLOC_MAX_FACES = 16384
 FLAG_DENSITY, FLAG_PRESSURE, FLAG_WAVE_SPEED, FLAG_FLUX = 1, 2, 4, 8
 FLAG_ROE_DENSITY, FLAG_ROE_PRESSURE, FLAG_NEW_STATE, FLAG_TIMEOUT = 16, 32, 64, 128
@@ -232,6 +233,21 @@ class Context:
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
 
+    def save_dc(self, path: str, step: int, time: float, proton_mass: float = 1.0, start=(0.0, 0.0, 0.0)):
+        """Writes the current state as a reference .dc file (pamhd_dc_write)."""
+        c = self.cfg
+        write_dc(path, self.get_state(), step=step, time=time, adiabatic_index=c.adiabatic_index,
+                 proton_mass=proton_mass, vacuum_permeability=c.vacuum_permeability, cell_length=c.cell_length,
+                 periodic=tuple(c.bc_lo[d] == BC_PERIODIC for d in range(3)), start=start)
+
+    def load_dc(self, path: str) -> dict:
+        """Sets the state from a reference .dc file of this grid's size; returns its header."""
+        info, U = read_dc(path)
+        if info["n"] != tuple(int(v) for v in self.cfg.n):
+            raise PamhdError(ERR_ARGUMENT, f"load_dc: {path} holds {info['n']} cells, the grid {tuple(self.cfg.n)}")
+        self.set_state(U)
+        return info
+
     def halo(self, side: int, ghost: int):
         """Device addresses of the eight variables' z plane (pamhd_gpu_halo) in the current state
         and the plane length in doubles."""
@@ -356,6 +372,67 @@ def face_flux_noalloc(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, devic
     if rc not in (OK, ERR_PHYSICS):
         raise PamhdError(rc, "pamhd_gpu_face_flux_noalloc")
     return flux, speed, flags
+
+
+class DcInfo(ctypes.Structure):
+    """pamhd_dc_info of include/pamhd_gpu.h: the header of a .dc file."""
+
+    _fields_ = [
+        ("step", ctypes.c_uint64),
+        ("time", ctypes.c_double),
+        ("adiabatic_index", ctypes.c_double),
+        ("proton_mass", ctypes.c_double),
+        ("vacuum_permeability", ctypes.c_double),
+        ("n", ctypes.c_int32 * 3),
+        ("periodic", ctypes.c_int32 * 3),
+        ("start", ctypes.c_double * 3),
+        ("cell_length", ctypes.c_double * 3),
+        ("cells", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {"step": int(self.step), "time": self.time, "adiabatic_index": self.adiabatic_index,
+                "proton_mass": self.proton_mass, "vacuum_permeability": self.vacuum_permeability,
+                "n": tuple(self.n), "periodic": tuple(bool(p) for p in self.periodic),
+                "start": tuple(self.start), "cell_length": tuple(self.cell_length), "cells": int(self.cells)}
+
+
+def write_dc(path: str, U: np.ndarray, *, step: int, time: float, adiabatic_index: float, proton_mass: float,
+             vacuum_permeability: float, cell_length, periodic=(True, True, True), start=(0.0, 0.0, 0.0)):
+    """Writes the state U (8, nz, ny, nx) as a reference .dc file (pamhd_dc_write)."""
+    L = lib()
+    L.pamhd_dc_write.argtypes = [ctypes.c_char_p, _P(DcInfo), ctypes.c_void_p]
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    info = DcInfo()
+    info.step = int(step)
+    info.time = float(time)
+    info.adiabatic_index = float(adiabatic_index)
+    info.proton_mass = float(proton_mass)
+    info.vacuum_permeability = float(vacuum_permeability)
+    for d in range(3):
+        info.n[d] = int(U.shape[3 - d])
+        info.periodic[d] = int(bool(periodic[d]))
+        info.start[d] = float(start[d])
+        info.cell_length[d] = float(cell_length[d])
+    rc = L.pamhd_dc_write(os.fsencode(path), ctypes.byref(info), _pointers([U[k].ctypes.data for k in range(8)]))
+    if rc != OK:
+        raise PamhdError(rc, "pamhd_dc_write")
+
+
+def read_dc(path: str):
+    """Reads a reference .dc file of a uniform grid: (header dict, state (8, nz, ny, nx))."""
+    L = lib()
+    L.pamhd_dc_read_info.argtypes = [ctypes.c_char_p, _P(DcInfo)]
+    L.pamhd_dc_read.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    info = DcInfo()
+    rc = L.pamhd_dc_read_info(os.fsencode(path), ctypes.byref(info))
+    if rc != OK:
+        raise PamhdError(rc, "pamhd_dc_read_info")
+    U = np.empty((8, info.n[2], info.n[1], info.n[0]))
+    rc = L.pamhd_dc_read(os.fsencode(path), _pointers([U[k].ctypes.data for k in range(8)]))
+    if rc != OK:
+        raise PamhdError(rc, "pamhd_dc_read")
+    return info.as_dict(), U
 
 
 class Batch:

@@ -149,6 +149,7 @@ const char* pamhd_gpu_errstr(const int code)
 	case PAMHD_ERR_STATE: return "call made in the wrong order";
 	case PAMHD_ERR_TIMEOUT: return "a bounded device wait expired";
 	case PAMHD_ERR_TOO_LARGE: return "request larger than the fixed scratch of a no-alloc entry point; split it";
+	case PAMHD_ERR_IO: return "a file could not be opened, read or written";
 	default: return "unknown error";
 	}
 }

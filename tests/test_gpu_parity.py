@@ -358,3 +358,14 @@ def test_reproduces_reference_program_output(case, vx):
     ref = g[case + "_state"]
     scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert (np.abs(out - ref).max(axis=1) / scale).max() <= STEP_TOL
+    # the same state through the reference's file format, and back into a context
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "mhd_000000917.dc")
+        ctx.save_dc(path, step=int(g[case + "_step"]), time=t, proton_mass=float(g[case + "_proton_mass"]))
+        info, U = pg.read_dc(path)
+        assert info["step"] == int(g[case + "_step"]) and info["periodic"] == (True, True, True)
+        assert np.array_equal(U.reshape(8, n), out)
+        ctx2 = pg.Context(cfg)
+        ctx2.load_dc(path)
+        assert np.array_equal(ctx2.get_state().reshape(8, n), out)
