@@ -183,6 +183,20 @@ No reference counterpart (the reference has no device streams).
 int pamhd_gpu_get_stream(pamhd_ctx* ctx, void** stream);
 
 /*
+Time-stamped inflow of a VALUE side (dim 0..2, side 0 = low, 1 = high), as
+the solar-wind boundary of mhd/solar_wind_box.hpp:227-268: with count
+increasing timestamps times[0..count-1] and count + 1 conservative states
+states[(count + 1) * 8], the side's ghosts hold states[i] while i of the
+timestamps are <= the simulation time.  The step writes them for the time
+its new state holds, on the device (no host round trip, graph replay
+unchanged); the current state's ghosts take the value of the current time
+at once.  Replaces the side's constant value; count = 0 with one state sets
+a constant.  Not with pamhd_gpu_adjoint (rejected).
+*/
+int pamhd_gpu_set_inflow(pamhd_ctx* ctx, int32_t dim, int32_t side, int32_t count, const double* times,
+                         const double* states);
+
+/*
 Halo planes of a z slab, for the exchange between slabs of one grid split
 along z (one slab per GPU; the cut sides are PAMHD_BC_EXTERNAL).  The
 dccrg halo update the reference does between steps (mhd/solve.hpp:
@@ -337,6 +351,10 @@ candidate number of z planes per work item and resident grid size, keeps
 the fastest and restores the state it started from.
 */
 int pamhd_gpu_batch_tune(pamhd_batch* batch, int32_t trial_steps, int32_t* planes, int32_t* grid);
+
+/* Time-stamped inflow of a VALUE side of one box (see pamhd_gpu_set_inflow). */
+int pamhd_gpu_batch_set_inflow(pamhd_batch* batch, int32_t box, int32_t dim, int32_t side, int32_t count,
+                               const double* times, const double* states);
 
 int pamhd_gpu_batch_sync(pamhd_batch* batch);
 int pamhd_gpu_batch_get_stream(pamhd_batch* batch, void** stream);

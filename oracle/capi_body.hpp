@@ -11,6 +11,7 @@ ORACLE_FLUX (the solver dispatch functor type).
 */
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "mode_c.hpp"
 
@@ -137,6 +138,27 @@ int ORACLE_API(grid_step)(void* grid, double max_dt, double* dt_taken,
 		for (int d = 0; d < 3; d++) cell[d] = c[d];
 		*dir = g.failure.dir;
 		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+/*
+Time-stamped inflow of a VALUE side (see Mode_C_Grid::set_inflow): count
+timestamps and count + 1 states of 8 doubles.
+*/
+int ORACLE_API(grid_set_inflow)(void* grid, int32_t dim, int32_t side, int32_t count, const double* times,
+                                const double* states)
+{
+	if (count < 0 or (count > 0 and times == nullptr) or states == nullptr) return fail_with("inflow arguments");
+	std::vector<double> t(times, times + count);
+	std::vector<std::array<double, 8>> u(size_t(count) + 1);
+	for (size_t i = 0; i < u.size(); i++) {
+		for (int v = 0; v < 8; v++) u[i][v] = states[8 * i + v];
+	}
+	try {
+		static_cast<Grid*>(grid)->set_inflow(dim, side, t, u);
 	} catch (const std::exception& e) {
 		return fail_with(e.what());
 	}

@@ -84,6 +84,18 @@ public:
 	std::vector<int8_t> CType;
 	int threads = 1;
 	Failure failure;
+	/*
+	Time-stamped inflow of VALUE sides, as the solar-wind boundary of
+	mhd/solar_wind_box.hpp:227-268: states[i] holds while i timestamps are
+	<= the simulation time (states has one more entry than times).  Empty:
+	the side keeps cfg.value_lo / value_hi.
+	*/
+	struct Inflow {
+		std::vector<double> times;
+		std::vector<std::array<double, 8>> states;
+	};
+	Inflow inflow[3][2];
+	double time = 0;  // simulation time since set_interior
 
 	explicit Mode_C_Grid(const pamhd_cfg& c) : cfg(c)
 	{
@@ -166,6 +178,29 @@ public:
 		}
 		for (auto& m: Max_v) m = {0, 0, 0, 0, 0, 0};
 		failure = Failure();
+		time = 0;
+		apply_boundaries();
+	}
+
+	// the value of a VALUE side at the current time
+	const double* value_of(const int d, const bool lo) const
+	{
+		const Inflow& t = inflow[d][lo ? 0 : 1];
+		if (t.states.empty()) return lo ? cfg.value_lo[d] : cfg.value_hi[d];
+		size_t i = 0;
+		while (i < t.times.size() and time >= t.times[i]) i++;
+		return t.states[i].data();
+	}
+
+	void set_inflow(const int d, const int side, const std::vector<double>& times,
+	                const std::vector<std::array<double, 8>>& states)
+	{
+		if (d < 0 or d > 2 or (side != 0 and side != 1)) throw std::invalid_argument("side");
+		if ((side == 0 ? cfg.bc_lo[d] : cfg.bc_hi[d]) != PAMHD_BC_VALUE) {
+			throw std::invalid_argument("inflow tables are for VALUE sides");
+		}
+		if (states.size() != times.size() + 1) throw std::invalid_argument("states: one more than times");
+		inflow[d][side] = {times, states};
 		apply_boundaries();
 	}
 
@@ -224,7 +259,7 @@ public:
 			const bool lo = c[d] < 0;
 			const int kind = lo ? cfg.bc_lo[d] : cfg.bc_hi[d];
 			if (kind == PAMHD_BC_VALUE) {
-				const double* v = lo ? cfg.value_lo[d] : cfg.value_hi[d];
+				const double* v = value_of(d, lo);
 				MHD& u = U[idx];
 				u.rho = v[0];
 				u.mom = {v[1], v[2], v[3]};
@@ -340,6 +375,7 @@ public:
 			throw Domain_Error(failure.flag, failure.what);
 		}
 		update();
+		time += dt;
 		apply_boundaries();
 		return dt;
 	}

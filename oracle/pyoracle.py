@@ -126,6 +126,8 @@ class Oracle:
         self._run = getattr(L, p + "grid_run")
         self._run.restype = ctypes.c_int64
         self._run.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int64, _DP, _DP]
+        self._set_inflow = getattr(L, p + "grid_set_inflow")
+        self._set_inflow.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
         self._last_error = getattr(L, p + "last_error")
         self._last_error.restype = ctypes.c_char_p
         if kind == "port":
@@ -195,6 +197,15 @@ class OracleGrid:
             ptrs[k] = U[k].ctypes.data
         self.o._get(self.h, ptrs)
         return U
+
+    def set_inflow(self, dim, side, times, states):
+        """Time-stamped states of a VALUE side: states[i] (8 conservative values) holds while i of
+        the timestamps are <= the simulation time; len(states) == len(times) + 1."""
+        times = np.ascontiguousarray(times, dtype=np.float64).reshape(-1)
+        states = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+        rc = self.o._set_inflow(self.h, dim, side, len(times), times.ctypes.data_as(_DP), states.ctypes.data_as(_DP))
+        if rc != 0:
+            raise ValueError(self.o.last_error())
 
     def step(self, max_dt):
         """Returns (dt, flag, cell, dir); flag != 0 when a face failed (state not updated)."""

@@ -233,6 +233,18 @@ class Context:
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
 
+    def set_inflow(self, dim: int, side: int, times, states):
+        """Time-stamped inflow of a VALUE side (pamhd_gpu_set_inflow): states[i] (8 conservative
+        values) holds while i of the increasing timestamps are <= the simulation time."""
+        fn = self.L.pamhd_gpu_set_inflow
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
+        times = np.ascontiguousarray(times, dtype=np.float64).reshape(-1)
+        states = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+        if len(states) != len(times) + 1:
+            raise ValueError("set_inflow: one state more than timestamps")
+        self._check(fn(self.h, dim, side, len(times), times.ctypes.data_as(_DP), states.ctypes.data_as(_DP)),
+                    "pamhd_gpu_set_inflow")
+
     def save_dc(self, path: str, step: int, time: float, proton_mass: float = 1.0, start=(0.0, 0.0, 0.0)):
         """Writes the current state as a reference .dc file (pamhd_dc_write)."""
         c = self.cfg
@@ -473,6 +485,17 @@ class Batch:
         U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shapes[box])
         self._check(self.L.pamhd_gpu_batch_set_state(self.h, box, _pointers([U[k].ctypes.data for k in range(8)])),
                     "pamhd_gpu_batch_set_state")
+
+    def set_inflow(self, box: int, dim: int, side: int, times, states):
+        """Time-stamped inflow of a VALUE side of one box (pamhd_gpu_batch_set_inflow)."""
+        fn = self.L.pamhd_gpu_batch_set_inflow
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
+        times = np.ascontiguousarray(times, dtype=np.float64).reshape(-1)
+        states = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+        if len(states) != len(times) + 1:
+            raise ValueError("set_inflow: one state more than timestamps")
+        self._check(fn(self.h, box, dim, side, len(times), times.ctypes.data_as(_DP), states.ctypes.data_as(_DP)),
+                    "pamhd_gpu_batch_set_inflow", box)
 
     def get_state(self, box: int) -> np.ndarray:
         U = np.empty((8,) + self.shapes[box])

@@ -63,6 +63,10 @@ struct pamhd_batch {
 	int cur = 0;
 	bool loaded = false;
 	cudaGraphExec_t graph = nullptr;
+	// time-stamped inflow of VALUE sides, per box and side (index 6 box + 2 dimension + side)
+	std::vector<Inflow_Table> inflow;
+	std::vector<double*> inflow_dev;
+	std::vector<std::vector<double>> inflow_times, inflow_states;
 };
 
 namespace {
@@ -79,6 +83,28 @@ int check(const cudaError_t e)
 long long cells_of(const pamhd_cfg& c)
 {
 	return (long long)c.n[0] * c.n[1] * c.n[2];
+}
+
+// ghost states of a box's VALUE sides at time t: configured values or time-stamped inflow
+void box_values_at(const pamhd_batch& b, const int box, const double t, double lo[3][8], double hi[3][8])
+{
+	for (int d = 0; d < 3; d++) {
+		for (int side = 0; side < 2; side++) {
+			double* out = side == 0 ? lo[d] : hi[d];
+			const double* v = side == 0 ? b.cfg[box].value_lo[d] : b.cfg[box].value_hi[d];
+			if (not b.inflow.empty()) {
+				const size_t k = 6 * size_t(box) + 2 * d + side;
+				const std::vector<double>& times = b.inflow_times[k];
+				const std::vector<double>& states = b.inflow_states[k];
+				if (not states.empty()) {
+					size_t i = 0;
+					while (i < times.size() and t >= times[i]) i++;
+					v = states.data() + 8 * i;
+				}
+			}
+			for (int q = 0; q < 8; q++) out[q] = v[q];
+		}
+	}
 }
 
 // per-box parameters and the work-item table for a given number of z planes per item
@@ -102,6 +128,11 @@ int build_work(pamhd_batch& b, const int planes)
 		for (int d = 0; d < 3; d++) {
 			for (int e = 0; e < 3; e++) {
 				if (e != d) b.largest_plane = std::max(b.largest_plane, b.cfg[i].n[d] * b.cfg[i].n[e]);
+			}
+		}
+		for (int d = 0; d < 3; d++) {
+			for (int side = 0; side < 2; side++) {
+				if (not b.inflow.empty()) P.inflow[d][side] = b.inflow[6 * i + 2 * d + side];
 			}
 		}
 		P.red = b.red + 3 * i;
@@ -308,6 +339,7 @@ int pamhd_gpu_batch_destroy(pamhd_batch* b)
 	cudaFree(b->d_params[1]);
 	cudaFree(b->d_items);
 	cudaFree(b->staging);
+	for (double* p: b->inflow_dev) cudaFree(p);
 	if (b->stream != nullptr) cudaStreamDestroy(b->stream);
 	delete b;
 	return PAMHD_OK;
@@ -329,11 +361,67 @@ int pamhd_gpu_batch_set_state(pamhd_batch* b, const int32_t box, const double* c
 				PAMHD_TRY(launch_scatter(b->staging, base + v * L.var, L, b->stream));
 			}
 		}
-		PAMHD_TRY(launch_fill_ghosts_values(b->params[0][box], base, b->cfg[box].value_lo, b->cfg[box].value_hi,
-		                                    b->stream));
+		double lo[3][8], hi[3][8];
+		box_values_at(*b, box, 0.0, lo, hi);
+		PAMHD_TRY(launch_fill_ghosts_values(b->params[0][box], base, lo, hi, b->stream));
 	}
 	b->loaded = true;
 	return reset_run_state(*b);
+}
+
+int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t dim, const int32_t side,
+                               const int32_t count, const double* times, const double* states)
+{
+	PAMHD_TRY(box_ok(b, box));
+	if (dim < 0 or dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
+	if ((count > 0 and times == nullptr) or states == nullptr) return PAMHD_ERR_ARGUMENT;
+	const pamhd_cfg& c = b->cfg[box];
+	if ((side == 0 ? c.bc_lo[dim] : c.bc_hi[dim]) != PAMHD_BC_VALUE or c.n[dim] < 2) return PAMHD_ERR_ARGUMENT;
+	for (int i = 0; i < count; i++) {
+		if (not std::isfinite(times[i]) or (i > 0 and not (times[i] > times[i - 1]))) return PAMHD_ERR_ARGUMENT;
+	}
+	PAMHD_TRY(check(cudaSetDevice(b->device)));
+	const size_t nt = size_t(count), ns = 8 * (size_t(count) + 1);
+	double* dev = nullptr;
+	PAMHD_TRY(check(cudaMalloc(&dev, (nt + ns) * sizeof(double))));
+	if ((nt > 0 and cudaMemcpy(dev, times, nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+		or cudaMemcpy(dev + nt, states, ns * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+		cudaFree(dev);
+		return PAMHD_ERR_CUDA;
+	}
+	PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+	if (b->inflow.empty()) {
+		b->inflow.assign(6 * size_t(b->nboxes), Inflow_Table{nullptr, nullptr, 0});
+		b->inflow_dev.assign(6 * size_t(b->nboxes), nullptr);
+		b->inflow_times.assign(6 * size_t(b->nboxes), {});
+		b->inflow_states.assign(6 * size_t(b->nboxes), {});
+	}
+	const size_t k = 6 * size_t(box) + 2 * dim + side;
+	cudaFree(b->inflow_dev[k]);
+	b->inflow_dev[k] = dev;
+	b->inflow[k] = Inflow_Table{dev, dev + nt, count};
+	b->inflow_times[k].assign(times, times + nt);
+	b->inflow_states[k].assign(states, states + ns);
+	for (int parity = 0; parity < 2; parity++) {
+		b->params[parity][box].inflow[dim][side] = b->inflow[k];
+		PAMHD_TRY(check(cudaMemcpy(b->d_params[parity] + box, &b->params[parity][box], sizeof(Step_Params),
+		                           cudaMemcpyHostToDevice)));
+	}
+	if (b->graph != nullptr) {
+		cudaGraphExecDestroy(b->graph);
+		b->graph = nullptr;
+	}
+	if (b->loaded) {
+		Clock clk;
+		PAMHD_TRY(check(cudaMemcpy(&clk, b->clock + 3 * size_t(box) + b->steps % 3, sizeof clk,
+		                           cudaMemcpyDeviceToHost)));
+		double lo[3][8], hi[3][8];
+		box_values_at(*b, box, clk.t, lo, hi);
+		PAMHD_TRY(launch_fill_ghosts_values(b->params[b->cur][box], b->state[b->cur] + b->off[box], lo, hi,
+		                                    b->stream));
+		PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+	}
+	return PAMHD_OK;
 }
 
 int pamhd_gpu_batch_get_state(pamhd_batch* b, const int32_t box, double* const soa[8])

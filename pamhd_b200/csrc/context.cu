@@ -102,11 +102,33 @@ int set_control(pamhd_ctx& x, const double max_dt, const double t_end)
 	return check(cudaStreamSynchronize(x.stream));
 }
 
+// ghost states of the VALUE sides at time t: the configured values, or the time-stamped inflow
+void values_at(const pamhd_ctx& x, const double t, double lo[3][8], double hi[3][8])
+{
+	for (int d = 0; d < 3; d++) {
+		for (int side = 0; side < 2; side++) {
+			double* out = side == 0 ? lo[d] : hi[d];
+			const double* v = side == 0 ? x.cfg.value_lo[d] : x.cfg.value_hi[d];
+			const std::vector<double>& times = x.inflow_times[d][side];
+			const std::vector<double>& states = x.inflow_states[d][side];
+			if (not states.empty()) {
+				size_t i = 0;
+				while (i < times.size() and t >= times[i]) i++;
+				v = states.data() + 8 * i;
+			}
+			for (int k = 0; k < 8; k++) out[k] = v[k];
+		}
+	}
+}
+
+// ghosts of both state copies after set_state (simulation time 0)
 int fill_ghosts(pamhd_ctx& x)
 {
 	const Step_Params P = x.base;
-	PAMHD_TRY(launch_fill_ghosts_values(P, x.state[0], x.cfg.value_lo, x.cfg.value_hi, x.stream));
-	return launch_fill_ghosts_values(P, x.state[1], x.cfg.value_lo, x.cfg.value_hi, x.stream);
+	double lo[3][8], hi[3][8];
+	values_at(x, 0.0, lo, hi);
+	PAMHD_TRY(launch_fill_ghosts_values(P, x.state[0], lo, hi, x.stream));
+	return launch_fill_ghosts_values(P, x.state[1], lo, hi, x.stream);
 }
 
 int capture_graph(pamhd_ctx& x)
@@ -204,6 +226,10 @@ int pamhd_gpu_destroy(pamhd_ctx* x)
 	if (x->stream != nullptr) cudaStreamSynchronize(x->stream);
 	if (x->graph != nullptr) cudaGraphExecDestroy(x->graph);
 	release_adjoint(*x);
+	for (int d = 0; d < 3; d++) {
+		cudaFree(x->inflow_dev[d][0]);
+		cudaFree(x->inflow_dev[d][1]);
+	}
 	cudaFree(x->state[0]);
 	cudaFree(x->state[1]);
 	cudaFree(x->red);
@@ -305,6 +331,55 @@ int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
 	while (left > 0) {
 		PAMHD_TRY(issue_step(*x));
 		left--;
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_set_inflow(pamhd_ctx* x, const int32_t dim, const int32_t side, const int32_t count,
+                         const double* times, const double* states)
+{
+	if (x == nullptr or dim < 0 or dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
+	if ((count > 0 and times == nullptr) or states == nullptr) return PAMHD_ERR_ARGUMENT;
+	if ((side == 0 ? x->cfg.bc_lo[dim] : x->cfg.bc_hi[dim]) != PAMHD_BC_VALUE or x->cfg.n[dim] < 2) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	for (int i = 0; i < count; i++) {
+		if (not std::isfinite(times[i]) or (i > 0 and not (times[i] > times[i - 1]))) return PAMHD_ERR_ARGUMENT;
+	}
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	const size_t nt = size_t(count), ns = 8 * (size_t(count) + 1);
+	double* dev = nullptr;
+	PAMHD_TRY(check(cudaMalloc(&dev, (nt + ns) * sizeof(double))));
+	if (nt > 0 and cudaMemcpy(dev, times, nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+		cudaFree(dev);
+		return PAMHD_ERR_CUDA;
+	}
+	if (cudaMemcpy(dev + nt, states, ns * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+		cudaFree(dev);
+		return PAMHD_ERR_CUDA;
+	}
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	cudaFree(x->inflow_dev[dim][side]);
+	x->inflow_dev[dim][side] = dev;
+	x->inflow_times[dim][side].assign(times, times + nt);
+	x->inflow_states[dim][side].assign(states, states + ns);
+	x->base.inflow[dim][side].times = dev;
+	x->base.inflow[dim][side].states = dev + nt;
+	x->base.inflow[dim][side].count = count;
+	// the captured steps hold the old parameters
+	if (x->graph != nullptr) {
+		cudaGraphExecDestroy(x->graph);
+		x->graph = nullptr;
+	}
+	// the current state's ghosts take the value of the current time
+	if (x->loaded) {
+		Clock c;
+		PAMHD_TRY(check(cudaMemcpyAsync(&c, x->clock + x->steps % 3, sizeof c, cudaMemcpyDeviceToHost, x->stream)));
+		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+		double lo[3][8], hi[3][8];
+		values_at(*x, c.t, lo, hi);
+		PAMHD_TRY(launch_fill_ghosts_values(x->base, x->state[x->cur], lo, hi, x->stream));
+		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
 	}
 	return PAMHD_OK;
 }

@@ -7,6 +7,8 @@ the entry points of context.cu and the adjoint driver of adjoint.cu.
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "grid_setup.cuh"
 #include "step.cuh"
 
@@ -36,6 +38,9 @@ struct pamhd_ctx {
 	cudaGraphExec_t graph = nullptr;
 	bool loaded = false;
 	Adjoint_Work* adjoint = nullptr;  // adjoint workspace, kept between pamhd_gpu_adjoint calls
+	// time-stamped inflow of VALUE sides: host copies and the device tables (times, then states)
+	std::vector<double> inflow_times[3][2], inflow_states[3][2];
+	double* inflow_dev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
 };
 
 namespace pamhd_b200 {

@@ -62,6 +62,18 @@ struct Control {
 	double t_end;
 };
 
+/*
+Time-stamped inflow of a VALUE side (the solar-wind boundary of
+mhd/solar_wind_box.hpp:227-268): states[i] (8 conservative values) holds
+while i of the count timestamps are <= the simulation time.  Device
+memory; states == nullptr: the side keeps its constant ghost values.
+*/
+struct Inflow_Table {
+	const double* times;
+	const double* states;   // (count + 1) x 8
+	int count;
+};
+
 struct Step_Params {
 	const double* __restrict__ in;
 	double* __restrict__ out;
@@ -84,6 +96,7 @@ struct Step_Params {
 	int phase;           // step index mod 3
 	int kchunk;          // z planes per block
 	double forced_dt;    // >= 0: the step's dt (a prescribed schedule); < 0: the CFL rule
+	Inflow_Table inflow[3][2];  // per dimension and side (lo, hi)
 };
 
 // launchers (step_kernels.cu)
