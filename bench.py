@@ -54,6 +54,7 @@ def args_():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
     return p.parse_args()
 
 
@@ -230,6 +231,87 @@ def cpu_model():
     except OSError:
         pass
     return "unknown"
+
+
+def configs_section(local, cpu=True):
+    """The other configured workloads, GPU beside the reference's solver headers on the host cores
+    (a bounded sample each): cell-updates/s of the shock tube run to its end time and of 100
+    Orszag-Tang 512^2 steps with each solver (the reference scheme keeps positivity that long)."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+    from oracle import pyoracle as po
+
+    def gpu_rate(cfg, U, steps, t_end):
+        ctx = pg.Context(cfg)
+        st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        # the steps that advance time (a run to t_end stops moving once there)
+        ctx.set_state(U)
+        ctx.steps(steps + 1, t_end)
+        ctx.sync()
+        steps = int((ctx.dt_history(steps + 1) > 0).sum())
+        best = None
+        for _ in range(3):
+            ctx.set_state(U)
+            ctx.steps(1, t_end)
+            ctx.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            ctx.steps(steps, t_end)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        ctx.sync()
+        ctx.close()
+        return best, steps
+
+    def cpu_rate(ocfg, U, steps, t_end, threads):
+        try:
+            o = po.Oracle("reference")
+        except Exception:
+            o = po.Oracle("port")
+        g = o.grid(ocfg, threads=threads)
+        g.set_state(U)
+        g.step(t_end)
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(steps):
+            dt, flag, _, _ = g.step(t_end)
+            if flag or dt == 0.0:
+                break
+            done += 1
+        return (time.perf_counter() - t0) * 1e3, done
+
+    out = {}
+    # shock tube: 1000 cells, gamma 2, HLLD, CFL 0.5, copy boundaries, to t = 0.1
+    U = states.brio_wu(1000)
+    cfg = pg.Config(n=(1000, 1, 1), solver=pg.HLLD, cell_length=(1e-3, 1.0, 1.0), adiabatic_index=2.0,
+                    time_step_factor=0.5, bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0), device=local)
+    ms, steps = gpu_rate(cfg, U, 2000, 0.1)
+    entry = {"workload": "Brio-Wu 1000 cells, HLLD, CFL 0.5, to t = 0.1", "steps": steps,
+             "gpu": 1000 * steps / (ms / 1e3), "gpu_ms": ms, "unit": UNIT}
+    if cpu:
+        ocfg = po.make_cfg((1000, 1, 1), po.HLLD, (1e-3, 1.0, 1.0), 2.0, 1.0, 0.5, (1, 0, 0), (1, 0, 0))
+        cms, csteps = cpu_rate(ocfg, U, 2000, 0.1, 1)
+        entry.update(cpu_one_core=1000 * csteps / (cms / 1e3), cpu_sample=f"{csteps} steps, 1 thread")
+    out["brio_wu"] = entry
+    # Orszag-Tang 512^2, each solver, 100 steps
+    n = 512
+    U = states.orszag_tang(n)
+    for name, sid in po.SOLVERS.items():
+        cfg = pg.Config(n=(n, n, 1), solver=sid, cell_length=(1 / n, 1 / n, 1.0), adiabatic_index=5 / 3,
+                        time_step_factor=0.4, device=local)
+        ms, steps = gpu_rate(cfg, U, 100, 10.0)
+        entry = {"workload": f"Orszag-Tang {n}^2 periodic, {name}, CFL 0.4, 100 steps", "steps": steps,
+                 "gpu": n * n * steps / (ms / 1e3), "gpu_ms": ms, "unit": UNIT}
+        if cpu:
+            threads = cpu_threads()
+            ocfg = po.make_cfg((n, n, 1), sid, (1 / n, 1 / n, 1.0), 5 / 3, 1.0, 0.4)
+            cms, csteps = cpu_rate(ocfg, U, 5, 10.0, threads)
+            entry.update(cpu=n * n * csteps / (cms / 1e3), cpu_cores=threads, cpu_sample=f"{csteps} steps")
+        out[f"orszag_tang_{name}"] = entry
+    return out
 
 
 def batched_section(local, steps=500):
@@ -621,6 +703,8 @@ def run_b200(a):
         line["batched"] = batched_section(local)
     if not a.no_adjoint:
         line["adjoint"] = adjoint_section(local)
+    if not a.no_configs and world == 1:
+        line["configs"] = configs_section(local, cpu=rank == 0 and not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)

@@ -370,10 +370,8 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 	for (int v = 0; v < 8; v++) if (seed[v] == nullptr or grad[v] == nullptr) return PAMHD_ERR_ARGUMENT;
 	if (x->cfg.solver == PAMHD_ROE_ATHENA) return PAMHD_ERR_ARGUMENT;  // no Roe adjoint
 	if (x->cfg.bc_lo[2] == PAMHD_BC_EXTERNAL or x->cfg.bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
-	for (int d = 0; d < 3; d++) {
-		// the inflow-state gradient is of one constant state per side
-		if (x->base.inflow[d][0].states != nullptr or x->base.inflow[d][1].states != nullptr) return PAMHD_ERR_ARGUMENT;
-	}
+	// the inflow-state gradient is of one constant state per side
+	if (x->base.inflow != nullptr) return PAMHD_ERR_ARGUMENT;
 	if (not x->loaded) return PAMHD_ERR_STATE;
 	if (dt_in != nullptr) {
 		for (int n = 0; n < nsteps; n++) if (not (dt_in[n] >= 0.0)) return PAMHD_ERR_ARGUMENT;

@@ -65,6 +65,7 @@ struct pamhd_batch {
 	cudaGraphExec_t graph = nullptr;
 	// time-stamped inflow of VALUE sides, per box and side (index 6 box + 2 dimension + side)
 	std::vector<Inflow_Table> inflow;
+	Inflow_Table* d_inflow = nullptr;   // the same tables in device memory
 	std::vector<double*> inflow_dev;
 	std::vector<std::vector<double>> inflow_times, inflow_states;
 };
@@ -130,10 +131,10 @@ int build_work(pamhd_batch& b, const int planes)
 				if (e != d) b.largest_plane = std::max(b.largest_plane, b.cfg[i].n[d] * b.cfg[i].n[e]);
 			}
 		}
-		for (int d = 0; d < 3; d++) {
-			for (int side = 0; side < 2; side++) {
-				if (not b.inflow.empty()) P.inflow[d][side] = b.inflow[6 * i + 2 * d + side];
-			}
+		if (b.d_inflow != nullptr) {
+			bool any = false;
+			for (int k = 0; k < 6; k++) any = any or b.inflow[6 * size_t(i) + k].states != nullptr;
+			if (any) P.inflow = b.d_inflow + 6 * size_t(i);
 		}
 		P.red = b.red + 3 * i;
 		P.clock = b.clock + 3 * i;
@@ -340,6 +341,7 @@ int pamhd_gpu_batch_destroy(pamhd_batch* b)
 	cudaFree(b->d_items);
 	cudaFree(b->staging);
 	for (double* p: b->inflow_dev) cudaFree(p);
+	cudaFree(b->d_inflow);
 	if (b->stream != nullptr) cudaStreamDestroy(b->stream);
 	delete b;
 	return PAMHD_OK;
@@ -395,6 +397,8 @@ int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t 
 		b->inflow_dev.assign(6 * size_t(b->nboxes), nullptr);
 		b->inflow_times.assign(6 * size_t(b->nboxes), {});
 		b->inflow_states.assign(6 * size_t(b->nboxes), {});
+		PAMHD_TRY(check(cudaMalloc(&b->d_inflow, 6 * size_t(b->nboxes) * sizeof(Inflow_Table))));
+		PAMHD_TRY(check(cudaMemset(b->d_inflow, 0, 6 * size_t(b->nboxes) * sizeof(Inflow_Table))));
 	}
 	const size_t k = 6 * size_t(box) + 2 * dim + side;
 	cudaFree(b->inflow_dev[k]);
@@ -402,8 +406,9 @@ int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t 
 	b->inflow[k] = Inflow_Table{dev, dev + nt, count};
 	b->inflow_times[k].assign(times, times + nt);
 	b->inflow_states[k].assign(states, states + ns);
+	PAMHD_TRY(check(cudaMemcpy(b->d_inflow + k, &b->inflow[k], sizeof(Inflow_Table), cudaMemcpyHostToDevice)));
 	for (int parity = 0; parity < 2; parity++) {
-		b->params[parity][box].inflow[dim][side] = b->inflow[k];
+		b->params[parity][box].inflow = b->d_inflow + 6 * size_t(box);
 		PAMHD_TRY(check(cudaMemcpy(b->d_params[parity] + box, &b->params[parity][box], sizeof(Step_Params),
 		                           cudaMemcpyHostToDevice)));
 	}

@@ -230,6 +230,7 @@ int pamhd_gpu_destroy(pamhd_ctx* x)
 		cudaFree(x->inflow_dev[d][0]);
 		cudaFree(x->inflow_dev[d][1]);
 	}
+	cudaFree(x->inflow_tables);
 	cudaFree(x->state[0]);
 	cudaFree(x->state[1]);
 	cudaFree(x->red);
@@ -363,9 +364,13 @@ int pamhd_gpu_set_inflow(pamhd_ctx* x, const int32_t dim, const int32_t side, co
 	x->inflow_dev[dim][side] = dev;
 	x->inflow_times[dim][side].assign(times, times + nt);
 	x->inflow_states[dim][side].assign(states, states + ns);
-	x->base.inflow[dim][side].times = dev;
-	x->base.inflow[dim][side].states = dev + nt;
-	x->base.inflow[dim][side].count = count;
+	if (x->inflow_tables == nullptr) {
+		PAMHD_TRY(check(cudaMalloc(&x->inflow_tables, 6 * sizeof(Inflow_Table))));
+		PAMHD_TRY(check(cudaMemset(x->inflow_tables, 0, 6 * sizeof(Inflow_Table))));
+	}
+	const Inflow_Table table{dev, dev + nt, count};
+	PAMHD_TRY(check(cudaMemcpy(x->inflow_tables + 2 * dim + side, &table, sizeof table, cudaMemcpyHostToDevice)));
+	x->base.inflow = x->inflow_tables;
 	// the captured steps hold the old parameters
 	if (x->graph != nullptr) {
 		cudaGraphExecDestroy(x->graph);

@@ -41,6 +41,7 @@ struct pamhd_ctx {
 	// time-stamped inflow of VALUE sides: host copies and the device tables (times, then states)
 	std::vector<double> inflow_times[3][2], inflow_states[3][2];
 	double* inflow_dev[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+	Inflow_Table* inflow_tables = nullptr;  // [3][2] in device memory, pointed to by the step parameters
 };
 
 namespace pamhd_b200 {

@@ -96,7 +96,7 @@ struct Step_Params {
 	int phase;           // step index mod 3
 	int kchunk;          // z planes per block
 	double forced_dt;    // >= 0: the step's dt (a prescribed schedule); < 0: the CFL rule
-	Inflow_Table inflow[3][2];  // per dimension and side (lo, hi)
+	const Inflow_Table* inflow;  // [3][2] by dimension and side (lo, hi) in device memory, or nullptr
 };
 
 // launchers (step_kernels.cu)

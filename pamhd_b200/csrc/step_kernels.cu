@@ -210,10 +210,11 @@ __device__ __forceinline__ const double* inflow_at(const Inflow_Table& T, const 
 
 /*
 New state of an interior cell plus its periodic image / COPY ghost, and the
-ghost of a time-stamped VALUE side at the time the new state holds, t_next.
+ghost of a time-stamped VALUE side at the time the new state holds: the
+step's start time plus dt, as begin_step advances the clock.
 */
 __device__ void write_cell(const Step_Params& P, const int i, const int j, const int k, const double U[8],
-                           const double t_next)
+                           const double dt)
 {
 	store_cell(P.out, P.L, i, j, k, U);
 	const int c[3] = {i, j, k};
@@ -231,9 +232,9 @@ __device__ void write_cell(const Step_Params& P, const int i, const int j, const
 				copy_state(U, P.gas, C);
 				t[d] = -1;
 				store_cell(P.out, P.L, t[0], t[1], t[2], C);
-			} else if (P.bc_lo[d] == PAMHD_BC_VALUE and P.inflow[d][0].states != nullptr) {
+			} else if (P.bc_lo[d] == PAMHD_BC_VALUE and P.inflow != nullptr and P.inflow[2 * d].states != nullptr) {
 				t[d] = -1;
-				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[d][0], t_next));
+				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d], P.clock[P.phase].t + dt));
 			}
 		}
 		if (c[d] == n - 1) {
@@ -246,9 +247,9 @@ __device__ void write_cell(const Step_Params& P, const int i, const int j, const
 				copy_state(U, P.gas, C);
 				t[d] = n;
 				store_cell(P.out, P.L, t[0], t[1], t[2], C);
-			} else if (P.bc_hi[d] == PAMHD_BC_VALUE and P.inflow[d][1].states != nullptr) {
+			} else if (P.bc_hi[d] == PAMHD_BC_VALUE and P.inflow != nullptr and P.inflow[2 * d + 1].states != nullptr) {
 				t[d] = n;
-				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[d][1], t_next));
+				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d + 1], P.clock[P.phase].t + dt));
 			}
 		}
 	}
@@ -365,8 +366,6 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 	const int kfirst = zact ? kb - 1 : kb;
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
-	// the time of the new state (as begin_step advances the clock)
-	const double t_next = P.clock[P.phase].t + dt;
 
 	double Up[8], Fzm[8];
 	#pragma unroll
@@ -452,7 +451,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 				double Un[8];
 				#pragma unroll
 				for (int v = 0; v < 8; v++) Un[v] = Up[v] + (Fzm[v] - Fz[v]) * P.inv_len[2];
-				write_cell(P, gx, gy, k - 1, Un, t_next);
+				write_cell(P, gx, gy, k - 1, Un, dt);
 			}
 			if (inner) {
 				#pragma unroll
@@ -471,7 +470,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 					#pragma unroll
 					for (int v = 0; v < 8; v++) Fzm[v] = Fz[v];
 				} else {
-					write_cell(P, gx, gy, k, Up, t_next);
+					write_cell(P, gx, gy, k, Up, dt);
 				}
 			}
 		}
