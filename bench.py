@@ -55,6 +55,13 @@ def args_():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
+    p.add_argument("--only", choices=["batched", "adjoint", "configs"],
+                   help="run one section alone and print it (for profiling)")
+    p.add_argument("--boxes", type=int, default=64, help="boxes of the batched section")
+    p.add_argument("--batched-steps", type=int, default=500)
+    p.add_argument("--no-tune", action="store_true", help="batched section without the autotuner")
+    p.add_argument("--adjoint-steps", type=int, default=200)
+    p.add_argument("--no-fd-check", action="store_true")
     return p.parse_args()
 
 
@@ -314,14 +321,14 @@ def configs_section(local, cpu=True):
     return out
 
 
-def batched_section(local, steps=500):
+def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
     """Batched ensemble (64 uneven SI solar-wind boxes, HLL, 500 steps) in one batch against the same
     boxes run one after another, each in its own context (sequential per-box launches)."""
     import torch
     import pamhd_b200 as pg
     import states
 
-    boxes = states.solar_wind_ensemble()
+    boxes = states.solar_wind_ensemble(nboxes=nboxes)
     cfgs = [pg.Config(n=(b["n"],) * 3, solver=pg.HLL, cell_length=(states.EARTH_RADIUS_CELL,) * 3,
                       adiabatic_index=5 / 3, vacuum_permeability=states.MU0_SI, time_step_factor=0.5,
                       bc_lo=(pg.BC_VALUE, pg.BC_COPY, pg.BC_COPY), bc_hi=(pg.BC_COPY,) * 3,
@@ -332,7 +339,7 @@ def batched_section(local, steps=500):
     batch = pg.Batch(cfgs, device=local)
     for i, b in enumerate(boxes):
         batch.set_state(i, states.ensemble_state(b))
-    planes, grid = batch.tune(3)
+    planes, grid = batch.tune(3) if tune else (None, None)
     st = torch.cuda.ExternalStream(batch.stream(), device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -348,7 +355,7 @@ def batched_section(local, steps=500):
     batch.close()
 
     plain_ms = 0.0
-    for cfg, b in zip(cfgs, boxes):
+    for cfg, b in zip(cfgs, boxes if sequential else []):
         ctx = pg.Context(cfg)
         ctx.set_state(states.ensemble_state(b))
         cs = torch.cuda.ExternalStream(ctx.stream(), device=dev)
@@ -363,7 +370,7 @@ def batched_section(local, steps=500):
             failed_steps[len(failed_steps)] = True
         ctx.close()
     batched = cells * steps / (batched_ms / 1e3)
-    plain = cells * steps / (plain_ms / 1e3)
+    plain = cells * steps / (plain_ms / 1e3) if sequential else None
     return {
         "workload": f"{len(boxes)} independent SI solar-wind boxes, edges from {{32,48,64,96,128}} "
                     f"({cells} cells), HLL, inflow -x, copy elsewhere, per-box CFL 0.5 timestep, {steps} steps",
@@ -372,7 +379,7 @@ def batched_section(local, steps=500):
         "ms": batched_ms,
         "plain_sequential": plain,
         "plain_ms": plain_ms,
-        "batched_over_plain": batched / plain,
+        "batched_over_plain": batched / plain if sequential else None,
         "tuned": {"planes_per_item": planes, "grid": grid},
         "boxes_failed": failed,
         "boxes_failed_note": "boxes whose state hit the positivity check of the reference scheme within the "
@@ -383,7 +390,7 @@ def batched_section(local, steps=500):
     }
 
 
-def adjoint_section(local, n=256, steps=200, every=20):
+def adjoint_section(local, n=256, steps=200, every=20, fd=True):
     """Discrete adjoint cost: Orszag-Tang n^2, HLLD, `steps` steps, checkpoints every `every` steps,
     J = magnetic energy in [0.4, 0.6]^2 at the last step.  Forward: the steps alone.  Gradient: the
     adjoint call, i.e. its forward run with checkpoints, the recompute of every segment and the
@@ -434,6 +441,10 @@ def adjoint_section(local, n=256, steps=200, every=20):
 
     adj_ms()
     gradient = min(adj_ms() for _ in range(3))
+
+    if not fd:
+        ctx.close()
+        return {"forward_ms": forward, "gradient_ms": gradient, "adjoint_over_forward": gradient / forward}
 
     # gradient check: 16 seeded Gaussian directions in (rho, v) at fixed p and B, central
     # differences at h = 1e-6 of the field rms and h/2 on the frozen dt schedule, Richardson-combined
@@ -700,9 +711,9 @@ def run_b200(a):
         "clocks": clocks.summary(),
     }
     if not a.no_batched:
-        line["batched"] = batched_section(local)
+        line["batched"] = batched_section(local, steps=a.batched_steps, nboxes=a.boxes, tune=not a.no_tune)
     if not a.no_adjoint:
-        line["adjoint"] = adjoint_section(local)
+        line["adjoint"] = adjoint_section(local, steps=a.adjoint_steps, fd=not a.no_fd_check)
     if not a.no_configs and world == 1:
         line["configs"] = configs_section(local, cpu=rank == 0 and not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -720,10 +731,27 @@ def run_b200(a):
     return 0
 
 
+def run_only(a):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if a.only == "batched":
+        out = batched_section(local, steps=a.batched_steps, nboxes=a.boxes, tune=not a.no_tune,
+                              sequential=False)
+    elif a.only == "adjoint":
+        out = adjoint_section(local, steps=a.adjoint_steps, fd=not a.no_fd_check)
+    else:
+        out = configs_section(local, cpu=not a.no_cpu_baseline)
+    print(json.dumps({a.only: out}), flush=True)
+    return 0
+
+
 def main():
     a = args_()
     if a.impl == "reference":
         return run_reference(a)
+    if a.only:
+        return run_only(a)
     return run_b200(a)
 
 
