@@ -339,7 +339,9 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
     batch = pg.Batch(cfgs, device=local)
     for i, b in enumerate(boxes):
         batch.set_state(i, states.ensemble_state(b))
-    planes, grid = batch.tune(3) if tune else (None, None)
+    if tune:
+        batch.tune(3)
+    tiling = batch.tiling()
     st = torch.cuda.ExternalStream(batch.stream(), device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -380,7 +382,8 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
         "plain_sequential": plain,
         "plain_ms": plain_ms,
         "batched_over_plain": batched / plain if sequential else None,
-        "tuned": {"planes_per_item": planes, "grid": grid},
+        "tuned": {"tile": f"32x{tiling[0]}", "planes_per_item": tiling[1], "grid": tiling[2],
+                  "by": "autotuner" if tune else "defaults"},
         "boxes_failed": failed,
         "boxes_failed_note": "boxes whose state hit the positivity check of the reference scheme within the "
                              "run (the CPU oracle fails box 24 at step 236, like the GPU); same count in the "

@@ -347,10 +347,18 @@ int pamhd_gpu_batch_steps(pamhd_batch* batch, int32_t nsteps, double t_end);
 
 /*
 Autotuner: times trial_steps steps of the loaded ensemble for each
-candidate number of z planes per work item and resident grid size, keeps
-the fastest and restores the state it started from.
+candidate tile shape (32 x 4 or 32 x 8 cells per block, 32 x 1 when y is
+inactive), number of z planes per work item (8, 16, 32, 64) and resident
+grid size (one wave, two waves, one block per item), keeps the fastest and
+restores the state it started from.
 */
 int pamhd_gpu_batch_tune(pamhd_batch* batch, int32_t trial_steps, int32_t* planes, int32_t* grid);
+
+/* The work split in use: tile rows (cells per block = 32 x tile_rows), z planes per item, grid. */
+int pamhd_gpu_batch_tiling(pamhd_batch* batch, int32_t* tile_rows, int32_t* planes, int32_t* grid);
+
+/* Sets the work split directly (a tiling found by an earlier pamhd_gpu_batch_tune, say). */
+int pamhd_gpu_batch_set_tiling(pamhd_batch* batch, int32_t tile_rows, int32_t planes, int32_t grid);
 
 /* Time-stamped inflow of a VALUE side of one box (see pamhd_gpu_set_inflow). */
 int pamhd_gpu_batch_set_inflow(pamhd_batch* batch, int32_t box, int32_t dim, int32_t side, int32_t count,

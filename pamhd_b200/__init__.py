@@ -486,6 +486,20 @@ class Batch:
         self._check(self.L.pamhd_gpu_batch_set_state(self.h, box, _pointers([U[k].ctypes.data for k in range(8)])),
                     "pamhd_gpu_batch_set_state")
 
+    def tiling(self):
+        """(tile rows, z planes per work item, grid) in use (pamhd_gpu_batch_tiling)."""
+        fn = self.L.pamhd_gpu_batch_tiling
+        fn.argtypes = [ctypes.c_void_p, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        t, p, g = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        self._check(fn(self.h, ctypes.byref(t), ctypes.byref(p), ctypes.byref(g)), "pamhd_gpu_batch_tiling")
+        return t.value, p.value, g.value
+
+    def set_tiling(self, tile_rows: int, planes: int, grid: int):
+        """Sets the work split (pamhd_gpu_batch_set_tiling)."""
+        fn = self.L.pamhd_gpu_batch_set_tiling
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+        self._check(fn(self.h, tile_rows, planes, grid), "pamhd_gpu_batch_set_tiling")
+
     def set_inflow(self, box: int, dim: int, side: int, times, states):
         """Time-stamped inflow of a VALUE side of one box (pamhd_gpu_batch_set_inflow)."""
         fn = self.L.pamhd_gpu_batch_set_inflow

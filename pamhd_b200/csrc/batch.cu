@@ -56,6 +56,7 @@ struct pamhd_batch {
 	int nitems = 0;
 	int grid = 0;
 	int planes_per_item = 32;
+	int ty = 1;                      // tile rows of the work items (autotuned when y is active)
 	bool needs_boundary = false;
 	int largest_plane = 0;
 	double* staging = nullptr;
@@ -86,6 +87,13 @@ long long cells_of(const pamhd_cfg& c)
 	return (long long)c.n[0] * c.n[1] * c.n[2];
 }
 
+// the tile shapes the autotuner chooses among: 32 x 4 and 32 x 8 (32 x 1 when y is inactive)
+std::vector<int> tile_choices(const pamhd_batch& b)
+{
+	if (not b.yact) return {1};
+	return {step_tile_rows(), 8};
+}
+
 // ghost states of a box's VALUE sides at time t: configured values or time-stamped inflow
 void box_values_at(const pamhd_batch& b, const int box, const double t, double lo[3][8], double hi[3][8])
 {
@@ -112,7 +120,7 @@ void box_values_at(const pamhd_batch& b, const int box, const double t, double l
 int build_work(pamhd_batch& b, const int planes)
 {
 	b.planes_per_item = planes;
-	const int ty = b.yact ? step_tile_rows() : 1;
+	const int ty = b.ty;
 	std::vector<int> order(b.nboxes);
 	std::iota(order.begin(), order.end(), 0);
 	std::stable_sort(order.begin(), order.end(),
@@ -199,7 +207,7 @@ int issue_step(pamhd_batch& b)
 		PAMHD_TRY(launch_batch_boundary_speeds(b.d_params[b.cur], b.nboxes, b.largest_plane, phase, b.solver,
 		                                       b.stream));
 	}
-	PAMHD_TRY(launch_batch_step(b.d_params[b.cur], b.d_items, b.nitems, phase, b.grid, b.solver, b.yact, b.stream));
+	PAMHD_TRY(launch_batch_step(b.d_params[b.cur], b.d_items, b.nitems, phase, b.grid, b.solver, b.ty, b.stream));
 	b.cur ^= 1;
 	b.steps++;
 	return PAMHD_OK;
@@ -311,9 +319,12 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 		or cudaMemset(b->dt_hist, 0, size_t(b->hist_len) * nboxes * sizeof(double)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
-	if (prepare_batch_kernels(b->solver, b->yact) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+	b->ty = b->yact ? step_tile_rows() : 1;
+	for (const int ty: tile_choices(*b)) {
+		if (prepare_batch_kernels(b->solver, ty) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+	}
 	int per_sm = 0;
-	if (batch_blocks_per_sm(b->solver, b->yact, &per_sm) != PAMHD_OK or per_sm < 1) return fail(PAMHD_ERR_CUDA);
+	if (batch_blocks_per_sm(b->solver, b->ty, &per_sm) != PAMHD_OK or per_sm < 1) return fail(PAMHD_ERR_CUDA);
 	int sms = 0;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
 	if (build_work(*b, 32) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
@@ -465,18 +476,21 @@ int pamhd_gpu_batch_tune(pamhd_batch* b, const int32_t trial_steps, int32_t* pla
 	PAMHD_TRY(check(cudaMalloc(&backup, size_t(b->total) * sizeof(double))));
 	int rc = check(cudaMemcpyAsync(backup, b->state[b->cur], size_t(b->total) * sizeof(double),
 	                               cudaMemcpyDeviceToDevice, b->stream));
-	int per_sm = 0, sms = 0;
-	if (rc == PAMHD_OK) rc = batch_blocks_per_sm(b->solver, b->yact, &per_sm);
+	int sms = 0;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
 	float best = 3.0e38f;
-	int best_planes = b->planes_per_item, best_grid = b->grid;
+	int best_planes = b->planes_per_item, best_grid = b->grid, best_ty = b->ty;
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	cudaEventCreate(&e0);
 	cudaEventCreate(&e1);
 	if (rc == PAMHD_OK) rc = set_control(*b, -1.0, 1.0e300);
+	for (const int ty: tile_choices(*b))
 	for (const int planes: {8, 16, 32, 64}) {
 		if (rc != PAMHD_OK) break;
-		rc = build_work(*b, planes);
+		b->ty = ty;
+		int per_sm = 0;
+		rc = batch_blocks_per_sm(b->solver, ty, &per_sm);
+		if (rc == PAMHD_OK) rc = build_work(*b, planes);
 		for (const int waves: {1, 2, 0}) {
 			if (rc != PAMHD_OK) break;
 			b->grid = waves == 0 ? b->nitems : std::min(b->nitems, std::max(1, waves * sms * per_sm));
@@ -493,6 +507,7 @@ int pamhd_gpu_batch_tune(pamhd_batch* b, const int32_t trial_steps, int32_t* pla
 				best = ms;
 				best_planes = planes;
 				best_grid = b->grid;
+				best_ty = ty;
 			}
 			// the trial steps advanced the state: go back to the starting buffer parity
 			if (rc == PAMHD_OK and b->cur != 0) {
@@ -503,6 +518,7 @@ int pamhd_gpu_batch_tune(pamhd_batch* b, const int32_t trial_steps, int32_t* pla
 			if (rc == PAMHD_OK) rc = reset_run_state(*b);
 		}
 	}
+	b->ty = best_ty;
 	if (rc == PAMHD_OK) rc = build_work(*b, best_planes);
 	b->grid = best_grid;
 	if (rc == PAMHD_OK) {
@@ -516,6 +532,28 @@ int pamhd_gpu_batch_tune(pamhd_batch* b, const int32_t trial_steps, int32_t* pla
 	if (planes_chosen != nullptr) *planes_chosen = best_planes;
 	if (grid_chosen != nullptr) *grid_chosen = best_grid;
 	return rc;
+}
+
+int pamhd_gpu_batch_set_tiling(pamhd_batch* b, const int32_t tile_rows, const int32_t planes, const int32_t grid)
+{
+	if (b == nullptr or planes < 1 or grid < 1) return PAMHD_ERR_ARGUMENT;
+	const std::vector<int> choices = tile_choices(*b);
+	if (std::find(choices.begin(), choices.end(), int(tile_rows)) == choices.end()) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(b->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+	b->ty = tile_rows;
+	PAMHD_TRY(build_work(*b, planes));
+	b->grid = std::min(b->nitems, int(grid));
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_batch_tiling(pamhd_batch* b, int32_t* tile_rows, int32_t* planes, int32_t* grid)
+{
+	if (b == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (tile_rows != nullptr) *tile_rows = b->ty;
+	if (planes != nullptr) *planes = b->planes_per_item;
+	if (grid != nullptr) *grid = b->grid;
+	return PAMHD_OK;
 }
 
 int pamhd_gpu_batch_sync(pamhd_batch* b)

@@ -113,10 +113,10 @@ int launch_totals(const double* state, const Layout& L, double volume, double* p
                   cudaStream_t stream);
 int step_smem_bytes(int ty);
 int step_tile_rows();
-int prepare_batch_kernels(int solver, bool y_active);
-int batch_blocks_per_sm(int solver, bool y_active, int* blocks);
+int prepare_batch_kernels(int solver, int tile_rows);
+int batch_blocks_per_sm(int solver, int tile_rows, int* blocks);
 int launch_batch_step(const Step_Params* boxes, const int4* items, int nitems, int phase, int grid, int solver,
-                      bool y_active, cudaStream_t stream);
+                      int tile_rows, cudaStream_t stream);
 int launch_batch_boundary_speeds(const Step_Params* boxes, int nboxes, int largest, int phase, int solver,
                                  cudaStream_t stream);
 

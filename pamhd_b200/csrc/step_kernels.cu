@@ -835,40 +835,71 @@ int launch_step(const Step_Params& P, const int solver, cudaStream_t stream)
 	}
 }
 
+// tile rows the batched step is built for (the autotuner picks one): 1 when y is inactive
+constexpr int TY_WIDE = 8;
+constexpr int MINB_WIDE = 2;   // resident blocks per SM of the 32 x 8 tile
+
+template <int TY> struct Batch_Build { static constexpr int MINB_OF = MINB; };
+template <> struct Batch_Build<TY_WIDE> { static constexpr int MINB_OF = MINB_WIDE; };
+
 template <int SOLVER, int TY>
 static int prepare_batch_t()
 {
-	const cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<SOLVER, TY, MINB>,
+	const cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
 	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tile<TY>::BYTES));
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
-int prepare_batch_kernels(const int solver, const bool y)
+template <int SOLVER>
+static int prepare_batch_s(const int ty)
 {
-	switch (solver) {
-	case PAMHD_RUSANOV: return y ? prepare_batch_t<PAMHD_RUSANOV, TY_3D>() : prepare_batch_t<PAMHD_RUSANOV, 1>();
-	case PAMHD_HLL_ATHENA: return y ? prepare_batch_t<PAMHD_HLL_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_HLL_ATHENA, 1>();
-	case PAMHD_HLLD_ATHENA: return y ? prepare_batch_t<PAMHD_HLLD_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_HLLD_ATHENA, 1>();
-	case PAMHD_ROE_ATHENA: return y ? prepare_batch_t<PAMHD_ROE_ATHENA, TY_3D>() : prepare_batch_t<PAMHD_ROE_ATHENA, 1>();
+	switch (ty) {
+	case 1: return prepare_batch_t<SOLVER, 1>();
+	case TY_3D: return prepare_batch_t<SOLVER, TY_3D>();
+	case TY_WIDE: return prepare_batch_t<SOLVER, TY_WIDE>();
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 }
 
-int batch_blocks_per_sm(const int solver, const bool y, int* blocks)
+int prepare_batch_kernels(const int solver, const int ty)
 {
-	cudaError_t e = cudaErrorInvalidValue;
-	#define PAMHD_OCC(S) \
-		e = y ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<S, TY_3D, MINB>, \
-		                                                    TX * TY_3D, Tile<TY_3D>::BYTES) \
-		      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<S, 1, MINB>, TX, Tile<1>::BYTES)
 	switch (solver) {
-	case PAMHD_RUSANOV: PAMHD_OCC(PAMHD_RUSANOV); break;
-	case PAMHD_HLL_ATHENA: PAMHD_OCC(PAMHD_HLL_ATHENA); break;
-	case PAMHD_HLLD_ATHENA: PAMHD_OCC(PAMHD_HLLD_ATHENA); break;
-	case PAMHD_ROE_ATHENA: PAMHD_OCC(PAMHD_ROE_ATHENA); break;
+	case PAMHD_RUSANOV: return prepare_batch_s<PAMHD_RUSANOV>(ty);
+	case PAMHD_HLL_ATHENA: return prepare_batch_s<PAMHD_HLL_ATHENA>(ty);
+	case PAMHD_HLLD_ATHENA: return prepare_batch_s<PAMHD_HLLD_ATHENA>(ty);
+	case PAMHD_ROE_ATHENA: return prepare_batch_s<PAMHD_ROE_ATHENA>(ty);
 	default: return PAMHD_ERR_ARGUMENT;
 	}
-	#undef PAMHD_OCC
+}
+
+template <int SOLVER, int TY>
+static cudaError_t occupancy_t(int* blocks)
+{
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
+	                                                     TX * TY, Tile<TY>::BYTES);
+}
+
+template <int SOLVER>
+static cudaError_t occupancy_s(const int ty, int* blocks)
+{
+	switch (ty) {
+	case 1: return occupancy_t<SOLVER, 1>(blocks);
+	case TY_3D: return occupancy_t<SOLVER, TY_3D>(blocks);
+	case TY_WIDE: return occupancy_t<SOLVER, TY_WIDE>(blocks);
+	default: return cudaErrorInvalidValue;
+	}
+}
+
+int batch_blocks_per_sm(const int solver, const int ty, int* blocks)
+{
+	cudaError_t e = cudaErrorInvalidValue;
+	switch (solver) {
+	case PAMHD_RUSANOV: e = occupancy_s<PAMHD_RUSANOV>(ty, blocks); break;
+	case PAMHD_HLL_ATHENA: e = occupancy_s<PAMHD_HLL_ATHENA>(ty, blocks); break;
+	case PAMHD_HLLD_ATHENA: e = occupancy_s<PAMHD_HLLD_ATHENA>(ty, blocks); break;
+	case PAMHD_ROE_ATHENA: e = occupancy_s<PAMHD_ROE_ATHENA>(ty, blocks); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -876,23 +907,35 @@ template <int SOLVER, int TY>
 static void launch_batch_t(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
                            const int grid, cudaStream_t stream)
 {
-	batch_step_kernel<SOLVER, TY, MINB><<<grid, dim3(TX, TY), Tile<TY>::BYTES, stream>>>(boxes, items, nitems, phase);
+	batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF><<<grid, dim3(TX, TY), Tile<TY>::BYTES, stream>>>(
+		boxes, items, nitems, phase);
+}
+
+template <int SOLVER>
+static int launch_batch_s(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
+                          const int grid, const int ty, cudaStream_t stream)
+{
+	switch (ty) {
+	case 1: launch_batch_t<SOLVER, 1>(boxes, items, nitems, phase, grid, stream); break;
+	case TY_3D: launch_batch_t<SOLVER, TY_3D>(boxes, items, nitems, phase, grid, stream); break;
+	case TY_WIDE: launch_batch_t<SOLVER, TY_WIDE>(boxes, items, nitems, phase, grid, stream); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return PAMHD_OK;
 }
 
 int launch_batch_step(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
-                      const int grid, const int solver, const bool y, cudaStream_t stream)
+                      const int grid, const int solver, const int ty, cudaStream_t stream)
 {
+	int rc = PAMHD_ERR_ARGUMENT;
 	switch (solver) {
-	case PAMHD_RUSANOV: y ? launch_batch_t<PAMHD_RUSANOV, TY_3D>(boxes, items, nitems, phase, grid, stream)
-	                      : launch_batch_t<PAMHD_RUSANOV, 1>(boxes, items, nitems, phase, grid, stream); break;
-	case PAMHD_HLL_ATHENA: y ? launch_batch_t<PAMHD_HLL_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
-	                         : launch_batch_t<PAMHD_HLL_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
-	case PAMHD_HLLD_ATHENA: y ? launch_batch_t<PAMHD_HLLD_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
-	                          : launch_batch_t<PAMHD_HLLD_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
-	case PAMHD_ROE_ATHENA: y ? launch_batch_t<PAMHD_ROE_ATHENA, TY_3D>(boxes, items, nitems, phase, grid, stream)
-	                         : launch_batch_t<PAMHD_ROE_ATHENA, 1>(boxes, items, nitems, phase, grid, stream); break;
+	case PAMHD_RUSANOV: rc = launch_batch_s<PAMHD_RUSANOV>(boxes, items, nitems, phase, grid, ty, stream); break;
+	case PAMHD_HLL_ATHENA: rc = launch_batch_s<PAMHD_HLL_ATHENA>(boxes, items, nitems, phase, grid, ty, stream); break;
+	case PAMHD_HLLD_ATHENA: rc = launch_batch_s<PAMHD_HLLD_ATHENA>(boxes, items, nitems, phase, grid, ty, stream); break;
+	case PAMHD_ROE_ATHENA: rc = launch_batch_s<PAMHD_ROE_ATHENA>(boxes, items, nitems, phase, grid, ty, stream); break;
 	default: return PAMHD_ERR_ARGUMENT;
 	}
+	if (rc != PAMHD_OK) return rc;
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 

@@ -105,6 +105,27 @@ def test_tuner_restores_state():
         np.testing.assert_array_equal(tuned.get_state(i), plain.get_state(i))
 
 
+@pytest.mark.parametrize("tile_rows", [4, 8])
+@pytest.mark.parametrize("planes", [8, 64])
+def test_every_tiling_gives_the_same_bits(tile_rows, planes):
+    """The tile shapes and work splits the autotuner chooses among compute every face with the
+    same arithmetic: the same bits as each box in its own context."""
+    cfgs, U0s = small_ensemble()
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.set_tiling(tile_rows, planes, 1 << 20)
+    assert batch.tiling()[:2] == (tile_rows, planes)
+    batch.steps(9)
+    batch.sync()
+    for i, (cfg, U) in enumerate(zip(cfgs, U0s)):
+        ctx = pg.Context(cfg)
+        ctx.set_state(U)
+        ctx.steps(9, 1e300)
+        ctx.sync()
+        np.testing.assert_array_equal(batch.get_state(i), ctx.get_state())
+
+
 def test_batch_reports_failing_box():
     cfgs, U0s = small_ensemble()
     U0s[2] = U0s[2].copy()
