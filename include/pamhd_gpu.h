@@ -101,7 +101,9 @@ factor (mhd/options.hpp:119-132, "mhd-time-step-factor"), the adiabatic
 index and vacuum permeability (simulation_options.hpp:59-60), the uniform
 cell size (grid/options.hpp) and the boundary kinds.
 A dimension with n == 1 is inactive: it has no faces and does not enter
-the timestep.
+the timestep.  Any set of active dimensions is accepted (grids that are
+not x, x-y or x-y-z run with their axes relabelled internally; every array,
+side, state, status and gradient of this ABI stays in the caller's axes).
 */
 typedef struct pamhd_cfg {
 	int32_t n[3];                /* interior cells in x, y, z */

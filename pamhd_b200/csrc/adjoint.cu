@@ -363,11 +363,18 @@ int pamhd_gpu_steps_dt(pamhd_ctx* x, const int32_t nsteps, const double* dts)
 	return PAMHD_OK;
 }
 
-int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, const double* const seed[8],
-                      double* const grad[8], double* grad_value, const double* dt_in, double* dt_out)
+int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, const double* const user_seed[8],
+                      double* const user_grad[8], double* grad_value, const double* dt_in, double* dt_out)
 {
-	if (x == nullptr or nsteps < 1 or every < 1 or seed == nullptr or grad == nullptr) return PAMHD_ERR_ARGUMENT;
-	for (int v = 0; v < 8; v++) if (seed[v] == nullptr or grad[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x == nullptr or nsteps < 1 or every < 1 or user_seed == nullptr or user_grad == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (user_seed[v] == nullptr or user_grad[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	// the caller's arrays in the internal component order (see Axis_Map)
+	const double* seed[8];
+	double* grad[8];
+	for (int v = 0; v < 8; v++) {
+		seed[v] = user_seed[x->map.user_var(v)];
+		grad[v] = user_grad[x->map.user_var(v)];
+	}
 	if (x->cfg.solver == PAMHD_ROE_ATHENA) return PAMHD_ERR_ARGUMENT;  // no Roe adjoint
 	if (x->cfg.bc_lo[2] == PAMHD_BC_EXTERNAL or x->cfg.bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
 	// the inflow-state gradient is of one constant state per side
@@ -525,11 +532,23 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 		PAMHD_TRY(check(cudaMemcpyAsync(grad[v], x->staging, cells * sizeof(double), cudaMemcpyDeviceToHost,
 		                                x->stream)));
 	}
+	double internal_value[48];
 	if (grad_value != nullptr) {
-		PAMHD_TRY(check(cudaMemcpyAsync(grad_value, W.acc.p, 48 * sizeof(double), cudaMemcpyDeviceToHost,
+		PAMHD_TRY(check(cudaMemcpyAsync(internal_value, W.acc.p, 48 * sizeof(double), cudaMemcpyDeviceToHost,
 		                                x->stream)));
 	}
-	return check(cudaStreamSynchronize(x->stream));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	if (grad_value != nullptr) {
+		// [dimension][side][variable] in the caller's axes and component order
+		for (int d = 0; d < 3; d++) {
+			for (int side = 0; side < 2; side++) {
+				for (int v = 0; v < 8; v++) {
+					grad_value[(2 * x->map.perm[d] + side) * 8 + x->map.user_var(v)] = internal_value[(2 * d + side) * 8 + v];
+				}
+			}
+		}
+	}
+	return PAMHD_OK;
 }
 
 } // extern "C"

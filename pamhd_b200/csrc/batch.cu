@@ -64,6 +64,7 @@ struct pamhd_batch {
 	int cur = 0;
 	bool loaded = false;
 	cudaGraphExec_t graph = nullptr;
+	Axis_Map map{{0, 1, 2}};        // the boxes' axes as the kernels see them
 	// time-stamped inflow of VALUE sides, per box and side (index 6 box + 2 dimension + side)
 	std::vector<Inflow_Table> inflow;
 	Inflow_Table* d_inflow = nullptr;   // the same tables in device memory
@@ -273,16 +274,25 @@ int box_ok(const pamhd_batch* b, const int box)
 
 extern "C" {
 
-int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pamhd_cfg* cfgs, pamhd_batch** out)
+int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pamhd_cfg* user_cfgs, pamhd_batch** out)
 {
-	if (out == nullptr or cfgs == nullptr or nboxes < 1) return PAMHD_ERR_ARGUMENT;
+	if (out == nullptr or user_cfgs == nullptr or nboxes < 1) return PAMHD_ERR_ARGUMENT;
 	*out = nullptr;
+	// every box with the same active dimensions, relabelled the same way (see Axis_Map)
+	const Axis_Map map = axis_map(user_cfgs[0]);
+	std::vector<pamhd_cfg> internal(nboxes);
 	for (int i = 0; i < nboxes; i++) {
-		PAMHD_TRY(validate(cfgs[i]));
-		if (cfgs[i].bc_lo[2] == PAMHD_BC_EXTERNAL or cfgs[i].bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
-		if (cfgs[i].solver != cfgs[0].solver) return PAMHD_ERR_ARGUMENT;
-		if ((cfgs[i].n[1] > 1) != (cfgs[0].n[1] > 1)) return PAMHD_ERR_ARGUMENT;
+		for (int d = 0; d < 3; d++) {
+			if ((user_cfgs[i].n[d] > 1) != (user_cfgs[0].n[d] > 1)) return PAMHD_ERR_ARGUMENT;
+			if (user_cfgs[i].bc_lo[d] == PAMHD_BC_EXTERNAL or user_cfgs[i].bc_hi[d] == PAMHD_BC_EXTERNAL) {
+				return PAMHD_ERR_ARGUMENT;
+			}
+		}
+		internal[i] = relabelled(user_cfgs[i], map);
+		PAMHD_TRY(validate(internal[i]));
+		if (internal[i].solver != internal[0].solver) return PAMHD_ERR_ARGUMENT;
 	}
+	const pamhd_cfg* cfgs = internal.data();
 	pamhd_batch* b = new (std::nothrow) pamhd_batch;
 	if (b == nullptr) return PAMHD_ERR_ARGUMENT;
 	auto fail = [&](const int rc) {
@@ -290,6 +300,7 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 		return rc;
 	};
 	b->device = device;
+	b->map = map;
 	b->nboxes = nboxes;
 	b->solver = cfgs[0].solver;
 	b->yact = cfgs[0].n[1] > 1;
@@ -358,11 +369,13 @@ int pamhd_gpu_batch_destroy(pamhd_batch* b)
 	return PAMHD_OK;
 }
 
-int pamhd_gpu_batch_set_state(pamhd_batch* b, const int32_t box, const double* const soa[8])
+int pamhd_gpu_batch_set_state(pamhd_batch* b, const int32_t box, const double* const user[8])
 {
 	PAMHD_TRY(box_ok(b, box));
-	if (soa == nullptr) return PAMHD_ERR_ARGUMENT;
-	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (user == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (user[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	const double* soa[8];
+	for (int v = 0; v < 8; v++) soa[v] = user[b->map.user_var(v)];
 	PAMHD_TRY(check(cudaSetDevice(b->device)));
 	const Layout& L = b->L[box];
 	const size_t bytes = size_t(cells_of(b->cfg[box])) * sizeof(double);
@@ -382,12 +395,20 @@ int pamhd_gpu_batch_set_state(pamhd_batch* b, const int32_t box, const double* c
 	return reset_run_state(*b);
 }
 
-int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t dim, const int32_t side,
-                               const int32_t count, const double* times, const double* states)
+int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t user_dim, const int32_t side,
+                               const int32_t count, const double* times, const double* user_states)
 {
 	PAMHD_TRY(box_ok(b, box));
-	if (dim < 0 or dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
-	if ((count > 0 and times == nullptr) or states == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (user_dim < 0 or user_dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
+	if ((count > 0 and times == nullptr) or user_states == nullptr) return PAMHD_ERR_ARGUMENT;
+	// the internal axis and component order
+	int dim = 0;
+	while (b->map.perm[dim] != user_dim) dim++;
+	std::vector<double> internal_states(8 * (size_t(count) + 1));
+	for (size_t i = 0; i <= size_t(count); i++) {
+		for (int v = 0; v < 8; v++) internal_states[8 * i + v] = user_states[8 * i + b->map.user_var(v)];
+	}
+	const double* states = internal_states.data();
 	const pamhd_cfg& c = b->cfg[box];
 	if ((side == 0 ? c.bc_lo[dim] : c.bc_hi[dim]) != PAMHD_BC_VALUE or c.n[dim] < 2) return PAMHD_ERR_ARGUMENT;
 	for (int i = 0; i < count; i++) {
@@ -440,11 +461,13 @@ int pamhd_gpu_batch_set_inflow(pamhd_batch* b, const int32_t box, const int32_t 
 	return PAMHD_OK;
 }
 
-int pamhd_gpu_batch_get_state(pamhd_batch* b, const int32_t box, double* const soa[8])
+int pamhd_gpu_batch_get_state(pamhd_batch* b, const int32_t box, double* const user[8])
 {
 	PAMHD_TRY(box_ok(b, box));
-	if (soa == nullptr) return PAMHD_ERR_ARGUMENT;
-	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (user == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (user[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	double* soa[8];
+	for (int v = 0; v < 8; v++) soa[v] = user[b->map.user_var(v)];
 	PAMHD_TRY(check(cudaSetDevice(b->device)));
 	const Layout& L = b->L[box];
 	const size_t bytes = size_t(cells_of(b->cfg[box])) * sizeof(double);
@@ -627,12 +650,11 @@ int pamhd_gpu_batch_status(pamhd_batch* b, const int32_t box, uint32_t* flags, i
 		c[1] = int32_t(lin % ny) - P.ext[1];
 		c[2] = int32_t(lin / ny) - P.ext[2];
 	}
+	// in the caller's axes
 	if (cell != nullptr) {
-		cell[0] = c[0];
-		cell[1] = c[1];
-		cell[2] = c[2];
+		for (int a = 0; a < 3; a++) cell[b->map.perm[a]] = c[a];
 	}
-	if (dir != nullptr) *dir = d;
+	if (dir != nullptr) *dir = d > 0 ? b->map.perm[d - 1] + 1 : 0;
 	return PAMHD_OK;
 }
 

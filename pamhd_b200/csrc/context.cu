@@ -180,12 +180,21 @@ int pamhd_gpu_create(const pamhd_cfg* cfg, pamhd_ctx** out)
 {
 	if (cfg == nullptr or out == nullptr) return PAMHD_ERR_ARGUMENT;
 	*out = nullptr;
-	PAMHD_TRY(validate(*cfg));
+	const Axis_Map map = axis_map(*cfg);
+	if (not map.identity()) {
+		// slab cuts are z sides of grids with the usual axes
+		for (int d = 0; d < 3; d++) {
+			if (cfg->bc_lo[d] == PAMHD_BC_EXTERNAL or cfg->bc_hi[d] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
+		}
+	}
+	const pamhd_cfg internal = relabelled(*cfg, map);
+	PAMHD_TRY(validate(internal));
 	pamhd_ctx* x = new (std::nothrow) pamhd_ctx;
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
-	x->cfg = *cfg;
+	x->cfg = internal;
+	x->map = map;
 	x->device = cfg->device;
-	x->L = make_layout(*cfg);
+	x->L = make_layout(internal);
 	auto fail = [&](const int rc) {
 		pamhd_gpu_destroy(x);
 		return rc;
@@ -245,10 +254,12 @@ int pamhd_gpu_destroy(pamhd_ctx* x)
 	return PAMHD_OK;
 }
 
-static int set_state_impl(pamhd_ctx* x, const double* const soa[8], const cudaMemcpyKind kind)
+static int set_state_impl(pamhd_ctx* x, const double* const user[8], const cudaMemcpyKind kind)
 {
-	if (x == nullptr or soa == nullptr) return PAMHD_ERR_ARGUMENT;
-	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x == nullptr or user == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (user[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	const double* soa[8];
+	for (int v = 0; v < 8; v++) soa[v] = user[x->map.user_var(v)];
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const size_t bytes = size_t(x->L.n[0]) * x->L.n[1] * x->L.n[2] * sizeof(double);
 	for (int v = 0; v < 8; v++) {
@@ -261,10 +272,12 @@ static int set_state_impl(pamhd_ctx* x, const double* const soa[8], const cudaMe
 	return check(cudaStreamSynchronize(x->stream));
 }
 
-static int get_state_impl(pamhd_ctx* x, double* const soa[8], const cudaMemcpyKind kind)
+static int get_state_impl(pamhd_ctx* x, double* const user[8], const cudaMemcpyKind kind)
 {
-	if (x == nullptr or soa == nullptr) return PAMHD_ERR_ARGUMENT;
-	for (int v = 0; v < 8; v++) if (soa[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x == nullptr or user == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (user[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	double* soa[8];
+	for (int v = 0; v < 8; v++) soa[v] = user[x->map.user_var(v)];
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const size_t bytes = size_t(x->L.n[0]) * x->L.n[1] * x->L.n[2] * sizeof(double);
 	for (int v = 0; v < 8; v++) {
@@ -336,11 +349,21 @@ int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
 	return PAMHD_OK;
 }
 
-int pamhd_gpu_set_inflow(pamhd_ctx* x, const int32_t dim, const int32_t side, const int32_t count,
-                         const double* times, const double* states)
+int pamhd_gpu_set_inflow(pamhd_ctx* x, const int32_t user_dim, const int32_t side, const int32_t count,
+                         const double* times, const double* user_states)
 {
-	if (x == nullptr or dim < 0 or dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
-	if ((count > 0 and times == nullptr) or states == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x == nullptr or user_dim < 0 or user_dim > 2 or (side != 0 and side != 1) or count < 0) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	if ((count > 0 and times == nullptr) or user_states == nullptr) return PAMHD_ERR_ARGUMENT;
+	// the internal axis and component order
+	int dim = 0;
+	while (x->map.perm[dim] != user_dim) dim++;
+	std::vector<double> internal(8 * (size_t(count) + 1));
+	for (size_t i = 0; i <= size_t(count); i++) {
+		for (int v = 0; v < 8; v++) internal[8 * i + v] = user_states[8 * i + x->map.user_var(v)];
+	}
+	const double* states = internal.data();
 	if ((side == 0 ? x->cfg.bc_lo[dim] : x->cfg.bc_hi[dim]) != PAMHD_BC_VALUE or x->cfg.n[dim] < 2) {
 		return PAMHD_ERR_ARGUMENT;
 	}
@@ -477,12 +500,11 @@ int pamhd_gpu_status(pamhd_ctx* x, uint32_t* flags, int32_t cell[3], int32_t* di
 		c[1] = int32_t(lin % ny) - P.ext[1];
 		c[2] = int32_t(lin / ny) - P.ext[2];
 	}
+	// in the caller's axes
 	if (cell != nullptr) {
-		cell[0] = c[0];
-		cell[1] = c[1];
-		cell[2] = c[2];
+		for (int a = 0; a < 3; a++) cell[x->map.perm[a]] = c[a];
 	}
-	if (dir != nullptr) *dir = d;
+	if (dir != nullptr) *dir = d > 0 ? x->map.perm[d - 1] + 1 : 0;
 	return PAMHD_OK;
 }
 
@@ -504,7 +526,7 @@ int pamhd_gpu_totals(pamhd_ctx* x, double totals[8])
 			comp = (t - sum) - y;
 			sum = t;
 		}
-		totals[v] = sum * volume;
+		totals[x->map.user_var(v)] = sum * volume;
 	}
 	return PAMHD_OK;
 }

@@ -17,7 +17,8 @@ using namespace pamhd_b200;
 struct Adjoint_Work;
 
 struct pamhd_ctx {
-	pamhd_cfg cfg;
+	pamhd_cfg cfg;        // the internal configuration (axes relabelled, see Axis_Map)
+	Axis_Map map{{0, 1, 2}};
 	int device = 0;
 	cudaStream_t stream = nullptr;
 	Layout L;

@@ -35,13 +35,66 @@ inline int validate(const pamhd_cfg& c)
 			return PAMHD_ERR_ARGUMENT;
 		}
 	}
-	// active dimensions must be x, x-y or x-y-z
+	// active dimensions must be x, x-y or x-y-z (other sets are relabelled first, see axis_map)
 	if (c.n[0] < 2) return PAMHD_ERR_ARGUMENT;
 	if (c.n[1] < 2 and c.n[2] > 1) return PAMHD_ERR_ARGUMENT;
 	if (not (c.adiabatic_index > 1.0) or not (c.vacuum_permeability > 0.0) or not (c.time_step_factor > 0.0)) {
 		return PAMHD_ERR_ARGUMENT;
 	}
 	return PAMHD_OK;
+}
+
+/*
+Axis relabelling.  The step kernels tile along x and march along z, so they
+need the active dimensions to be x, x-y or x-y-z.  A grid whose active
+dimensions are another set (y, z, y-z or x-z: the reference's 2-D tests
+often use a y-z plane) runs with its axes relabelled: internal axis a is
+the caller's axis perm[a], vector components (momentum, field) follow
+their axes.  With the inactive axes one cell long, the x-fastest order of
+the caller's cells is also the internal order, so state arrays only swap
+which array holds which component.  y, z and y-z use a rotation of the
+axes, whose face frames equal the caller's (the reference's
+get_rotated_vector), so every face sees the same numbers; x-z swaps y and
+z, a reflection, under which ideal MHD is invariant and the faces see
+their two tangential components in the other order.
+*/
+struct Axis_Map {
+	int perm[3];
+	bool identity() const { return perm[0] == 0 and perm[1] == 1 and perm[2] == 2; }
+	// the caller's variable held in internal variable v
+	int user_var(const int v) const
+	{
+		if (v >= 1 and v <= 3) return 1 + perm[v - 1];
+		if (v >= 5 and v <= 7) return 5 + perm[v - 5];
+		return v;
+	}
+};
+
+inline Axis_Map axis_map(const pamhd_cfg& c)
+{
+	const bool ax = c.n[0] > 1, ay = c.n[1] > 1, az = c.n[2] > 1;
+	if (not ax and ay) return Axis_Map{{1, 2, 0}};             // y, y-z
+	if (not ax and not ay and az) return Axis_Map{{2, 0, 1}};  // z
+	if (ax and not ay and az) return Axis_Map{{0, 2, 1}};      // x-z
+	return Axis_Map{{0, 1, 2}};
+}
+
+// the internal configuration of a caller's configuration
+inline pamhd_cfg relabelled(const pamhd_cfg& c, const Axis_Map& m)
+{
+	pamhd_cfg r = c;
+	for (int a = 0; a < 3; a++) {
+		const int u = m.perm[a];
+		r.n[a] = c.n[u];
+		r.cell_length[a] = c.cell_length[u];
+		r.bc_lo[a] = c.bc_lo[u];
+		r.bc_hi[a] = c.bc_hi[u];
+		for (int v = 0; v < 8; v++) {
+			r.value_lo[a][v] = c.value_lo[u][m.user_var(v)];
+			r.value_hi[a][v] = c.value_hi[u][m.user_var(v)];
+		}
+	}
+	return r;
 }
 
 inline Layout make_layout(const pamhd_cfg& c)

@@ -55,8 +55,7 @@ def test_cfg_layout_matches_oracle():
 @pytest.mark.parametrize("change", [
     dict(solver=1),                       # rusanov_staggered aborts in the reference dispatcher
     dict(solver=9),
-    dict(n=(1, 8, 8)),                    # x must be active
-    dict(n=(8, 1, 8)),                    # active dimensions are x, x-y or x-y-z
+    dict(n=(1, 1, 1)),                    # no active dimension
     dict(cell_length=(0.0, 1.0, 1.0)),
     dict(adiabatic_index=1.0),
     dict(vacuum_permeability=0.0),
@@ -76,3 +75,15 @@ def test_null_arguments_rejected(lib):
     assert lib.pamhd_gpu_create(None, None) == pg.ERR_ARGUMENT
     assert lib.pamhd_gpu_step(None, 0.0, None) == pg.ERR_ARGUMENT
     assert lib.pamhd_gpu_destroy(None) == pg.OK
+
+
+@pytest.mark.parametrize("n", [(1, 8, 8), (8, 1, 8), (1, 8, 1), (1, 1, 8)])
+def test_any_active_dimensions_pass_the_checks(lib, n):
+    """Grids whose active dimensions are not x, x-y or x-y-z are relabelled, not rejected (without
+    a GPU the call then fails at its first CUDA call, not at the argument checks)."""
+    cfg = pg.Config(n=n, solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1)).to_c()
+    h = ctypes.c_void_p()
+    rc = lib.pamhd_gpu_create(ctypes.byref(cfg), ctypes.byref(h))
+    assert rc != pg.ERR_ARGUMENT
+    if h.value:
+        lib.pamhd_gpu_destroy(h)
