@@ -2,7 +2,8 @@
 C entry points of the CPU oracle, shared by the two oracle libraries:
   oracle/_build/liboracle.so   - the restated solvers of mhd_oracle.hpp
   oracle/_ref/libpamhd_ref.so  - the reference's own solver headers
-Both drive them with the same Mode C grid restatement (mode_c.hpp).
+Both drive them with the same grid restatements: Mode C (mode_c.hpp) and
+the staggered-field step (mode_s.hpp).
 
 TEST INFRASTRUCTURE - see mhd_oracle.hpp for who may use this.
 
@@ -13,11 +14,12 @@ ORACLE_FLUX (the solver dispatch functor type).
 #include <cstring>
 #include <vector>
 
-#include "mode_c.hpp"
+#include "mode_s.hpp"
 
 namespace {
 
 using Grid = oracle::Mode_C_Grid<ORACLE_FLUX>;
+using SGrid = oracle::Mode_S_Grid<ORACLE_FLUX>;
 
 thread_local std::string last_error;
 
@@ -202,6 +204,60 @@ int64_t ORACLE_API(grid_run)(void* grid, double t_start, double t_end, int64_t m
 	}
 	*t_reached = t;
 	return steps;
+}
+
+// a staggered-field grid (periodic in every dimension); NULL on an invalid configuration
+void* ORACLE_API(sgrid_create)(const pamhd_cfg* cfg)
+{
+	try {
+		return new SGrid(*cfg);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return nullptr;
+	}
+}
+
+void ORACLE_API(sgrid_destroy)(void* grid)
+{
+	delete static_cast<SGrid*>(grid);
+}
+
+// cell state (8 arrays) and the normal field of every cell's -x, -y, -z face (3 arrays)
+int ORACLE_API(sgrid_set_state)(void* grid, const double* const soa[8], const double* const faces[3])
+{
+	try {
+		static_cast<SGrid*>(grid)->set_state(soa, faces);
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+int ORACLE_API(sgrid_get_state)(void* grid, double* const soa[8], double* const faces[3])
+{
+	static_cast<SGrid*>(grid)->get_state(soa, faces);
+	return PAMHD_OK;
+}
+
+// one staggered step (see Mode_S_Grid::step); failures as grid_step
+int ORACLE_API(sgrid_step)(void* grid, double max_dt, double* dt_taken,
+                           uint32_t* flag, int32_t cell[3], int32_t* dir)
+{
+	SGrid& g = *static_cast<SGrid*>(grid);
+	*flag = 0;
+	try {
+		*dt_taken = g.step(max_dt);
+	} catch (const oracle::Domain_Error& e) {
+		*flag = e.flag;
+		int c[3];
+		g.coords(size_t(g.failure.cell), c);
+		for (int d = 0; d < 3; d++) cell[d] = c[d];
+		*dir = g.failure.dir;
+		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
 }
 
 } // extern "C"

@@ -7,7 +7,8 @@ thing measured or shipped.
 Two libraries expose the same entry points (oracle/capi_body.hpp):
   port       oracle/_build/liboracle.so   restated solvers (mhd_oracle.hpp)
   reference  oracle/_ref/libpamhd_ref.so  the reference's own solver headers
-Both drive the solvers with the same Mode C grid restatement (mode_c.hpp).
+Both drive the solvers with the same grid restatements: Mode C (mode_c.hpp)
+and the staggered-field step (mode_s.hpp).
 """
 from __future__ import annotations
 
@@ -128,6 +129,18 @@ class Oracle:
         self._run.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int64, _DP, _DP]
         self._set_inflow = getattr(L, p + "grid_set_inflow")
         self._set_inflow.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
+        self._screate = getattr(L, p + "sgrid_create")
+        self._screate.restype = ctypes.c_void_p
+        self._screate.argtypes = [_P(Cfg)]
+        self._sdestroy = getattr(L, p + "sgrid_destroy")
+        self._sdestroy.argtypes = [ctypes.c_void_p]
+        self._sset = getattr(L, p + "sgrid_set_state")
+        self._sset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self._sget = getattr(L, p + "sgrid_get_state")
+        self._sget.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self._sstep = getattr(L, p + "sgrid_step")
+        self._sstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
+                                _P(ctypes.c_int32)]
         self._last_error = getattr(L, p + "last_error")
         self._last_error.restype = ctypes.c_char_p
         if kind == "port":
@@ -164,6 +177,9 @@ class Oracle:
 
     def grid(self, cfg: Cfg, threads: int = 1) -> "OracleGrid":
         return OracleGrid(self, cfg, threads)
+
+    def staggered_grid(self, cfg: Cfg) -> "OracleStaggeredGrid":
+        return OracleStaggeredGrid(self, cfg)
 
 
 class OracleGrid:
@@ -233,3 +249,58 @@ class OracleGrid:
         if steps < 0:
             raise RuntimeError(self.o.last_error())
         return t.value, hist[:steps]
+
+
+class OracleStaggeredGrid:
+    """A staggered-field grid in the oracle (periodic in every dimension).  Cell state arrays are
+    (8, nz, ny, nx); face field arrays (3, nz, ny, nx): the normal field of every cell's -x, -y
+    and -z face."""
+
+    def __init__(self, oracle: Oracle, cfg: Cfg):
+        self.o = oracle
+        self.cfg = cfg
+        self.shape = (cfg.n[2], cfg.n[1], cfg.n[0])
+        self.h = oracle._screate(ctypes.byref(cfg))
+        if not self.h:
+            raise ValueError(oracle.last_error())
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.o._sdestroy(h)
+            self.h = None
+
+    def set_state(self, U, faces):
+        ptrs, keep = _soa_in([U[k].reshape(-1) for k in range(8)])
+        fptrs = (ctypes.c_void_p * 3)()
+        fkeep = []
+        for d in range(3):
+            a = np.ascontiguousarray(faces[d], dtype=np.float64).reshape(-1)
+            fkeep.append(a)
+            fptrs[d] = a.ctypes.data
+        rc = self.o._sset(self.h, ptrs, fptrs)
+        if rc != 0:
+            raise ValueError(self.o.last_error())
+
+    def get_state(self):
+        U = np.zeros((8,) + self.shape)
+        faces = np.zeros((3,) + self.shape)
+        ptrs = (ctypes.c_void_p * 8)()
+        for k in range(8):
+            ptrs[k] = U[k].ctypes.data
+        fptrs = (ctypes.c_void_p * 3)()
+        for d in range(3):
+            fptrs[d] = faces[d].ctypes.data
+        self.o._sget(self.h, ptrs, fptrs)
+        return U, faces
+
+    def step(self, max_dt):
+        """Returns (dt, flag, cell, dir); flag != 0 when a face failed (state not updated)."""
+        dt = ctypes.c_double(0)
+        flag = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.o._sstep(self.h, max_dt, ctypes.byref(dt), ctypes.byref(flag), cell, ctypes.byref(d))
+        if rc not in (0, 3):
+            raise ValueError(self.o.last_error())
+        return dt.value, flag.value, tuple(cell), d.value

@@ -5,15 +5,25 @@ reference's tests) into tests/golden/dc_goldens.npz, with the reference's own re
 Run where the reference tree exists:
     python tests/golden/make_dc_golden.py
 
-The cases are those whose magnetic field is zero, for which the reference's staggered-field
-("Mode S") program reduces to the cell-centred step of this library: the hydrodynamic part of
-the update is the same flux difference (mhd/solve.hpp:1543-1576) and the field terms vanish.
+Zero-field cases, for which the reference's staggered-field ("Mode S") program reduces to the
+cell-centred step of this library (the hydrodynamic part of the update is the same flux
+difference, mhd/solve.hpp:1543-1576, and the field terms vanish):
 
   da_px, da_mx  tests/mhd/reference/hydrodynamic/density_advection/1d/{+x,-x}/rusanov/
                 mhd_000000917.dc: 200 periodic cells on [0, 1], gamma 1.6666666667, mu0 1,
                 proton mass 1, CFL 0.5, Rusanov, run from t = 0 to t = 1
                 (tests/mhd/config_files/hydrodynamic/density_advection/1d/{+x,-x}/rusanov.json)
-Each case stores: step, time, gamma, mu0, proton mass, the state (8, nx) in the reference's
+
+Alfven waves, which pin the staggered-field step itself (Rusanov, CFL 0.5, t = 0 .. 1,
+uniform level-0 grids, periodic):
+
+  alf_px, alf_mx  tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/1d/{+x,-x}/small_rusanov/
+                  mhd_000000202.dc: 100 x 1 x 1 cells on [0, 1]^3
+  alf_r1, alf_r2  tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov{1,2}/
+                  mhd_0000000{18,33}.dc: 1 x 10 x 10 cells, volume (1, 2/sqrt 3, 2), travelling
+                  and standing wave
+
+Each case stores: step, time, gamma, mu0, proton mass, the state (8, cells) in the reference's
 variable order (rho, mom xyz, E, B xyz) ordered by cell id, and the cell length.
 """
 import os
@@ -26,6 +36,10 @@ REF = "/root/reference"
 CASES = {
     "da_px": "tests/mhd/reference/hydrodynamic/density_advection/1d/+x/rusanov/mhd_000000917.dc",
     "da_mx": "tests/mhd/reference/hydrodynamic/density_advection/1d/-x/rusanov/mhd_000000917.dc",
+    "alf_px": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/1d/+x/small_rusanov/mhd_000000202.dc",
+    "alf_mx": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/1d/-x/small_rusanov/mhd_000000202.dc",
+    "alf_r1": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov1/mhd_000000018.dc",
+    "alf_r2": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov2/mhd_000000033.dc",
 }
 
 

@@ -2,6 +2,8 @@
 the benchmark inputs (numpy only)."""
 from __future__ import annotations
 
+import functools
+
 import numpy as np
 
 GAMMA_53 = 5.0 / 3.0
@@ -239,3 +241,182 @@ def density_advection(n, gamma, vx, proton_mass=1.0):
     U[1, 0, 0] = rho * vx
     U[4, 0, 0] = 1.0 / (gamma - 1) + 0.5 * rho * vx * vx
     return U
+
+
+@functools.lru_cache(maxsize=None)
+def gauss_legendre_7():
+    """Nodes (x >= 0, ascending) and weights of the 7-point Gauss-Legendre rule on [-1, 1], each
+    the double nearest to the exact value: Newton iteration on the Legendre polynomial P7 in
+    60-digit decimal arithmetic from the Chebyshev-like first guesses cos(pi (i - 1/4) / (7 + 1/2)),
+    weights 2 / ((1 - x^2) P7'(x)^2)."""
+    import decimal
+    import math
+
+    ctx = decimal.Context(prec=60)
+    D = decimal.Decimal
+
+    def legendre(x):
+        p0, p1 = D(1), x
+        for k in range(2, 8):
+            p0, p1 = p1, ctx.divide(ctx.subtract(ctx.multiply(D(2 * k - 1) * x, p1), D(k - 1) * p0), D(k))
+        # derivative: n (x P_n - P_{n-1}) / (x^2 - 1)
+        dp = ctx.divide(D(7) * (x * p1 - p0), x * x - 1)
+        return p1, dp
+
+    nodes, weights = [], []
+    for i in range(1, 5):
+        x = D(repr(math.cos(math.pi * (i - 0.25) / 7.5)))
+        for _ in range(100):
+            p, dp = legendre(x)
+            step = ctx.divide(p, dp)
+            x = ctx.subtract(x, step)
+            if abs(step) < D(10) ** -55:
+                break
+        if abs(x) < D(10) ** -50:
+            x = D(0)
+        _, dp = legendre(x)
+        w = ctx.divide(D(2), (1 - x * x) * dp * dp)
+        nodes.append(float(x))
+        weights.append(float(w))
+    order = np.argsort(nodes)
+    return [nodes[i] for i in order], [weights[i] for i in order]
+
+
+def gauss_average(f, a, b):
+    """Integral of f over [a, b] by the 7-point Gauss-Legendre rule, in the summation order of
+    boost::math::quadrature::gauss<double, 7>::integrate (the rule mhd/initialize.hpp:361-486
+    uses): scale * (f(mid) w0 + sum_i (f(mid + scale x_i) + f(mid - scale x_i)) w_i)."""
+    x, w = gauss_legendre_7()
+    mid = (a + b) * 0.5
+    scale = (b - a) * 0.5
+    total = f(mid + scale * x[0]) * w[0]
+    for i in range(1, 4):
+        fp = f(mid + scale * x[i])
+        fm = f(mid + scale * -x[i])
+        total += (fp + fm) * w[i]
+    return scale * total
+
+
+def staggered_state(n, length, start, number_density, velocity, pressure, field, gamma, mu0,
+                    proton_mass=1.0):
+    """Initial cell state and face field of the reference's MHD program (tests/mhd/test.cpp:422-456)
+    on a uniform periodic grid: the normal field of every face is its 7-point Gauss-Legendre
+    average over the face (initialize_magnetic_field, mhd/initialize.hpp:361-547), in a dimension
+    of one cell taken at the grid's middle (get_cell_geom_emulated, grid/amr.hpp:288-310); the
+    volume field is the mean of each cell's two faces (update_vol_B); the fluid is set at the
+    cell centres (initialize_fluid, mhd/initialize.hpp:77-160: rho = m_p n, mom = rho v, E from
+    the pressure, v and the volume field).  The functions take (x, y, z) scalars and return a
+    scalar (number density, pressure) or a 3-sequence (velocity, field).
+    Returns U (8, nz, ny, nx) and faces (3, nz, ny, nx): the field of each cell's -x, -y, -z face."""
+    n = [int(v) for v in n]
+    L = [float(v) for v in length]
+    s = [float(v) for v in start]
+    mid = [(s[d] + n[d] * L[d] + s[d]) / 2 for d in range(3)]
+
+    def bounds(d, i):
+        if n[d] == 1:
+            return mid[d], mid[d], mid[d]
+        lo = s[d] + i * L[d]
+        hi = s[d] + (i + 1) * L[d]
+        return lo + L[d] / 2, lo, hi
+
+    faces = np.zeros((3, n[2], n[1], n[0]))
+    U = np.zeros((8, n[2], n[1], n[0]))
+    for k in range(n[2]):
+        for j in range(n[1]):
+            for i in range(n[0]):
+                geo = [bounds(0, i), bounds(1, j), bounds(2, k)]
+                for d in range(3):
+                    a, b = [e for e in range(3) if e != d]   # the two dimensions across the face
+
+                    def point(u, v, d=d, a=a, b=b):
+                        c = [0.0, 0.0, 0.0]
+                        c[d] = geo[d][1]
+                        c[a] = u
+                        c[b] = v
+                        return field(*c)[d]
+
+                    ua, ea = geo[a][1], geo[a][2]
+                    ub, eb = geo[b][1], geo[b][2]
+                    wa, wb = ea - ua, eb - ub
+                    if wa == 0 and wb == 0:
+                        val = point(ua, ub)
+                    elif wa == 0:
+                        val = gauss_average(lambda v: point(ua, v), ub, eb) / wb
+                    elif wb == 0:
+                        val = gauss_average(lambda u: point(u, ub), ua, ea) / wa
+                    else:
+                        val = gauss_average(lambda v: gauss_average(lambda u: point(u, v), ua, ea), ub, eb) / wa / wb
+                    faces[d, k, j, i] = val
+    for k in range(n[2]):
+        for j in range(n[1]):
+            for i in range(n[0]):
+                c = [bounds(0, i)[0], bounds(1, j)[0], bounds(2, k)[0]]
+                B = [0.5 * (faces[0, k, j, i] + faces[0, k, j, (i + 1) % n[0]]),
+                     0.5 * (faces[1, k, j, i] + faces[1, k, (j + 1) % n[1], i]),
+                     0.5 * (faces[2, k, j, i] + faces[2, (k + 1) % n[2], j, i])]
+                rho = proton_mass * number_density(*c)
+                v = velocity(*c)
+                p = pressure(*c)
+                U[0, k, j, i] = rho
+                for e in range(3):
+                    U[1 + e, k, j, i] = rho * v[e]
+                    U[5 + e, k, j, i] = B[e]
+                if rho > 0 and p > 0:
+                    kinetic = 0.5 * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+                    magnetic = 0.5 / mu0 * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2])
+                    U[4, k, j, i] = p / (gamma - 1) + kinetic + magnetic
+    return U, faces
+
+
+def alfven_1d(n=100, sign=1):
+    """The reference's 1-D Alfven wave (tests/mhd/config_files/magnetohydrodynamic/Alfven_wave/1d/
+    {+x,-x}/small_rusanov.json): n x 1 x 1 periodic cells on [0, 1]^3, gamma 5/3, mu0 1, number
+    density 1, pressure 0.1, v = sign (0, 0.1 sin 2 pi x, 0.1 cos 2 pi x),
+    B = (1, 0.1 sin 2 pi x, 0.1 cos 2 pi x).  Returns U, faces, cell lengths."""
+    import math
+    tau = 2 * math.pi
+    gamma = 1.6666666666666667
+
+    def vel(x, y, z):
+        return (0.0, sign * (0.1 * math.sin(tau * x)), sign * (0.1 * math.cos(tau * x)))
+
+    def mag(x, y, z):
+        return (1.0, 0.1 * math.sin(tau * x), 0.1 * math.cos(tau * x))
+
+    L = (1.0 / n, 1.0, 1.0)
+    U, faces = staggered_state((n, 1, 1), L, (0, 0, 0), lambda x, y, z: 1.0, vel, lambda x, y, z: 0.1,
+                               mag, gamma, 1.0)
+    return U, faces, L
+
+
+def alfven_2d(standing=False):
+    """The reference's 2-D Alfven wave on 1 x 10 x 10 level-0 cells (tests/mhd/config_files/
+    magnetohydrodynamic/Alfven_wave/2d/x/small_rusanov1.json, travelling; small_rusanov2.json,
+    standing): periodic, volume (1, 2/sqrt 3, 2), gamma 5/3, mu0 1, number density 1, pressure
+    0.1, with phase = pi (sqrt 3 y + z):
+    v = (sin(phase)/1000, -cos(phase)/2000, sqrt 3 cos(phase)/2000), or for the standing wave
+    (sin(phase)/1000, sqrt 3/2 - cos(phase)/2000, 0.5 + sqrt 3 cos(phase)/2000);
+    B = (sin(phase)/1000, sqrt 3/2 + cos(phase)/2000, 0.5 - sqrt 3 cos(phase)/2000).
+    Returns U, faces, cell lengths."""
+    import math
+    r3 = math.sqrt(3)
+    gamma = 1.6666666666666667
+
+    def phase(y, z):
+        return math.pi * (r3 * y + z)
+
+    def vel(x, y, z):
+        s, c = math.sin(phase(y, z)), math.cos(phase(y, z))
+        if standing:
+            return (s / 1000, r3 / 2 - c / 2000, 0.5 + r3 * c / 2000)
+        return (s / 1000, -c / 2000, r3 * c / 2000)
+
+    def mag(x, y, z):
+        s, c = math.sin(phase(y, z)), math.cos(phase(y, z))
+        return (s / 1000, r3 / 2 + c / 2000, 0.5 - r3 * c / 2000)
+
+    L = (1.0, 2 / r3 / 10, 0.2)
+    U, faces = staggered_state((1, 10, 10), L, (0, 0, 0), lambda x, y, z: 1.0, vel, lambda x, y, z: 0.1,
+                               mag, gamma, 1.0)
+    return U, faces, L

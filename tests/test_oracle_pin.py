@@ -11,7 +11,10 @@ reference's solvers and step.  These tests hold it to:
   - the reference program's own output files (tests/mhd/reference/**/*.dc, extracted into
     tests/golden/dc_goldens.npz by tests/golden/make_dc_golden.py with the reference's reader)
     for the cases whose field is zero, where its staggered-field step reduces to the
-    cell-centred one: same step count, state within a few ulps after 917 steps.
+    cell-centred one: same step count, state within a few ulps after 917 steps;
+  - the same program's Alfven-wave outputs, which pin the staggered-field step
+    (oracle/mode_s.hpp): same step count, every cell within the tolerances of the
+    reference's own comparison (tests/mhd/mhd_diff.py:232-241).
 Bit-for-bit equality is required wherever both sides run the same
 arithmetic (the oracle is built with -ffp-contract=off, as the reference).
 """
@@ -233,3 +236,143 @@ def test_mode_c_reproduces_reference_program_output(port, case, vx):
     ref = g[case + "_state"]
     scale = np.maximum(np.abs(ref).max(axis=1), 1e-300)
     assert (np.abs(out - ref).max(axis=1) / scale).max() <= 1e-14
+
+
+def _mhd_diff_ok(out, ref, tol=1e-15, floor=1e-15):
+    """The per-cell comparison of tests/mhd/mhd_diff.py:189-225 with its default tolerances:
+    (|a - b| - floor) / max(|a|, |b|) <= tol for mass density, |v|, total energy and |B|."""
+    def within(a, b):
+        denom = np.maximum(np.abs(a), np.abs(b))
+        diff = np.abs(a - b) - floor
+        return bool(np.all((denom == 0) | (diff / np.where(denom == 0, 1, denom) <= tol)))
+
+    v1 = np.linalg.norm(out[1:4] / out[0], axis=0)
+    v2 = np.linalg.norm(ref[1:4] / ref[0], axis=0)
+    return (within(out[0], ref[0]) and within(v1, v2) and within(out[4], ref[4])
+            and within(np.linalg.norm(out[5:8], axis=0), np.linalg.norm(ref[5:8], axis=0)))
+
+
+STAGGERED_CASES = {
+    "alf_px": lambda: states.alfven_1d(100, 1),
+    "alf_mx": lambda: states.alfven_1d(100, -1),
+    "alf_r1": lambda: states.alfven_2d(False),
+    "alf_r2": lambda: states.alfven_2d(True),
+}
+
+
+def run_staggered(grid_owner, case, solver=po.RUSANOV):
+    """Runs a staggered-field golden case as the reference's program does (tests/mhd/test.cpp:
+    422-537): initial state, the dt = 0 priming step, then steps capped by the time left until
+    t = 1.  Returns (state (8, cells), faces (3, cells), steps, t)."""
+    g = _load("dc_goldens.npz")
+    U0, faces, _ = STAGGERED_CASES[case]()
+    n = (U0.shape[3], U0.shape[2], U0.shape[1])
+    cfg = po.make_cfg(n, solver, tuple(g[case + "_cell_length"]), float(g[case + "_gamma"]),
+                      float(g[case + "_mu0"]), 0.5)
+    grid = grid_owner.staggered_grid(cfg)
+    grid.set_state(U0, faces)
+    grid.step(0.0)
+    t, steps, t_end = 0.0, 0, float(g[case + "_time"])
+    while t < t_end:
+        dt, flag, _, _ = grid.step(t_end - t)
+        assert flag == 0
+        t += dt
+        steps += 1
+    U, F = grid.get_state()
+    return U.reshape(8, -1), F.reshape(3, -1), steps, t
+
+
+@pytest.mark.parametrize("case", list(STAGGERED_CASES))
+def test_mode_s_reproduces_reference_program_output(port, case):
+    """The reference program's staggered-field Alfven waves (Rusanov, CFL 0.5, t = 0 .. 1): the
+    oracle takes the same number of steps to the same time and every cell passes the reference's
+    own comparison against the program's output at its default 1e-15 tolerances."""
+    g = _load("dc_goldens.npz")
+    out, _, steps, t = run_staggered(port, case)
+    assert steps == int(g[case + "_step"])
+    assert t == float(g[case + "_time"])
+    ref = g[case + "_state"]
+    assert _mhd_diff_ok(out, ref)
+    # every conservative value within 2e-15 absolute (all are of order 1 or less here)
+    assert np.abs(out - ref).max() <= 2e-15
+
+
+@pytest.mark.parametrize("case", ["alf_px", "alf_r1"])
+def test_mode_s_restated_solvers_equal_reference_headers(port, ref, case):
+    """The staggered step driven by the reference's own solver headers computes the same bits."""
+    a = run_staggered(port, case)
+    b = run_staggered(ref, case)
+    assert a[2] == b[2]
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def _curl_faces(shape, L, rng, amp):
+    """Face field of a random periodic vector potential: the discrete curl of edge values, whose
+    discrete divergence is zero up to rounding."""
+    nz, ny, nx = shape
+    A = rng.normal(size=(3,) + shape) * amp
+    dx, dy, dz = L
+    r = lambda a, ax: np.roll(a, -1, axis=ax)
+    # A[0] on x edges, A[1] on y edges, A[2] on z edges (at the cell's low corner lines)
+    bx = (r(A[2], 1) - A[2]) / dy - (r(A[1], 0) - A[1]) / dz
+    by = (r(A[0], 0) - A[0]) / dz - (r(A[2], 2) - A[2]) / dx
+    bz = (r(A[1], 2) - A[1]) / dx - (r(A[0], 1) - A[0]) / dy
+    return np.stack([bx, by, bz])
+
+
+def _div(faces, L):
+    r = lambda a, ax: np.roll(a, -1, axis=ax)
+    return ((r(faces[0], 2) - faces[0]) / L[0] + (r(faces[1], 1) - faces[1]) / L[1]
+            + (r(faces[2], 0) - faces[2]) / L[2])
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena"])
+def test_mode_s_keeps_divergence(port, solver):
+    """Constrained transport: the discrete divergence of the face field does not change."""
+    rng = np.random.default_rng(7)
+    shape, L = (6, 5, 7), (0.1, 0.12, 0.09)
+    faces = _curl_faces(shape, L, rng, 0.01) + np.array([0.3, -0.2, 0.1])[:, None, None, None]
+    U = states.smooth_3d(shape, rng, amp=0.05)
+    r = lambda a, ax: np.roll(a, -1, axis=ax)
+    U[5] = 0.5 * (faces[0] + r(faces[0], 2))
+    U[6] = 0.5 * (faces[1] + r(faces[1], 1))
+    U[7] = 0.5 * (faces[2] + r(faces[2], 0))
+    cfg = po.make_cfg((7, 5, 6), po.SOLVERS[solver], L, states.GAMMA_53, 1.0, 0.4)
+    grid = port.staggered_grid(cfg)
+    grid.set_state(U, faces)
+    div0 = _div(faces, L)
+    grid.step(0.0)
+    for _ in range(10):
+        dt, flag, _, _ = grid.step(1.0)
+        assert flag == 0 and dt > 0
+    _, F = grid.get_state()
+    assert np.abs(_div(F, L) - div0).max() <= 1e-12 * np.abs(F).max() / min(L)
+
+
+def test_mode_s_cyclic_rotation(port):
+    """The staggered step commutes with the cyclic relabelling x -> y -> z of axes, vector
+    components and faces (the property the reference's rotated golden checks use,
+    mhd_diff.py --rotate).  The face fluxes and face-field changes are relabelled bit for bit;
+    the pressure sums of update_vol_B add the components in grid order, so the states agree to
+    rounding."""
+    U0, faces, L = states.alfven_1d(20, 1)
+
+    def run(U, faces, L):
+        n = (U.shape[3], U.shape[2], U.shape[1])
+        grid = port.staggered_grid(po.make_cfg(n, po.HLLD, L, 1.6666666666666667, 1.0, 0.5))
+        grid.set_state(U, faces)
+        grid.step(0.0)
+        for _ in range(15):
+            grid.step(1.0)
+        return grid.get_state()
+
+    def to_y(U, F):
+        # data along x -> along y; components (x, y, z) -> (z, x, y)
+        return np.moveaxis(U, 3, 2)[[0, 3, 1, 2, 4, 7, 5, 6]], np.moveaxis(F, 3, 2)[[2, 0, 1]]
+
+    a_U, a_F = run(U0, faces, L)
+    U1, F1 = to_y(U0, faces)
+    b_U, b_F = run(U1, F1, (L[2], L[0], L[1]))
+    e_U, e_F = to_y(a_U, a_F)
+    np.testing.assert_allclose(b_U, e_U, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(b_F, e_F, rtol=0, atol=1e-14)
