@@ -406,6 +406,43 @@ int pamhd_dc_read_info(const char* path, pamhd_dc_info* info);
 /* Reads the "mhd     " variable of a .dc file into eight arrays of info.cells doubles. */
 int pamhd_dc_read(const char* path, double* const soa[8]);
 
+/*
+Staggered-field step: the reference's timestep() with the normal magnetic
+field of every face (Face_B) advanced by constrained transport
+(mhd/solve.hpp:1837-1924: get_fluxes with assign_face_dBs_f{x,y,z},
+update_mhd_state, update_vol_B with constant thermal pressure before and
+after sync_magnetic_field), on a uniform grid periodic in every dimension.
+A dimension of one cell is its own neighbour, as in the reference's
+emulated 1-D and 2-D runs.  Solvers: Rusanov, HLL, HLLD, Roe.
+
+  - create: cfg as pamhd_gpu_create, every side PAMHD_BC_PERIODIC
+    (else PAMHD_ERR_ARGUMENT); replaces the state a PAMHD program keeps in
+    Mas, Mom, Nrj, Vol_B and Face_B (tests/mhd/test.cpp:422-456).
+  - set_state / get_state: cells as pamhd_gpu_set_state (eight arrays, x
+    fastest; cells[5..7] is the volume field Vol_B) and faces[d] the normal
+    field of every cell's -d face (Face_B(-d); a cell's +d face is the -d
+    face of its +d neighbour).  set_state resets the clock; the first step
+    after it is the reference's dt = 0 priming step when called with
+    max_dt = 0.  get_state may be given faces == NULL.
+  - step: one step with dt = min(lagged CFL dt, max_dt) as pamhd_gpu_step;
+    PAMHD_ERR_PHYSICS when a face failed (the state is left as it was).
+  - steps: nsteps steps launched on the context's stream, each capped by
+    t_end - t; steps once t >= t_end leave the state unchanged.  Returns
+    at once; sync waits and reports failures.
+*/
+typedef struct pamhd_stag pamhd_stag;
+
+int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** ctx);
+int pamhd_gpu_staggered_destroy(pamhd_stag* ctx);
+int pamhd_gpu_staggered_set_state(pamhd_stag* ctx, const double* const cells[8], const double* const faces[3]);
+int pamhd_gpu_staggered_get_state(pamhd_stag* ctx, double* const cells[8], double* const faces[3]);
+int pamhd_gpu_staggered_step(pamhd_stag* ctx, double max_dt, double* dt_taken);
+int pamhd_gpu_staggered_steps(pamhd_stag* ctx, int32_t nsteps, double t_end);
+int pamhd_gpu_staggered_sync(pamhd_stag* ctx);
+int pamhd_gpu_staggered_time(pamhd_stag* ctx, double* time, int64_t* steps, double* last_dt);
+int pamhd_gpu_staggered_status(pamhd_stag* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
+int pamhd_gpu_staggered_get_stream(pamhd_stag* ctx, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -339,6 +339,102 @@ class Context:
         return out
 
 
+class StaggeredContext:
+    """A pamhd_stag: the staggered-field step (face magnetic field by constrained transport) on
+    one uniform grid periodic in every dimension.  Cell arrays are (8, nz, ny, nx) as Context;
+    face arrays (3, nz, ny, nx): the normal field of every cell's -x, -y and -z face."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.L = lib()
+        L = self.L
+        V = ctypes.c_void_p
+        L.pamhd_gpu_staggered_create.argtypes = [_P(_Cfg), _P(V)]
+        L.pamhd_gpu_staggered_destroy.argtypes = [V]
+        L.pamhd_gpu_staggered_set_state.argtypes = [V, V, V]
+        L.pamhd_gpu_staggered_get_state.argtypes = [V, V, V]
+        L.pamhd_gpu_staggered_step.argtypes = [V, _D, _DP]
+        L.pamhd_gpu_staggered_steps.argtypes = [V, ctypes.c_int32, _D]
+        L.pamhd_gpu_staggered_sync.argtypes = [V]
+        L.pamhd_gpu_staggered_time.argtypes = [V, _DP, _P(ctypes.c_int64), _DP]
+        L.pamhd_gpu_staggered_status.argtypes = [V, _P(ctypes.c_uint32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        L.pamhd_gpu_staggered_get_stream.argtypes = [V, _P(V)]
+        self.shape = (int(cfg.n[2]), int(cfg.n[1]), int(cfg.n[0]))
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        rc = L.pamhd_gpu_staggered_create(ctypes.byref(self._c), ctypes.byref(h))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_staggered_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pamhd_gpu_staggered_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == ERR_PHYSICS:
+            flags, cell, d = self.status()
+            raise PhysicsError(rc, what, flags, cell, d)
+        if rc != OK:
+            raise PamhdError(rc, what)
+
+    def set_state(self, U: np.ndarray, faces: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shape)
+        faces = np.ascontiguousarray(faces, dtype=np.float64).reshape((3,) + self.shape)
+        fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
+        self._check(self.L.pamhd_gpu_staggered_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
+                    "pamhd_gpu_staggered_set_state")
+
+    def get_state(self):
+        U = np.empty((8,) + self.shape)
+        faces = np.empty((3,) + self.shape)
+        fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
+        self._check(self.L.pamhd_gpu_staggered_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
+                    "pamhd_gpu_staggered_get_state")
+        return U, faces
+
+    def step(self, max_dt: float) -> float:
+        dt = ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_staggered_step(self.h, max_dt, ctypes.byref(dt)), "pamhd_gpu_staggered_step")
+        return dt.value
+
+    def steps(self, n: int, t_end: float):
+        self._check(self.L.pamhd_gpu_staggered_steps(self.h, int(n), float(t_end)), "pamhd_gpu_staggered_steps")
+
+    def sync(self):
+        self._check(self.L.pamhd_gpu_staggered_sync(self.h), "pamhd_gpu_staggered_sync")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.pamhd_gpu_staggered_get_stream(self.h, ctypes.byref(s)), "pamhd_gpu_staggered_get_stream")
+        return s.value or 0
+
+    def time(self):
+        t, n, dt = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_staggered_time(self.h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(dt)),
+                    "pamhd_gpu_staggered_time")
+        return t.value, n.value, dt.value
+
+    def status(self):
+        f = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.L.pamhd_gpu_staggered_status(self.h, ctypes.byref(f), cell, ctypes.byref(d))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_staggered_status")
+        return f.value, tuple(cell), d.value
+
+
 def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
     """Solver-level entry point (pamhd_gpu_face_flux).  neg, pos: (n, 8); bg: (n, 3) or None.
     Returns flux (n, 8), speed (n,), flags (n,); failed faces have flags != 0 (no exception)."""

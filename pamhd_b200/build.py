@@ -3,7 +3,7 @@
     python -m pamhd_b200.build          # builds pamhd_b200/libpamhd_gpu.so in-tree
 
 Compiles every .cu under pamhd_b200/csrc with nvcc for compute_100a/sm_100a
-(FP64 arithmetic, FMA contraction on), links them into one shared library
+(FP64 arithmetic, FMA contraction on except in the files of FILE_FLAGS), links them into one shared library
 with the CUDA runtime linked statically, so the library has no dependency
 besides the driver.  Rebuilds only when a source or header is newer than
 the library.
@@ -26,6 +26,8 @@ OBJ = os.path.join(PKG, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "-I", os.path.join(ROOT, "include")]
+# per-file flags: the staggered step rounds every operation as the CPU oracle does
+FILE_FLAGS = {"staggered.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -53,7 +55,7 @@ def up_to_date() -> bool:
 
 def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
-    cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + ARCH + FLAGS + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,655 @@
+/*
+The staggered-field MHD step (the reference's timestep() with face magnetic
+field, mhd/solve.hpp:1837-1924) on uniform grids periodic in every
+dimension, behind pamhd_gpu_staggered_* of include/pamhd_gpu.h.
+
+Data in HBM, every array x fastest over the n0 x n1 x n2 cells, no ghosts
+(neighbours wrap around):
+  U[2]  cell state, 8 arrays (rho, mom xyz, E, volume B xyz), ping-pong;
+  B[2]  normal field of every cell's -x, -y and -z face, 3 arrays, ping-pong
+        (the +d face of a cell is the -d face of its +d neighbour);
+  F     raw flux through every cell's -d face, 3 x 8 arrays.
+A dimension of one cell is its own neighbour, as in the reference's emulated
+1-D and 2-D runs: its faces are solved with the cell on both sides.
+
+One step is two launches on the context's stream:
+  faces_kernel   every cell solves its three -d faces (the +d faces of its
+                 -d neighbours, get_fluxes, mhd/solve.hpp:217-392), stores
+                 the unrotated flux, and max-reduces the face speeds per
+                 axis into a three-slot ring, as the fused cell-centred step;
+  update_kernel  dt from the previous step's speeds and the cap (lagged CFL
+                 rule, mhd/solve.hpp:1933-2007, substepping.hpp:285-338);
+                 the cell update of update_mhd_state (mhd/solve.hpp:
+                 1543-1602); the new normal field of the cell's six faces from
+                 the twelve edge terms of assign_face_dBs_f{x,y,z}
+                 (mhd/solve.hpp:587-1494, equal-size neighbours); the cell
+                 writes its own three -d faces; then update_vol_B with
+                 constant thermal pressure twice (mhd/solve.hpp:1631-1683,
+                 :1895-1918), the volume field the mean of each pair of faces.
+This file is compiled without FMA contraction and writes the cell and face
+updates in the same operation order as the CPU oracle, so that given the same
+face fluxes both compute the same bits.
+*/
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "pamhd_gpu.h"
+#include "step.cuh"
+
+using namespace pamhd_b200;
+
+namespace {
+
+constexpr int THREADS = 256;
+
+struct Stag_Params {
+	const double* __restrict__ U;    // 8 x N
+	double* __restrict__ Uo;
+	const double* __restrict__ B;    // 3 x N
+	double* __restrict__ Bo;
+	double* __restrict__ F;          // (3 x 8) x N
+	int n[3];
+	long long N;
+	Gas gas;
+	double len[3];
+	double inv_len[3];
+	double area[3];
+	double cfl;
+	Speed_Max* red;                  // [3], ring by step phase
+	Clock* clock;                    // [3]
+	Status* status;
+	int phase;
+	double max_dt;                   // >= 0: cap of dt; < 0: the cap is t_end - t
+	double t_end;
+};
+
+__device__ __forceinline__ long long wrap_index(const Stag_Params& P, int i, int j, int k)
+{
+	i = i < 0 ? i + P.n[0] : (i >= P.n[0] ? i - P.n[0] : i);
+	j = j < 0 ? j + P.n[1] : (j >= P.n[1] ? j - P.n[1] : j);
+	k = k < 0 ? k + P.n[2] : (k >= P.n[2] ? k - P.n[2] : k);
+	return (long long)i + (long long)P.n[0] * ((long long)j + (long long)P.n[1] * k);
+}
+
+__device__ __forceinline__ void cell_coords(const Stag_Params& P, const long long c, int& i, int& j, int& k)
+{
+	i = int(c % P.n[0]);
+	j = int((c / P.n[0]) % P.n[1]);
+	k = int(c / ((long long)P.n[0] * P.n[1]));
+}
+
+template <int A>
+__device__ __forceinline__ Side make_side(const double U[8], const Derived& d)
+{
+	Side s;
+	s.rho = U[0];
+	rotate<A>(U[1], U[2], U[3], s.m0, s.m1, s.m2);
+	s.E = U[4];
+	rotate<A>(U[5], U[6], U[7], s.b0, s.b1, s.b2);
+	s.rinv = d.rinv;
+	s.p = d.p;
+	s.cf = d.cf[A];
+	s.v0 = s.m0 * s.rinv;
+	s.v1 = s.m1 * s.rinv;
+	s.v2 = s.m2 * s.rinv;
+	s.bad = d.bad;
+	return s;
+}
+
+__device__ __forceinline__ void record_failure(const Stag_Params& P, const uint32_t flag, const long long cell,
+                                               const int axis)
+{
+	atomicOr(&P.status->flags, flag);
+	const unsigned long long key = ((unsigned long long)(cell * 3 + axis) << 8) | flag;
+	atomicMin(&P.status->first, key);
+}
+
+// the -A face of cell c: solved between its -A neighbour (left) and c (right)
+template <int SOLVER, int A>
+__device__ __forceinline__ void solve_minus_face(const Stag_Params& P, const long long c, const int i, const int j,
+                                                 const int k, const double Uc[8], const Derived& dc,
+                                                 double& smax, bool& zero)
+{
+	const long long m = wrap_index(P, i - (A == 0), j - (A == 1), k - (A == 2));
+	double Um[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + m);
+	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7],
+	                                                  P.gas);
+	const Side L = make_side<A>(Um, dm);
+	const Side R = make_side<A>(Uc, dc);
+	double G[8];
+	uint32_t flag = 0;
+	const double s = solve_face<SOLVER>(L, R, P.gas, G, flag);
+	if (flag != 0) record_failure(P, flag, m, A);
+	smax = fmax(smax, s);
+	zero = zero or not (s > 0.0);
+	double out[8];
+	out[0] = G[0];
+	unrotate<A>(G[1], G[2], G[3], out[1], out[2], out[3]);
+	out[4] = G[4];
+	unrotate<A>(G[5], G[6], G[7], out[5], out[6], out[7]);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) P.F[(A * 8 + v) * P.N + c] = out[v];
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+	#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+
+template <int SOLVER>
+__global__ void __launch_bounds__(THREADS) faces_kernel(const Stag_Params P)
+{
+	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+	bool zero = false;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		int i, j, k;
+		cell_coords(P, c, i, j, k);
+		double Uc[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) Uc[v] = __ldg(P.U + v * P.N + c);
+		const Derived dc = derive<true, true, true>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
+		solve_minus_face<SOLVER, 0>(P, c, i, j, k, Uc, dc, s0, zero);
+		solve_minus_face<SOLVER, 1>(P, c, i, j, k, Uc, dc, s1, zero);
+		solve_minus_face<SOLVER, 2>(P, c, i, j, k, Uc, dc, s2, zero);
+	}
+	// per-axis maxima of the non-negative speeds, as bit patterns
+	s0 = warp_max(s0);
+	s1 = warp_max(s1);
+	s2 = warp_max(s2);
+	const bool any_zero = __any_sync(0xffffffffu, zero);
+	if ((threadIdx.x & 31) == 0) {
+		Speed_Max& r = P.red[(P.phase + 1) % 3];
+		atomicMax(&r.smax[0], (unsigned long long)__double_as_longlong(s0));
+		atomicMax(&r.smax[1], (unsigned long long)__double_as_longlong(s1));
+		atomicMax(&r.smax[2], (unsigned long long)__double_as_longlong(s2));
+		if (any_zero) atomicOr(&r.zero, 1u);
+	}
+}
+
+// dt of the step from the previous step's speeds (solve.hpp:1983-2003, substepping.hpp:331-338)
+__device__ __forceinline__ double step_dt(const Stag_Params& P)
+{
+	const Speed_Max& r = P.red[P.phase];
+	bool zero = r.zero != 0;
+	double smallest = 1.7976931348623157e308;
+	#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		const double s = __longlong_as_double((long long)r.smax[d]);
+		if (not (s > 0.0)) {
+			zero = true;
+		} else {
+			smallest = fmin(smallest, (P.cfl * P.len[d]) / s);
+		}
+	}
+	if (zero) smallest = 0.0;
+	const double t = P.clock[P.phase].t;
+	const double cap = P.max_dt >= 0.0 ? P.max_dt : P.t_end - t;
+	return (cap <= smallest) ? cap : smallest;
+}
+
+__device__ __forceinline__ double fluxB(const Stag_Params& P, const int axis, const int comp, const long long cell)
+{
+	return P.F[(axis * 8 + 5 + comp) * P.N + cell];
+}
+
+/*
+Change of the normal field of the -d face of cell (i, j, k), times the face
+area: the twelve edge terms of assign_face_dBs_f{x,y,z} that reach the face,
+in the order of the oracle (d-directed fluxes one cell away along a and b,
+then the a- and b-directed fluxes of the faces sharing an edge with it).
+*/
+template <int D>
+__device__ __forceinline__ double face_dB(const Stag_Params& P, const int i, const int j, const int k, const double dt)
+{
+	constexpr int A = (D + 1) % 3, Bd = (D + 2) % 3;
+	const double La = P.len[A], Lb = P.len[Bd];
+	const int c[3] = {i, j, k};
+	auto cell = [&](const int da, const int db, const int dd) {
+		int m[3] = {c[0], c[1], c[2]};
+		m[A] += da;
+		m[Bd] += db;
+		m[D] += dd;
+		return wrap_index(P, m[0], m[1], m[2]);
+	};
+	auto e1 = [&](const long long s) { return fluxB(P, D, A, s) * dt * Lb / 4; };
+	auto e2 = [&](const long long s) { return -(fluxB(P, D, Bd, s) * dt * La / 4); };
+	auto e3 = [&](const long long s) { return -(fluxB(P, A, D, s) * dt * Lb / 4); };
+	auto e4 = [&](const long long s) { return fluxB(P, Bd, D, s) * dt * La / 4; };
+	double dB = 0;
+	dB += e1(cell(+1, 0, 0));
+	dB -= e1(cell(-1, 0, 0));
+	dB -= e2(cell(0, +1, 0));
+	dB += e2(cell(0, -1, 0));
+	dB += e3(cell(+1, 0, 0));
+	dB += e3(cell(+1, 0, -1));
+	dB -= e3(cell(0, 0, 0));
+	dB -= e3(cell(0, 0, -1));
+	dB -= e4(cell(0, +1, 0));
+	dB -= e4(cell(0, +1, -1));
+	dB += e4(cell(0, 0, 0));
+	dB += e4(cell(0, 0, -1));
+	return dB;
+}
+
+// get_pressure, mhd/common.hpp:79-118
+__device__ __forceinline__ double pressure(const double u[8], const Gas& g)
+{
+	const double kinetic = 0.5 / u[0] * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]);
+	const double magnetic = 0.5 / g.mu0 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
+	return (u[4] - kinetic - magnetic) * (g.gamma - 1);
+}
+
+// update_vol_B with constant thermal pressure for one cell (mhd/solve.hpp:1646-1672)
+__device__ __forceinline__ void vol_B_constant_pressure(double u[8], const double mean[3], const Gas& g)
+{
+	if (u[0] <= 0) return;
+	const double p = pressure(u, g);
+	u[5] = mean[0];
+	u[6] = mean[1];
+	u[7] = mean[2];
+	const double inv = 1 / u[0];
+	const double v0 = u[1] * inv, v1 = u[2] * inv, v2 = u[3] * inv;
+	const double kinetic = 0.5 * u[0] * (v0 * v0 + v1 * v1 + v2 * v2);
+	const double magnetic = 0.5 / g.mu0 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
+	u[4] = p / (g.gamma - 1) + kinetic + magnetic;
+}
+
+__global__ void __launch_bounds__(THREADS) update_kernel(const Stag_Params P)
+{
+	__shared__ double s_dt;
+	__shared__ int s_skip;
+	if (threadIdx.x == 0) {
+		const Clock c = P.clock[P.phase];
+		// a failed face leaves the state as it was; so does a step past t_end
+		const bool skip = P.status->flags != 0u or (P.max_dt < 0.0 and c.t >= P.t_end);
+		const double dt = skip ? 0.0 : step_dt(P);
+		s_dt = dt;
+		s_skip = skip ? 1 : 0;
+		if (blockIdx.x == 0) {
+			Clock& next = P.clock[(P.phase + 1) % 3];
+			next.t = skip ? c.t : c.t + dt;
+			next.dt = skip ? c.dt : dt;
+			next.steps = skip ? c.steps : c.steps + 1;
+			Speed_Max& z = P.red[(P.phase + 2) % 3];
+			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
+			z.zero = 0u;
+		}
+	}
+	__syncthreads();
+	const double dt = s_dt;
+	const bool skip = s_skip != 0;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		if (skip) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) P.Uo[v * P.N + c] = P.U[v * P.N + c];
+			#pragma unroll
+			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
+			continue;
+		}
+		int i, j, k;
+		cell_coords(P, c, i, j, k);
+		const long long up[3] = {wrap_index(P, i + 1, j, k), wrap_index(P, i, j + 1, k), wrap_index(P, i, j, k + 1)};
+		double u[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) u[v] = P.U[v * P.N + c];
+		// dt-scaled fluxes of the -d and +d faces, as the flux slots of the reference (0 + dt F)
+		double fm[3][8], fp[3][8];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				fm[d][v] = 0 + dt * P.F[(d * 8 + v) * P.N + c];
+				fp[d][v] = 0 + dt * P.F[(d * 8 + v) * P.N + up[d]];
+			}
+		}
+		// update_mhd_state: mass, momentum, energy, volume field; x, then y, then z
+		#pragma unroll
+		for (int d = 0; d < 3; d++) u[0] += (fm[d][0] - fp[d][0]) / P.len[d];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int e = 1; e <= 3; e++) u[e] = u[e] + P.inv_len[d] * (fm[d][e] + (-fp[d][e]));
+		}
+		#pragma unroll
+		for (int d = 0; d < 3; d++) u[4] += (fm[d][4] - fp[d][4]) / P.len[d];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (fm[d][e] + (-fp[d][e]));
+		}
+		// Face_B += Face_dB / area for the six faces of the cell
+		const double bm0 = P.B[c] + face_dB<0>(P, i, j, k, dt) / P.area[0];
+		const double bm1 = P.B[P.N + c] + face_dB<1>(P, i, j, k, dt) / P.area[1];
+		const double bm2 = P.B[2 * P.N + c] + face_dB<2>(P, i, j, k, dt) / P.area[2];
+		const double bp0 = P.B[up[0]] + face_dB<0>(P, i + 1, j, k, dt) / P.area[0];
+		const double bp1 = P.B[P.N + up[1]] + face_dB<1>(P, i, j + 1, k, dt) / P.area[1];
+		const double bp2 = P.B[2 * P.N + up[2]] + face_dB<2>(P, i, j, k + 1, dt) / P.area[2];
+		P.Bo[c] = bm0;
+		P.Bo[P.N + c] = bm1;
+		P.Bo[2 * P.N + c] = bm2;
+		const double mean[3] = {0.5 * (bm0 + bp0), 0.5 * (bm1 + bp1), 0.5 * (bm2 + bp2)};
+		vol_B_constant_pressure(u, mean, P.gas);
+		vol_B_constant_pressure(u, mean, P.gas);
+		#pragma unroll
+		for (int v = 0; v < 8; v++) P.Uo[v * P.N + c] = u[v];
+	}
+}
+
+template <int SOLVER>
+int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
+{
+	faces_kernel<SOLVER><<<grid, THREADS, 0, stream>>>(P);
+	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
+	update_kernel<<<grid, THREADS, 0, stream>>>(P);
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int check(const cudaError_t e)
+{
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+#define PAMHD_TRY(expr) do { const int rc_ = (expr); if (rc_ != PAMHD_OK) return rc_; } while (0)
+
+} // namespace
+
+struct pamhd_stag {
+	pamhd_cfg cfg;
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	long long N = 0;
+	double* U[2] = {nullptr, nullptr};
+	double* B[2] = {nullptr, nullptr};
+	double* F = nullptr;
+	Speed_Max* red = nullptr;
+	Clock* clock = nullptr;
+	Status* status = nullptr;
+	double* staging = nullptr;   // pinned host buffer of 11 x N doubles
+	int cur = 0;
+	long long steps = 0;         // launched steps since set_state (the ring phase)
+	int grid = 0;
+	bool loaded = false;
+	Stag_Params base;
+};
+
+namespace {
+
+Stag_Params params_of(const pamhd_stag& x, const double max_dt, const double t_end)
+{
+	Stag_Params P = x.base;
+	P.U = x.U[x.cur];
+	P.Uo = x.U[x.cur ^ 1];
+	P.B = x.B[x.cur];
+	P.Bo = x.B[x.cur ^ 1];
+	P.phase = int(x.steps % 3);
+	P.max_dt = max_dt;
+	P.t_end = t_end;
+	return P;
+}
+
+int issue(pamhd_stag& x, const double max_dt, const double t_end)
+{
+	const Stag_Params P = params_of(x, max_dt, t_end);
+	int rc = PAMHD_ERR_ARGUMENT;
+	switch (x.cfg.solver) {
+	case PAMHD_RUSANOV: rc = launch_pair<PAMHD_RUSANOV>(P, x.grid, x.stream); break;
+	case PAMHD_HLL_ATHENA: rc = launch_pair<PAMHD_HLL_ATHENA>(P, x.grid, x.stream); break;
+	case PAMHD_HLLD_ATHENA: rc = launch_pair<PAMHD_HLLD_ATHENA>(P, x.grid, x.stream); break;
+	case PAMHD_ROE_ATHENA: rc = launch_pair<PAMHD_ROE_ATHENA>(P, x.grid, x.stream); break;
+	default: break;
+	}
+	if (rc != PAMHD_OK) return rc;
+	x.cur ^= 1;
+	x.steps++;
+	return PAMHD_OK;
+}
+
+int reset_ring(pamhd_stag& x)
+{
+	Speed_Max r[3] = {};
+	r[0].zero = 1u;   // no speeds yet: the first step's dt is 0 unless capped lower
+	const Clock c[3] = {};
+	const Status s{0u, 0u, ~0ull};
+	PAMHD_TRY(check(cudaMemcpyAsync(x.red, r, sizeof r, cudaMemcpyHostToDevice, x.stream)));
+	PAMHD_TRY(check(cudaMemcpyAsync(x.clock, c, sizeof c, cudaMemcpyHostToDevice, x.stream)));
+	PAMHD_TRY(check(cudaMemcpyAsync(x.status, &s, sizeof s, cudaMemcpyHostToDevice, x.stream)));
+	x.steps = 0;
+	return check(cudaStreamSynchronize(x.stream));
+}
+
+int validate_stag(const pamhd_cfg& c)
+{
+	if (c.solver != PAMHD_RUSANOV and c.solver != PAMHD_HLL_ATHENA and c.solver != PAMHD_HLLD_ATHENA
+		and c.solver != PAMHD_ROE_ATHENA) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	for (int d = 0; d < 3; d++) {
+		if (c.n[d] < 1 or not (c.cell_length[d] > 0.0)) return PAMHD_ERR_ARGUMENT;
+		if (c.bc_lo[d] != PAMHD_BC_PERIODIC or c.bc_hi[d] != PAMHD_BC_PERIODIC) return PAMHD_ERR_ARGUMENT;
+	}
+	if (not (c.adiabatic_index > 1.0) or not (c.vacuum_permeability > 0.0) or not (c.time_step_factor > 0.0)) {
+		return PAMHD_ERR_ARGUMENT;
+	}
+	const long long N = (long long)c.n[0] * c.n[1] * c.n[2];
+	if (N > (1ll << 31)) return PAMHD_ERR_ARGUMENT;
+	return PAMHD_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
+{
+	if (cfg == nullptr or out == nullptr) return PAMHD_ERR_ARGUMENT;
+	*out = nullptr;
+	PAMHD_TRY(validate_stag(*cfg));
+	pamhd_stag* x = new (std::nothrow) pamhd_stag;
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	x->cfg = *cfg;
+	x->device = cfg->device;
+	x->N = (long long)cfg->n[0] * cfg->n[1] * cfg->n[2];
+	auto fail = [&](const int rc) {
+		pamhd_gpu_staggered_destroy(x);
+		return rc;
+	};
+	if (cudaSetDevice(x->device) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+	if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+	const size_t n = size_t(x->N);
+	if (cudaMalloc(&x->U[0], 8 * n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->U[1], 8 * n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->B[0], 3 * n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->B[1], 3 * n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->F, 24 * n * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
+		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
+		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess
+		or cudaMallocHost(&x->staging, 11 * n * sizeof(double)) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	int sms = 0;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	const long long blocks = (x->N + THREADS - 1) / THREADS;
+	x->grid = int(blocks < 8ll * sms ? blocks : 8ll * sms);
+	Stag_Params& P = x->base;
+	P = Stag_Params{};
+	for (int d = 0; d < 3; d++) {
+		P.n[d] = cfg->n[d];
+		P.len[d] = cfg->cell_length[d];
+		P.inv_len[d] = 1 / cfg->cell_length[d];
+	}
+	P.area[0] = cfg->cell_length[1] * cfg->cell_length[2];
+	P.area[1] = cfg->cell_length[0] * cfg->cell_length[2];
+	P.area[2] = cfg->cell_length[0] * cfg->cell_length[1];
+	P.N = x->N;
+	P.gas.gamma = cfg->adiabatic_index;
+	P.gas.mu0 = cfg->vacuum_permeability;
+	P.gas.inv_mu0 = 1.0 / cfg->vacuum_permeability;
+	P.gas.sqrt_mu0 = std::sqrt(cfg->vacuum_permeability);
+	P.gas.inv_sqrt_mu0 = 1.0 / P.gas.sqrt_mu0;
+	P.cfl = cfg->time_step_factor;
+	P.F = x->F;
+	P.red = x->red;
+	P.clock = x->clock;
+	P.status = x->status;
+	if (cudaMemsetAsync(x->U[0], 0, 8 * n * sizeof(double), x->stream) != cudaSuccess
+		or cudaMemsetAsync(x->B[0], 0, 3 * n * sizeof(double), x->stream) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	if (reset_ring(*x) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+	*out = x;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_destroy(pamhd_stag* x)
+{
+	if (x == nullptr) return PAMHD_OK;
+	cudaSetDevice(x->device);
+	if (x->stream != nullptr) cudaStreamSynchronize(x->stream);
+	cudaFree(x->U[0]);
+	cudaFree(x->U[1]);
+	cudaFree(x->B[0]);
+	cudaFree(x->B[1]);
+	cudaFree(x->F);
+	cudaFree(x->red);
+	cudaFree(x->clock);
+	cudaFree(x->status);
+	cudaFreeHost(x->staging);
+	if (x->stream != nullptr) cudaStreamDestroy(x->stream);
+	delete x;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_set_state(pamhd_stag* x, const double* const cells[8], const double* const faces[3])
+{
+	if (x == nullptr or cells == nullptr or faces == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (cells[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int d = 0; d < 3; d++) if (faces[d] == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	const size_t n = size_t(x->N);
+	for (int v = 0; v < 8; v++) std::memcpy(x->staging + v * n, cells[v], n * sizeof(double));
+	for (int d = 0; d < 3; d++) std::memcpy(x->staging + (8 + d) * n, faces[d], n * sizeof(double));
+	x->cur = 0;
+	PAMHD_TRY(check(cudaMemcpyAsync(x->U[0], x->staging, 8 * n * sizeof(double), cudaMemcpyHostToDevice, x->stream)));
+	PAMHD_TRY(check(cudaMemcpyAsync(x->B[0], x->staging + 8 * n, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
+	                                x->stream)));
+	PAMHD_TRY(reset_ring(*x));
+	x->loaded = true;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_get_state(pamhd_stag* x, double* const cells[8], double* const faces[3])
+{
+	if (x == nullptr or cells == nullptr) return PAMHD_ERR_ARGUMENT;
+	for (int v = 0; v < 8; v++) if (cells[v] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (faces != nullptr) {
+		for (int d = 0; d < 3; d++) if (faces[d] == nullptr) return PAMHD_ERR_ARGUMENT;
+	}
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	const size_t n = size_t(x->N);
+	PAMHD_TRY(check(cudaMemcpyAsync(x->staging, x->U[x->cur], 8 * n * sizeof(double), cudaMemcpyDeviceToHost,
+	                                x->stream)));
+	if (faces != nullptr) {
+		PAMHD_TRY(check(cudaMemcpyAsync(x->staging + 8 * n, x->B[x->cur], 3 * n * sizeof(double),
+		                                cudaMemcpyDeviceToHost, x->stream)));
+	}
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	for (int v = 0; v < 8; v++) std::memcpy(cells[v], x->staging + v * n, n * sizeof(double));
+	if (faces != nullptr) {
+		for (int d = 0; d < 3; d++) std::memcpy(faces[d], x->staging + (8 + d) * n, n * sizeof(double));
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_sync(pamhd_stag* x)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	Status s;
+	PAMHD_TRY(check(cudaMemcpy(&s, x->status, sizeof s, cudaMemcpyDeviceToHost)));
+	return s.flags != 0u ? PAMHD_ERR_PHYSICS : PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_step(pamhd_stag* x, const double max_dt, double* dt_taken)
+{
+	if (x == nullptr or not (max_dt >= 0.0)) return PAMHD_ERR_ARGUMENT;
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(issue(*x, max_dt, 0.0));
+	const int rc = pamhd_gpu_staggered_sync(x);
+	if (dt_taken != nullptr) {
+		Clock c;
+		PAMHD_TRY(check(cudaMemcpy(&c, x->clock + (x->steps % 3), sizeof c, cudaMemcpyDeviceToHost)));
+		*dt_taken = rc == PAMHD_OK ? c.dt : 0.0;
+	}
+	return rc;
+}
+
+int pamhd_gpu_staggered_steps(pamhd_stag* x, const int32_t nsteps, const double t_end)
+{
+	if (x == nullptr or nsteps < 0 or not (t_end == t_end)) return PAMHD_ERR_ARGUMENT;
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	for (int32_t s = 0; s < nsteps; s++) PAMHD_TRY(issue(*x, -1.0, t_end));
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_time(pamhd_stag* x, double* time, int64_t* steps, double* last_dt)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	Clock c;
+	PAMHD_TRY(check(cudaMemcpy(&c, x->clock + (x->steps % 3), sizeof c, cudaMemcpyDeviceToHost)));
+	if (time != nullptr) *time = c.t;
+	if (steps != nullptr) *steps = c.steps;
+	if (last_dt != nullptr) *last_dt = c.dt;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_status(pamhd_stag* x, uint32_t* flags, int32_t cell[3], int32_t* dir)
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	Status s;
+	PAMHD_TRY(check(cudaMemcpy(&s, x->status, sizeof s, cudaMemcpyDeviceToHost)));
+	if (flags != nullptr) *flags = s.flags;
+	if (s.flags != 0u and s.first != ~0ull) {
+		const long long key = (long long)(s.first >> 8);
+		const long long c = key / 3;
+		if (cell != nullptr) {
+			cell[0] = int32_t(c % x->cfg.n[0]);
+			cell[1] = int32_t((c / x->cfg.n[0]) % x->cfg.n[1]);
+			cell[2] = int32_t(c / ((long long)x->cfg.n[0] * x->cfg.n[1]));
+		}
+		if (dir != nullptr) *dir = int32_t(key % 3) + 1;
+	} else {
+		if (cell != nullptr) cell[0] = cell[1] = cell[2] = -1;
+		if (dir != nullptr) *dir = 0;
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_get_stream(pamhd_stag* x, void** stream)
+{
+	if (x == nullptr or stream == nullptr) return PAMHD_ERR_ARGUMENT;
+	*stream = static_cast<void*>(x->stream);
+	return PAMHD_OK;
+}
+
+} // extern "C"

@@ -420,3 +420,33 @@ def alfven_2d(standing=False):
     U, faces = staggered_state((1, 10, 10), L, (0, 0, 0), lambda x, y, z: 1.0, vel, lambda x, y, z: 0.1,
                                mag, gamma, 1.0)
     return U, faces, L
+
+
+def face_divergence(faces, L):
+    """Discrete divergence of a face field (3, nz, ny, nx) on a periodic grid, per cell."""
+    r = lambda a, ax: np.roll(a, -1, axis=ax)
+    return ((r(faces[0], 2) - faces[0]) / L[0] + (r(faces[1], 1) - faces[1]) / L[1]
+            + (r(faces[2], 0) - faces[2]) / L[2])
+
+
+def staggered_random(shape, L, rng, amp=0.05, field_amp=0.01, mean_field=(0.3, -0.2, 0.1), gamma=GAMMA_53):
+    """A smooth random cell state with a face field of zero discrete divergence: a uniform field
+    plus the discrete curl of a random periodic vector potential on the cell edges.  The volume
+    field is the mean of each cell's two faces, the total energy recomputed with it at the
+    state's pressure.  Returns U (8, nz, ny, nx), faces (3, nz, ny, nx), L."""
+    A = rng.normal(size=(3,) + tuple(shape)) * field_amp
+    dx, dy, dz = L
+    r = lambda a, ax: np.roll(a, -1, axis=ax)
+    bx = (r(A[2], 1) - A[2]) / dy - (r(A[1], 0) - A[1]) / dz
+    by = (r(A[0], 0) - A[0]) / dz - (r(A[2], 2) - A[2]) / dx
+    bz = (r(A[1], 2) - A[1]) / dx - (r(A[0], 1) - A[0]) / dy
+    faces = np.stack([bx, by, bz]) + np.asarray(mean_field, dtype=float)[:, None, None, None]
+    U = smooth_3d(tuple(shape), rng, gamma=gamma, amp=amp)
+    rho = U[0]
+    v = U[1:4] / rho
+    p = (U[4] - 0.5 * rho * (v ** 2).sum(axis=0) - 0.5 * (U[5:8] ** 2).sum(axis=0)) * (gamma - 1)
+    U[5] = 0.5 * (faces[0] + r(faces[0], 2))
+    U[6] = 0.5 * (faces[1] + r(faces[1], 1))
+    U[7] = 0.5 * (faces[2] + r(faces[2], 0))
+    U[4] = energy(rho, v, p, U[5:8], gamma)
+    return U, faces, L

@@ -87,3 +87,23 @@ def test_any_active_dimensions_pass_the_checks(lib, n):
     assert rc != pg.ERR_ARGUMENT
     if h.value:
         lib.pamhd_gpu_destroy(h)
+
+
+@pytest.mark.parametrize("change", [
+    dict(bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0)),   # the staggered step is periodic only
+    dict(bc_lo=(0, 0, pg.BC_VALUE)),
+    dict(solver=1),
+    dict(n=(0, 4, 4)),
+    dict(cell_length=(0.1, -0.1, 0.1)),
+    dict(adiabatic_index=0.5),
+])
+def test_staggered_create_rejects_invalid_config(lib, change):
+    lib.pamhd_gpu_staggered_create.argtypes = [ctypes.POINTER(pg._Cfg), ctypes.POINTER(ctypes.c_void_p)]
+    kw = dict(n=(4, 4, 4), solver=pg.RUSANOV, cell_length=(0.1, 0.1, 0.1))
+    kw.update(change)
+    cfg = pg.Config(**kw).to_c()
+    h = ctypes.c_void_p()
+    assert lib.pamhd_gpu_staggered_create(ctypes.byref(cfg), ctypes.byref(h)) == pg.ERR_ARGUMENT
+    assert not h.value
+    assert lib.pamhd_gpu_staggered_create(None, None) == pg.ERR_ARGUMENT
+    assert lib.pamhd_gpu_staggered_destroy(None) == pg.OK

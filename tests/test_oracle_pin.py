@@ -306,47 +306,20 @@ def test_mode_s_restated_solvers_equal_reference_headers(port, ref, case):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-def _curl_faces(shape, L, rng, amp):
-    """Face field of a random periodic vector potential: the discrete curl of edge values, whose
-    discrete divergence is zero up to rounding."""
-    nz, ny, nx = shape
-    A = rng.normal(size=(3,) + shape) * amp
-    dx, dy, dz = L
-    r = lambda a, ax: np.roll(a, -1, axis=ax)
-    # A[0] on x edges, A[1] on y edges, A[2] on z edges (at the cell's low corner lines)
-    bx = (r(A[2], 1) - A[2]) / dy - (r(A[1], 0) - A[1]) / dz
-    by = (r(A[0], 0) - A[0]) / dz - (r(A[2], 2) - A[2]) / dx
-    bz = (r(A[1], 2) - A[1]) / dx - (r(A[0], 1) - A[0]) / dy
-    return np.stack([bx, by, bz])
-
-
-def _div(faces, L):
-    r = lambda a, ax: np.roll(a, -1, axis=ax)
-    return ((r(faces[0], 2) - faces[0]) / L[0] + (r(faces[1], 1) - faces[1]) / L[1]
-            + (r(faces[2], 0) - faces[2]) / L[2])
-
-
 @pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena"])
 def test_mode_s_keeps_divergence(port, solver):
     """Constrained transport: the discrete divergence of the face field does not change."""
-    rng = np.random.default_rng(7)
-    shape, L = (6, 5, 7), (0.1, 0.12, 0.09)
-    faces = _curl_faces(shape, L, rng, 0.01) + np.array([0.3, -0.2, 0.1])[:, None, None, None]
-    U = states.smooth_3d(shape, rng, amp=0.05)
-    r = lambda a, ax: np.roll(a, -1, axis=ax)
-    U[5] = 0.5 * (faces[0] + r(faces[0], 2))
-    U[6] = 0.5 * (faces[1] + r(faces[1], 1))
-    U[7] = 0.5 * (faces[2] + r(faces[2], 0))
+    U, faces, L = states.staggered_random((6, 5, 7), (0.1, 0.12, 0.09), np.random.default_rng(7))
     cfg = po.make_cfg((7, 5, 6), po.SOLVERS[solver], L, states.GAMMA_53, 1.0, 0.4)
     grid = port.staggered_grid(cfg)
     grid.set_state(U, faces)
-    div0 = _div(faces, L)
+    div0 = states.face_divergence(faces, L)
     grid.step(0.0)
     for _ in range(10):
         dt, flag, _, _ = grid.step(1.0)
         assert flag == 0 and dt > 0
     _, F = grid.get_state()
-    assert np.abs(_div(F, L) - div0).max() <= 1e-12 * np.abs(F).max() / min(L)
+    assert np.abs(states.face_divergence(F, L) - div0).max() <= 1e-12 * np.abs(F).max() / min(L)
 
 
 def test_mode_s_cyclic_rotation(port):
