@@ -55,13 +55,16 @@ def args_():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
-    p.add_argument("--only", choices=["batched", "adjoint", "configs"],
+    p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered"],
                    help="run one section alone and print it (for profiling)")
     p.add_argument("--boxes", type=int, default=64, help="boxes of the batched section")
     p.add_argument("--batched-steps", type=int, default=500)
     p.add_argument("--no-tune", action="store_true", help="batched section without the autotuner")
     p.add_argument("--adjoint-steps", type=int, default=200)
     p.add_argument("--no-fd-check", action="store_true")
+    p.add_argument("--no-staggered", action="store_true", help="skip the staggered-field section")
+    p.add_argument("--staggered-n", type=int, default=256)
+    p.add_argument("--staggered-steps", type=int, default=20)
     return p.parse_args()
 
 
@@ -501,6 +504,65 @@ def adjoint_section(local, n=256, steps=200, every=20, fd=True):
     }
 
 
+def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
+    """Staggered-field step (face field by constrained transport): n^3 periodic cells (n a multiple
+    of 64 or below it), a smooth seeded 64^3 state with a divergence-free face field
+    (states.staggered_random) repeated periodically, CFL 0.4.  Timed:
+    `steps` steps launched back to back on the context's stream (two kernels per step), CUDA
+    events.  CPU: the oracle's staggered step on one core on a 32^3 sample."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+
+    sid = pg.SOLVERS[solver]
+    L = (1.0 / n,) * 3
+    # a 64^3 periodic pattern repeated to n^3 (periodic, divergence-free faces; fast to build)
+    m = min(n, 64)
+    reps = (1, n // m, n // m, n // m)
+    U, faces, _ = states.staggered_random((m, m, m), L, np.random.default_rng(20261206), field_amp=0.001 / n)
+    U, faces = np.tile(U, reps), np.tile(faces, reps)
+    cfg = pg.Config(n=(n, n, n), solver=sid, cell_length=L, adiabatic_index=5 / 3, vacuum_permeability=1.0,
+                    time_step_factor=0.4, device=local)
+    with pg.StaggeredContext(cfg) as ctx:
+        ctx.set_state(U, faces)
+        ctx.step(0.0)
+        ctx.steps(3, T_END)
+        ctx.sync()
+        st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        ctx.steps(steps, T_END)
+        e1.record(st)
+        ctx.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+    out = {
+        "workload": f"{n}^3 periodic, {solver}, smooth state with a divergence-free face field, CFL 0.4",
+        "value": n ** 3 / (ms * 1e-3),
+        "unit": UNIT,
+        "ms_per_step": ms,
+        "steps": steps,
+        "gpu_launches": 2 * steps,
+    }
+    if cpu:
+        from oracle import pyoracle as po
+        m = 32
+        Uc, Fc, Lc = states.staggered_random((m, m, m), (1.0 / m,) * 3, np.random.default_rng(20261206),
+                                             field_amp=0.001 / m)
+        g = po.Oracle("port").staggered_grid(po.make_cfg((m, m, m), sid, Lc, 5 / 3, 1.0, 0.4))
+        g.set_state(Uc, Fc)
+        g.step(0.0)
+        t0 = time.perf_counter()
+        k = 3
+        for _ in range(k):
+            g.step(T_END)
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": m ** 3 * k / sec, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"oracle staggered step, {m}^3, {k} steps"}
+    return out
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -719,6 +781,9 @@ def run_b200(a):
         line["adjoint"] = adjoint_section(local, steps=a.adjoint_steps, fd=not a.no_fd_check)
     if not a.no_configs and world == 1:
         line["configs"] = configs_section(local, cpu=rank == 0 and not a.no_cpu_baseline)
+    if not a.no_staggered and world == 1:
+        line["staggered"] = staggered_section(local, n=a.staggered_n, steps=a.staggered_steps,
+                                              cpu=rank == 0 and not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)
@@ -743,6 +808,8 @@ def run_only(a):
                               sequential=False)
     elif a.only == "adjoint":
         out = adjoint_section(local, steps=a.adjoint_steps, fd=not a.no_fd_check)
+    elif a.only == "staggered":
+        out = staggered_section(local, n=a.staggered_n, steps=a.staggered_steps, cpu=not a.no_cpu_baseline)
     else:
         out = configs_section(local, cpu=not a.no_cpu_baseline)
     print(json.dumps({a.only: out}), flush=True)

@@ -12,20 +12,22 @@ Data in HBM, every array x fastest over the n0 x n1 x n2 cells, no ghosts
 A dimension of one cell is its own neighbour, as in the reference's emulated
 1-D and 2-D runs: its faces are solved with the cell on both sides.
 
-One step is two launches on the context's stream:
+One step is three launches on the context's stream:
   faces_kernel   every cell solves its three -d faces (the +d faces of its
                  -d neighbours, get_fluxes, mhd/solve.hpp:217-392), stores
                  the unrotated flux, and max-reduces the face speeds per
                  axis into a three-slot ring, as the fused cell-centred step;
-  update_kernel  dt from the previous step's speeds and the cap (lagged CFL
+  field_kernel   dt from the previous step's speeds and the cap (lagged CFL
                  rule, mhd/solve.hpp:1933-2007, substepping.hpp:285-338);
-                 the cell update of update_mhd_state (mhd/solve.hpp:
-                 1543-1602); the new normal field of the cell's six faces from
+                 the new normal field of every cell's three -d faces from
                  the twelve edge terms of assign_face_dBs_f{x,y,z}
-                 (mhd/solve.hpp:587-1494, equal-size neighbours); the cell
-                 writes its own three -d faces; then update_vol_B with
-                 constant thermal pressure twice (mhd/solve.hpp:1631-1683,
-                 :1895-1918), the volume field the mean of each pair of faces.
+                 (mhd/solve.hpp:587-1494, equal-size neighbours) and
+                 Face_B += Face_dB / area (mhd/solve.hpp:1589-1593);
+  cell_kernel    the same dt; the cell update of update_mhd_state
+                 (mhd/solve.hpp:1543-1587), then update_vol_B with constant
+                 thermal pressure twice (mhd/solve.hpp:1631-1683,
+                 :1895-1918), the volume field the mean of each pair of new
+                 faces; advances the clock ring.
 This file is compiled without FMA contraction and writes the cell and face
 updates in the same operation order as the CPU oracle, so that given the same
 face fluxes both compute the same bits.
@@ -44,6 +46,8 @@ using namespace pamhd_b200;
 namespace {
 
 constexpr int THREADS = 256;
+// the face solves: 128 threads, three resident blocks per SM (two for Roe's larger register set)
+constexpr int FACE_THREADS = 128;
 
 struct Stag_Params {
 	const double* __restrict__ U;    // 8 x N
@@ -144,7 +148,7 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 template <int SOLVER>
-__global__ void __launch_bounds__(THREADS) faces_kernel(const Stag_Params P)
+__global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3) faces_kernel(const Stag_Params P)
 {
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	bool zero = false;
@@ -262,18 +266,58 @@ __device__ __forceinline__ void vol_B_constant_pressure(double u[8], const doubl
 	u[4] = p / (g.gamma - 1) + kinetic + magnetic;
 }
 
-__global__ void __launch_bounds__(THREADS) update_kernel(const Stag_Params P)
+// the step's dt, or whether it is skipped: a failed face leaves the state as it was; so does a step past t_end
+__device__ __forceinline__ double step_start(const Stag_Params& P, bool& skip)
+{
+	const Clock c = P.clock[P.phase];
+	skip = P.status->flags != 0u or (P.max_dt < 0.0 and c.t >= P.t_end);
+	return skip ? 0.0 : step_dt(P);
+}
+
+// Face_B += Face_dB / area for the three -d faces of every cell
+__global__ void __launch_bounds__(THREADS) field_kernel(const Stag_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
 	if (threadIdx.x == 0) {
-		const Clock c = P.clock[P.phase];
-		// a failed face leaves the state as it was; so does a step past t_end
-		const bool skip = P.status->flags != 0u or (P.max_dt < 0.0 and c.t >= P.t_end);
-		const double dt = skip ? 0.0 : step_dt(P);
+		bool skip;
+		s_dt = step_start(P, skip);
+		s_skip = skip ? 1 : 0;
+	}
+	__syncthreads();
+	const double dt = s_dt;
+	const bool skip = s_skip != 0;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		if (skip) {
+			#pragma unroll
+			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
+			continue;
+		}
+		int i, j, k;
+		cell_coords(P, c, i, j, k);
+		P.Bo[c] = P.B[c] + face_dB<0>(P, i, j, k, dt) / P.area[0];
+		P.Bo[P.N + c] = P.B[P.N + c] + face_dB<1>(P, i, j, k, dt) / P.area[1];
+		P.Bo[2 * P.N + c] = P.B[2 * P.N + c] + face_dB<2>(P, i, j, k, dt) / P.area[2];
+	}
+}
+
+/*
+The cell update of update_mhd_state (mass, momentum, energy, volume field;
+x, then y, then z, each flux slot 0 + dt F as the reference accumulates it),
+then update_vol_B twice with the new faces.  Block 0 advances the clock ring.
+*/
+__global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
+{
+	__shared__ double s_dt;
+	__shared__ int s_skip;
+	if (threadIdx.x == 0) {
+		bool skip;
+		const double dt = step_start(P, skip);
 		s_dt = dt;
 		s_skip = skip ? 1 : 0;
 		if (blockIdx.x == 0) {
+			const Clock c = P.clock[P.phase];
 			Clock& next = P.clock[(P.phase + 1) % 3];
 			next.t = skip ? c.t : c.t + dt;
 			next.dt = skip ? c.dt : dt;
@@ -286,70 +330,54 @@ __global__ void __launch_bounds__(THREADS) update_kernel(const Stag_Params P)
 	__syncthreads();
 	const double dt = s_dt;
 	const bool skip = s_skip != 0;
+	const long long N = P.N;
 	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
 		if (skip) {
 			#pragma unroll
-			for (int v = 0; v < 8; v++) P.Uo[v * P.N + c] = P.U[v * P.N + c];
-			#pragma unroll
-			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
+			for (int v = 0; v < 8; v++) P.Uo[v * N + c] = P.U[v * N + c];
 			continue;
 		}
 		int i, j, k;
 		cell_coords(P, c, i, j, k);
 		const long long up[3] = {wrap_index(P, i + 1, j, k), wrap_index(P, i, j + 1, k), wrap_index(P, i, j, k + 1)};
+		auto fm = [&](const int d, const int v) { return 0 + dt * P.F[(d * 8 + v) * N + c]; };
+		auto fp = [&](const int d, const int v) { return 0 + dt * P.F[(d * 8 + v) * N + up[d]]; };
 		double u[8];
 		#pragma unroll
-		for (int v = 0; v < 8; v++) u[v] = P.U[v * P.N + c];
-		// dt-scaled fluxes of the -d and +d faces, as the flux slots of the reference (0 + dt F)
-		double fm[3][8], fp[3][8];
+		for (int v = 0; v < 8; v++) u[v] = P.U[v * N + c];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) u[0] += (fm(d, 0) - fp(d, 0)) / P.len[d];
 		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			#pragma unroll
-			for (int v = 0; v < 8; v++) {
-				fm[d][v] = 0 + dt * P.F[(d * 8 + v) * P.N + c];
-				fp[d][v] = 0 + dt * P.F[(d * 8 + v) * P.N + up[d]];
-			}
+			for (int e = 1; e <= 3; e++) u[e] = u[e] + P.inv_len[d] * (fm(d, e) + (-fp(d, e)));
 		}
-		// update_mhd_state: mass, momentum, energy, volume field; x, then y, then z
 		#pragma unroll
-		for (int d = 0; d < 3; d++) u[0] += (fm[d][0] - fp[d][0]) / P.len[d];
+		for (int d = 0; d < 3; d++) u[4] += (fm(d, 4) - fp(d, 4)) / P.len[d];
 		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			#pragma unroll
-			for (int e = 1; e <= 3; e++) u[e] = u[e] + P.inv_len[d] * (fm[d][e] + (-fp[d][e]));
+			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (fm(d, e) + (-fp(d, e)));
 		}
-		#pragma unroll
-		for (int d = 0; d < 3; d++) u[4] += (fm[d][4] - fp[d][4]) / P.len[d];
-		#pragma unroll
-		for (int d = 0; d < 3; d++) {
-			#pragma unroll
-			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (fm[d][e] + (-fp[d][e]));
-		}
-		// Face_B += Face_dB / area for the six faces of the cell
-		const double bm0 = P.B[c] + face_dB<0>(P, i, j, k, dt) / P.area[0];
-		const double bm1 = P.B[P.N + c] + face_dB<1>(P, i, j, k, dt) / P.area[1];
-		const double bm2 = P.B[2 * P.N + c] + face_dB<2>(P, i, j, k, dt) / P.area[2];
-		const double bp0 = P.B[up[0]] + face_dB<0>(P, i + 1, j, k, dt) / P.area[0];
-		const double bp1 = P.B[P.N + up[1]] + face_dB<1>(P, i, j + 1, k, dt) / P.area[1];
-		const double bp2 = P.B[2 * P.N + up[2]] + face_dB<2>(P, i, j, k + 1, dt) / P.area[2];
-		P.Bo[c] = bm0;
-		P.Bo[P.N + c] = bm1;
-		P.Bo[2 * P.N + c] = bm2;
-		const double mean[3] = {0.5 * (bm0 + bp0), 0.5 * (bm1 + bp1), 0.5 * (bm2 + bp2)};
+		const double mean[3] = {0.5 * (P.Bo[c] + P.Bo[up[0]]),
+		                        0.5 * (P.Bo[N + c] + P.Bo[N + up[1]]),
+		                        0.5 * (P.Bo[2 * N + c] + P.Bo[2 * N + up[2]])};
 		vol_B_constant_pressure(u, mean, P.gas);
 		vol_B_constant_pressure(u, mean, P.gas);
 		#pragma unroll
-		for (int v = 0; v < 8; v++) P.Uo[v * P.N + c] = u[v];
+		for (int v = 0; v < 8; v++) P.Uo[v * N + c] = u[v];
 	}
 }
 
 template <int SOLVER>
 int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 {
-	faces_kernel<SOLVER><<<grid, THREADS, 0, stream>>>(P);
+	faces_kernel<SOLVER><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
-	update_kernel<<<grid, THREADS, 0, stream>>>(P);
+	field_kernel<<<grid, THREADS, 0, stream>>>(P);
+	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
+	cell_kernel<<<grid, THREADS, 0, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
