@@ -508,7 +508,7 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
     """Staggered-field step (face field by constrained transport): n^3 periodic cells (n a multiple
     of 64 or below it), a smooth seeded 64^3 state with a divergence-free face field
     (states.staggered_random) repeated periodically, CFL 0.4.  Timed:
-    `steps` steps launched back to back on the context's stream (two kernels per step), CUDA
+    `steps` steps launched back to back on the context's stream (three kernels per step), CUDA
     events.  CPU: the oracle's staggered step on one core on a 32^3 sample."""
     import torch
     import pamhd_b200 as pg
@@ -543,7 +543,7 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
         "unit": UNIT,
         "ms_per_step": ms,
         "steps": steps,
-        "gpu_launches": 2 * steps,
+        "gpu_launches": 3 * steps,
     }
     if cpu:
         from oracle import pyoracle as po

@@ -4,7 +4,9 @@ pamhd_gpu.h - C ABI of the B200 (sm_100a) finite-volume MHD step.
 This is the drop-in boundary for PAMHD's cell-centred ("Mode C") MHD step
 on uniform Cartesian grids: the conservative state (mass density, momentum
 density, total energy density, magnetic field), the Rusanov / HLL / HLLD /
-Roe face fluxes, flux application and the lagged CFL timestep rule.
+Roe face fluxes, flux application and the lagged CFL timestep rule; and for
+its staggered-field step (face magnetic field by constrained transport,
+pamhd_gpu_staggered_*) on uniform periodic grids.
 Host code (C or C++) calls these entry points with plain pointers and
 sizes; no C++ types, exceptions or torch types cross this boundary.
 
@@ -436,6 +438,13 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** ctx);
 int pamhd_gpu_staggered_destroy(pamhd_stag* ctx);
 int pamhd_gpu_staggered_set_state(pamhd_stag* ctx, const double* const cells[8], const double* const faces[3]);
 int pamhd_gpu_staggered_get_state(pamhd_stag* ctx, double* const cells[8], double* const faces[3]);
+/*
+Background magnetic field of every face (the reference's Bg_B, mhd/solve.hpp:120-121):
+bg[3 d + c][cell] is component c at the cell's -d face; NULL removes it.  Rusanov and HLL
+use it in the flux and the fast speeds, HLLD and Roe ignore it (as the reference's solvers,
+mhd/hlld_athena.hpp:77).  The cell state and the faces hold the field without it.
+*/
+int pamhd_gpu_staggered_set_background(pamhd_stag* ctx, const double* const bg[9]);
 int pamhd_gpu_staggered_step(pamhd_stag* ctx, double max_dt, double* dt_taken);
 int pamhd_gpu_staggered_steps(pamhd_stag* ctx, int32_t nsteps, double t_end);
 int pamhd_gpu_staggered_sync(pamhd_stag* ctx);

@@ -233,6 +233,13 @@ int ORACLE_API(sgrid_set_state)(void* grid, const double* const soa[8], const do
 	return PAMHD_OK;
 }
 
+// background field: bg[3 d + c] = component c at every cell's -d face; NULL clears it
+int ORACLE_API(sgrid_set_background)(void* grid, const double* const bg[9])
+{
+	static_cast<SGrid*>(grid)->set_background(bg);
+	return PAMHD_OK;
+}
+
 int ORACLE_API(sgrid_get_state)(void* grid, double* const soa[8], double* const faces[3])
 {
 	static_cast<SGrid*>(grid)->get_state(soa, faces);

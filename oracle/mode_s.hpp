@@ -32,6 +32,14 @@ keep those dimensions, tests/mhd/config_files/.../Alfvén_wave):
   - the lagged CFL rule and the time cap as Mode C.
 Face storage: Bf[d][cell] is the normal field of the cell's -d face; the
 +d face of a cell is the -d face of its +d neighbour.
+
+Background field (optional): Bg[d][cell] is the background field vector at
+the cell's -d face (the reference's Bg_B of the face, integrated over it at
+initialisation, mhd/initialize.hpp:517-530).  The face between a cell and its
++d neighbour is solved with that face's vector, rotated into the face frame
+(mhd/solve.hpp:120-121); the solvers use it as the reference's do (Rusanov
+and HLL in the flux and the fast speeds, HLLD and Roe not at all).  The cell
+state and Face_B hold the field without the background, as in the reference.
 */
 #ifndef PAMHD_ORACLE_MODE_S_HPP
 #define PAMHD_ORACLE_MODE_S_HPP
@@ -54,6 +62,7 @@ public:
 
 	std::vector<double> Bf[3];   // normal field of each cell's -d face
 	std::vector<MHD> FF[3];      // raw flux through each cell's -d face, unrotated
+	std::vector<Vec3> Bg[3];     // background field at each cell's -d face (empty: none)
 
 	explicit Mode_S_Grid(const pamhd_cfg& c) : Base(c)
 	{
@@ -87,6 +96,37 @@ public:
 				Bf[d][this->index(i, j, k)] = faces[d][size_t(i) + size_t(n[0]) * (size_t(j) + size_t(n[1]) * k)];
 			}
 		}
+	}
+
+	// bg[3 d + c]: component c of the background field at every cell's -d face; nullptr clears it
+	void set_background(const double* const bg[9])
+	{
+		for (int d = 0; d < 3; d++) {
+			Bg[d].clear();
+			if (bg == nullptr) continue;
+			Bg[d].resize(U.size());
+			for (int k = 0; k < n[2]; k++)
+			for (int j = 0; j < n[1]; j++)
+			for (int i = 0; i < n[0]; i++) {
+				const size_t src = size_t(i) + size_t(n[0]) * (size_t(j) + size_t(n[1]) * k);
+				Bg[d][this->index(i, j, k)] = {bg[3 * d][src], bg[3 * d + 1][src], bg[3 * d + 2][src]};
+			}
+		}
+	}
+
+	// the face of cell a with its +d neighbour b, with the face's background field (mhd/solve.hpp:80-188)
+	Face_Flux solve_face_bg(const MHD& a, const MHD& b, const int d, const Vec3& bg) const
+	{
+		MHD neg = a, pos = b;
+		neg.mom = get_rotated_vector(a.mom, d + 1);
+		neg.mag = get_rotated_vector(a.mag, d + 1);
+		pos.mom = get_rotated_vector(b.mom, d + 1);
+		pos.mag = get_rotated_vector(b.mag, d + 1);
+		const Vec3 rbg = get_rotated_vector(bg, d + 1);
+		Face_Flux r = this->flux(cfg.solver, neg, pos, rbg, cfg.adiabatic_index, cfg.vacuum_permeability);
+		r.flux.mom = get_rotated_vector(r.flux.mom, -(d + 1));
+		r.flux.mag = get_rotated_vector(r.flux.mag, -(d + 1));
+		return r;
 	}
 
 	void get_state(double* const soa[8], double* const faces[3]) const
@@ -186,7 +226,8 @@ public:
 				const int64_t up = this->plus_neighbor(c, d);
 				Face_Flux r;
 				try {
-					r = this->solve_face(U[idx], U[up], d);
+					r = Bg[d].empty() ? this->solve_face(U[idx], U[up], d)
+					                  : solve_face_bg(U[idx], U[up], d, Bg[d][up]);
 				} catch (const Domain_Error& e) {
 					if (failure.flag == 0) failure = {e.flag, int64_t(idx), d + 1, e.what()};
 					continue;

@@ -138,6 +138,8 @@ class Oracle:
         self._sset.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         self._sget = getattr(L, p + "sgrid_get_state")
         self._sget.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        self._sbg = getattr(L, p + "sgrid_set_background")
+        self._sbg.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         self._sstep = getattr(L, p + "sgrid_step")
         self._sstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                 _P(ctypes.c_int32)]
@@ -281,6 +283,17 @@ class OracleStaggeredGrid:
         rc = self.o._sset(self.h, ptrs, fptrs)
         if rc != 0:
             raise ValueError(self.o.last_error())
+
+    def set_background(self, bg):
+        """bg: (3, 3, nz, ny, nx): bg[d, c] = component c of the background field at every cell's
+        -d face; None clears it."""
+        if bg is None:
+            self.o._sbg(self.h, None)
+            return
+        bg = np.ascontiguousarray(bg, dtype=np.float64).reshape((9,) + self.shape)
+        ptrs = (ctypes.c_void_p * 9)(*[bg[k].ctypes.data for k in range(9)])
+        self._bg_keep = bg
+        self.o._sbg(self.h, ptrs)
 
     def get_state(self):
         U = np.zeros((8,) + self.shape)

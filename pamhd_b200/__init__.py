@@ -353,6 +353,7 @@ class StaggeredContext:
         L.pamhd_gpu_staggered_destroy.argtypes = [V]
         L.pamhd_gpu_staggered_set_state.argtypes = [V, V, V]
         L.pamhd_gpu_staggered_get_state.argtypes = [V, V, V]
+        L.pamhd_gpu_staggered_set_background.argtypes = [V, V]
         L.pamhd_gpu_staggered_step.argtypes = [V, _D, _DP]
         L.pamhd_gpu_staggered_steps.argtypes = [V, ctypes.c_int32, _D]
         L.pamhd_gpu_staggered_sync.argtypes = [V]
@@ -394,6 +395,16 @@ class StaggeredContext:
         fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
         self._check(self.L.pamhd_gpu_staggered_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
                     "pamhd_gpu_staggered_set_state")
+
+    def set_background(self, bg):
+        """bg: (3, 3, nz, ny, nx), bg[d, c] = component c of the background field at every cell's
+        -d face; None removes it."""
+        if bg is None:
+            self._check(self.L.pamhd_gpu_staggered_set_background(self.h, None), "pamhd_gpu_staggered_set_background")
+            return
+        bg = np.ascontiguousarray(bg, dtype=np.float64).reshape((9,) + self.shape)
+        ptrs = (ctypes.c_void_p * 9)(*[bg[k].ctypes.data for k in range(9)])
+        self._check(self.L.pamhd_gpu_staggered_set_background(self.h, ptrs), "pamhd_gpu_staggered_set_background")
 
     def get_state(self):
         U = np.empty((8,) + self.shape)

@@ -55,6 +55,7 @@ struct Stag_Params {
 	const double* __restrict__ B;    // 3 x N
 	double* __restrict__ Bo;
 	double* __restrict__ F;          // (3 x 8) x N
+	const double* __restrict__ bg;   // (3 x 3) x N background field at every cell's -d face, or nullptr
 	int n[3];
 	long long N;
 	Gas gas;
@@ -111,8 +112,32 @@ __device__ __forceinline__ void record_failure(const Stag_Params& P, const uint3
 	atomicMin(&P.status->first, key);
 }
 
-// the -A face of cell c: solved between its -A neighbour (left) and c (right)
-template <int SOLVER, int A>
+/*
+The fast speed of a side with the total field (own + background, in the face
+frame), as get_fast_magnetosonic_speed with a background field
+(mhd/common.hpp:433-490), and its check.
+*/
+__device__ __forceinline__ void with_background(Side& s, const double bg[3], const Gas& g)
+{
+	const double t0 = s.b0 + bg[0], t1 = s.b1 + bg[1], t2 = s.b2 + bg[2];
+	const double t2s = t0 * t0 + t1 * t1 + t2 * t2;
+	const double cs2 = g.gamma * s.p * s.rinv;
+	if (t2s > 0.0) {
+		const double va2 = t2s * g.inv_mu0 * s.rinv;
+		const double sum2 = cs2 + va2;
+		const double to_sqrt = cs2 * cs2 + va2 * va2 + 2.0 * cs2 * va2 * (1.0 - 2.0 * (t0 * t0 / t2s));
+		if (s.bad == 0 and not (is_normal(sum2) and to_sqrt > 0.0 and is_normal(to_sqrt))) {
+			s.bad = PAMHD_FLAG_WAVE_SPEED;
+		}
+		s.cf = sqrt(0.5 * (sum2 + sqrt(fmax(to_sqrt, 0.0))));
+	} else {
+		s.cf = sqrt(fmax(cs2, 0.0));
+	}
+}
+
+// the -A face of cell c: solved between its -A neighbour (left) and c (right); BG: with the
+// face's background field (Rusanov and HLL use it; the reference's HLLD and Roe ignore it)
+template <int SOLVER, int A, bool BG>
 __device__ __forceinline__ void solve_minus_face(const Stag_Params& P, const long long c, const int i, const int j,
                                                  const int k, const double Uc[8], const Derived& dc,
                                                  double& smax, bool& zero)
@@ -123,11 +148,25 @@ __device__ __forceinline__ void solve_minus_face(const Stag_Params& P, const lon
 	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + m);
 	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7],
 	                                                  P.gas);
-	const Side L = make_side<A>(Um, dm);
-	const Side R = make_side<A>(Uc, dc);
+	Side L = make_side<A>(Um, dm);
+	Side R = make_side<A>(Uc, dc);
 	double G[8];
 	uint32_t flag = 0;
-	const double s = solve_face<SOLVER>(L, R, P.gas, G, flag);
+	double s;
+	if (BG) {
+		double b[3];
+		rotate<A>(P.bg[(3 * A) * P.N + c], P.bg[(3 * A + 1) * P.N + c], P.bg[(3 * A + 2) * P.N + c],
+		          b[0], b[1], b[2]);
+		with_background(L, b, P.gas);
+		with_background(R, b, P.gas);
+		flag = L.bad | R.bad;
+		if (flag & PAMHD_FLAG_DENSITY) flag = PAMHD_FLAG_DENSITY;
+		else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
+		s = SOLVER == PAMHD_RUSANOV ? flux_rusanov<true>(L, R, P.gas, G, flag, b)
+		                            : flux_hll<true>(L, R, P.gas, G, flag, b);
+	} else {
+		s = solve_face<SOLVER>(L, R, P.gas, G, flag);
+	}
 	if (flag != 0) record_failure(P, flag, m, A);
 	smax = fmax(smax, s);
 	zero = zero or not (s > 0.0);
@@ -147,7 +186,7 @@ __device__ __forceinline__ double warp_max(double v)
 	return v;
 }
 
-template <int SOLVER>
+template <int SOLVER, bool BG>
 __global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3) faces_kernel(const Stag_Params P)
 {
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -160,9 +199,9 @@ __global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_ROE_ATHENA ? 2 :
 		#pragma unroll
 		for (int v = 0; v < 8; v++) Uc[v] = __ldg(P.U + v * P.N + c);
 		const Derived dc = derive<true, true, true>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
-		solve_minus_face<SOLVER, 0>(P, c, i, j, k, Uc, dc, s0, zero);
-		solve_minus_face<SOLVER, 1>(P, c, i, j, k, Uc, dc, s1, zero);
-		solve_minus_face<SOLVER, 2>(P, c, i, j, k, Uc, dc, s2, zero);
+		solve_minus_face<SOLVER, 0, BG>(P, c, i, j, k, Uc, dc, s0, zero);
+		solve_minus_face<SOLVER, 1, BG>(P, c, i, j, k, Uc, dc, s1, zero);
+		solve_minus_face<SOLVER, 2, BG>(P, c, i, j, k, Uc, dc, s2, zero);
 	}
 	// per-axis maxima of the non-negative speeds, as bit patterns
 	s0 = warp_max(s0);
@@ -373,7 +412,12 @@ __global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
 template <int SOLVER>
 int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 {
-	faces_kernel<SOLVER><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+	constexpr bool USES_BG = SOLVER == PAMHD_RUSANOV or SOLVER == PAMHD_HLL_ATHENA;
+	if (USES_BG and P.bg != nullptr) {
+		faces_kernel<SOLVER, USES_BG><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+	} else {
+		faces_kernel<SOLVER, false><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+	}
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	field_kernel<<<grid, THREADS, 0, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
@@ -398,6 +442,7 @@ struct pamhd_stag {
 	double* U[2] = {nullptr, nullptr};
 	double* B[2] = {nullptr, nullptr};
 	double* F = nullptr;
+	double* bg = nullptr;        // background field, 9 x N, allocated by set_background
 	Speed_Max* red = nullptr;
 	Clock* clock = nullptr;
 	Status* status = nullptr;
@@ -550,6 +595,7 @@ int pamhd_gpu_staggered_destroy(pamhd_stag* x)
 	cudaFree(x->B[0]);
 	cudaFree(x->B[1]);
 	cudaFree(x->F);
+	cudaFree(x->bg);
 	cudaFree(x->red);
 	cudaFree(x->clock);
 	cudaFree(x->status);
@@ -575,6 +621,25 @@ int pamhd_gpu_staggered_set_state(pamhd_stag* x, const double* const cells[8], c
 	                                x->stream)));
 	PAMHD_TRY(reset_ring(*x));
 	x->loaded = true;
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_staggered_set_background(pamhd_stag* x, const double* const bg[9])
+{
+	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	if (bg == nullptr) {
+		x->base.bg = nullptr;
+		return PAMHD_OK;
+	}
+	for (int k = 0; k < 9; k++) if (bg[k] == nullptr) return PAMHD_ERR_ARGUMENT;
+	const size_t n = size_t(x->N);
+	if (x->bg == nullptr) PAMHD_TRY(check(cudaMalloc(&x->bg, 9 * n * sizeof(double))));
+	for (int k = 0; k < 9; k++) {
+		PAMHD_TRY(check(cudaMemcpy(x->bg + k * n, bg[k], n * sizeof(double), cudaMemcpyHostToDevice)));
+	}
+	x->base.bg = x->bg;
 	return PAMHD_OK;
 }
 

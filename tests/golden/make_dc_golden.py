@@ -22,6 +22,8 @@ uniform level-0 grids, periodic):
   alf_r1, alf_r2  tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov{1,2}/
                   mhd_0000000{18,33}.dc: 1 x 10 x 10 cells, volume (1, 2/sqrt 3, 2), travelling
                   and standing wave
+  alf_b1, alf_b2  .../2d/x/small_rusanov_bgB{1,2}/mhd_0000000{18,33}.dc: the same waves with the
+                  field split into a constant background (0, 0.86603, 0.5) and the perturbation
 
 Each case stores: step, time, gamma, mu0, proton mass, the state (8, cells) in the reference's
 variable order (rho, mom xyz, E, B xyz) ordered by cell id, and the cell length.
@@ -40,6 +42,8 @@ CASES = {
     "alf_mx": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/1d/-x/small_rusanov/mhd_000000202.dc",
     "alf_r1": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov1/mhd_000000018.dc",
     "alf_r2": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov2/mhd_000000033.dc",
+    "alf_b1": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov_bgB1/mhd_000000018.dc",
+    "alf_b2": "tests/mhd/reference/magnetohydrodynamic/Alfvén_wave/2d/x/small_rusanov_bgB2/mhd_000000033.dc",
 }
 
 

@@ -298,7 +298,7 @@ def gauss_average(f, a, b):
 
 
 def staggered_state(n, length, start, number_density, velocity, pressure, field, gamma, mu0,
-                    proton_mass=1.0):
+                    proton_mass=1.0, background=None):
     """Initial cell state and face field of the reference's MHD program (tests/mhd/test.cpp:422-456)
     on a uniform periodic grid: the normal field of every face is its 7-point Gauss-Legendre
     average over the face (initialize_magnetic_field, mhd/initialize.hpp:361-547), in a dimension
@@ -306,8 +306,10 @@ def staggered_state(n, length, start, number_density, velocity, pressure, field,
     volume field is the mean of each cell's two faces (update_vol_B); the fluid is set at the
     cell centres (initialize_fluid, mhd/initialize.hpp:77-160: rho = m_p n, mom = rho v, E from
     the pressure, v and the volume field).  The functions take (x, y, z) scalars and return a
-    scalar (number density, pressure) or a 3-sequence (velocity, field).
-    Returns U (8, nz, ny, nx) and faces (3, nz, ny, nx): the field of each cell's -x, -y, -z face."""
+    scalar (number density, pressure) or a 3-sequence (velocity, field, background).
+    Returns U (8, nz, ny, nx) and faces (3, nz, ny, nx): the field of each cell's -x, -y, -z face;
+    with a background field function also bg (3, 3, nz, ny, nx): every component of the
+    background field averaged over each cell's -d face the same way (mhd/initialize.hpp:517-530)."""
     n = [int(v) for v in n]
     L = [float(v) for v in length]
     s = [float(v) for v in start]
@@ -321,33 +323,40 @@ def staggered_state(n, length, start, number_density, velocity, pressure, field,
         return lo + L[d] / 2, lo, hi
 
     faces = np.zeros((3, n[2], n[1], n[0]))
+    bg = None if background is None else np.zeros((3, 3, n[2], n[1], n[0]))
     U = np.zeros((8, n[2], n[1], n[0]))
+
+    def face_average(func, comp, d, geo):
+        # integrate_face_B of mhd/initialize.hpp:361-486 for the cell's -d face
+        a, b = [e for e in range(3) if e != d]   # the two dimensions across the face
+
+        def point(u, v):
+            c = [0.0, 0.0, 0.0]
+            c[d] = geo[d][1]
+            c[a] = u
+            c[b] = v
+            return func(*c)[comp]
+
+        ua, ea = geo[a][1], geo[a][2]
+        ub, eb = geo[b][1], geo[b][2]
+        wa, wb = ea - ua, eb - ub
+        if wa == 0 and wb == 0:
+            return point(ua, ub)
+        if wa == 0:
+            return gauss_average(lambda v: point(ua, v), ub, eb) / wb
+        if wb == 0:
+            return gauss_average(lambda u: point(u, ub), ua, ea) / wa
+        return gauss_average(lambda v: gauss_average(lambda u: point(u, v), ua, ea), ub, eb) / wa / wb
+
     for k in range(n[2]):
         for j in range(n[1]):
             for i in range(n[0]):
                 geo = [bounds(0, i), bounds(1, j), bounds(2, k)]
                 for d in range(3):
-                    a, b = [e for e in range(3) if e != d]   # the two dimensions across the face
-
-                    def point(u, v, d=d, a=a, b=b):
-                        c = [0.0, 0.0, 0.0]
-                        c[d] = geo[d][1]
-                        c[a] = u
-                        c[b] = v
-                        return field(*c)[d]
-
-                    ua, ea = geo[a][1], geo[a][2]
-                    ub, eb = geo[b][1], geo[b][2]
-                    wa, wb = ea - ua, eb - ub
-                    if wa == 0 and wb == 0:
-                        val = point(ua, ub)
-                    elif wa == 0:
-                        val = gauss_average(lambda v: point(ua, v), ub, eb) / wb
-                    elif wb == 0:
-                        val = gauss_average(lambda u: point(u, ub), ua, ea) / wa
-                    else:
-                        val = gauss_average(lambda v: gauss_average(lambda u: point(u, v), ua, ea), ub, eb) / wa / wb
-                    faces[d, k, j, i] = val
+                    faces[d, k, j, i] = face_average(field, d, d, geo)
+                    if bg is not None:
+                        for comp in range(3):
+                            bg[d, comp, k, j, i] = face_average(background, comp, d, geo)
     for k in range(n[2]):
         for j in range(n[1]):
             for i in range(n[0]):
@@ -366,6 +375,8 @@ def staggered_state(n, length, start, number_density, velocity, pressure, field,
                     kinetic = 0.5 * rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
                     magnetic = 0.5 / mu0 * (B[0] * B[0] + B[1] * B[1] + B[2] * B[2])
                     U[4, k, j, i] = p / (gamma - 1) + kinetic + magnetic
+    if bg is not None:
+        return U, faces, bg
     return U, faces
 
 
@@ -390,7 +401,7 @@ def alfven_1d(n=100, sign=1):
     return U, faces, L
 
 
-def alfven_2d(standing=False):
+def alfven_2d(standing=False, background=False):
     """The reference's 2-D Alfven wave on 1 x 10 x 10 level-0 cells (tests/mhd/config_files/
     magnetohydrodynamic/Alfven_wave/2d/x/small_rusanov1.json, travelling; small_rusanov2.json,
     standing): periodic, volume (1, 2/sqrt 3, 2), gamma 5/3, mu0 1, number density 1, pressure
@@ -398,7 +409,9 @@ def alfven_2d(standing=False):
     v = (sin(phase)/1000, -cos(phase)/2000, sqrt 3 cos(phase)/2000), or for the standing wave
     (sin(phase)/1000, sqrt 3/2 - cos(phase)/2000, 0.5 + sqrt 3 cos(phase)/2000);
     B = (sin(phase)/1000, sqrt 3/2 + cos(phase)/2000, 0.5 - sqrt 3 cos(phase)/2000).
-    Returns U, faces, cell lengths."""
+    With background=True (small_rusanov_bgB{1,2}.json): B = (sin(phase)/1000, cos(phase)/2000,
+    -sqrt 3 cos(phase)/2000) on the constant background field (0, 0.86603, 0.5).
+    Returns U, faces, cell lengths (and the background field per face, (3, 3, 10, 10, 1))."""
     import math
     r3 = math.sqrt(3)
     gamma = 1.6666666666666667
@@ -414,11 +427,17 @@ def alfven_2d(standing=False):
 
     def mag(x, y, z):
         s, c = math.sin(phase(y, z)), math.cos(phase(y, z))
+        if background:
+            return (s / 1000, c / 2000, -r3 * c / 2000)
         return (s / 1000, r3 / 2 + c / 2000, 0.5 - r3 * c / 2000)
 
     L = (1.0, 2 / r3 / 10, 0.2)
-    U, faces = staggered_state((1, 10, 10), L, (0, 0, 0), lambda x, y, z: 1.0, vel, lambda x, y, z: 0.1,
-                               mag, gamma, 1.0)
+    out = staggered_state((1, 10, 10), L, (0, 0, 0), lambda x, y, z: 1.0, vel, lambda x, y, z: 0.1,
+                          mag, gamma, 1.0, background=(lambda x, y, z: (0.0, 0.86603, 0.5)) if background else None)
+    if background:
+        U, faces, bg = out
+        return U, faces, L, bg
+    U, faces = out
     return U, faces, L
 
 

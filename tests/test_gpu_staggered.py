@@ -65,17 +65,19 @@ def test_steps_match_oracle(port, solver, shape):
 
 @pytest.mark.parametrize("case", list(STAGGERED_CASES))
 def test_reproduces_reference_program_output(case):
-    """The reference program's Alfven waves (Rusanov, CFL 0.5, t = 0 .. 1), run through the C ABI as
-    the program runs them: same step count and time, every cell within the reference's own
-    comparison (tests/mhd/mhd_diff.py, 1e-15 defaults)."""
+    """The reference program's Alfven waves (Rusanov, CFL 0.5, t = 0 .. 1; with and without a
+    background field), run through the C ABI as the program runs them: same step count and time,
+    every cell within the reference's own comparison (tests/mhd/mhd_diff.py, 1e-15 defaults)."""
     g = _load("dc_goldens.npz")
-    U0, faces, _ = STAGGERED_CASES[case]()
+    U0, faces, _, *bg = STAGGERED_CASES[case]()
     n = (U0.shape[3], U0.shape[2], U0.shape[1])
     cfg = pg.Config(n=n, solver=pg.RUSANOV, cell_length=tuple(g[case + "_cell_length"]),
                     adiabatic_index=float(g[case + "_gamma"]), vacuum_permeability=float(g[case + "_mu0"]),
                     time_step_factor=0.5)
     with pg.StaggeredContext(cfg) as ctx:
         ctx.set_state(U0, faces)
+        if bg:
+            ctx.set_background(bg[0])
         ctx.step(0.0)
         t, steps, t_end = 0.0, 0, float(g[case + "_time"])
         while t < t_end:
@@ -87,6 +89,33 @@ def test_reproduces_reference_program_output(case):
     ref = g[case + "_state"]
     assert _mhd_diff_ok(out, ref)
     assert np.abs(out - ref).max() <= 2e-15
+
+
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+def test_background_field_matches_oracle(port, solver):
+    """A background field that varies over the faces (a uniform field plus a random one), every
+    solver (Rusanov and HLL use it, HLLD and Roe ignore it, as the reference's): per step against
+    the oracle."""
+    L = (0.1, 0.12, 0.09)
+    shape = (5, 6, 7)
+    rng = np.random.default_rng(8)
+    U, faces, _ = states.staggered_random(shape, L, rng)
+    bg = rng.normal(0, 0.05, (3, 3) + shape) + np.array([0.2, 0.4, -0.3])[None, :, None, None, None]
+    gpu, ora = pair(port, (7, 6, 5), po.SOLVERS[solver], L)
+    gpu.set_state(U, faces)
+    ora.set_state(U, faces)
+    gpu.set_background(bg)
+    ora.set_background(bg)
+    for s in range(8):
+        cap = 0.0 if s == 0 else 1.0
+        dg = gpu.step(cap)
+        do, flag, _, _ = ora.step(cap)
+        assert flag == 0
+        assert abs(dg - do) <= 1e-13 * max(do, 1e-300)
+        Ug, Fg = gpu.get_state()
+        Uo, Fo = ora.get_state()
+        assert state_err(Ug, Uo) <= STEP_TOL, s
+        assert face_err(Fg, Fo) <= STEP_TOL, s
 
 
 def test_batched_steps_equal_single_steps(port):

@@ -13,8 +13,8 @@ reference's solvers and step.  These tests hold it to:
     for the cases whose field is zero, where its staggered-field step reduces to the
     cell-centred one: same step count, state within a few ulps after 917 steps;
   - the same program's Alfven-wave outputs, which pin the staggered-field step
-    (oracle/mode_s.hpp): same step count, every cell within the tolerances of the
-    reference's own comparison (tests/mhd/mhd_diff.py:232-241).
+    (oracle/mode_s.hpp), with and without a background field: same step count, every cell
+    within the tolerances of the reference's own comparison (tests/mhd/mhd_diff.py:232-241).
 Bit-for-bit equality is required wherever both sides run the same
 arithmetic (the oracle is built with -ffp-contract=off, as the reference).
 """
@@ -257,6 +257,8 @@ STAGGERED_CASES = {
     "alf_mx": lambda: states.alfven_1d(100, -1),
     "alf_r1": lambda: states.alfven_2d(False),
     "alf_r2": lambda: states.alfven_2d(True),
+    "alf_b1": lambda: states.alfven_2d(False, background=True),
+    "alf_b2": lambda: states.alfven_2d(True, background=True),
 }
 
 
@@ -265,12 +267,14 @@ def run_staggered(grid_owner, case, solver=po.RUSANOV):
     422-537): initial state, the dt = 0 priming step, then steps capped by the time left until
     t = 1.  Returns (state (8, cells), faces (3, cells), steps, t)."""
     g = _load("dc_goldens.npz")
-    U0, faces, _ = STAGGERED_CASES[case]()
+    U0, faces, _, *bg = STAGGERED_CASES[case]()
     n = (U0.shape[3], U0.shape[2], U0.shape[1])
     cfg = po.make_cfg(n, solver, tuple(g[case + "_cell_length"]), float(g[case + "_gamma"]),
                       float(g[case + "_mu0"]), 0.5)
     grid = grid_owner.staggered_grid(cfg)
     grid.set_state(U0, faces)
+    if bg:
+        grid.set_background(bg[0])
     grid.step(0.0)
     t, steps, t_end = 0.0, 0, float(g[case + "_time"])
     while t < t_end:
@@ -297,7 +301,7 @@ def test_mode_s_reproduces_reference_program_output(port, case):
     assert np.abs(out - ref).max() <= 2e-15
 
 
-@pytest.mark.parametrize("case", ["alf_px", "alf_r1"])
+@pytest.mark.parametrize("case", ["alf_px", "alf_r1", "alf_b2"])
 def test_mode_s_restated_solvers_equal_reference_headers(port, ref, case):
     """The staggered step driven by the reference's own solver headers computes the same bits."""
     a = run_staggered(port, case)
