@@ -7,19 +7,22 @@ the staggered-field step (mode_s.hpp).
 
 TEST INFRASTRUCTURE - see mhd_oracle.hpp for who may use this.
 
-The including file defines ORACLE_API(name) (the exported symbol name) and
-ORACLE_FLUX (the solver dispatch functor type).
+The including file defines ORACLE_API(name) (the exported symbol name),
+ORACLE_FLUX (the solver dispatch functor type) and ORACLE_SPLIT (the
+two-population split solver functor type).
 */
 #include <cstdio>
 #include <cstring>
 #include <vector>
 
 #include "mode_s.hpp"
+#include "n_solve.hpp"
 
 namespace {
 
 using Grid = oracle::Mode_C_Grid<ORACLE_FLUX>;
 using SGrid = oracle::Mode_S_Grid<ORACLE_FLUX>;
+using NGrid = oracle::N_Grid<ORACLE_SPLIT>;
 
 thread_local std::string last_error;
 
@@ -260,6 +263,117 @@ int ORACLE_API(sgrid_step)(void* grid, double max_dt, double* dt_taken,
 		g.coords(size_t(g.failure.cell), c);
 		for (int d = 0; d < 3; d++) cell[d] = c[d];
 		*dir = g.failure.dir;
+		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+/*
+Split fluxes of n two-population face problems (total states, face frame):
+neg, pos n x 8; flux_neg, flux_pos n x 8 (already times area and dt);
+speed n; flags n.  Returns the number of failed faces.
+*/
+int64_t ORACLE_API(face_flux_N)(
+	int32_t solver, int64_t n, const double* neg, const double* pos, double area, double dt,
+	double gamma, double mu0, double* flux_neg, double* flux_pos, double* speed, uint32_t* flags)
+{
+	const ORACLE_SPLIT split{};
+	int64_t failed = 0;
+	for (int64_t i = 0; i < n; i++) {
+		oracle::MHD a, b;
+		const double* x = neg + 8 * i;
+		const double* y = pos + 8 * i;
+		a.rho = x[0]; a.mom = {x[1], x[2], x[3]}; a.nrj = x[4]; a.mag = {x[5], x[6], x[7]};
+		b.rho = y[0]; b.mom = {y[1], y[2], y[3]}; b.nrj = y[4]; b.mag = {y[5], y[6], y[7]};
+		double* on = flux_neg + 8 * i;
+		double* op = flux_pos + 8 * i;
+		try {
+			const oracle::Split_Flux r = split(solver, a, b, oracle::Vec3{0, 0, 0}, area, dt, gamma, mu0);
+			const double rn[8] = {r.neg.rho, r.neg.mom[0], r.neg.mom[1], r.neg.mom[2],
+			                      r.neg.nrj, r.neg.mag[0], r.neg.mag[1], r.neg.mag[2]};
+			const double rp[8] = {r.pos.rho, r.pos.mom[0], r.pos.mom[1], r.pos.mom[2],
+			                      r.pos.nrj, r.pos.mag[0], r.pos.mag[1], r.pos.mag[2]};
+			std::memcpy(on, rn, sizeof rn);
+			std::memcpy(op, rp, sizeof rp);
+			speed[i] = r.speed;
+			flags[i] = 0;
+		} catch (const oracle::Domain_Error& e) {
+			for (int k = 0; k < 8; k++) on[k] = op[k] = 0;
+			speed[i] = 0;
+			flags[i] = e.flag;
+			failed++;
+		} catch (const std::exception&) {
+			for (int k = 0; k < 8; k++) on[k] = op[k] = 0;
+			speed[i] = 0;
+			flags[i] = 0x80000000u;
+			failed++;
+		}
+	}
+	return failed;
+}
+
+/*
+The scheme of tests/mhd/two_reference.cpp (see oracle::reference_2pop_1d)
+with this library's split solvers; returns the number of steps or -1.
+*/
+int32_t ORACLE_API(reference_2pop_1d)(int32_t solver, int32_t cells, double t_end, double length, double* out)
+{
+	try {
+		return oracle::reference_2pop_1d(ORACLE_SPLIT{}, solver, cells, t_end, length, out);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return -1;
+	}
+}
+
+// a two-population grid (periodic); NULL on an invalid configuration
+void* ORACLE_API(ngrid_create)(const int32_t n[3], const double len[3], int32_t solver, double gamma, double mu0,
+                               double min_pressure)
+{
+	try {
+		return new NGrid(n[0], n[1], n[2], len[0], len[1], len[2], solver, gamma, mu0, min_pressure);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return nullptr;
+	}
+}
+
+void ORACLE_API(ngrid_destroy)(void* grid)
+{
+	delete static_cast<NGrid*>(grid);
+}
+
+// 13 arrays: rho1, mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz
+int ORACLE_API(ngrid_set_state)(void* grid, const double* const a[13])
+{
+	static_cast<NGrid*>(grid)->set_state(a);
+	return PAMHD_OK;
+}
+
+int ORACLE_API(ngrid_get_state)(void* grid, double* const a[13])
+{
+	static_cast<NGrid*>(grid)->get_state(a);
+	return PAMHD_OK;
+}
+
+// one step of length dt; *max_dt receives the next step's limit; failures as grid_step
+int ORACLE_API(ngrid_step)(void* grid, double dt, double* max_dt, uint32_t* flag, int32_t cell[3], int32_t* dir)
+{
+	NGrid& g = *static_cast<NGrid*>(grid);
+	*flag = 0;
+	try {
+		*max_dt = g.step(dt);
+	} catch (const oracle::Domain_Error& e) {
+		*flag = e.flag;
+		if (g.failure.cell >= 0) {
+			const int64_t c = g.failure.cell;
+			cell[0] = int32_t(c % g.n[0]);
+			cell[1] = int32_t((c / g.n[0]) % g.n[1]);
+			cell[2] = int32_t(c / (int64_t(g.n[0]) * g.n[1]));
+			*dir = g.failure.dir;
+		}
 		return PAMHD_ERR_PHYSICS;
 	} catch (const std::exception& e) {
 		return fail_with(e.what());

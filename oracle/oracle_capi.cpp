@@ -6,6 +6,7 @@ TEST INFRASTRUCTURE - see mhd_oracle.hpp for who may use this.
 */
 #define ORACLE_API(name) oracle_##name
 #define ORACLE_FLUX oracle::Restated_Solvers
+#define ORACLE_SPLIT oracle::Restated_Split_Solvers
 #include "capi_body.hpp"
 
 extern "C" {

@@ -143,6 +143,25 @@ class Oracle:
         self._sstep = getattr(L, p + "sgrid_step")
         self._sstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                 _P(ctypes.c_int32)]
+        self._face_flux_N = getattr(L, p + "face_flux_N")
+        self._face_flux_N.restype = ctypes.c_int64
+        self._face_flux_N.argtypes = [ctypes.c_int32, ctypes.c_int64, _DP, _DP, _D, _D, _D, _D, _DP, _DP, _DP,
+                                      _P(ctypes.c_uint32)]
+        self._ref2 = getattr(L, p + "reference_2pop_1d")
+        self._ref2.restype = ctypes.c_int32
+        self._ref2.argtypes = [ctypes.c_int32, ctypes.c_int32, _D, _D, _DP]
+        self._ncreate = getattr(L, p + "ngrid_create")
+        self._ncreate.restype = ctypes.c_void_p
+        self._ncreate.argtypes = [_P(ctypes.c_int32), _DP, ctypes.c_int32, _D, _D, _D]
+        self._ndestroy = getattr(L, p + "ngrid_destroy")
+        self._ndestroy.argtypes = [ctypes.c_void_p]
+        self._nset = getattr(L, p + "ngrid_set_state")
+        self._nset.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._nget = getattr(L, p + "ngrid_get_state")
+        self._nget.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._nstep = getattr(L, p + "ngrid_step")
+        self._nstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
+                                _P(ctypes.c_int32)]
         self._last_error = getattr(L, p + "last_error")
         self._last_error.restype = ctypes.c_char_p
         if kind == "port":
@@ -176,6 +195,31 @@ class Oracle:
         if steps < 0:
             raise RuntimeError(self.last_error())
         return out, steps
+
+    def face_flux_N(self, solver, neg, pos, area=1.0, dt=1.0, gamma=5.0 / 3.0, mu0=1.0):
+        """Two-population split solver on total states (n, 8): returns flux_neg, flux_pos (n, 8),
+        speed (n,), flags (n,)."""
+        neg = np.ascontiguousarray(neg, dtype=np.float64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        n = neg.shape[0]
+        fn, fp = np.zeros((n, 8)), np.zeros((n, 8))
+        speed = np.zeros(n)
+        flags = np.zeros(n, dtype=np.uint32)
+        self._face_flux_N(solver, n, neg.ctypes.data_as(_DP), pos.ctypes.data_as(_DP), area, dt, gamma, mu0,
+                          fn.ctypes.data_as(_DP), fp.ctypes.data_as(_DP), speed.ctypes.data_as(_DP),
+                          flags.ctypes.data_as(_P(ctypes.c_uint32)))
+        return fn, fp, speed, flags
+
+    def reference_2pop_1d(self, solver, cells=1002, t_end=1.0, length=1e5):
+        """The scheme of tests/mhd/two_reference.cpp: (cells, 13) state and the step count."""
+        out = np.zeros((cells, 13))
+        steps = self._ref2(solver, cells, t_end, length, out.ctypes.data_as(_DP))
+        if steps < 0:
+            raise RuntimeError(self.last_error())
+        return out, steps
+
+    def two_population_grid(self, n, length, solver, gamma, mu0, min_pressure) -> "OracleTwoPopulationGrid":
+        return OracleTwoPopulationGrid(self, n, length, solver, gamma, mu0, min_pressure)
 
     def grid(self, cfg: Cfg, threads: int = 1) -> "OracleGrid":
         return OracleGrid(self, cfg, threads)
@@ -317,3 +361,46 @@ class OracleStaggeredGrid:
         if rc not in (0, 3):
             raise ValueError(self.o.last_error())
         return dt.value, flag.value, tuple(cell), d.value
+
+
+class OracleTwoPopulationGrid:
+    """A two-population grid in the oracle (N_solve + apply_fluxes_N, periodic).  State arrays are
+    (13, nz, ny, nx): rho1, mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz."""
+
+    def __init__(self, oracle: Oracle, n, length, solver, gamma, mu0, min_pressure):
+        self.o = oracle
+        self.shape = (int(n[2]), int(n[1]), int(n[0]))
+        nn = (ctypes.c_int32 * 3)(*[int(v) for v in n])
+        ll = (ctypes.c_double * 3)(*[float(v) for v in length])
+        self.h = oracle._ncreate(nn, ll, solver, gamma, mu0, min_pressure)
+        if not self.h:
+            raise ValueError(oracle.last_error())
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.o._ndestroy(h)
+            self.h = None
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((13,) + self.shape)
+        ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
+        self._keep = U
+        self.o._nset(self.h, ptrs)
+
+    def get_state(self):
+        U = np.zeros((13,) + self.shape)
+        ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
+        self.o._nget(self.h, ptrs)
+        return U
+
+    def step(self, dt):
+        """Returns (max_dt for the next step, flag, cell, dir)."""
+        m = ctypes.c_double(0)
+        flag = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.o._nstep(self.h, dt, ctypes.byref(m), ctypes.byref(flag), cell, ctypes.byref(d))
+        if rc not in (0, 3):
+            raise ValueError(self.o.last_error())
+        return m.value, flag.value, tuple(cell), d.value

@@ -54,6 +54,9 @@ using HD_Primitive = gensimcell::Cell<
 
 struct HD_State_Conservative { using data_type = HD_Conservative; };
 struct HD_Flux_Conservative { using data_type = HD_Conservative; };
+// the second population of tests/mhd/two_reference.cpp (mhd/variables.hpp:163-164)
+struct HD2_State_Conservative { using data_type = HD_Conservative; };
+struct HD2_Flux_Conservative { using data_type = HD_Conservative; };
 
 namespace detail {
 using MHD = gensimcell::Cell<

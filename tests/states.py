@@ -469,3 +469,24 @@ def staggered_random(shape, L, rng, amp=0.05, field_amp=0.01, mean_field=(0.3, -
     U[7] = 0.5 * (faces[2] + r(faces[2], 0))
     U[4] = energy(rho, v, p, U[5:8], gamma)
     return U, faces, L
+
+
+def two_population_random(shape, rng, gamma=GAMMA_53, mu0=1.0, amp=0.1):
+    """Two fluid populations sharing one field, smooth and periodic: (13, nz, ny, nx) with rho1,
+    mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz.  Each population's energy holds its own thermal and
+    kinetic energy plus its mass fraction's share of the field energy, so that the total state has
+    the total pressure of both."""
+    a = smooth_3d(tuple(shape), rng, gamma=gamma, amp=amp)
+    b = smooth_3d(tuple(shape), rng, gamma=gamma, amp=amp)
+    B = a[5:8]
+    rho1, rho2 = a[0], 0.5 * b[0]
+    v1, v2 = a[1:4] / a[0], b[1:4] / b[0] + np.array([0.05, -0.02, 0.01])[:, None, None, None]
+    p1 = (a[4] - 0.5 * a[0] * (v1 ** 2).sum(axis=0) - 0.5 / mu0 * (B ** 2).sum(axis=0)) * (gamma - 1)
+    p2 = 0.5 * p1
+    f1, f2 = rho1 / (rho1 + rho2), rho2 / (rho1 + rho2)
+    pb = 0.5 / mu0 * (B ** 2).sum(axis=0)
+    U = np.zeros((13,) + tuple(shape))
+    U[0], U[1:4], U[4] = rho1, rho1 * v1, p1 / (gamma - 1) + 0.5 * rho1 * (v1 ** 2).sum(axis=0) + f1 * pb
+    U[5], U[6:9], U[9] = rho2, rho2 * v2, p2 / (gamma - 1) + 0.5 * rho2 * (v2 ** 2).sum(axis=0) + f2 * pb
+    U[10:13] = B
+    return U
