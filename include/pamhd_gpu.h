@@ -452,6 +452,45 @@ int pamhd_gpu_staggered_time(pamhd_stag* ctx, double* time, int64_t* steps, doub
 int pamhd_gpu_staggered_status(pamhd_stag* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
 int pamhd_gpu_staggered_get_stream(pamhd_stag* ctx, void** stream);
 
+/*
+Two-population step: the reference's N_solve + apply_fluxes_N
+(mhd/N_solve.hpp:79-587) on a uniform grid periodic in every dimension
+(dimensions of one cell have no faces).  Two fluid populations share one
+magnetic field; every face is solved for the two cells' total states with
+the split solvers get_flux_N_rusanov (mhd/N_rusanov.hpp:61) or
+get_flux_N_hll (mhd/N_hll_athena.hpp:47, as the reference computes it,
+including its second scaling of the positive side's momentum flux and its
+unscaled field flux), the populations taking their mass fractions' share.
+
+  - create: n, cell_length as pamhd_cfg, solver PAMHD_RUSANOV or
+    PAMHD_HLL_ATHENA, min_pressure the floor apply_fluxes_N raises the
+    total thermal pressure to (mhd/N_solve.hpp:553-583).
+  - set_state / get_state: 13 arrays of n0 n1 n2 doubles, x fastest:
+    rho1, mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz (each population's energy
+    as the reference keeps it; the total state is their sum).
+  - step: one N_solve + apply_fluxes_N with the caller's dt;
+    *max_dt receives the next step's limit, min over faces of
+    d_len / signal speed (what N_solve returns); PAMHD_ERR_PHYSICS when a
+    face failed (the state is left as it was).
+  - run: nsteps steps on the context's stream with the loop of
+    tests/mhd/two_reference.cpp: dt = min(cfl * max_dt, t_end - t), max_dt
+    the previous step's limit (0 before the first step); steps once
+    t >= t_end leave the state unchanged.  Returns at once; sync waits.
+*/
+typedef struct pamhd_npop pamhd_npop;
+
+int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], int32_t solver, double gamma, double mu0,
+                          double min_pressure, int32_t device, pamhd_npop** ctx);
+int pamhd_gpu_npop_destroy(pamhd_npop* ctx);
+int pamhd_gpu_npop_set_state(pamhd_npop* ctx, const double* const state[13]);
+int pamhd_gpu_npop_get_state(pamhd_npop* ctx, double* const state[13]);
+int pamhd_gpu_npop_step(pamhd_npop* ctx, double dt, double* max_dt);
+int pamhd_gpu_npop_run(pamhd_npop* ctx, int32_t nsteps, double cfl, double t_end);
+int pamhd_gpu_npop_sync(pamhd_npop* ctx);
+int pamhd_gpu_npop_time(pamhd_npop* ctx, double* time, int64_t* steps, double* last_dt);
+int pamhd_gpu_npop_status(pamhd_npop* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
+int pamhd_gpu_npop_get_stream(pamhd_npop* ctx, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

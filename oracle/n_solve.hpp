@@ -353,13 +353,14 @@ public:
 		failure = Failure();
 		const double area[3] = {len[1] * len[2], len[0] * len[2], len[0] * len[1]};
 		double max_dt = std::numeric_limits<double>::max();
+		// each cell's +d faces in cell order, as N_solve visits them (mhd/N_solve.hpp:127-172)
 		for (int k = 0; k < n[2]; k++)
 		for (int j = 0; j < n[1]; j++)
 		for (int i = 0; i < n[0]; i++) {
-			const size_t c = at(i, j, k);
+			const size_t m = at(i, j, k);
 			for (int d = 0; d < 3; d++) {
 				if (not active[d]) continue;
-				const size_t m = at(i - (d == 0), j - (d == 1), k - (d == 2));
+				const size_t c = at(i + (d == 0), j + (d == 1), k + (d == 2));
 				Split_Flux f;
 				try {
 					f = solve(U[m], U[c], d, area[d], dt);

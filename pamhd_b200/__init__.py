@@ -446,6 +446,101 @@ class StaggeredContext:
         return f.value, tuple(cell), d.value
 
 
+class TwoPopulationContext:
+    """A pamhd_npop: the two-population step (N_solve + apply_fluxes_N) on one uniform periodic
+    grid.  State arrays are (13, nz, ny, nx): rho1, mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz."""
+
+    def __init__(self, n, cell_length, solver=RUSANOV, adiabatic_index=5.0 / 3.0, vacuum_permeability=1.0,
+                 min_pressure=0.0, device=0):
+        self.L = lib()
+        L = self.L
+        V = ctypes.c_void_p
+        I3 = ctypes.c_int32 * 3
+        D3 = ctypes.c_double * 3
+        L.pamhd_gpu_npop_create.argtypes = [I3, D3, ctypes.c_int32, _D, _D, _D, ctypes.c_int32, _P(V)]
+        L.pamhd_gpu_npop_destroy.argtypes = [V]
+        L.pamhd_gpu_npop_set_state.argtypes = [V, V]
+        L.pamhd_gpu_npop_get_state.argtypes = [V, V]
+        L.pamhd_gpu_npop_step.argtypes = [V, _D, _DP]
+        L.pamhd_gpu_npop_run.argtypes = [V, ctypes.c_int32, _D, _D]
+        L.pamhd_gpu_npop_sync.argtypes = [V]
+        L.pamhd_gpu_npop_time.argtypes = [V, _DP, _P(ctypes.c_int64), _DP]
+        L.pamhd_gpu_npop_status.argtypes = [V, _P(ctypes.c_uint32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        L.pamhd_gpu_npop_get_stream.argtypes = [V, _P(V)]
+        self.shape = (int(n[2]), int(n[1]), int(n[0]))
+        h = ctypes.c_void_p()
+        rc = L.pamhd_gpu_npop_create(I3(*[int(v) for v in n]), D3(*[float(v) for v in cell_length]), int(solver),
+                                     float(adiabatic_index), float(vacuum_permeability), float(min_pressure),
+                                     int(device), ctypes.byref(h))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_npop_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pamhd_gpu_npop_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == ERR_PHYSICS:
+            flags, cell, d = self.status()
+            raise PhysicsError(rc, what, flags, cell, d)
+        if rc != OK:
+            raise PamhdError(rc, what)
+
+    def set_state(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((13,) + self.shape)
+        ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
+        self._check(self.L.pamhd_gpu_npop_set_state(self.h, ptrs), "pamhd_gpu_npop_set_state")
+
+    def get_state(self) -> np.ndarray:
+        U = np.empty((13,) + self.shape)
+        ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
+        self._check(self.L.pamhd_gpu_npop_get_state(self.h, ptrs), "pamhd_gpu_npop_get_state")
+        return U
+
+    def step(self, dt: float) -> float:
+        """One step of length dt; returns the next step's limit (min over faces of d_len / speed)."""
+        m = ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_npop_step(self.h, float(dt), ctypes.byref(m)), "pamhd_gpu_npop_step")
+        return m.value
+
+    def run(self, n: int, cfl: float, t_end: float):
+        self._check(self.L.pamhd_gpu_npop_run(self.h, int(n), float(cfl), float(t_end)), "pamhd_gpu_npop_run")
+
+    def sync(self):
+        self._check(self.L.pamhd_gpu_npop_sync(self.h), "pamhd_gpu_npop_sync")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.pamhd_gpu_npop_get_stream(self.h, ctypes.byref(s)), "pamhd_gpu_npop_get_stream")
+        return s.value or 0
+
+    def time(self):
+        t, n, dt = ctypes.c_double(0), ctypes.c_int64(0), ctypes.c_double(0)
+        self._check(self.L.pamhd_gpu_npop_time(self.h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(dt)),
+                    "pamhd_gpu_npop_time")
+        return t.value, n.value, dt.value
+
+    def status(self):
+        f = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.L.pamhd_gpu_npop_status(self.h, ctypes.byref(f), cell, ctypes.byref(d))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_npop_status")
+        return f.value, tuple(cell), d.value
+
+
 def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
     """Solver-level entry point (pamhd_gpu_face_flux).  neg, pos: (n, 8); bg: (n, 3) or None.
     Returns flux (n, 8), speed (n,), flags (n,); failed faces have flags != 0 (no exception)."""

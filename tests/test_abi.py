@@ -107,3 +107,24 @@ def test_staggered_create_rejects_invalid_config(lib, change):
     assert not h.value
     assert lib.pamhd_gpu_staggered_create(None, None) == pg.ERR_ARGUMENT
     assert lib.pamhd_gpu_staggered_destroy(None) == pg.OK
+
+
+@pytest.mark.parametrize("change", [
+    dict(solver=3),                 # the two-population step has Rusanov and HLL only
+    dict(n=(0, 4, 4)),
+    dict(length=(0.1, 0.0, 0.1)),
+    dict(gamma=1.0),
+    dict(mu0=-1.0),
+    dict(min_pressure=-1.0),
+])
+def test_two_population_create_rejects_invalid_arguments(lib, change):
+    I3, D3 = ctypes.c_int32 * 3, ctypes.c_double * 3
+    lib.pamhd_gpu_npop_create.argtypes = [I3, D3, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+    kw = dict(n=(4, 4, 4), length=(0.1, 0.1, 0.1), solver=pg.RUSANOV, gamma=5 / 3, mu0=1.0, min_pressure=0.0)
+    kw.update(change)
+    h = ctypes.c_void_p()
+    rc = lib.pamhd_gpu_npop_create(I3(*kw["n"]), D3(*kw["length"]), kw["solver"], kw["gamma"], kw["mu0"],
+                                   kw["min_pressure"], 0, ctypes.byref(h))
+    assert rc == pg.ERR_ARGUMENT and not h.value
+    assert lib.pamhd_gpu_npop_destroy(None) == pg.OK
