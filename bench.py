@@ -55,7 +55,7 @@ def args_():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
-    p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered"],
+    p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered", "two_population"],
                    help="run one section alone and print it (for profiling)")
     p.add_argument("--boxes", type=int, default=64, help="boxes of the batched section")
     p.add_argument("--batched-steps", type=int, default=500)
@@ -65,6 +65,8 @@ def args_():
     p.add_argument("--no-staggered", action="store_true", help="skip the staggered-field section")
     p.add_argument("--staggered-n", type=int, default=256)
     p.add_argument("--staggered-steps", type=int, default=20)
+    p.add_argument("--no-two-population", action="store_true", help="skip the two-population section")
+    p.add_argument("--two-population-n", type=int, default=256)
     return p.parse_args()
 
 
@@ -563,6 +565,56 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
     return out
 
 
+def two_population_section(local, n=256, steps=20, cpu=True):
+    """Two-population step (N_solve + apply_fluxes_N, split Rusanov): n^3 periodic cells (n a
+    multiple of 64 or below it), two smooth seeded populations sharing one field
+    (states.two_population_random, a 64^3 pattern repeated), the loop dt = min(0.4 max_dt, t_end - t)
+    on the device.  CPU: the oracle's step on one core on a 32^3 sample."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+
+    m = min(n, 64)
+    reps = (1, n // m, n // m, n // m)
+    U = np.tile(states.two_population_random((m, m, m), np.random.default_rng(20261208)), reps)
+    with pg.TwoPopulationContext((n, n, n), (1.0 / n,) * 3, pg.RUSANOV, 5 / 3, 1.0, 0.0, local) as ctx:
+        ctx.set_state(U)
+        ctx.run(4, 0.4, T_END)
+        ctx.sync()
+        st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        ctx.run(steps, 0.4, T_END)
+        e1.record(st)
+        ctx.sync()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+    out = {
+        "workload": f"{n}^3 periodic, two populations sharing one field, split Rusanov, CFL 0.4",
+        "value": n ** 3 / (ms * 1e-3),
+        "unit": UNIT,
+        "ms_per_step": ms,
+        "steps": steps,
+        "gpu_launches": 2 * steps,
+    }
+    if cpu:
+        from oracle import pyoracle as po
+        k = 32
+        Uc = states.two_population_random((k, k, k), np.random.default_rng(20261208))
+        g = po.Oracle("port").two_population_grid((k, k, k), (1.0 / k,) * 3, po.RUSANOV, 5 / 3, 1.0, 0.0)
+        g.set_state(Uc)
+        max_dt = g.step(0.0)[0]
+        t0 = time.perf_counter()
+        reps_cpu = 3
+        for _ in range(reps_cpu):
+            max_dt = g.step(0.4 * max_dt)[0]
+        sec = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k ** 3 * reps_cpu / sec, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": f"oracle two-population step, {k}^3, {reps_cpu} steps"}
+    return out
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -784,6 +836,9 @@ def run_b200(a):
     if not a.no_staggered and world == 1:
         line["staggered"] = staggered_section(local, n=a.staggered_n, steps=a.staggered_steps,
                                               cpu=rank == 0 and not a.no_cpu_baseline)
+    if not a.no_two_population and world == 1:
+        line["two_population"] = two_population_section(local, n=a.two_population_n,
+                                                        cpu=rank == 0 and not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)
@@ -810,6 +865,8 @@ def run_only(a):
         out = adjoint_section(local, steps=a.adjoint_steps, fd=not a.no_fd_check)
     elif a.only == "staggered":
         out = staggered_section(local, n=a.staggered_n, steps=a.staggered_steps, cpu=not a.no_cpu_baseline)
+    elif a.only == "two_population":
+        out = two_population_section(local, n=a.two_population_n, cpu=not a.no_cpu_baseline)
     else:
         out = configs_section(local, cpu=not a.no_cpu_baseline)
     print(json.dumps({a.only: out}), flush=True)

@@ -49,6 +49,8 @@ using namespace pamhd_b200;
 namespace {
 
 constexpr int THREADS = 256;
+// the face solves: 128 threads, three resident blocks per SM (two for HLL's larger register set)
+constexpr int FACE_THREADS = 128;
 constexpr int NV = 13;
 
 struct Npop_Control {
@@ -410,7 +412,7 @@ __device__ __forceinline__ void minus_face(const Npop_Params& P, const long long
 }
 
 template <int SOLVER>
-__global__ void __launch_bounds__(THREADS) npop_faces_kernel(const Npop_Params P)
+__global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_RUSANOV ? 3 : 2) npop_faces_kernel(const Npop_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
@@ -534,7 +536,7 @@ __global__ void __launch_bounds__(THREADS) npop_update_kernel(const Npop_Params 
 template <int SOLVER>
 int launch_pair(const Npop_Params& P, const int grid, cudaStream_t stream)
 {
-	npop_faces_kernel<SOLVER><<<grid, THREADS, 0, stream>>>(P);
+	npop_faces_kernel<SOLVER><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	npop_update_kernel<<<grid, THREADS, 0, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
