@@ -17,12 +17,14 @@ two-population split solver functor type).
 
 #include "mode_s.hpp"
 #include "n_solve.hpp"
+#include "substep.hpp"
 
 namespace {
 
 using Grid = oracle::Mode_C_Grid<ORACLE_FLUX>;
 using SGrid = oracle::Mode_S_Grid<ORACLE_FLUX>;
 using NGrid = oracle::N_Grid<ORACLE_SPLIT>;
+using LGrid = oracle::Substep_Grid<ORACLE_FLUX>;
 
 thread_local std::string last_error;
 
@@ -377,6 +379,70 @@ int ORACLE_API(ngrid_step)(void* grid, double dt, double* max_dt, uint32_t* flag
 		return PAMHD_ERR_PHYSICS;
 	} catch (const std::exception& e) {
 		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+// a grid with local time stepping (periodic); NULL on an invalid configuration
+void* ORACLE_API(lgrid_create)(const pamhd_cfg* cfg)
+{
+	try {
+		return new LGrid(*cfg);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return nullptr;
+	}
+}
+
+void ORACLE_API(lgrid_destroy)(void* grid)
+{
+	delete static_cast<LGrid*>(grid);
+}
+
+int ORACLE_API(lgrid_set_state)(void* grid, const double* const soa[8])
+{
+	try {
+		static_cast<LGrid*>(grid)->set_interior(soa);
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+int ORACLE_API(lgrid_get_state)(void* grid, double* const soa[8])
+{
+	static_cast<LGrid*>(grid)->get_interior(soa);
+	return PAMHD_OK;
+}
+
+// the substep exponents' bounds of every cell (the options substep-min / substep-max)
+int ORACLE_API(lgrid_set_exponents)(void* grid, const int32_t* mins, const int32_t* maxs)
+{
+	try {
+		static_cast<LGrid*>(grid)->set_exponents(mins, maxs);
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	return PAMHD_OK;
+}
+
+// one step with substeps; *dt_taken its length, *substeps their number, periods[c] each cell's period
+int ORACLE_API(lgrid_step)(void* grid, double max_dt, double* dt_taken, int32_t* substeps, int32_t* periods,
+                           uint32_t* flag)
+{
+	LGrid& g = *static_cast<LGrid*>(grid);
+	*flag = 0;
+	try {
+		*dt_taken = g.step(max_dt);
+	} catch (const oracle::Domain_Error& e) {
+		*flag = e.flag;
+		return PAMHD_ERR_PHYSICS;
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
+	*substeps = g.max_substep;
+	if (periods != nullptr) {
+		for (size_t c = 0; c < g.U.size(); c++) periods[c] = g.period[c];
 	}
 	return PAMHD_OK;
 }

@@ -162,6 +162,20 @@ class Oracle:
         self._nstep = getattr(L, p + "ngrid_step")
         self._nstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                 _P(ctypes.c_int32)]
+        self._lcreate = getattr(L, p + "lgrid_create")
+        self._lcreate.restype = ctypes.c_void_p
+        self._lcreate.argtypes = [_P(Cfg)]
+        self._ldestroy = getattr(L, p + "lgrid_destroy")
+        self._ldestroy.argtypes = [ctypes.c_void_p]
+        self._lset = getattr(L, p + "lgrid_set_state")
+        self._lset.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._lget = getattr(L, p + "lgrid_get_state")
+        self._lget.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._lexp = getattr(L, p + "lgrid_set_exponents")
+        self._lexp.argtypes = [ctypes.c_void_p, _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        self._lstep = getattr(L, p + "lgrid_step")
+        self._lstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_int32), _P(ctypes.c_int32),
+                                _P(ctypes.c_uint32)]
         self._last_error = getattr(L, p + "last_error")
         self._last_error.restype = ctypes.c_char_p
         if kind == "port":
@@ -220,6 +234,9 @@ class Oracle:
 
     def two_population_grid(self, n, length, solver, gamma, mu0, min_pressure) -> "OracleTwoPopulationGrid":
         return OracleTwoPopulationGrid(self, n, length, solver, gamma, mu0, min_pressure)
+
+    def substep_grid(self, cfg: Cfg) -> "OracleSubstepGrid":
+        return OracleSubstepGrid(self, cfg)
 
     def grid(self, cfg: Cfg, threads: int = 1) -> "OracleGrid":
         return OracleGrid(self, cfg, threads)
@@ -404,3 +421,52 @@ class OracleTwoPopulationGrid:
         if rc not in (0, 3):
             raise ValueError(self.o.last_error())
         return m.value, flag.value, tuple(cell), d.value
+
+
+class OracleSubstepGrid:
+    """A cell-centred grid with local time stepping in the oracle (periodic); state (8, nz, ny, nx),
+    exponent bounds (nz, ny, nx) int32."""
+
+    def __init__(self, oracle: Oracle, cfg: Cfg):
+        self.o = oracle
+        self.shape = (cfg.n[2], cfg.n[1], cfg.n[0])
+        self.h = oracle._lcreate(ctypes.byref(cfg))
+        if not self.h:
+            raise ValueError(oracle.last_error())
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.o._ldestroy(h)
+            self.h = None
+
+    def set_state(self, U):
+        ptrs, keep = _soa_in([U[k].reshape(-1) for k in range(8)])
+        if self.o._lset(self.h, ptrs) != 0:
+            raise ValueError(self.o.last_error())
+
+    def get_state(self):
+        U = np.zeros((8,) + self.shape)
+        ptrs = (ctypes.c_void_p * 8)()
+        for k in range(8):
+            ptrs[k] = U[k].ctypes.data
+        self.o._lget(self.h, ptrs)
+        return U
+
+    def set_exponents(self, mins, maxs):
+        a = np.ascontiguousarray(mins, dtype=np.int32).reshape(-1)
+        b = np.ascontiguousarray(maxs, dtype=np.int32).reshape(-1)
+        if self.o._lexp(self.h, a.ctypes.data_as(_P(ctypes.c_int32)), b.ctypes.data_as(_P(ctypes.c_int32))) != 0:
+            raise ValueError(self.o.last_error())
+
+    def step(self, max_dt):
+        """Returns (dt, substeps, periods (nz, ny, nx), flag)."""
+        dt = ctypes.c_double(0)
+        k = ctypes.c_int32(0)
+        periods = np.zeros(self.shape, dtype=np.int32)
+        flag = ctypes.c_uint32(0)
+        rc = self.o._lstep(self.h, max_dt, ctypes.byref(dt), ctypes.byref(k),
+                           periods.ctypes.data_as(_P(ctypes.c_int32)), ctypes.byref(flag))
+        if rc not in (0, 3):
+            raise ValueError(self.o.last_error())
+        return dt.value, k.value, periods, flag.value
