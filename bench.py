@@ -55,7 +55,7 @@ def args_():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
-    p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered", "two_population"],
+    p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered", "two_population", "substep"],
                    help="run one section alone and print it (for profiling)")
     p.add_argument("--boxes", type=int, default=64, help="boxes of the batched section")
     p.add_argument("--batched-steps", type=int, default=500)
@@ -67,6 +67,7 @@ def args_():
     p.add_argument("--staggered-steps", type=int, default=20)
     p.add_argument("--no-two-population", action="store_true", help="skip the two-population section")
     p.add_argument("--two-population-n", type=int, default=256)
+    p.add_argument("--no-substep", action="store_true", help="skip the local time stepping section")
     return p.parse_args()
 
 
@@ -615,6 +616,64 @@ def two_population_section(local, n=256, steps=20, cpu=True):
     return out
 
 
+def substep_section(local, n=128, steps=10, solver="hlld_athena", cpu=True):
+    """Local time stepping: n^3 periodic cells, a smooth seeded state, exponent 0 where y < 0 and 1
+    elsewhere (the regions of tests/mhd/config_files/hydrodynamic/substep/100cells/x2.json), CFL 0.4.
+    Timed: `steps` host-driven steps (each plans its periods on the device, then runs its
+    substeps).  value: cells advanced per second over the step length (every cell once per step);
+    updates_per_s counts each cell's updates (two per step in the period-1 region).  CPU: the
+    oracle on one core on a 24^3 sample."""
+    import torch
+    import pamhd_b200 as pg
+    import states
+
+    m = min(n, 64)
+    reps = (1, n // m, n // m, n // m)
+    U = np.tile(states.smooth_3d((m, m, m), np.random.default_rng(20261209), amp=0.05), reps)
+    y = (np.arange(n) + 0.5) / n - 0.5
+    e = np.broadcast_to(np.where(y < 0, 0, 1)[None, :, None], (n, n, n)).astype(np.int32)
+    cfg = pg.Config(n=(n, n, n), solver=pg.SOLVERS[solver], cell_length=(1.0 / n,) * 3, adiabatic_index=5 / 3,
+                    vacuum_permeability=1.0, time_step_factor=0.4, device=local)
+    with pg.SubstepContext(cfg) as ctx:
+        ctx.set_state(U)
+        ctx.set_exponents(e, e)
+        ctx.step(0.0)
+        ctx.step(T_END)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        subs = 0
+        for _ in range(steps):
+            subs += ctx.step(T_END)[1]
+        sec = time.perf_counter() - t0
+        periods = ctx.periods()
+    updates = float((subs / steps) * (1.0 / periods).sum())
+    out = {
+        "workload": f"{n}^3 periodic, {solver}, exponent 0 for y < 0 and 1 elsewhere, CFL 0.4",
+        "value": n ** 3 * steps / sec,
+        "unit": "cell-steps/s",
+        "updates_per_s": updates * steps / sec,
+        "ms_per_step": 1e3 * sec / steps,
+        "substeps_per_step": subs / steps,
+        "timing": "host clock around synchronous steps (each step plans on the device and reads the plan back)",
+    }
+    if cpu:
+        from oracle import pyoracle as po
+        k = 24
+        Uc = states.smooth_3d((k, k, k), np.random.default_rng(20261209), amp=0.05)
+        yc = (np.arange(k) + 0.5) / k - 0.5
+        ec = np.broadcast_to(np.where(yc < 0, 0, 1)[None, :, None], (k, k, k)).astype(np.int32)
+        g = po.Oracle("port").substep_grid(po.make_cfg((k, k, k), pg.SOLVERS[solver], (1.0 / k,) * 3, 5 / 3, 1.0, 0.4))
+        g.set_state(Uc)
+        g.set_exponents(ec, ec)
+        g.step(0.0)
+        t0 = time.perf_counter()
+        for _ in range(2):
+            g.step(T_END)
+        out["cpu_baseline"] = {"value": k ** 3 * 2 / (time.perf_counter() - t0), "unit": "cell-steps/s",
+                               "cores": 1, "kind": "port", "sample": f"oracle substepped step, {k}^3, 2 steps"}
+    return out
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -839,6 +898,8 @@ def run_b200(a):
     if not a.no_two_population and world == 1:
         line["two_population"] = two_population_section(local, n=a.two_population_n,
                                                         cpu=rank == 0 and not a.no_cpu_baseline)
+    if not a.no_substep and world == 1:
+        line["substep"] = substep_section(local, cpu=rank == 0 and not a.no_cpu_baseline)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(U, n)
@@ -867,6 +928,8 @@ def run_only(a):
         out = staggered_section(local, n=a.staggered_n, steps=a.staggered_steps, cpu=not a.no_cpu_baseline)
     elif a.only == "two_population":
         out = two_population_section(local, n=a.two_population_n, cpu=not a.no_cpu_baseline)
+    elif a.only == "substep":
+        out = substep_section(local, cpu=not a.no_cpu_baseline)
     else:
         out = configs_section(local, cpu=not a.no_cpu_baseline)
     print(json.dumps({a.only: out}), flush=True)

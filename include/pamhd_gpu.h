@@ -491,6 +491,37 @@ int pamhd_gpu_npop_time(pamhd_npop* ctx, double* time, int64_t* steps, double* l
 int pamhd_gpu_npop_status(pamhd_npop* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
 int pamhd_gpu_npop_get_stream(pamhd_npop* ctx, void** stream);
 
+/*
+Cell-centred step with local time stepping: the reference's timestep() with
+substeps (mhd/solve.hpp:1837-1924, substepping.hpp) on a uniform grid
+periodic in every dimension.  Every cell advances with a period of 2^k
+substeps of one common substep length; k is bounded by the caller's
+per-cell exponents (the reference's "substep-min" and "substep-max"
+options evaluated at the cell), by the cell's CFL limit against the
+substep and by its neighbours' (at most one above any face or edge
+neighbour).  With every exponent 0 this is pamhd_gpu_step's rule.
+
+  - create: cfg as pamhd_gpu_create, every side PAMHD_BC_PERIODIC.
+  - set_state / get_state: as pamhd_gpu_set_state; set_state clears the
+    face speeds, so the next step is the dt = 0 priming step when called
+    with max_dt = 0.
+  - set_exponents: n0 n1 n2 int32 minima and maxima, 0 .. 30 (default 0).
+  - step: one step capped by max_dt; *dt_taken its length (the substep
+    added once per substep), *substeps their number; PAMHD_ERR_PHYSICS
+    when a face failed (the step stops at that substep).  Synchronises.
+  - periods: the last step's period of every cell.
+*/
+typedef struct pamhd_sub pamhd_sub;
+
+int pamhd_gpu_substep_create(const pamhd_cfg* cfg, pamhd_sub** ctx);
+int pamhd_gpu_substep_destroy(pamhd_sub* ctx);
+int pamhd_gpu_substep_set_state(pamhd_sub* ctx, const double* const cells[8]);
+int pamhd_gpu_substep_get_state(pamhd_sub* ctx, double* const cells[8]);
+int pamhd_gpu_substep_set_exponents(pamhd_sub* ctx, const int32_t* mins, const int32_t* maxs);
+int pamhd_gpu_substep_step(pamhd_sub* ctx, double max_dt, double* dt_taken, int32_t* substeps);
+int pamhd_gpu_substep_periods(pamhd_sub* ctx, int32_t* periods);
+int pamhd_gpu_substep_status(pamhd_sub* ctx, uint32_t* flags, int32_t cell[3], int32_t* dir);
+
 #ifdef __cplusplus
 }
 #endif

@@ -541,6 +541,95 @@ class TwoPopulationContext:
         return f.value, tuple(cell), d.value
 
 
+class SubstepContext:
+    """A pamhd_sub: the cell-centred step with local time stepping on one uniform periodic grid.
+    State arrays (8, nz, ny, nx) as Context; exponent bounds (nz, ny, nx) int32."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.L = lib()
+        L = self.L
+        V = ctypes.c_void_p
+        I = _P(ctypes.c_int32)
+        L.pamhd_gpu_substep_create.argtypes = [_P(_Cfg), _P(V)]
+        L.pamhd_gpu_substep_destroy.argtypes = [V]
+        L.pamhd_gpu_substep_set_state.argtypes = [V, V]
+        L.pamhd_gpu_substep_get_state.argtypes = [V, V]
+        L.pamhd_gpu_substep_set_exponents.argtypes = [V, I, I]
+        L.pamhd_gpu_substep_step.argtypes = [V, _D, _DP, I]
+        L.pamhd_gpu_substep_periods.argtypes = [V, I]
+        L.pamhd_gpu_substep_status.argtypes = [V, _P(ctypes.c_uint32), I, I]
+        self.shape = (int(cfg.n[2]), int(cfg.n[1]), int(cfg.n[0]))
+        self._c = cfg.to_c()
+        h = ctypes.c_void_p()
+        rc = L.pamhd_gpu_substep_create(ctypes.byref(self._c), ctypes.byref(h))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_substep_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pamhd_gpu_substep_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == ERR_PHYSICS:
+            flags, cell, d = self.status()
+            raise PhysicsError(rc, what, flags, cell, d)
+        if rc != OK:
+            raise PamhdError(rc, what)
+
+    def set_state(self, U: np.ndarray):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shape)
+        self._check(self.L.pamhd_gpu_substep_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_substep_set_state")
+
+    def get_state(self) -> np.ndarray:
+        U = np.empty((8,) + self.shape)
+        self._check(self.L.pamhd_gpu_substep_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
+                    "pamhd_gpu_substep_get_state")
+        return U
+
+    def set_exponents(self, mins, maxs):
+        a = np.ascontiguousarray(mins, dtype=np.int32).reshape(-1)
+        b = np.ascontiguousarray(maxs, dtype=np.int32).reshape(-1)
+        I = _P(ctypes.c_int32)
+        self._check(self.L.pamhd_gpu_substep_set_exponents(self.h, a.ctypes.data_as(I), b.ctypes.data_as(I)),
+                    "pamhd_gpu_substep_set_exponents")
+
+    def step(self, max_dt: float):
+        """Returns (dt, substeps)."""
+        dt = ctypes.c_double(0)
+        k = ctypes.c_int32(0)
+        self._check(self.L.pamhd_gpu_substep_step(self.h, float(max_dt), ctypes.byref(dt), ctypes.byref(k)),
+                    "pamhd_gpu_substep_step")
+        return dt.value, k.value
+
+    def periods(self) -> np.ndarray:
+        p = np.empty(self.shape, dtype=np.int32)
+        self._check(self.L.pamhd_gpu_substep_periods(self.h, p.ctypes.data_as(_P(ctypes.c_int32))),
+                    "pamhd_gpu_substep_periods")
+        return p
+
+    def status(self):
+        f = ctypes.c_uint32(0)
+        cell = (ctypes.c_int32 * 3)()
+        d = ctypes.c_int32(0)
+        rc = self.L.pamhd_gpu_substep_status(self.h, ctypes.byref(f), cell, ctypes.byref(d))
+        if rc != OK:
+            raise PamhdError(rc, "pamhd_gpu_substep_status")
+        return f.value, tuple(cell), d.value
+
+
 def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
     """Solver-level entry point (pamhd_gpu_face_flux).  neg, pos: (n, 8); bg: (n, 3) or None.
     Returns flux (n, 8), speed (n,), flags (n,); failed faces have flags != 0 (no exception)."""

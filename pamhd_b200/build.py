@@ -26,8 +26,8 @@ OBJ = os.path.join(PKG, "_build")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "-I", os.path.join(ROOT, "include")]
-# per-file flags: the staggered and two-population steps round every operation as the CPU oracle does
-FILE_FLAGS = {"staggered.cu": ["-fmad=false"], "npop.cu": ["-fmad=false"]}
+# per-file flags: these steps round their updates as the CPU oracle does
+FILE_FLAGS = {"staggered.cu": ["-fmad=false"], "npop.cu": ["-fmad=false"], "substep.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

@@ -171,6 +171,25 @@ __device__ __forceinline__ void unrotate(const double r0, const double r1, const
 	if (AXIS == 2) { a = r1; b = r2; c = r0; }
 }
 
+// a cell's state (8 values, xyz frame) and derived quantities seen from a face normal to axis A
+template <int A>
+__device__ __forceinline__ Side side_of(const double U[8], const Derived& d)
+{
+	Side s;
+	s.rho = U[0];
+	rotate<A>(U[1], U[2], U[3], s.m0, s.m1, s.m2);
+	s.E = U[4];
+	rotate<A>(U[5], U[6], U[7], s.b0, s.b1, s.b2);
+	s.rinv = d.rinv;
+	s.p = d.p;
+	s.cf = d.cf[A];
+	s.v0 = s.m0 * s.rinv;
+	s.v1 = s.m1 * s.rinv;
+	s.v2 = s.m2 * s.rinv;
+	s.bad = d.bad;
+	return s;
+}
+
 /*
 Ideal-MHD flux along the face normal, mhd/common.hpp:146-244, with the
 background field zero (every configuration of the fused step).  pb is the

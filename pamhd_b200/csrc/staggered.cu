@@ -86,24 +86,6 @@ __device__ __forceinline__ void cell_coords(const Stag_Params& P, const long lon
 	k = int(c / ((long long)P.n[0] * P.n[1]));
 }
 
-template <int A>
-__device__ __forceinline__ Side make_side(const double U[8], const Derived& d)
-{
-	Side s;
-	s.rho = U[0];
-	rotate<A>(U[1], U[2], U[3], s.m0, s.m1, s.m2);
-	s.E = U[4];
-	rotate<A>(U[5], U[6], U[7], s.b0, s.b1, s.b2);
-	s.rinv = d.rinv;
-	s.p = d.p;
-	s.cf = d.cf[A];
-	s.v0 = s.m0 * s.rinv;
-	s.v1 = s.m1 * s.rinv;
-	s.v2 = s.m2 * s.rinv;
-	s.bad = d.bad;
-	return s;
-}
-
 __device__ __forceinline__ void record_failure(const Stag_Params& P, const uint32_t flag, const long long cell,
                                                const int axis)
 {
@@ -148,8 +130,8 @@ __device__ __forceinline__ void solve_minus_face(const Stag_Params& P, const lon
 	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + m);
 	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7],
 	                                                  P.gas);
-	Side L = make_side<A>(Um, dm);
-	Side R = make_side<A>(Uc, dc);
+	Side L = side_of<A>(Um, dm);
+	Side R = side_of<A>(Uc, dc);
 	double G[8];
 	uint32_t flag = 0;
 	double s;

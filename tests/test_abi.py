@@ -128,3 +128,20 @@ def test_two_population_create_rejects_invalid_arguments(lib, change):
                                    kw["min_pressure"], 0, ctypes.byref(h))
     assert rc == pg.ERR_ARGUMENT and not h.value
     assert lib.pamhd_gpu_npop_destroy(None) == pg.OK
+
+
+@pytest.mark.parametrize("change", [
+    dict(bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0)),   # local time stepping is periodic only
+    dict(solver=1),
+    dict(n=(1, 1, 1)),
+    dict(time_step_factor=0.0),
+])
+def test_substep_create_rejects_invalid_config(lib, change):
+    lib.pamhd_gpu_substep_create.argtypes = [ctypes.POINTER(pg._Cfg), ctypes.POINTER(ctypes.c_void_p)]
+    kw = dict(n=(4, 4, 4), solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1))
+    kw.update(change)
+    cfg = pg.Config(**kw).to_c()
+    h = ctypes.c_void_p()
+    assert lib.pamhd_gpu_substep_create(ctypes.byref(cfg), ctypes.byref(h)) == pg.ERR_ARGUMENT
+    assert not h.value
+    assert lib.pamhd_gpu_substep_destroy(None) == pg.OK
