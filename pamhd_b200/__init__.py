@@ -419,6 +419,14 @@ class StaggeredContext:
         self._check(self.L.pamhd_gpu_staggered_step(self.h, max_dt, ctypes.byref(dt)), "pamhd_gpu_staggered_step")
         return dt.value
 
+    def save_dc(self, path: str, step: int, time: float, proton_mass: float = 1.0, start=(0.0, 0.0, 0.0)):
+        """Writes the cell state (mass, momentum, energy, volume field) as a reference .dc file,
+        the variable the reference's MHD program saves (mhd/save.hpp:75-375)."""
+        c = self.cfg
+        write_dc(path, self.get_state()[0], step=step, time=time, adiabatic_index=c.adiabatic_index,
+                 proton_mass=proton_mass, vacuum_permeability=c.vacuum_permeability, cell_length=c.cell_length,
+                 periodic=(True, True, True), start=start)
+
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_staggered_steps(self.h, int(n), float(t_end)), "pamhd_gpu_staggered_steps")
 

@@ -64,7 +64,7 @@ def test_steps_match_oracle(port, solver, shape):
 
 
 @pytest.mark.parametrize("case", list(STAGGERED_CASES))
-def test_reproduces_reference_program_output(case):
+def test_reproduces_reference_program_output(case, tmp_path):
     """The reference program's Alfven waves (Rusanov, CFL 0.5, t = 0 .. 1; with and without a
     background field), run through the C ABI as the program runs them: same step count and time,
     every cell within the reference's own comparison (tests/mhd/mhd_diff.py, 1e-15 defaults)."""
@@ -84,6 +84,12 @@ def test_reproduces_reference_program_output(case):
             t += ctx.step(t_end - t)
             steps += 1
         U, _ = ctx.get_state()
+        # the result as the program saves it: a .dc file, read back
+        path = str(tmp_path / f"mhd_{steps:09d}.dc")
+        ctx.save_dc(path, steps, t)
+        head, back = pg.read_dc(path)
+        assert head["step"] == steps and head["time"] == t
+        np.testing.assert_array_equal(back, U)
     assert steps == int(g[case + "_step"]) and t == t_end
     out = U.reshape(8, -1)
     ref = g[case + "_state"]
