@@ -9,8 +9,8 @@ length.  A step is planned on the device and driven from the host:
   limits_kernel    each cell's CFL limit from the last face speeds
                    (minimize_timestep, mhd/solve.hpp:1933-2007), the smallest
                    limit and the smallest limit / 2^min over cells
-                   (substepping.hpp:312-353), both by atomicMin on the bits of
-                   the non-negative doubles;
+                   (substepping.hpp:312-353), reduced per warp, then one
+                   atomicMin per warp on the bits of the non-negative doubles;
   exponent_kernel  floor(log2(min(limit, max_dt) / substep)) capped by the
                    cell's largest exponent (substepping.hpp:364-390);
   restrict_kernel  a cell's exponent at most one above any face or edge
@@ -119,9 +119,18 @@ __device__ __forceinline__ unsigned long long bits(const double x)
 	return (unsigned long long)__double_as_longlong(x);
 }
 
+__device__ __forceinline__ double warp_min(double v)
+{
+	#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+	return v;
+}
+
 // each cell's CFL limit (0 when a face speed is <= 0), the smallest limit and limit / 2^min
+// (reduced per warp, then one atomicMin per warp on the bits of the non-negative doubles)
 __global__ void limits_kernel(const Sub_Params P)
 {
+	double smallest = DBL_MAX, ret = DBL_MAX;
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
 		int i, j, k;
@@ -141,8 +150,14 @@ __global__ void limits_kernel(const Sub_Params P)
 		if (zero) t = 0.0;
 		P.T[c] = t;
 		const int smin = P.user_min[c] - P.min_offset;
-		atomicMin(&P.plan->smallest, bits(t));
-		atomicMin(&P.plan->ret, bits(t / (1 << smin)));
+		smallest = fmin(smallest, t);
+		ret = fmin(ret, t / (1 << smin));
+	}
+	smallest = warp_min(smallest);
+	ret = warp_min(ret);
+	if ((threadIdx.x & 31) == 0) {
+		atomicMin(&P.plan->smallest, bits(smallest));
+		atomicMin(&P.plan->ret, bits(ret));
 	}
 }
 
@@ -165,6 +180,7 @@ __global__ void exponent_kernel(const Sub_Params P, const double max_dt, const d
 
 __global__ void restrict_kernel(const Sub_Params P, const int32_t* __restrict__ in, int32_t* __restrict__ out)
 {
+	unsigned int changed = 0u;
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
 		int i, j, k;
@@ -172,18 +188,22 @@ __global__ void restrict_kernel(const Sub_Params P, const int32_t* __restrict__ 
 		int s = in[c];
 		for_neighbours(P, i, j, k, [&](const long long m) { s = min(s, in[m] + 1); });
 		out[c] = s;
-		if (s != in[c]) atomicOr(&P.plan->changed, 1u);
+		if (s != in[c]) changed = 1u;
 	}
+	if (__any_sync(0xffffffffu, changed != 0u) and (threadIdx.x & 31) == 0) atomicOr(&P.plan->changed, 1u);
 }
 
 __global__ void period_kernel(const Sub_Params P)
 {
+	unsigned int largest = 0u;
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
 		const int p = 1 << P.S[c];
 		P.P[c] = p;
-		atomicMax(&P.plan->max_period, (unsigned int)p);
+		largest = max(largest, (unsigned int)p);
 	}
+	largest = __reduce_max_sync(0xffffffffu, largest);
+	if ((threadIdx.x & 31) == 0) atomicMax(&P.plan->max_period, largest);
 }
 
 __global__ void reach_kernel(const Sub_Params P)
