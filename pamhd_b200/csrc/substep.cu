@@ -223,6 +223,15 @@ __device__ __forceinline__ void plus_face(const Sub_Params& P, const long long c
                                           const int k, const double Uc[8], const Derived& dc, const double min_dt)
 {
 	const long long up = wrap(P, i + (A == 0), j + (A == 1), k + (A == 2));
+	double* const plus = P.slot + (size_t(2 * A + 1) * 8) * P.N + c;   // the cell's +A slot
+	double* const minus = P.slot + (size_t(2 * A) * 8) * P.N + up;     // the neighbour's -A slot
+	// the slots are read before the solve, so that their latency overlaps its arithmetic
+	double pv[8], mv[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) {
+		pv[v] = plus[v * P.N];
+		mv[v] = minus[v * P.N];
+	}
 	double Uu[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) Uu[v] = P.U[v * P.N + up];
@@ -242,12 +251,10 @@ __device__ __forceinline__ void plus_face(const Sub_Params& P, const long long c
 	unrotate<A>(G[1], G[2], G[3], F[1], F[2], F[3]);
 	F[4] = G[4];
 	unrotate<A>(G[5], G[6], G[7], F[5], F[6], F[7]);
-	double* plus = P.slot + (size_t(2 * A + 1) * 8) * P.N + c;   // the cell's +A slot
-	double* minus = P.slot + (size_t(2 * A) * 8) * P.N + up;     // the neighbour's -A slot
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
-		plus[v * P.N] = plus[v * P.N] + min_dt * F[v];
-		minus[v * P.N] = minus[v * P.N] + min_dt * F[v];
+		plus[v * P.N] = pv[v] + min_dt * F[v];
+		minus[v * P.N] = mv[v] + min_dt * F[v];
 	}
 }
 
@@ -279,29 +286,43 @@ __global__ void update_kernel(const Sub_Params P, const int s)
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
 		if (s % P.P[c] != 0) continue;
-		auto f = [&](const int sl, const int v) -> double& { return P.slot[(size_t(sl) * 8 + v) * N + c]; };
+		// every slot read first: 48 independent loads in flight
+		double sl_[6][8];
+		#pragma unroll
+		for (int sl = 0; sl < 6; sl++) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) sl_[sl][v] = P.slot[(size_t(sl) * 8 + v) * N + c];
+		}
+		auto f = [&](const int sl, const int v) -> double { return sl_[sl][v]; };
 		double u[8];
 		#pragma unroll
 		for (int v = 0; v < 8; v++) u[v] = P.U[v * N + c];
+		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			if (P.active[d]) u[0] += (f(2 * d, 0) - f(2 * d + 1, 0)) / P.len[d];
 		}
+		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			if (not P.active[d]) continue;
+			#pragma unroll
 			for (int e = 1; e <= 3; e++) u[e] = u[e] + P.inv_len[d] * (f(2 * d, e) + (-f(2 * d + 1, e)));
 		}
+		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			if (P.active[d]) u[4] += (f(2 * d, 4) - f(2 * d + 1, 4)) / P.len[d];
 		}
+		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			if (not P.active[d]) continue;
+			#pragma unroll
 			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (f(2 * d, e) + (-f(2 * d + 1, e)));
 		}
 		#pragma unroll
 		for (int v = 0; v < 8; v++) P.U[v * N + c] = u[v];
+		#pragma unroll
 		for (int sl = 0; sl < 6; sl++) {
 			#pragma unroll
-			for (int v = 0; v < 8; v++) f(sl, v) = 0.0;
+			for (int v = 0; v < 8; v++) P.slot[(size_t(sl) * 8 + v) * N + c] = 0.0;
 		}
 	}
 }
