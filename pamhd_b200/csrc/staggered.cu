@@ -23,7 +23,7 @@ One step is three launches on the context's stream:
                  the twelve edge terms of assign_face_dBs_f{x,y,z}
                  (mhd/solve.hpp:587-1494, equal-size neighbours) and
                  Face_B += Face_dB / area (mhd/solve.hpp:1589-1593);
-  cell_kernel    the same dt; the cell update of update_mhd_state
+  cell_kernel    the same dt (all its inputs loaded first); the cell update of update_mhd_state
                  (mhd/solve.hpp:1543-1587), then update_vol_B with constant
                  thermal pressure twice (mhd/solve.hpp:1631-1683,
                  :1895-1918), the volume field the mean of each pair of new
@@ -328,7 +328,7 @@ The cell update of update_mhd_state (mass, momentum, energy, volume field;
 x, then y, then z, each flux slot 0 + dt F as the reference accumulates it),
 then update_vol_B twice with the new faces.  Block 0 advances the clock ring.
 */
-__global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
+__global__ void __launch_bounds__(THREADS, 1) cell_kernel(const Stag_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
@@ -362,8 +362,20 @@ __global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
 		int i, j, k;
 		cell_coords(P, c, i, j, k);
 		const long long up[3] = {wrap_index(P, i + 1, j, k), wrap_index(P, i, j + 1, k), wrap_index(P, i, j, k + 1)};
-		auto fm = [&](const int d, const int v) { return 0 + dt * P.F[(d * 8 + v) * N + c]; };
-		auto fp = [&](const int d, const int v) { return 0 + dt * P.F[(d * 8 + v) * N + up[d]]; };
+		// every input read first: 62 independent loads in flight
+		double Fm[3][8], Fp[3][8], bm[3], bp[3];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				Fm[d][v] = P.F[(d * 8 + v) * N + c];
+				Fp[d][v] = P.F[(d * 8 + v) * N + up[d]];
+			}
+			bm[d] = P.Bo[d * N + c];
+			bp[d] = P.Bo[d * N + up[d]];
+		}
+		auto fm = [&](const int d, const int v) { return 0 + dt * Fm[d][v]; };
+		auto fp = [&](const int d, const int v) { return 0 + dt * Fp[d][v]; };
 		double u[8];
 		#pragma unroll
 		for (int v = 0; v < 8; v++) u[v] = P.U[v * N + c];
@@ -381,9 +393,7 @@ __global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
 			#pragma unroll
 			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (fm(d, e) + (-fp(d, e)));
 		}
-		const double mean[3] = {0.5 * (P.Bo[c] + P.Bo[up[0]]),
-		                        0.5 * (P.Bo[N + c] + P.Bo[N + up[1]]),
-		                        0.5 * (P.Bo[2 * N + c] + P.Bo[2 * N + up[2]])};
+		const double mean[3] = {0.5 * (bm[0] + bp[0]), 0.5 * (bm[1] + bp[1]), 0.5 * (bm[2] + bp[2])};
 		vol_B_constant_pressure(u, mean, P.gas);
 		vol_B_constant_pressure(u, mean, P.gas);
 		#pragma unroll
