@@ -317,9 +317,13 @@ __global__ void __launch_bounds__(THREADS) field_kernel(const Stag_Params P)
 		}
 		int i, j, k;
 		cell_coords(P, c, i, j, k);
-		P.Bo[c] = P.B[c] + face_dB<0>(P, i, j, k, dt) / P.area[0];
-		P.Bo[P.N + c] = P.B[P.N + c] + face_dB<1>(P, i, j, k, dt) / P.area[1];
-		P.Bo[2 * P.N + c] = P.B[2 * P.N + c] + face_dB<2>(P, i, j, k, dt) / P.area[2];
+		// every read before the first store, so that the 39 loads are in flight together
+		const double d0 = face_dB<0>(P, i, j, k, dt), d1 = face_dB<1>(P, i, j, k, dt),
+		             d2 = face_dB<2>(P, i, j, k, dt);
+		const double b0 = P.B[c], b1 = P.B[P.N + c], b2 = P.B[2 * P.N + c];
+		P.Bo[c] = b0 + d0 / P.area[0];
+		P.Bo[P.N + c] = b1 + d1 / P.area[1];
+		P.Bo[2 * P.N + c] = b2 + d2 / P.area[2];
 	}
 }
 
