@@ -417,8 +417,8 @@ after sync_magnetic_field), on a uniform grid periodic in every dimension.
 A dimension of one cell is its own neighbour, as in the reference's
 emulated 1-D and 2-D runs.  Solvers: Rusanov, HLL, HLLD, Roe.
 
-  - create: cfg as pamhd_gpu_create, every side PAMHD_BC_PERIODIC
-    (else PAMHD_ERR_ARGUMENT); replaces the state a PAMHD program keeps in
+  - create: cfg as pamhd_gpu_create, every side PAMHD_BC_PERIODIC and
+    n[1] at most 262140 (else PAMHD_ERR_ARGUMENT); replaces the state a PAMHD program keeps in
     Mas, Mom, Nrj, Vol_B and Face_B (tests/mhd/test.cpp:422-456).
   - set_state / get_state: cells as pamhd_gpu_set_state (eight arrays, x
     fastest; cells[5..7] is the volume field Vol_B) and faces[d] the normal

@@ -14,9 +14,11 @@ A dimension of one cell is its own neighbour, as in the reference's emulated
 
 One step is three launches on the context's stream:
   faces_kernel   every cell solves its three -d faces (the +d faces of its
-                 -d neighbours, get_fluxes, mhd/solve.hpp:217-392), stores
-                 the unrotated flux, and max-reduces the face speeds per
-                 axis into a three-slot ring, as the fused cell-centred step;
+                 -d neighbours, get_fluxes, mhd/solve.hpp:217-392) from
+                 per-cell records staged in shared memory by z-marching
+                 tiles, stores the unrotated flux, and max-reduces the face
+                 speeds per axis into a three-slot ring, as the fused
+                 cell-centred step;
   field_kernel   dt from the previous step's speeds and the cap (lagged CFL
                  rule, mhd/solve.hpp:1933-2007, substepping.hpp:285-338);
                  the new normal field of every cell's three -d faces from
@@ -34,6 +36,7 @@ face fluxes both compute the same bits.
 */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -46,8 +49,6 @@ using namespace pamhd_b200;
 namespace {
 
 constexpr int THREADS = 256;
-// the face solves: 128 threads, three resident blocks per SM (two for Roe's larger register set)
-constexpr int FACE_THREADS = 128;
 
 struct Stag_Params {
 	const double* __restrict__ U;    // 8 x N
@@ -69,6 +70,7 @@ struct Stag_Params {
 	int phase;
 	double max_dt;                   // >= 0: cap of dt; < 0: the cap is t_end - t
 	double t_end;
+	int kchunk;                      // z planes per face-solve block
 };
 
 __device__ __forceinline__ long long wrap_index(const Stag_Params& P, int i, int j, int k)
@@ -117,21 +119,75 @@ __device__ __forceinline__ void with_background(Side& s, const double bg[3], con
 	}
 }
 
-// the -A face of cell c: solved between its -A neighbour (left) and c (right); BG: with the
-// face's background field (Rusanov and HLL use it; the reference's HLLD and Roe ignore it)
-template <int SOLVER, int A, bool BG>
-__device__ __forceinline__ void solve_minus_face(const Stag_Params& P, const long long c, const int i, const int j,
-                                                 const int k, const double Uc[8], const Derived& dc,
-                                                 double& smax, bool& zero)
+/*
+The face solves as tiles: a block of STX x STY threads owns a column of cells
+and marches it in z through a chunk of planes.  Each plane's cells, with the
+-x column and -y row next to the tile, are read and derived once into a
+shared-memory record (state, 1/rho, pressure, fast speed along each axis,
+validity per axis) instead of once per face; every cell then solves its three
+-d faces from the records, the -z face against the previous plane's record.
+Three record slots rotate over the planes, so one barrier per plane keeps a
+plane's stores apart from the reads of the plane two before it.
+*/
+constexpr int STX = 32, STY = 4;
+constexpr int SW = STX + 1;                 // a record row: the -x halo at column 0
+constexpr int SCELLS = SW * (STY + 1);      // record rows: the -y halo at row 0
+constexpr int SREC = 13;                    // rho, mom xyz, E, B xyz, 1/rho, p, c_f xyz
+constexpr int SSLOT = SREC * SCELLS;        // doubles of one slot
+constexpr int SSLOTS = 3;
+constexpr size_t SMEM_FACES = SSLOTS * (SSLOT * sizeof(double) + SCELLS * sizeof(uint32_t));
+
+// read cell c from HBM and derive its record into slot position r
+__device__ __forceinline__ void stage_cell(const Stag_Params& P, double* rec, uint32_t* bad, const int r,
+                                           const long long c)
 {
-	const long long m = wrap_index(P, i - (A == 0), j - (A == 1), k - (A == 2));
-	double Um[8];
+	double U[8];
 	#pragma unroll
-	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + m);
-	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7],
-	                                                  P.gas);
-	Side L = side_of<A>(Um, dm);
-	Side R = side_of<A>(Uc, dc);
+	for (int v = 0; v < 8; v++) U[v] = __ldg(P.U + v * P.N + c);
+	const Derived d = derive<true, true, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) rec[v * SCELLS + r] = U[v];
+	rec[8 * SCELLS + r] = d.rinv;
+	rec[9 * SCELLS + r] = d.p;
+	rec[10 * SCELLS + r] = d.cf[0];
+	rec[11 * SCELLS + r] = d.cf[1];
+	rec[12 * SCELLS + r] = d.cf[2];
+	// one byte of flags per face direction: the reference checks the fast speed of each face
+	// along that face's normal, so a failed speed belongs to the failing directions only
+	uint32_t packed = d.bad | (d.bad << 8) | (d.bad << 16);
+	if (d.bad == PAMHD_FLAG_WAVE_SPEED) {
+		packed = derive<true, false, false>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad
+			| (derive<false, true, false>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad << 8)
+			| (derive<false, false, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad << 16);
+	}
+	bad[r] = packed;
+}
+
+// the cell at slot position r seen from a face normal to axis A (as side_of<A>)
+template <int A>
+__device__ __forceinline__ Side side_rec(const double* rec, const uint32_t* bad, const int r)
+{
+	Side s;
+	s.rho = rec[r];
+	rotate<A>(rec[SCELLS + r], rec[2 * SCELLS + r], rec[3 * SCELLS + r], s.m0, s.m1, s.m2);
+	s.E = rec[4 * SCELLS + r];
+	rotate<A>(rec[5 * SCELLS + r], rec[6 * SCELLS + r], rec[7 * SCELLS + r], s.b0, s.b1, s.b2);
+	s.rinv = rec[8 * SCELLS + r];
+	s.p = rec[9 * SCELLS + r];
+	s.cf = rec[(10 + A) * SCELLS + r];
+	s.v0 = s.m0 * s.rinv;
+	s.v1 = s.m1 * s.rinv;
+	s.v2 = s.m2 * s.rinv;
+	s.bad = (bad[r] >> (8 * A)) & 0xffu;
+	return s;
+}
+
+// the -A face of cell c between its -A neighbour m (left) and c (right); BG: with the face's
+// background field (Rusanov and HLL use it; the reference's HLLD and Roe ignore it)
+template <int SOLVER, int A, bool BG>
+__device__ __forceinline__ void solve_minus_face(const Stag_Params& P, Side L, Side R, const long long c,
+                                                 const long long m, double& smax, bool& zero)
+{
 	double G[8];
 	uint32_t flag = 0;
 	double s;
@@ -169,28 +225,65 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 template <int SOLVER, bool BG>
-__global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3) faces_kernel(const Stag_Params P)
+__global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3) faces_kernel(const Stag_Params P)
 {
+	extern __shared__ __align__(16) double smem[];
+	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(smem + SSLOTS * SSLOT);
+	const int tx = threadIdx.x, ty = threadIdx.y;
+	const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+	const int gx0 = blockIdx.x * STX, gy0 = blockIdx.y * STY;
+	const int gx = gx0 + tx, gy = gy0 + ty;
+	const bool own = gx < nx and gy < ny;
+	const int kb = blockIdx.z * P.kchunk;
+	const int ke = min(nz, kb + P.kchunk);
+	const int ri = (ty + 1) * SW + tx + 1;
+	const long long plane = (long long)nx * ny;
+	const long long col = gx + (long long)nx * gy;
+	// this thread's halo cell, if any: warp 0 the row below the tile, warp 1 the column left of it
+	int hr = -1;
+	long long hcol = 0;
+	if (ty == 0 and gx < nx) {
+		hr = tx + 1;
+		hcol = gx + (long long)nx * (gy0 == 0 ? ny - 1 : gy0 - 1);
+	} else if (ty == 1 and tx < STY and gy0 + tx < ny) {
+		hr = (tx + 1) * SW;
+		hcol = (gx0 == 0 ? nx - 1 : gx0 - 1) + (long long)nx * (gy0 + tx);
+	}
+	// the -d neighbours' columns (failure reports name the face's negative cell)
+	const long long col_mx = (gx == 0 ? nx - 1 : gx - 1) + (long long)nx * gy;
+	const long long col_my = gx + (long long)nx * (gy == 0 ? ny - 1 : gy - 1);
+
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	bool zero = false;
-	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
-		int i, j, k;
-		cell_coords(P, c, i, j, k);
-		double Uc[8];
-		#pragma unroll
-		for (int v = 0; v < 8; v++) Uc[v] = __ldg(P.U + v * P.N + c);
-		const Derived dc = derive<true, true, true>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
-		solve_minus_face<SOLVER, 0, BG>(P, c, i, j, k, Uc, dc, s0, zero);
-		solve_minus_face<SOLVER, 1, BG>(P, c, i, j, k, Uc, dc, s1, zero);
-		solve_minus_face<SOLVER, 2, BG>(P, c, i, j, k, Uc, dc, s2, zero);
+	// the plane before the chunk, own cells only: the left sides of the first plane's -z faces
+	if (own) stage_cell(P, smem, bad_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
+	for (int k = kb; k < ke; k++) {
+		const int t = k - kb + 1;
+		double* const rec = smem + (t % SSLOTS) * SSLOT;
+		uint32_t* const bad = bad_base + (t % SSLOTS) * SCELLS;
+		const double* const prv = smem + ((t - 1) % SSLOTS) * SSLOT;
+		const uint32_t* const pbad = bad_base + ((t - 1) % SSLOTS) * SCELLS;
+		const long long kofs = plane * k;
+		if (own) stage_cell(P, rec, bad, ri, col + kofs);
+		if (hr >= 0) stage_cell(P, rec, bad, hr, hcol + kofs);
+		__syncthreads();
+		if (own) {
+			const long long c = col + kofs;
+			const long long mz = col + plane * (k == 0 ? nz - 1 : k - 1);
+			solve_minus_face<SOLVER, 0, BG>(P, side_rec<0>(rec, bad, ri - 1), side_rec<0>(rec, bad, ri), c,
+			                                col_mx + kofs, s0, zero);
+			solve_minus_face<SOLVER, 1, BG>(P, side_rec<1>(rec, bad, ri - SW), side_rec<1>(rec, bad, ri), c,
+			                                col_my + kofs, s1, zero);
+			solve_minus_face<SOLVER, 2, BG>(P, side_rec<2>(prv, pbad, ri), side_rec<2>(rec, bad, ri), c, mz,
+			                                s2, zero);
+		}
 	}
 	// per-axis maxima of the non-negative speeds, as bit patterns
 	s0 = warp_max(s0);
 	s1 = warp_max(s1);
 	s2 = warp_max(s2);
 	const bool any_zero = __any_sync(0xffffffffu, zero);
-	if ((threadIdx.x & 31) == 0) {
+	if (tx == 0) {
 		Speed_Max& r = P.red[(P.phase + 1) % 3];
 		atomicMax(&r.smax[0], (unsigned long long)__double_as_longlong(s0));
 		atomicMax(&r.smax[1], (unsigned long long)__double_as_longlong(s1));
@@ -405,14 +498,32 @@ __global__ void __launch_bounds__(THREADS, 1) cell_kernel(const Stag_Params P)
 	}
 }
 
+// the face kernels' shared memory above the default 48 KB, once per kernel
+template <int SOLVER>
+int allow_face_smem()
+{
+	constexpr bool USES_BG = SOLVER == PAMHD_RUSANOV or SOLVER == PAMHD_HLL_ATHENA;
+	if (cudaFuncSetAttribute(faces_kernel<SOLVER, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                         int(SMEM_FACES)) != cudaSuccess) {
+		return PAMHD_ERR_CUDA;
+	}
+	if (USES_BG and cudaFuncSetAttribute(faces_kernel<SOLVER, USES_BG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                     int(SMEM_FACES)) != cudaSuccess) {
+		return PAMHD_ERR_CUDA;
+	}
+	return PAMHD_OK;
+}
+
 template <int SOLVER>
 int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 {
 	constexpr bool USES_BG = SOLVER == PAMHD_RUSANOV or SOLVER == PAMHD_HLL_ATHENA;
+	const dim3 tiles((P.n[0] + STX - 1) / STX, (P.n[1] + STY - 1) / STY, (P.n[2] + P.kchunk - 1) / P.kchunk);
+	const dim3 block(STX, STY);
 	if (USES_BG and P.bg != nullptr) {
-		faces_kernel<SOLVER, USES_BG><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+		faces_kernel<SOLVER, USES_BG><<<tiles, block, SMEM_FACES, stream>>>(P);
 	} else {
-		faces_kernel<SOLVER, false><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+		faces_kernel<SOLVER, false><<<tiles, block, SMEM_FACES, stream>>>(P);
 	}
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	field_kernel<<<grid, THREADS, 0, stream>>>(P);
@@ -510,6 +621,7 @@ int validate_stag(const pamhd_cfg& c)
 	}
 	const long long N = (long long)c.n[0] * c.n[1] * c.n[2];
 	if (N > (1ll << 31)) return PAMHD_ERR_ARGUMENT;
+	if ((c.n[1] + STY - 1) / STY > 65535) return PAMHD_ERR_ARGUMENT;   // rows of face tiles: the grid's y extent
 	return PAMHD_OK;
 }
 
@@ -551,8 +663,21 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 	}
 	const long long blocks = (x->N + THREADS - 1) / THREADS;
 	x->grid = int(blocks < 8ll * sms ? blocks : 8ll * sms);
+	int rc = PAMHD_ERR_ARGUMENT;
+	switch (cfg->solver) {
+	case PAMHD_RUSANOV: rc = allow_face_smem<PAMHD_RUSANOV>(); break;
+	case PAMHD_HLL_ATHENA: rc = allow_face_smem<PAMHD_HLL_ATHENA>(); break;
+	case PAMHD_HLLD_ATHENA: rc = allow_face_smem<PAMHD_HLLD_ATHENA>(); break;
+	case PAMHD_ROE_ATHENA: rc = allow_face_smem<PAMHD_ROE_ATHENA>(); break;
+	default: break;
+	}
+	if (rc != PAMHD_OK) return fail(rc);
 	Stag_Params& P = x->base;
 	P = Stag_Params{};
+	// z chunks so that the face tiles fill the SMs about six times over
+	const long long tiles = (long long)((cfg->n[0] + STX - 1) / STX) * ((cfg->n[1] + STY - 1) / STY);
+	const long long chunks = std::max(1ll, std::min((long long)cfg->n[2], 18ll * sms / tiles));
+	P.kchunk = int((cfg->n[2] + chunks - 1) / chunks);
 	for (int d = 0; d < 3; d++) {
 		P.n[d] = cfg->n[d];
 		P.len[d] = cfg->cell_length[d];
