@@ -22,8 +22,11 @@ One step, two launches:
   npop_faces_kernel   dt (given, or min(CFL max_dt, t_end - t) from the
                       previous step's face speeds, the loop of
                       tests/mhd/two_reference.cpp:936-960); every cell solves
-                      its -d faces, stores their contributions and max-reduces
-                      the signal speeds per axis into a three-slot ring;
+                      its -d faces from per-cell records staged in shared
+                      memory by z-marching tiles (the fast speed of a cell
+                      along each axis computed once, not once per face side),
+                      stores their contributions and max-reduces the signal
+                      speeds per axis into a three-slot ring;
   npop_update_kernel  the same dt; every cell sums its faces' contributions
                       in the order -x, +x, -y, +y, -z, +z, applies them times
                       1/volume (apply_fluxes_N, mhd/N_solve.hpp:505-546) and
@@ -37,6 +40,7 @@ computes the oracle's bits.
 */
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 #include <new>
@@ -49,8 +53,6 @@ using namespace pamhd_b200;
 namespace {
 
 constexpr int THREADS = 256;
-// the face solves: 128 threads, three resident blocks per SM (two for HLL's larger register set)
-constexpr int FACE_THREADS = 128;
 constexpr int NV = 13;
 
 struct Npop_Control {
@@ -74,6 +76,7 @@ struct Npop_Params {
 	Status* status;
 	Npop_Control control;
 	int phase;
+	int kchunk;                     // z planes per face-solve block
 };
 
 // a total state: mass, momentum, energy, field
@@ -201,18 +204,31 @@ __device__ __forceinline__ void state_row(const St& s, double u[8])
 	u[4] = s.e; u[5] = s.b[0]; u[6] = s.b[1]; u[7] = s.b[2];
 }
 
+/*
+The fast speed of a side along the face normal is computed once per cell and
+axis (fast_speed of the rotated total state, with the flag it raises from a
+clear start); the split solvers take it with that flag.
+*/
+struct Fast {
+	double speed;
+	uint32_t flag;
+};
+
 // get_flux_N_rusanov (mhd/N_rusanov.hpp:61-170)
-__device__ double split_rusanov(const St& L, const St& R, const double area, const double dt, const double gamma,
-                                const double mu0, double fn[8], double fp[8], uint32_t& flag)
+__device__ double split_rusanov(const St& L, const St& R, const Fast& fl, const Fast& fr, const double area,
+                                const double dt, const double gamma, const double mu0, double fn[8], double fp[8],
+                                uint32_t& flag)
 {
 	if (not (is_normal(L.rho) and not (L.rho < 0)) or not (is_normal(R.rho) and not (R.rho < 0))) {
 		flag = PAMHD_FLAG_DENSITY;
 		return 0;
 	}
-	const double fast_neg = fast_speed(L, gamma, mu0, flag);
+	flag = fl.flag;
 	if (flag) return 0;
-	const double fast_pos = fast_speed(R, gamma, mu0, flag);
+	const double fast_neg = fl.speed;
+	flag = fr.flag;
 	if (flag) return 0;
+	const double fast_pos = fr.speed;
 	const double max_fast = max_of(fast_neg, fast_pos);
 	double vl[3], vr[3];
 	velocity(L.m, L.rho, vl);
@@ -243,8 +259,9 @@ __device__ double split_rusanov(const St& L, const St& R, const double area, con
 }
 
 // get_flux_N_hll (mhd/N_hll_athena.hpp:47-231)
-__device__ double split_hll(const St& L, const St& R, const double area, const double dt, const double gamma,
-                            const double mu0, double fn[8], double fp[8], uint32_t& flag)
+__device__ double split_hll(const St& L, const St& R, const Fast& fl, const Fast& fr, const double area,
+                            const double dt, const double gamma, const double mu0, double fn[8], double fp[8],
+                            uint32_t& flag)
 {
 	double vn[3], vp[3];
 	velocity(L.m, L.rho, vn);
@@ -255,10 +272,12 @@ __device__ double split_hll(const St& L, const St& R, const double area, const d
 	const double
 		pb_neg = (L.b[0] * L.b[0] + L.b[1] * L.b[1] + L.b[2] * L.b[2]) / (2 * mu0),
 		pb_pos = (R.b[0] * R.b[0] + R.b[1] * R.b[1] + R.b[2] * R.b[2]) / (2 * mu0);
-	const double fast_neg = fast_speed(L, gamma, mu0, flag);
+	flag = fl.flag;
 	if (flag) return 0;
-	const double fast_pos = fast_speed(R, gamma, mu0, flag);
+	const double fast_neg = fl.speed;
+	flag = fr.flag;
 	if (flag) return 0;
+	const double fast_pos = fr.speed;
 	const double
 		max_signal = max_of(fast_neg, fast_pos),
 		s_neg = (vn[0] <= vp[0]) ? vn[0] - max_signal : vp[0] - max_signal,
@@ -368,18 +387,69 @@ __device__ __forceinline__ double warp_max(double v)
 	return v;
 }
 
-template <int SOLVER, int A>
-__device__ __forceinline__ void minus_face(const Npop_Params& P, const long long c, const int i, const int j,
-                                           const int k, const double uc[NV], const double dt, double& smax)
+/*
+The face solves as tiles: a block of NTX x NTY threads owns a column of cells
+and marches it in z through a chunk of planes.  Each plane's cells, with the
+-x column and -y row next to the tile, are read once into a shared-memory
+record (the 13 state values and, per active axis, the fast speed of the
+rotated total state with its check flag); every cell then solves its -d
+faces from the records, the -z face against the previous plane's record.
+Three record slots rotate over the planes, so one barrier per plane keeps a
+plane's stores apart from the reads of the plane two before it.
+*/
+constexpr int NTX = 32, NTY = 4;
+constexpr int NW = NTX + 1;                 // a record row: the -x halo at column 0
+constexpr int NCELLS = NW * (NTY + 1);      // record rows: the -y halo at row 0
+constexpr int NREC = NV + 3;                // state, fast speed along x, y, z
+constexpr int NSLOT = NREC * NCELLS;
+constexpr int NSLOTS = 3;
+constexpr size_t SMEM_FACES = NSLOTS * (NSLOT * sizeof(double) + NCELLS * sizeof(uint32_t));
+
+template <int A>
+__device__ __forceinline__ void stage_fast(const Npop_Params& P, const double u[NV], double* rec, const int r,
+                                           uint32_t& flags)
 {
-	const long long m = wrap(P, i - (A == 0), j - (A == 1), k - (A == 2));
-	double um[NV];
-	load13(P, m, um);
+	if (not P.active[A]) return;
+	uint32_t f = 0;
+	rec[(NV + A) * NCELLS + r] = fast_speed(total_rotated<A>(u), P.gamma, P.mu0, f);
+	flags |= f << (8 * A);
+}
+
+// read cell c into slot position r
+__device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, uint32_t* flg, const int r,
+                                           const long long c)
+{
+	double u[NV];
+	load13(P, c, u);
+	#pragma unroll
+	for (int v = 0; v < NV; v++) rec[v * NCELLS + r] = u[v];
+	uint32_t flags = 0;
+	stage_fast<0>(P, u, rec, r, flags);
+	stage_fast<1>(P, u, rec, r, flags);
+	stage_fast<2>(P, u, rec, r, flags);
+	flg[r] = flags;
+}
+
+// the -A face of cell c between its -A neighbour m (record rl) and c (record rr)
+template <int SOLVER, int A>
+__device__ __forceinline__ void minus_face(const Npop_Params& P, const double* recl, const uint32_t* flgl,
+                                           const int rl, const double* recr, const uint32_t* flgr, const int rr,
+                                           const long long c, const long long m, const double dt, double& smax)
+{
+	double um[NV], uc[NV];
+	#pragma unroll
+	for (int v = 0; v < NV; v++) {
+		um[v] = recl[v * NCELLS + rl];
+		uc[v] = recr[v * NCELLS + rr];
+	}
 	const St L = total_rotated<A>(um), R = total_rotated<A>(uc);
+	const Fast fl{recl[(NV + A) * NCELLS + rl], (flgl[rl] >> (8 * A)) & 0xffu};
+	const Fast fr{recr[(NV + A) * NCELLS + rr], (flgr[rr] >> (8 * A)) & 0xffu};
 	double fn[8], fp[8];
 	uint32_t flag = 0;
-	const double s = SOLVER == PAMHD_RUSANOV ? split_rusanov(L, R, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag)
-	                                         : split_hll(L, R, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag);
+	const double s = SOLVER == PAMHD_RUSANOV
+		? split_rusanov(L, R, fl, fr, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag)
+		: split_hll(L, R, fl, fr, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag);
 	if (flag != 0) {
 		atomicOr(&P.status->flags, flag);
 		atomicMin(&P.status->first, ((unsigned long long)(m * 3 + A) << 8) | flag);
@@ -412,11 +482,14 @@ __device__ __forceinline__ void minus_face(const Npop_Params& P, const long long
 }
 
 template <int SOLVER>
-__global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_RUSANOV ? 3 : 2) npop_faces_kernel(const Npop_Params P)
+__global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) npop_faces_kernel(const Npop_Params P)
 {
+	extern __shared__ __align__(16) double smem[];
+	uint32_t* const flg_base = reinterpret_cast<uint32_t*>(smem + NSLOTS * NSLOT);
 	__shared__ double s_dt;
 	__shared__ int s_skip;
-	if (threadIdx.x == 0) {
+	const int tx = threadIdx.x, ty = threadIdx.y;
+	if (tx == 0 and ty == 0) {
 		const Clock c = P.clock[P.phase];
 		const bool skip = P.control.dt < 0.0 and c.t >= P.control.t_end;
 		s_skip = skip ? 1 : 0;
@@ -426,22 +499,55 @@ __global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_RUSANOV ? 3 : 2)
 	const double dt = s_dt;
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	if (s_skip == 0) {
-		const long long stride = (long long)gridDim.x * blockDim.x;
-		for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
-			const int i = int(c % P.n[0]);
-			const int j = int((c / P.n[0]) % P.n[1]);
-			const int k = int(c / ((long long)P.n[0] * P.n[1]));
-			double uc[NV];
-			load13(P, c, uc);
-			if (P.active[0]) minus_face<SOLVER, 0>(P, c, i, j, k, uc, dt, s0);
-			if (P.active[1]) minus_face<SOLVER, 1>(P, c, i, j, k, uc, dt, s1);
-			if (P.active[2]) minus_face<SOLVER, 2>(P, c, i, j, k, uc, dt, s2);
+		const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+		const int gx0 = blockIdx.x * NTX, gy0 = blockIdx.y * NTY;
+		const int gx = gx0 + tx, gy = gy0 + ty;
+		const bool own = gx < nx and gy < ny;
+		const int kb = blockIdx.z * P.kchunk;
+		const int ke = min(nz, kb + P.kchunk);
+		const int ri = (ty + 1) * NW + tx + 1;
+		const long long plane = (long long)nx * ny;
+		const long long col = gx + (long long)nx * gy;
+		// this thread's halo cell, if any: warp 0 the row below the tile, warp 1 the column left of it
+		int hr = -1;
+		long long hcol = 0;
+		if (ty == 0 and gx < nx) {
+			hr = tx + 1;
+			hcol = gx + (long long)nx * (gy0 == 0 ? ny - 1 : gy0 - 1);
+		} else if (ty == 1 and tx < NTY and gy0 + tx < ny) {
+			hr = (tx + 1) * NW;
+			hcol = (gx0 == 0 ? nx - 1 : gx0 - 1) + (long long)nx * (gy0 + tx);
+		}
+		// the -d neighbours' columns (failure reports name the face's negative cell)
+		const long long col_mx = (gx == 0 ? nx - 1 : gx - 1) + (long long)nx * gy;
+		const long long col_my = gx + (long long)nx * (gy == 0 ? ny - 1 : gy - 1);
+		// the plane before the chunk, own cells only: the left sides of the first plane's -z faces
+		if (own and P.active[2]) stage_cell(P, smem, flg_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
+		for (int k = kb; k < ke; k++) {
+			const int t = k - kb + 1;
+			double* const rec = smem + (t % NSLOTS) * NSLOT;
+			uint32_t* const flg = flg_base + (t % NSLOTS) * NCELLS;
+			const double* const prv = smem + ((t - 1) % NSLOTS) * NSLOT;
+			const uint32_t* const pflg = flg_base + ((t - 1) % NSLOTS) * NCELLS;
+			const long long kofs = plane * k;
+			if (own) stage_cell(P, rec, flg, ri, col + kofs);
+			if (hr >= 0) stage_cell(P, rec, flg, hr, hcol + kofs);
+			__syncthreads();
+			if (own) {
+				const long long c = col + kofs;
+				if (P.active[0]) minus_face<SOLVER, 0>(P, rec, flg, ri - 1, rec, flg, ri, c, col_mx + kofs, dt, s0);
+				if (P.active[1]) minus_face<SOLVER, 1>(P, rec, flg, ri - NW, rec, flg, ri, c, col_my + kofs, dt, s1);
+				if (P.active[2]) {
+					minus_face<SOLVER, 2>(P, prv, pflg, ri, rec, flg, ri, c, col + plane * (k == 0 ? nz - 1 : k - 1),
+					                      dt, s2);
+				}
+			}
 		}
 	}
 	s0 = warp_max(s0);
 	s1 = warp_max(s1);
 	s2 = warp_max(s2);
-	if ((threadIdx.x & 31) == 0) {
+	if (tx == 0) {
 		Speed_Max& r = P.red[(P.phase + 1) % 3];
 		atomicMax(&r.smax[0], (unsigned long long)__double_as_longlong(s0));
 		atomicMax(&r.smax[1], (unsigned long long)__double_as_longlong(s1));
@@ -449,7 +555,7 @@ __global__ void __launch_bounds__(FACE_THREADS, SOLVER == PAMHD_RUSANOV ? 3 : 2)
 	}
 }
 
-__global__ void __launch_bounds__(THREADS) npop_update_kernel(const Npop_Params P)
+__global__ void __launch_bounds__(THREADS, 1) npop_update_kernel(const Npop_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
@@ -481,17 +587,28 @@ __global__ void __launch_bounds__(THREADS) npop_update_kernel(const Npop_Params 
 			const int i = int(c % P.n[0]);
 			const int j = int((c / P.n[0]) % P.n[1]);
 			const int k = int(c / ((long long)P.n[0] * P.n[1]));
-			double f[NV];
-			#pragma unroll
-			for (int v = 0; v < NV; v++) f[v] = 0;
+			// every contribution read first: 78 independent loads in flight
+			double xm[3][NV], xp[3][NV];
 			#pragma unroll
 			for (int d = 0; d < 3; d++) {
 				if (not P.active[d]) continue;
 				const long long hi = wrap(P, i + (d == 0), j + (d == 1), k + (d == 2));
 				#pragma unroll
 				for (int v = 0; v < NV; v++) {
-					f[v] += P.X[(d * NV + v) * N + c];
-					f[v] -= P.X[(d * NV + v) * N + hi];
+					xm[d][v] = P.X[(d * NV + v) * N + c];
+					xp[d][v] = P.X[(d * NV + v) * N + hi];
+				}
+			}
+			double f[NV];
+			#pragma unroll
+			for (int v = 0; v < NV; v++) f[v] = 0;
+			#pragma unroll
+			for (int d = 0; d < 3; d++) {
+				if (not P.active[d]) continue;
+				#pragma unroll
+				for (int v = 0; v < NV; v++) {
+					f[v] += xm[d][v];
+					f[v] -= xp[d][v];
 				}
 			}
 			// apply_fluxes_N: rho1, rho2, mom1, mom2, E1, E2, B
@@ -536,7 +653,8 @@ __global__ void __launch_bounds__(THREADS) npop_update_kernel(const Npop_Params 
 template <int SOLVER>
 int launch_pair(const Npop_Params& P, const int grid, cudaStream_t stream)
 {
-	npop_faces_kernel<SOLVER><<<2 * grid, FACE_THREADS, 0, stream>>>(P);
+	const dim3 tiles((P.n[0] + NTX - 1) / NTX, (P.n[1] + NTY - 1) / NTY, (P.n[2] + P.kchunk - 1) / P.kchunk);
+	npop_faces_kernel<SOLVER><<<tiles, dim3(NTX, NTY), SMEM_FACES, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	npop_update_kernel<<<grid, THREADS, 0, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
@@ -615,6 +733,7 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	if (not (gamma > 1.0) or not (mu0 > 0.0) or not (min_pressure >= 0.0)) return PAMHD_ERR_ARGUMENT;
 	const long long N = (long long)n[0] * n[1] * n[2];
 	if (N > (1ll << 31)) return PAMHD_ERR_ARGUMENT;
+	if ((n[1] + NTY - 1) / NTY > 65535) return PAMHD_ERR_ARGUMENT;   // rows of face tiles: the grid's y extent
 	pamhd_npop* x = new (std::nothrow) pamhd_npop;
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
 	x->device = device;
@@ -639,8 +758,18 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
 	const long long blocks = (N + THREADS - 1) / THREADS;
 	x->grid = int(blocks < 8ll * sms ? blocks : 8ll * sms);
+	const cudaError_t attr = solver == PAMHD_RUSANOV
+		? cudaFuncSetAttribute(npop_faces_kernel<PAMHD_RUSANOV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                       int(SMEM_FACES))
+		: cudaFuncSetAttribute(npop_faces_kernel<PAMHD_HLL_ATHENA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                       int(SMEM_FACES));
+	if (attr != cudaSuccess) return fail(PAMHD_ERR_CUDA);
 	Npop_Params& P = x->base;
 	std::memset(&P, 0, sizeof P);
+	// z chunks so that the face tiles fill the SMs about six times over
+	const long long tiles = (long long)((n[0] + NTX - 1) / NTX) * ((n[1] + NTY - 1) / NTY);
+	const long long chunks = std::max(1ll, std::min((long long)n[2], 18ll * sms / tiles));
+	P.kchunk = int((n[2] + chunks - 1) / chunks);
 	for (int d = 0; d < 3; d++) {
 		P.n[d] = n[d];
 		P.active[d] = n[d] > 1;

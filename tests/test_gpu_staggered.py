@@ -63,6 +63,32 @@ def test_steps_match_oracle(port, solver, shape):
         assert face_err(Fg, Fo) <= STEP_TOL, s
 
 
+@pytest.mark.parametrize("solver", ["rusanov", "hlld_athena"])
+def test_tiled_grid_matches_oracle(port, solver):
+    """A grid of 100 x 254 x 48 cells: the face solves run as 32 x 4 tiles marching several z planes
+    each (five per block on a 148-SM GPU, the last chunk three), with partial tiles at the +x and +y
+    edges; the priming step and two steps against the oracle.  The state is a random 24 x 127 x 50
+    pattern repeated twice along each axis, whose periods fall across the tile edges."""
+    L = (0.1, 0.12, 0.09)
+    U, faces, _ = states.staggered_random((24, 127, 50), L, np.random.default_rng(11))
+    U, faces = np.tile(U, (1, 2, 2, 2)), np.tile(faces, (1, 2, 2, 2))
+    shape = U.shape[1:]
+    n = (shape[2], shape[1], shape[0])
+    gpu, ora = pair(port, n, po.SOLVERS[solver], L)
+    gpu.set_state(U, faces)
+    ora.set_state(U, faces)
+    for s in range(3):
+        cap = 0.0 if s == 0 else 1.0
+        dg = gpu.step(cap)
+        do, flag, _, _ = ora.step(cap)
+        assert flag == 0
+        assert abs(dg - do) <= 1e-13 * max(do, 1e-300)
+        Ug, Fg = gpu.get_state()
+        Uo, Fo = ora.get_state()
+        assert state_err(Ug, Uo) <= STEP_TOL, s
+        assert face_err(Fg, Fo) <= STEP_TOL, s
+
+
 @pytest.mark.parametrize("case", list(STAGGERED_CASES))
 def test_reproduces_reference_program_output(case, tmp_path):
     """The reference program's Alfven waves (Rusanov, CFL 0.5, t = 0 .. 1; with and without a

@@ -39,6 +39,27 @@ def test_rusanov_steps_are_bitwise(port, shape):
         dt = 0.4 * mo
 
 
+@pytest.mark.parametrize("solver", [pg.RUSANOV, pg.HLL])
+def test_tiled_grid_is_bitwise(port, solver):
+    """A grid of 100 x 254 x 48 cells: the face solves run as 32 x 4 tiles marching several z planes
+    each (five per block on a 148-SM GPU, the last chunk three), with partial tiles at the +x and +y
+    edges; Rusanov three steps, HLL one.  The state is a random 24 x 127 x 50 pattern repeated twice
+    along each axis, whose periods fall across the tile edges."""
+    L = (0.1, 0.12, 0.09)
+    U0 = np.tile(states.two_population_random((24, 127, 50), np.random.default_rng(7)), (1, 2, 2, 2))
+    gpu, ora = pair(port, U0.shape[1:], L, solver)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    dt = 1e-4
+    for s in range(3 if solver == pg.RUSANOV else 1):
+        mg = gpu.step(dt)
+        mo, flag, _, _ = ora.step(dt)
+        assert flag == 0
+        assert mg == mo, s
+        np.testing.assert_array_equal(gpu.get_state(), ora.get_state())
+        dt = 0.4 * mo
+
+
 def test_hll_step_is_bitwise(port):
     """One HLL step (the reference's split HLL does not keep a state positive for long, see
     test_two_population_oracle.py)."""
