@@ -415,7 +415,8 @@ __device__ __forceinline__ void stage_fast(const Npop_Params& P, const double u[
 	flags |= f << (8 * A);
 }
 
-// read cell c into slot position r
+// read cell c into slot position r, with its fast speeds along the axes its faces in the tile need
+template <bool CX, bool CY, bool CZ>
 __device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, uint32_t* flg, const int r,
                                            const long long c)
 {
@@ -424,9 +425,9 @@ __device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, ui
 	#pragma unroll
 	for (int v = 0; v < NV; v++) rec[v * NCELLS + r] = u[v];
 	uint32_t flags = 0;
-	stage_fast<0>(P, u, rec, r, flags);
-	stage_fast<1>(P, u, rec, r, flags);
-	stage_fast<2>(P, u, rec, r, flags);
+	if (CX) stage_fast<0>(P, u, rec, r, flags);
+	if (CY) stage_fast<1>(P, u, rec, r, flags);
+	if (CZ) stage_fast<2>(P, u, rec, r, flags);
 	flg[r] = flags;
 }
 
@@ -508,7 +509,8 @@ __global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) np
 		const int ri = (ty + 1) * NW + tx + 1;
 		const long long plane = (long long)nx * ny;
 		const long long col = gx + (long long)nx * gy;
-		// this thread's halo cell, if any: warp 0 the row below the tile, warp 1 the column left of it
+		// this thread's halo cell, if any: warp 0 the row below the tile (its y speed), warp 1 the
+		// column left of it (its x speed)
 		int hr = -1;
 		long long hcol = 0;
 		if (ty == 0 and gx < nx) {
@@ -522,7 +524,9 @@ __global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) np
 		const long long col_mx = (gx == 0 ? nx - 1 : gx - 1) + (long long)nx * gy;
 		const long long col_my = gx + (long long)nx * (gy == 0 ? ny - 1 : gy - 1);
 		// the plane before the chunk, own cells only: the left sides of the first plane's -z faces
-		if (own and P.active[2]) stage_cell(P, smem, flg_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
+		if (own and P.active[2]) {
+			stage_cell<false, false, true>(P, smem, flg_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
+		}
 		for (int k = kb; k < ke; k++) {
 			const int t = k - kb + 1;
 			double* const rec = smem + (t % NSLOTS) * NSLOT;
@@ -530,8 +534,12 @@ __global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) np
 			const double* const prv = smem + ((t - 1) % NSLOTS) * NSLOT;
 			const uint32_t* const pflg = flg_base + ((t - 1) % NSLOTS) * NCELLS;
 			const long long kofs = plane * k;
-			if (own) stage_cell(P, rec, flg, ri, col + kofs);
-			if (hr >= 0) stage_cell(P, rec, flg, hr, hcol + kofs);
+			if (own) stage_cell<true, true, true>(P, rec, flg, ri, col + kofs);
+			if (ty == 0) {
+				if (hr >= 0) stage_cell<false, true, false>(P, rec, flg, hr, hcol + kofs);
+			} else if (hr >= 0) {
+				stage_cell<true, false, false>(P, rec, flg, hr, hcol + kofs);
+			}
 			__syncthreads();
 			if (own) {
 				const long long c = col + kofs;

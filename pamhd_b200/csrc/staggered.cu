@@ -137,25 +137,31 @@ constexpr int SSLOT = SREC * SCELLS;        // doubles of one slot
 constexpr int SSLOTS = 3;
 constexpr size_t SMEM_FACES = SSLOTS * (SSLOT * sizeof(double) + SCELLS * sizeof(uint32_t));
 
-// read cell c from HBM and derive its record into slot position r
+/*
+Read cell c from HBM and derive its record into slot position r, with the
+fast speeds along the axes its faces in the tile need (a halo cell only
+along the axis of the face it shares with the tile).
+*/
+template <bool CX, bool CY, bool CZ>
 __device__ __forceinline__ void stage_cell(const Stag_Params& P, double* rec, uint32_t* bad, const int r,
                                            const long long c)
 {
 	double U[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) U[v] = __ldg(P.U + v * P.N + c);
-	const Derived d = derive<true, true, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
+	const Derived d = derive<CX, CY, CZ>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
 	#pragma unroll
 	for (int v = 0; v < 8; v++) rec[v * SCELLS + r] = U[v];
 	rec[8 * SCELLS + r] = d.rinv;
 	rec[9 * SCELLS + r] = d.p;
-	rec[10 * SCELLS + r] = d.cf[0];
-	rec[11 * SCELLS + r] = d.cf[1];
-	rec[12 * SCELLS + r] = d.cf[2];
+	if (CX) rec[10 * SCELLS + r] = d.cf[0];
+	if (CY) rec[11 * SCELLS + r] = d.cf[1];
+	if (CZ) rec[12 * SCELLS + r] = d.cf[2];
 	// one byte of flags per face direction: the reference checks the fast speed of each face
-	// along that face's normal, so a failed speed belongs to the failing directions only
+	// along that face's normal, so a failed speed belongs to the failing directions only (with
+	// one axis derived, d.bad is that axis's)
 	uint32_t packed = d.bad | (d.bad << 8) | (d.bad << 16);
-	if (d.bad == PAMHD_FLAG_WAVE_SPEED) {
+	if (CX and CY and CZ and d.bad == PAMHD_FLAG_WAVE_SPEED) {
 		packed = derive<true, false, false>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad
 			| (derive<false, true, false>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad << 8)
 			| (derive<false, false, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas).bad << 16);
@@ -239,7 +245,8 @@ __global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3)
 	const int ri = (ty + 1) * SW + tx + 1;
 	const long long plane = (long long)nx * ny;
 	const long long col = gx + (long long)nx * gy;
-	// this thread's halo cell, if any: warp 0 the row below the tile, warp 1 the column left of it
+	// this thread's halo cell, if any: warp 0 the row below the tile (its y speed), warp 1 the column
+	// left of it (its x speed)
 	int hr = -1;
 	long long hcol = 0;
 	if (ty == 0 and gx < nx) {
@@ -256,7 +263,7 @@ __global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3)
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	bool zero = false;
 	// the plane before the chunk, own cells only: the left sides of the first plane's -z faces
-	if (own) stage_cell(P, smem, bad_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
+	if (own) stage_cell<false, false, true>(P, smem, bad_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
 	for (int k = kb; k < ke; k++) {
 		const int t = k - kb + 1;
 		double* const rec = smem + (t % SSLOTS) * SSLOT;
@@ -264,8 +271,12 @@ __global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3)
 		const double* const prv = smem + ((t - 1) % SSLOTS) * SSLOT;
 		const uint32_t* const pbad = bad_base + ((t - 1) % SSLOTS) * SCELLS;
 		const long long kofs = plane * k;
-		if (own) stage_cell(P, rec, bad, ri, col + kofs);
-		if (hr >= 0) stage_cell(P, rec, bad, hr, hcol + kofs);
+		if (own) stage_cell<true, true, true>(P, rec, bad, ri, col + kofs);
+		if (ty == 0) {
+			if (hr >= 0) stage_cell<false, true, false>(P, rec, bad, hr, hcol + kofs);
+		} else if (hr >= 0) {
+			stage_cell<true, false, false>(P, rec, bad, hr, hcol + kofs);
+		}
 		__syncthreads();
 		if (own) {
 			const long long c = col + kofs;
