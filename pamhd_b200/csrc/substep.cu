@@ -22,9 +22,13 @@ length.  A step is planned on the device and driven from the host:
 then for every substep s:
   faces_kernel     cells with s % M == 0 solve their +d faces and add
                    (substep M) F to both sides' flux slots (get_fluxes,
-                   mhd/solve.hpp:254-392);
+                   mhd/solve.hpp:254-392), a slot's first contribution
+                   since its cell's last update added to zero instead of
+                   to the slot's old value;
   update_kernel    cells whose period divides s apply their slots
-                   (update_mhd_state, mhd/solve.hpp:1543-1587) and zero them.
+                   (update_mhd_state, mhd/solve.hpp:1543-1587); the slots
+                   are not cleared (the reference zeroes them, :1596-1602),
+                   the faces kernel starts them afresh instead.
 Layout: state 8 x N, flux slots 6 x 8 x N (each cell's -x, +x, -y, +y, -z,
 +z), the speed of every cell's -d face 3 x N, exponents and periods
 N int32, x fastest, no ghosts.  A slow path: one host round trip per step
@@ -220,17 +224,26 @@ __global__ void reach_kernel(const Sub_Params P)
 
 template <int SOLVER, int A>
 __device__ __forceinline__ void plus_face(const Sub_Params& P, const long long c, const int i, const int j,
-                                          const int k, const double Uc[8], const Derived& dc, const double min_dt)
+                                          const int k, const double Uc[8], const Derived& dc, const double min_dt,
+                                          const bool fresh_plus, const int sub, const int m)
 {
 	const long long up = wrap(P, i + (A == 0), j + (A == 1), k + (A == 2));
 	double* const plus = P.slot + (size_t(2 * A + 1) * 8) * P.N + c;   // the cell's +A slot
 	double* const minus = P.slot + (size_t(2 * A) * 8) * P.N + up;     // the neighbour's -A slot
-	// the slots are read before the solve, so that their latency overlaps its arithmetic
+	/*
+	A slot holds the contributions since its cell's last update.  The face is
+	solved every m substeps and m divides the periods of both its cells, so its
+	first contribution after a cell's update comes at substep sub with (sub - m) a
+	multiple of that cell's period: there the slot starts from zero instead of
+	being read (the update does not clear it).  The slots are read before the
+	solve, so that their latency overlaps its arithmetic.
+	*/
+	const bool fresh_minus = (sub - m) % P.P[up] == 0;
 	double pv[8], mv[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
-		pv[v] = plus[v * P.N];
-		mv[v] = minus[v * P.N];
+		pv[v] = fresh_plus ? 0.0 : plus[v * P.N];
+		mv[v] = fresh_minus ? 0.0 : minus[v * P.N];
 	}
 	double Uu[8];
 	#pragma unroll
@@ -273,9 +286,10 @@ __global__ void __launch_bounds__(128, 3) faces_kernel(const Sub_Params P, const
 		for (int v = 0; v < 8; v++) Uc[v] = P.U[v * P.N + c];
 		const Derived dc = derive<true, true, true>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
 		const double min_dt = substep * m;
-		if (P.active[0]) plus_face<SOLVER, 0>(P, c, i, j, k, Uc, dc, min_dt);
-		if (P.active[1]) plus_face<SOLVER, 1>(P, c, i, j, k, Uc, dc, min_dt);
-		if (P.active[2]) plus_face<SOLVER, 2>(P, c, i, j, k, Uc, dc, min_dt);
+		const bool fresh = (s - m) % P.P[c] == 0;
+		if (P.active[0]) plus_face<SOLVER, 0>(P, c, i, j, k, Uc, dc, min_dt, fresh, s, m);
+		if (P.active[1]) plus_face<SOLVER, 1>(P, c, i, j, k, Uc, dc, min_dt, fresh, s, m);
+		if (P.active[2]) plus_face<SOLVER, 2>(P, c, i, j, k, Uc, dc, min_dt, fresh, s, m);
 	}
 }
 
@@ -319,11 +333,6 @@ __global__ void update_kernel(const Sub_Params P, const int s)
 		}
 		#pragma unroll
 		for (int v = 0; v < 8; v++) P.U[v * N + c] = u[v];
-		#pragma unroll
-		for (int sl = 0; sl < 6; sl++) {
-			#pragma unroll
-			for (int v = 0; v < 8; v++) P.slot[(size_t(sl) * 8 + v) * N + c] = 0.0;
-		}
 	}
 }
 
