@@ -129,6 +129,40 @@ def fp64_roof(n, kernel_ms, clocks):
             "peak_source": f"148 SMs x 64 FP64 FMA/cycle x 2 at {mhz:.0f} MHz (nominal rate, measured clock)"}
 
 
+def pinned(shape, like=None):
+    """A host array in pinned (page-locked) memory, as a numpy view of a torch tensor; returns the
+    tensor (to keep the memory alive) and the view, filled from `like` when given."""
+    import torch
+    t = torch.empty(tuple(shape), dtype=torch.float64, pin_memory=True)
+    v = t.numpy()
+    if like is not None:
+        v[...] = like
+    return t, v
+
+
+def section_roofline(n, key, alg_bytes, updates, ms, clk, scope):
+    """Roofline of a step of several kernels, taken as a whole: the algorithmic bytes of one step
+    (the state read and written once per cell-update) over the step's measured time against the
+    measured copy bandwidth; the DRAM traffic and the FP64 flops of one step from the committed
+    ncu counts (profiles/traffic.txt, scaled from the captured grid to n^3 cells); the FP64 roof at
+    the SM clock sampled during the timed region."""
+    peak, peak_kind = peaks()
+    achieved = alg_bytes * updates / (ms / 1e3) / 1e9
+    out = {"bound": "hbm", "scope": scope, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "traffic": ncu_count(n, key), "traffic_scope": "one step, all its kernels",
+           "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+           "algorithmic_bytes_per_cell_update": alg_bytes, "step_ms": ms}
+    flops = ncu_count(n, key + "_fp64")
+    if flops is not None:
+        mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+        fpeak = 148 * 64 * 2 * mhz * 1e6 / 1e12
+        fa = flops / (ms / 1e3) / 1e12
+        out["fp64"] = {"achieved": fa, "peak": fpeak, "unit": "TFLOP/s", "frac": fa / fpeak,
+                       "flop_per_cell_update": flops / updates,
+                       "peak_source": f"148 SMs x 64 FP64 FMA/cycle x 2 at {mhz:.0f} MHz (nominal rate, measured clock)"}
+    return out
+
+
 class ClockSampler:
     """Samples SM clock and throttle reasons with NVML while the timed region runs."""
 
@@ -534,12 +568,24 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
         st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        e0.record(st)
-        ctx.steps(steps, T_END)
-        e1.record(st)
-        ctx.sync()
-        torch.cuda.synchronize()
+        with ClockSampler(local) as clocks:
+            e0.record(st)
+            ctx.steps(steps, T_END)
+            e1.record(st)
+            ctx.sync()
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        # end to end through the Python API: pinned host arrays in, the priming step and `steps`
+        # steps, pinned host arrays out, host clock
+        keep = [pinned(U.shape, U), pinned(faces.shape, faces), pinned(U.shape), pinned(faces.shape)]
+        hU, hF, hUo, hFo = (k[1] for k in keep)
+        t0 = time.perf_counter()
+        ctx.set_state(hU, hF)
+        ctx.step(0.0)
+        ctx.steps(steps, T_END)
+        ctx.get_state(out=(hUo, hFo))
+        e2e_sec = time.perf_counter() - t0
+    moved = (U.nbytes + faces.nbytes) / (steps + 1)
     out = {
         "workload": f"{n}^3 periodic, {solver}, smooth state with a divergence-free face field, CFL 0.4",
         "value": n ** 3 / (ms * 1e-3),
@@ -547,6 +593,13 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
         "ms_per_step": ms,
         "steps": steps,
         "gpu_launches": 3 * steps,
+        "roofline": section_roofline(n, "staggered_step_hlld", 176, n ** 3, ms, clocks.summary(),
+                                     "whole step: faces_kernel + field_kernel + cell_kernel"),
+        "e2e": {"value": n ** 3 * (steps + 1) / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": moved,
+                "d2h_bytes_per_step": moved,
+                "what": f"StaggeredContext.set_state from pinned host arrays + the priming step + {steps} "
+                        f"steps + get_state to pinned host arrays, host clock"},
+        "clocks": clocks.summary(),
     }
     if cpu:
         from oracle import pyoracle as po
@@ -585,12 +638,22 @@ def two_population_section(local, n=256, steps=20, cpu=True):
         st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        e0.record(st)
-        ctx.run(steps, 0.4, T_END)
-        e1.record(st)
-        ctx.sync()
-        torch.cuda.synchronize()
+        with ClockSampler(local) as clocks:
+            e0.record(st)
+            ctx.run(steps, 0.4, T_END)
+            e1.record(st)
+            ctx.sync()
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
+        # end to end through the Python API: a pinned host array in, `steps` steps of the device loop,
+        # a pinned host array out, host clock
+        keep = [pinned(U.shape, U), pinned(U.shape)]
+        hU, hUo = (k[1] for k in keep)
+        t0 = time.perf_counter()
+        ctx.set_state(hU)
+        ctx.run(steps, 0.4, T_END)
+        ctx.get_state(out=hUo)
+        e2e_sec = time.perf_counter() - t0
     out = {
         "workload": f"{n}^3 periodic, two populations sharing one field, split Rusanov, CFL 0.4",
         "value": n ** 3 / (ms * 1e-3),
@@ -598,6 +661,13 @@ def two_population_section(local, n=256, steps=20, cpu=True):
         "ms_per_step": ms,
         "steps": steps,
         "gpu_launches": 2 * steps,
+        "roofline": section_roofline(n, "two_population_step_rusanov", 208, n ** 3, ms, clocks.summary(),
+                                     "whole step: npop_faces_kernel + npop_update_kernel"),
+        "e2e": {"value": n ** 3 * steps / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": U.nbytes / steps,
+                "d2h_bytes_per_step": U.nbytes / steps,
+                "what": f"TwoPopulationContext.set_state from a pinned host array + {steps} steps + "
+                        f"get_state to a pinned host array, host clock"},
+        "clocks": clocks.summary(),
     }
     if cpu:
         from oracle import pyoracle as po
@@ -640,21 +710,41 @@ def substep_section(local, n=128, steps=10, solver="hlld_athena", cpu=True):
         ctx.step(0.0)
         ctx.step(T_END)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        subs = 0
-        for _ in range(steps):
-            subs += ctx.step(T_END)[1]
-        sec = time.perf_counter() - t0
+        with ClockSampler(local) as clocks:
+            t0 = time.perf_counter()
+            subs = 0
+            for _ in range(steps):
+                subs += ctx.step(T_END)[1]
+            sec = time.perf_counter() - t0
         periods = ctx.periods()
+        # end to end through the Python API: a pinned host array in, the priming step and `steps`
+        # steps, a pinned host array out, host clock
+        keep = [pinned(U.shape, U), pinned(U.shape)]
+        hU, hUo = (k[1] for k in keep)
+        t0 = time.perf_counter()
+        ctx.set_state(hU)
+        ctx.step(0.0)
+        for _ in range(steps):
+            ctx.step(T_END)
+        ctx.get_state(out=hUo)
+        e2e_sec = time.perf_counter() - t0
     updates = float((subs / steps) * (1.0 / periods).sum())
+    ms = 1e3 * sec / steps
     out = {
         "workload": f"{n}^3 periodic, {solver}, exponent 0 for y < 0 and 1 elsewhere, CFL 0.4",
         "value": n ** 3 * steps / sec,
         "unit": "cell-steps/s",
         "updates_per_s": updates * steps / sec,
-        "ms_per_step": 1e3 * sec / steps,
+        "ms_per_step": ms,
         "substeps_per_step": subs / steps,
         "timing": "host clock around synchronous steps (each step plans on the device and reads the plan back)",
+        "roofline": section_roofline(n, "substep_step_hlld", 128, updates, ms, clocks.summary(),
+                                     "whole step: the plan's kernels and faces_kernel + update_kernel per substep"),
+        "e2e": {"value": n ** 3 * (steps + 1) / e2e_sec, "unit": "cell-steps/s",
+                "h2d_bytes_per_step": U.nbytes / (steps + 1), "d2h_bytes_per_step": U.nbytes / (steps + 1),
+                "what": f"SubstepContext.set_state from a pinned host array + the priming step + {steps} "
+                        f"steps + get_state to a pinned host array, host clock"},
+        "clocks": clocks.summary(),
     }
     if cpu:
         from oracle import pyoracle as po

@@ -406,9 +406,13 @@ class StaggeredContext:
         ptrs = (ctypes.c_void_p * 9)(*[bg[k].ctypes.data for k in range(9)])
         self._check(self.L.pamhd_gpu_staggered_set_background(self.h, ptrs), "pamhd_gpu_staggered_set_background")
 
-    def get_state(self):
-        U = np.empty((8,) + self.shape)
-        faces = np.empty((3,) + self.shape)
+    def get_state(self, out=None):
+        """Returns (U, faces); out: an optional pair of C-contiguous float64 arrays of those shapes to
+        fill (pinned host memory makes the copy run at full speed)."""
+        U, faces = out if out is not None else (np.empty((8,) + self.shape), np.empty((3,) + self.shape))
+        for a, rows in ((U, 8), (faces, 3)):
+            if a.shape != (rows,) + self.shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("get_state: out arrays must be C-contiguous float64 of the state's shapes")
         fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
         self._check(self.L.pamhd_gpu_staggered_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
                     "pamhd_gpu_staggered_get_state")
@@ -510,8 +514,11 @@ class TwoPopulationContext:
         ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
         self._check(self.L.pamhd_gpu_npop_set_state(self.h, ptrs), "pamhd_gpu_npop_set_state")
 
-    def get_state(self) -> np.ndarray:
-        U = np.empty((13,) + self.shape)
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Returns the state (13, nz, ny, nx); out: an optional C-contiguous float64 array to fill."""
+        U = out if out is not None else np.empty((13,) + self.shape)
+        if U.shape != (13,) + self.shape or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError("get_state: out must be C-contiguous float64 of shape (13, nz, ny, nx)")
         ptrs = (ctypes.c_void_p * 13)(*[U[k].ctypes.data for k in range(13)])
         self._check(self.L.pamhd_gpu_npop_get_state(self.h, ptrs), "pamhd_gpu_npop_get_state")
         return U
@@ -601,8 +608,11 @@ class SubstepContext:
         self._check(self.L.pamhd_gpu_substep_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
                     "pamhd_gpu_substep_set_state")
 
-    def get_state(self) -> np.ndarray:
-        U = np.empty((8,) + self.shape)
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Returns the state (8, nz, ny, nx); out: an optional C-contiguous float64 array to fill."""
+        U = out if out is not None else np.empty((8,) + self.shape)
+        if U.shape != (8,) + self.shape or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError("get_state: out must be C-contiguous float64 of shape (8, nz, ny, nx)")
         self._check(self.L.pamhd_gpu_substep_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)])),
                     "pamhd_gpu_substep_get_state")
         return U

@@ -687,7 +687,6 @@ struct pamhd_npop {
 	Speed_Max* red = nullptr;
 	Clock* clock = nullptr;
 	Status* status = nullptr;
-	double* staging = nullptr;   // pinned, 13 x N
 	int cur = 0;
 	long long steps = 0;
 	int grid = 0;
@@ -758,8 +757,7 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 		or cudaMalloc(&x->X, 3 * bytes) != cudaSuccess
 		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
 		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
-		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess
-		or cudaMallocHost(&x->staging, bytes) != cudaSuccess) {
+		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
 	int sms = 0;
@@ -811,7 +809,6 @@ int pamhd_gpu_npop_destroy(pamhd_npop* x)
 	cudaFree(x->red);
 	cudaFree(x->clock);
 	cudaFree(x->status);
-	cudaFreeHost(x->staging);
 	if (x->stream != nullptr) cudaStreamDestroy(x->stream);
 	delete x;
 	return PAMHD_OK;
@@ -824,9 +821,12 @@ int pamhd_gpu_npop_set_state(pamhd_npop* x, const double* const state[13])
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
 	const size_t n = size_t(x->N);
-	for (int v = 0; v < NV; v++) std::memcpy(x->staging + v * n, state[v], n * sizeof(double));
 	x->cur = 0;
-	PAMHD_TRY(check(cudaMemcpyAsync(x->U[0], x->staging, NV * n * sizeof(double), cudaMemcpyHostToDevice, x->stream)));
+	// one copy per array straight from the caller's memory (at full speed when it is pinned)
+	for (int v = 0; v < NV; v++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(x->U[0] + v * n, state[v], n * sizeof(double), cudaMemcpyHostToDevice,
+		                                x->stream)));
+	}
 	PAMHD_TRY(reset(*x));
 	x->loaded = true;
 	return PAMHD_OK;
@@ -839,11 +839,11 @@ int pamhd_gpu_npop_get_state(pamhd_npop* x, double* const state[13])
 	if (not x->loaded) return PAMHD_ERR_STATE;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const size_t n = size_t(x->N);
-	PAMHD_TRY(check(cudaMemcpyAsync(x->staging, x->U[x->cur], NV * n * sizeof(double), cudaMemcpyDeviceToHost,
-	                                x->stream)));
-	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
-	for (int v = 0; v < NV; v++) std::memcpy(state[v], x->staging + v * n, n * sizeof(double));
-	return PAMHD_OK;
+	for (int v = 0; v < NV; v++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(state[v], x->U[x->cur] + v * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+		                                x->stream)));
+	}
+	return check(cudaStreamSynchronize(x->stream));
 }
 
 int pamhd_gpu_npop_sync(pamhd_npop* x)

@@ -564,7 +564,6 @@ struct pamhd_stag {
 	Speed_Max* red = nullptr;
 	Clock* clock = nullptr;
 	Status* status = nullptr;
-	double* staging = nullptr;   // pinned host buffer of 11 x N doubles
 	int cur = 0;
 	long long steps = 0;         // launched steps since set_state (the ring phase)
 	int grid = 0;
@@ -664,8 +663,7 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 		or cudaMalloc(&x->F, 24 * n * sizeof(double)) != cudaSuccess
 		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
 		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
-		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess
-		or cudaMallocHost(&x->staging, 11 * n * sizeof(double)) != cudaSuccess) {
+		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
 	int sms = 0;
@@ -731,7 +729,6 @@ int pamhd_gpu_staggered_destroy(pamhd_stag* x)
 	cudaFree(x->red);
 	cudaFree(x->clock);
 	cudaFree(x->status);
-	cudaFreeHost(x->staging);
 	if (x->stream != nullptr) cudaStreamDestroy(x->stream);
 	delete x;
 	return PAMHD_OK;
@@ -745,12 +742,16 @@ int pamhd_gpu_staggered_set_state(pamhd_stag* x, const double* const cells[8], c
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
 	const size_t n = size_t(x->N);
-	for (int v = 0; v < 8; v++) std::memcpy(x->staging + v * n, cells[v], n * sizeof(double));
-	for (int d = 0; d < 3; d++) std::memcpy(x->staging + (8 + d) * n, faces[d], n * sizeof(double));
 	x->cur = 0;
-	PAMHD_TRY(check(cudaMemcpyAsync(x->U[0], x->staging, 8 * n * sizeof(double), cudaMemcpyHostToDevice, x->stream)));
-	PAMHD_TRY(check(cudaMemcpyAsync(x->B[0], x->staging + 8 * n, 3 * n * sizeof(double), cudaMemcpyHostToDevice,
-	                                x->stream)));
+	// one copy per array straight from the caller's memory (at full speed when it is pinned)
+	for (int v = 0; v < 8; v++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(x->U[0] + v * n, cells[v], n * sizeof(double), cudaMemcpyHostToDevice,
+		                                x->stream)));
+	}
+	for (int d = 0; d < 3; d++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(x->B[0] + d * n, faces[d], n * sizeof(double), cudaMemcpyHostToDevice,
+		                                x->stream)));
+	}
 	PAMHD_TRY(reset_ring(*x));
 	x->loaded = true;
 	return PAMHD_OK;
@@ -785,18 +786,17 @@ int pamhd_gpu_staggered_get_state(pamhd_stag* x, double* const cells[8], double*
 	if (not x->loaded) return PAMHD_ERR_STATE;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const size_t n = size_t(x->N);
-	PAMHD_TRY(check(cudaMemcpyAsync(x->staging, x->U[x->cur], 8 * n * sizeof(double), cudaMemcpyDeviceToHost,
-	                                x->stream)));
-	if (faces != nullptr) {
-		PAMHD_TRY(check(cudaMemcpyAsync(x->staging + 8 * n, x->B[x->cur], 3 * n * sizeof(double),
-		                                cudaMemcpyDeviceToHost, x->stream)));
+	for (int v = 0; v < 8; v++) {
+		PAMHD_TRY(check(cudaMemcpyAsync(cells[v], x->U[x->cur] + v * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+		                                x->stream)));
 	}
-	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
-	for (int v = 0; v < 8; v++) std::memcpy(cells[v], x->staging + v * n, n * sizeof(double));
 	if (faces != nullptr) {
-		for (int d = 0; d < 3; d++) std::memcpy(faces[d], x->staging + (8 + d) * n, n * sizeof(double));
+		for (int d = 0; d < 3; d++) {
+			PAMHD_TRY(check(cudaMemcpyAsync(faces[d], x->B[x->cur] + d * n, n * sizeof(double),
+			                                cudaMemcpyDeviceToHost, x->stream)));
+		}
 	}
-	return PAMHD_OK;
+	return check(cudaStreamSynchronize(x->stream));
 }
 
 int pamhd_gpu_staggered_sync(pamhd_stag* x)

@@ -510,9 +510,9 @@ int pamhd_gpu_substep_set_state(pamhd_sub* x, const double* const cells[8])
 		PAMHD_TRY(check(cudaMemcpyAsync(x->U + v * n, cells[v], n * sizeof(double), cudaMemcpyHostToDevice,
 		                                x->stream)));
 	}
-	// no face speeds yet (the first step is the reference's dt = 0 priming step), empty slots
+	// no face speeds yet (the first step is the reference's dt = 0 priming step); the flux slots
+	// need no clearing: each is written afresh before it is read
 	PAMHD_TRY(check(cudaMemsetAsync(x->speed, 0, 3 * n * sizeof(double), x->stream)));
-	PAMHD_TRY(check(cudaMemsetAsync(x->slot, 0, 48 * n * sizeof(double), x->stream)));
 	const Status s{0u, 0u, ~0ull};
 	PAMHD_TRY(check(cudaMemcpyAsync(x->status, &s, sizeof s, cudaMemcpyHostToDevice, x->stream)));
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));

@@ -171,8 +171,11 @@ def test_batched_steps_equal_single_steps(port):
     tb, nb, _ = b.time()
     assert tb == t and nb == n + 1   # the priming step counts
     Ua, Fa = a.get_state()
-    Ub, Fb = b.get_state()
+    Ub, Fb = np.zeros_like(Ua), np.zeros_like(Fa)
+    assert b.get_state(out=(Ub, Fb))[0] is Ub   # the caller's arrays, filled in place
     assert np.array_equal(Ua, Ub) and np.array_equal(Fa, Fb)
+    with pytest.raises(ValueError):
+        b.get_state(out=(Ub[:, ::2], Fb))
 
 
 def test_divergence_is_kept():

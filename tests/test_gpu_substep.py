@@ -64,6 +64,9 @@ def test_zero_exponents_are_the_plain_step():
         db = b.step(cap)
         assert k == 1 and abs(da - db) <= 1e-13 * max(db, 1e-300)
         assert err(a.get_state(), b.get_state()) <= STEP_TOL
+    out = np.zeros_like(U)
+    assert a.get_state(out=out) is out   # the caller's array, filled in place
+    assert np.array_equal(out, a.get_state())
 
 
 def test_failure_is_reported():

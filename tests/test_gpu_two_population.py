@@ -105,7 +105,11 @@ def test_device_loop_equals_host_loop(port):
     gpu.sync()
     tg, ng, _ = gpu.time()
     assert tg == t and ng == steps
-    np.testing.assert_array_equal(gpu.get_state(), ora.get_state())
+    out = np.zeros_like(U0)
+    assert gpu.get_state(out=out) is out   # the caller's array, filled in place
+    np.testing.assert_array_equal(out, ora.get_state())
+    with pytest.raises(ValueError):
+        gpu.get_state(out=out[:12])
 
 
 def test_failure_reports_oracle_face_and_keeps_state(port):
