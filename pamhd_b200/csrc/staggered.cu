@@ -23,7 +23,8 @@ One step is three launches on the context's stream:
                  rule, mhd/solve.hpp:1933-2007, substepping.hpp:285-338);
                  the new normal field of every cell's three -d faces from
                  the twelve edge terms of assign_face_dBs_f{x,y,z}
-                 (mhd/solve.hpp:587-1494, equal-size neighbours) and
+                 (mhd/solve.hpp:587-1494, equal-size neighbours), read from
+                 planes of tangential fluxes staged in shared memory, and
                  Face_B += Face_dB / area (mhd/solve.hpp:1589-1593);
   cell_kernel    the same dt (all its inputs loaded first); the cell update of update_mhd_state
                  (mhd/solve.hpp:1543-1587), then update_vol_B with constant
@@ -71,6 +72,7 @@ struct Stag_Params {
 	double max_dt;                   // >= 0: cap of dt; < 0: the cap is t_end - t
 	double t_end;
 	int kchunk;                      // z planes per face-solve block
+	int fchunk;                      // z planes per face-field block
 };
 
 __device__ __forceinline__ long long wrap_index(const Stag_Params& P, int i, int j, int k)
@@ -324,47 +326,43 @@ __device__ __forceinline__ double step_dt(const Stag_Params& P)
 	return (cap <= smallest) ? cap : smallest;
 }
 
-__device__ __forceinline__ double fluxB(const Stag_Params& P, const int axis, const int comp, const long long cell)
-{
-	return P.F[(axis * 8 + 5 + comp) * P.N + cell];
-}
-
 /*
-Change of the normal field of the -d face of cell (i, j, k), times the face
-area: the twelve edge terms of assign_face_dBs_f{x,y,z} that reach the face,
-in the order of the oracle (d-directed fluxes one cell away along a and b,
-then the a- and b-directed fluxes of the faces sharing an edge with it).
+Change of the normal field of the -D face of a cell, times the face area: the
+twelve edge terms of assign_face_dBs_f{x,y,z} that reach the face, in the
+order of the oracle (D-directed fluxes one cell away along a and b, then the
+a- and b-directed fluxes of the faces sharing an edge with it).
+get(axis, comp, ox, oy, oz) is the flux of field component comp through the
+-axis face of the cell at offset (ox, oy, oz) from this one.
 */
-template <int D>
-__device__ __forceinline__ double face_dB(const Stag_Params& P, const int i, const int j, const int k, const double dt)
+template <int D, class Get>
+__device__ __forceinline__ double face_dB(const Stag_Params& P, const Get& get, const double dt)
 {
 	constexpr int A = (D + 1) % 3, Bd = (D + 2) % 3;
 	const double La = P.len[A], Lb = P.len[Bd];
-	const int c[3] = {i, j, k};
-	auto cell = [&](const int da, const int db, const int dd) {
-		int m[3] = {c[0], c[1], c[2]};
-		m[A] += da;
-		m[Bd] += db;
-		m[D] += dd;
-		return wrap_index(P, m[0], m[1], m[2]);
+	auto at = [&](const int axis, const int comp, const int da, const int db, const int dd) {
+		int o[3] = {0, 0, 0};
+		o[A] += da;
+		o[Bd] += db;
+		o[D] += dd;
+		return get(axis, comp, o[0], o[1], o[2]);
 	};
-	auto e1 = [&](const long long s) { return fluxB(P, D, A, s) * dt * Lb / 4; };
-	auto e2 = [&](const long long s) { return -(fluxB(P, D, Bd, s) * dt * La / 4); };
-	auto e3 = [&](const long long s) { return -(fluxB(P, A, D, s) * dt * Lb / 4); };
-	auto e4 = [&](const long long s) { return fluxB(P, Bd, D, s) * dt * La / 4; };
+	auto e1 = [&](const int da, const int db, const int dd) { return at(D, A, da, db, dd) * dt * Lb / 4; };
+	auto e2 = [&](const int da, const int db, const int dd) { return -(at(D, Bd, da, db, dd) * dt * La / 4); };
+	auto e3 = [&](const int da, const int db, const int dd) { return -(at(A, D, da, db, dd) * dt * Lb / 4); };
+	auto e4 = [&](const int da, const int db, const int dd) { return at(Bd, D, da, db, dd) * dt * La / 4; };
 	double dB = 0;
-	dB += e1(cell(+1, 0, 0));
-	dB -= e1(cell(-1, 0, 0));
-	dB -= e2(cell(0, +1, 0));
-	dB += e2(cell(0, -1, 0));
-	dB += e3(cell(+1, 0, 0));
-	dB += e3(cell(+1, 0, -1));
-	dB -= e3(cell(0, 0, 0));
-	dB -= e3(cell(0, 0, -1));
-	dB -= e4(cell(0, +1, 0));
-	dB -= e4(cell(0, +1, -1));
-	dB += e4(cell(0, 0, 0));
-	dB += e4(cell(0, 0, -1));
+	dB += e1(+1, 0, 0);
+	dB -= e1(-1, 0, 0);
+	dB -= e2(0, +1, 0);
+	dB += e2(0, -1, 0);
+	dB += e3(+1, 0, 0);
+	dB += e3(+1, 0, -1);
+	dB -= e3(0, 0, 0);
+	dB -= e3(0, 0, -1);
+	dB -= e4(0, +1, 0);
+	dB -= e4(0, +1, -1);
+	dB += e4(0, 0, 0);
+	dB += e4(0, 0, -1);
 	return dB;
 }
 
@@ -399,35 +397,127 @@ __device__ __forceinline__ double step_start(const Stag_Params& P, bool& skip)
 	return skip ? 0.0 : step_dt(P);
 }
 
-// Face_B += Face_dB / area for the three -d faces of every cell
-__global__ void __launch_bounds__(THREADS) field_kernel(const Stag_Params P)
+/*
+Face_B += Face_dB / area for the three -d faces of every cell, as a z-marching
+stencil: a block of FTX x FTY threads owns a column of cells; the six
+tangential field fluxes (component b of every -a face, a != b) of each plane,
+with a one-cell halo in x and y, are staged once in shared memory, and the
+twelve terms of each face are read from the planes k - 1, k and k + 1 there.
+Four plane slots rotate, so one barrier per plane keeps a plane's stores
+apart from the reads of the three planes before it.
+*/
+constexpr int FTX = 32, FTY = 8;
+constexpr int FW = FTX + 2, FH = FTY + 2;
+constexpr int FPLANE = 6 * FW * FH;        // doubles of one staged plane
+constexpr int FSLOTS = 4;
+constexpr size_t SMEM_FIELD = FSLOTS * FPLANE * sizeof(double);
+
+// a thread's share of a staged plane: elements tid + i FTX FTY, i < FPER
+constexpr int FPER = (FPLANE + FTX * FTY - 1) / (FTX * FTY);
+
+/*
+The six arrays of a staged plane: 2 axis + j holds component (axis + 1 + j)
+mod 3 of the -axis faces.  off[i]: the global offset, within its z plane, of
+this thread's i-th element (-1 past the plane's end).
+*/
+__device__ __forceinline__ void plane_offsets(const Stag_Params& P, const int gx0, const int gy0, long long off[FPER])
 {
+	const int nx = P.n[0], ny = P.n[1];
+	const int tid = threadIdx.y * FTX + threadIdx.x;
+	#pragma unroll
+	for (int i = 0; i < FPER; i++) {
+		const int e = tid + i * FTX * FTY;
+		off[i] = -1;
+		if (e < FPLANE) {
+			const int arr = e / (FW * FH);
+			const int rem = e - arr * (FW * FH);
+			const int row = rem / FW, col = rem - row * FW;
+			const int axis = arr >> 1, comp = (axis + 1 + (arr & 1)) % 3;
+			const long long x = ((gx0 - 1 + col) % nx + nx) % nx;
+			const long long y = ((gy0 - 1 + row) % ny + ny) % ny;
+			off[i] = (long long)(axis * 8 + 5 + comp) * P.N + x + nx * y;
+		}
+	}
+}
+
+__device__ __forceinline__ void load_plane(const Stag_Params& P, const long long off[FPER], const int pz, double v[FPER])
+{
+	const int nz = P.n[2];
+	const long long z = (long long)P.n[0] * P.n[1] * (((pz % nz) + nz) % nz);
+	#pragma unroll
+	for (int i = 0; i < FPER; i++) v[i] = off[i] >= 0 ? P.F[off[i] + z] : 0.0;
+}
+
+__device__ __forceinline__ void store_plane(double* slot, const double v[FPER])
+{
+	const int tid = threadIdx.y * FTX + threadIdx.x;
+	#pragma unroll
+	for (int i = 0; i < FPER; i++) {
+		const int e = tid + i * FTX * FTY;
+		if (e < FPLANE) slot[e] = v[i];
+	}
+}
+
+__global__ void __launch_bounds__(FTX * FTY, 3) field_kernel(const Stag_Params P)
+{
+	extern __shared__ __align__(16) double fsm[];
 	__shared__ double s_dt;
 	__shared__ int s_skip;
-	if (threadIdx.x == 0) {
+	const int tx = threadIdx.x, ty = threadIdx.y;
+	if (tx == 0 and ty == 0) {
 		bool skip;
 		s_dt = step_start(P, skip);
 		s_skip = skip ? 1 : 0;
 	}
 	__syncthreads();
 	const double dt = s_dt;
-	const bool skip = s_skip != 0;
-	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
-		if (skip) {
-			#pragma unroll
-			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
-			continue;
+	const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+	const int gx0 = blockIdx.x * FTX, gy0 = blockIdx.y * FTY;
+	const int gx = gx0 + tx, gy = gy0 + ty;
+	const bool own = gx < nx and gy < ny;
+	const int kb = blockIdx.z * P.fchunk;
+	const int ke = min(nz, kb + P.fchunk);
+	const long long plane = (long long)nx * ny;
+	const long long col = gx + (long long)nx * gy;
+	if (s_skip != 0) {   // the same for the whole block: no barrier is skipped by some threads only
+		if (own) {
+			for (int k = kb; k < ke; k++) {
+				#pragma unroll
+				for (int d = 0; d < 3; d++) P.Bo[d * P.N + col + plane * k] = P.B[d * P.N + col + plane * k];
+			}
 		}
-		int i, j, k;
-		cell_coords(P, c, i, j, k);
-		// every read before the first store, so that the 39 loads are in flight together
-		const double d0 = face_dB<0>(P, i, j, k, dt), d1 = face_dB<1>(P, i, j, k, dt),
-		             d2 = face_dB<2>(P, i, j, k, dt);
-		const double b0 = P.B[c], b1 = P.B[P.N + c], b2 = P.B[2 * P.N + c];
-		P.Bo[c] = b0 + d0 / P.area[0];
-		P.Bo[P.N + c] = b1 + d1 / P.area[1];
-		P.Bo[2 * P.N + c] = b2 + d2 / P.area[2];
+		return;
+	}
+	long long off[FPER];
+	plane_offsets(P, gx0, gy0, off);
+	// global plane p sits in slot (p - kb + 1) mod 4; planes kb - 1 .. kb + 1 staged first, the
+	// loads of the next plane kept in flight in registers while a plane is computed
+	double v[FPER];
+	#pragma unroll 1
+	for (int t = 0; t < 3; t++) {
+		load_plane(P, off, kb - 1 + t, v);
+		store_plane(fsm + t * FPLANE, v);
+	}
+	load_plane(P, off, kb + 2, v);
+	for (int k = kb; k < ke; k++) {
+		const int t = k - kb + 1;
+		__syncthreads();
+		if (own) {
+			auto get = [&](const int axis, const int comp, const int ox, const int oy, const int oz) {
+				const int j = comp == (axis + 1) % 3 ? 0 : 1;
+				return fsm[((t + oz) & 3) * FPLANE + (2 * axis + j) * (FW * FH) + (ty + 1 + oy) * FW + tx + 1 + ox];
+			};
+			const long long c = col + plane * k;
+			const double d0 = face_dB<0>(P, get, dt), d1 = face_dB<1>(P, get, dt), d2 = face_dB<2>(P, get, dt);
+			const double b0 = P.B[c], b1 = P.B[P.N + c], b2 = P.B[2 * P.N + c];
+			P.Bo[c] = b0 + d0 / P.area[0];
+			P.Bo[P.N + c] = b1 + d1 / P.area[1];
+			P.Bo[2 * P.N + c] = b2 + d2 / P.area[2];
+		}
+		// plane k + 2 into its slot (not one of the three the slowest thread may still read), then
+		// the loads of plane k + 3
+		store_plane(fsm + ((t + 2) & 3) * FPLANE, v);
+		if (k + 1 < ke) load_plane(P, off, k + 3, v);
 	}
 }
 
@@ -537,7 +627,8 @@ int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 		faces_kernel<SOLVER, false><<<tiles, block, SMEM_FACES, stream>>>(P);
 	}
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
-	field_kernel<<<grid, THREADS, 0, stream>>>(P);
+	const dim3 field_tiles((P.n[0] + FTX - 1) / FTX, (P.n[1] + FTY - 1) / FTY, (P.n[2] + P.fchunk - 1) / P.fchunk);
+	field_kernel<<<field_tiles, dim3(FTX, FTY), SMEM_FIELD, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	cell_kernel<<<grid, THREADS, 0, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
@@ -687,6 +778,13 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 	const long long tiles = (long long)((cfg->n[0] + STX - 1) / STX) * ((cfg->n[1] + STY - 1) / STY);
 	const long long chunks = std::max(1ll, std::min((long long)cfg->n[2], 18ll * sms / tiles));
 	P.kchunk = int((cfg->n[2] + chunks - 1) / chunks);
+	const long long ftiles = (long long)((cfg->n[0] + FTX - 1) / FTX) * ((cfg->n[1] + FTY - 1) / FTY);
+	const long long fchunks = std::max(1ll, std::min((long long)cfg->n[2], 12ll * sms / ftiles));
+	P.fchunk = int((cfg->n[2] + fchunks - 1) / fchunks);
+	if (cudaFuncSetAttribute(field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_FIELD))
+		!= cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
 	for (int d = 0; d < 3; d++) {
 		P.n[d] = cfg->n[d];
 		P.len[d] = cfg->cell_length[d];
