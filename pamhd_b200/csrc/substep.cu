@@ -5,7 +5,8 @@ grids periodic in every dimension, behind pamhd_gpu_substep_* of
 include/pamhd_gpu.h.  Dimensions of one cell are inactive.
 
 Every cell advances with a period of 2^k substeps of one common substep
-length.  A step is planned on the device and driven from the host:
+length.  A step is planned on the device in one batch of launches, read back
+once (the substep count and length), and its substeps launched from the host:
   limits_kernel    each cell's CFL limit from the last face speeds
                    (minimize_timestep, mhd/solve.hpp:1933-2007), the smallest
                    limit and the smallest limit / 2^min over cells
@@ -16,7 +17,9 @@ length.  A step is planned on the device and driven from the host:
   restrict_kernel  a cell's exponent at most one above any face or edge
                    neighbour's, repeated until nothing changes (the largest
                    such assignment, which the reference's in-place passes reach
-                   too, substepping.hpp:104-176);
+                   too, substepping.hpp:104-176): one pass in the batch, the
+                   periods taken on the guess that it changed nothing, and
+                   more passes (each read back) only where it did;
   period_kernel,   periods 2^k and their largest value; each cell's smallest
   reach_kernel     period among itself and its face and edge neighbours, M;
 then for every substep s:
@@ -31,9 +34,9 @@ then for every substep s:
                    the faces kernel starts them afresh instead.
 Layout: state 8 x N, flux slots 6 x 8 x N (each cell's -x, +x, -y, +y, -z,
 +z), the speed of every cell's -d face 3 x N, exponents and periods
-N int32, x fastest, no ghosts.  A slow path: one host round trip per step
-for the plan.  Compiled without FMA contraction; the update follows the
-oracle's operation order.
+N int32, x fastest, no ghosts.  One host round trip per step for the plan
+(the host needs the substep count to launch the substeps).  Compiled without
+FMA contraction; the update follows the oracle's operation order.
 */
 #include <cuda_runtime.h>
 
@@ -56,6 +59,7 @@ constexpr int MAX_RESTRICT_PASSES = 64;
 struct Plan {
 	unsigned long long smallest;   // bits of the smallest CFL limit
 	unsigned long long ret;        // bits of the smallest limit / 2^min
+	unsigned long long substep;    // bits of the step's substep length (written by exponent_kernel)
 	unsigned int max_period;
 	unsigned int changed;
 	unsigned int bad_exponents;
@@ -165,10 +169,26 @@ __global__ void limits_kernel(const Sub_Params P)
 	}
 }
 
-__global__ void exponent_kernel(const Sub_Params P, const double max_dt, const double ret)
+/*
+The substep and the exponents (substepping.hpp:312-390): when max_dt is at
+most the smallest limit, every exponent is 0 and the substep is max_dt; else
+the substep is the smallest limit / 2^min and each cell's largest exponent is
+capped by floor(log2(min(limit, max_dt) / substep)).
+*/
+__global__ void exponent_kernel(const Sub_Params P, const double max_dt)
 {
+	const double smallest = __longlong_as_double((long long)P.plan->smallest);
+	const double ret = __longlong_as_double((long long)P.plan->ret);
+	const bool capped = max_dt <= smallest;
+	if (blockIdx.x == 0 and threadIdx.x == 0) {
+		P.plan->substep = (unsigned long long)__double_as_longlong(capped ? max_dt : ret);
+	}
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		if (capped) {
+			P.S[c] = 0;
+			continue;
+		}
 		const double dt = P.T[c];
 		int smin = P.user_min[c] - P.min_offset, smax = P.user_max[c];
 		if (dt > 0) {
@@ -272,9 +292,10 @@ __device__ __forceinline__ void plus_face(const Sub_Params& P, const long long c
 }
 
 template <int SOLVER>
-__global__ void __launch_bounds__(128, 3) faces_kernel(const Sub_Params P, const int s, const double substep)
+__global__ void __launch_bounds__(128, 3) faces_kernel(const Sub_Params P, const int s)
 {
 	if (P.status->flags != 0u) return;   // a face of an earlier substep failed: the step stops there
+	const double substep = __longlong_as_double((long long)P.plan->substep);
 	const long long stride = (long long)gridDim.x * blockDim.x;
 	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
 		const int m = P.M[c];
@@ -372,14 +393,14 @@ int launch(const pamhd_sub& x, K kernel, Args... args)
 	return check(cudaGetLastError());
 }
 
-int faces(const pamhd_sub& x, const int s, const double substep)
+int faces(const pamhd_sub& x, const int s)
 {
 	const int g = 2 * x.grid;
 	switch (x.cfg.solver) {
-	case PAMHD_RUSANOV: faces_kernel<PAMHD_RUSANOV><<<g, 128, 0, x.stream>>>(x.base, s, substep); break;
-	case PAMHD_HLL_ATHENA: faces_kernel<PAMHD_HLL_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s, substep); break;
-	case PAMHD_HLLD_ATHENA: faces_kernel<PAMHD_HLLD_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s, substep); break;
-	case PAMHD_ROE_ATHENA: faces_kernel<PAMHD_ROE_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s, substep); break;
+	case PAMHD_RUSANOV: faces_kernel<PAMHD_RUSANOV><<<g, 128, 0, x.stream>>>(x.base, s); break;
+	case PAMHD_HLL_ATHENA: faces_kernel<PAMHD_HLL_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s); break;
+	case PAMHD_HLLD_ATHENA: faces_kernel<PAMHD_HLLD_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s); break;
+	case PAMHD_ROE_ATHENA: faces_kernel<PAMHD_ROE_ATHENA><<<g, 128, 0, x.stream>>>(x.base, s); break;
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 	return check(cudaGetLastError());
@@ -556,45 +577,53 @@ int pamhd_gpu_substep_step(pamhd_sub* x, const double max_dt, double* dt_taken, 
 	if (not x->loaded) return PAMHD_ERR_STATE;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const Sub_Params& P = x->base;
-	Plan p{~0ull, ~0ull, 0u, 0u, 0u, 0u};
+	Plan p{~0ull, ~0ull, 0ull, 0u, 0u, 0u, 0u};
 	PAMHD_TRY(check(cudaMemcpyAsync(x->plan, &p, sizeof p, cudaMemcpyHostToDevice, x->stream)));
+	/*
+	The plan in one batch and one read-back: limits, substep and exponents, one
+	restriction pass (S -> S2), and the periods and their reach taken from S on
+	the guess that the pass changed nothing (then S2 equals S).  When it did,
+	the passes continue from S2 until nothing changes and the periods are
+	taken again.
+	*/
 	PAMHD_TRY(launch(*x, limits_kernel, P));
-	PAMHD_TRY(read_plan(*x, p));
-	const double smallest = from_bits(p.smallest);
-	double substep = max_dt;
-	if (max_dt <= smallest) {
-		PAMHD_TRY(check(cudaMemsetAsync(P.S, 0, size_t(x->N) * sizeof(int32_t), x->stream)));
-	} else {
-		substep = from_bits(p.ret);
-		PAMHD_TRY(launch(*x, exponent_kernel, P, max_dt, substep));
-		PAMHD_TRY(read_plan(*x, p));
-		if (p.bad_exponents != 0u) return PAMHD_ERR_ARGUMENT;
-	}
-	// restrict_substepping_period: passes until no exponent changes
-	int32_t* in = P.S;
-	int32_t* out = P.S2;
-	int pass = 0;
-	for (;; pass++) {
-		if (pass == MAX_RESTRICT_PASSES) return PAMHD_ERR_TIMEOUT;
-		const unsigned int zero = 0u;
-		PAMHD_TRY(check(cudaMemcpyAsync(&x->plan->changed, &zero, sizeof zero, cudaMemcpyHostToDevice, x->stream)));
-		PAMHD_TRY(launch(*x, restrict_kernel, P, static_cast<const int32_t*>(in), out));
-		PAMHD_TRY(read_plan(*x, p));
-		std::swap(in, out);
-		if (p.changed == 0u) break;
-	}
-	if (in != P.S) {
-		PAMHD_TRY(check(cudaMemcpyAsync(P.S, in, size_t(x->N) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
-		                                x->stream)));
-	}
+	PAMHD_TRY(launch(*x, exponent_kernel, P, max_dt));
+	PAMHD_TRY(launch(*x, restrict_kernel, P, static_cast<const int32_t*>(P.S), P.S2));
 	PAMHD_TRY(launch(*x, period_kernel, P));
 	PAMHD_TRY(launch(*x, reach_kernel, P));
 	PAMHD_TRY(read_plan(*x, p));
+	if (p.bad_exponents != 0u) return PAMHD_ERR_ARGUMENT;
+	if (p.changed != 0u) {
+		// restrict_substepping_period: passes until no exponent changes
+		int32_t* in = P.S2;
+		int32_t* out = P.S;
+		for (int pass = 1;; pass++) {
+			if (pass == MAX_RESTRICT_PASSES) return PAMHD_ERR_TIMEOUT;
+			const unsigned int zero = 0u;
+			PAMHD_TRY(check(cudaMemcpyAsync(&x->plan->changed, &zero, sizeof zero, cudaMemcpyHostToDevice,
+			                                x->stream)));
+			PAMHD_TRY(launch(*x, restrict_kernel, P, static_cast<const int32_t*>(in), out));
+			PAMHD_TRY(read_plan(*x, p));
+			std::swap(in, out);
+			if (p.changed == 0u) break;
+		}
+		if (in != P.S) {
+			PAMHD_TRY(check(cudaMemcpyAsync(P.S, in, size_t(x->N) * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+			                                x->stream)));
+		}
+		const unsigned int zero = 0u;
+		PAMHD_TRY(check(cudaMemcpyAsync(&x->plan->max_period, &zero, sizeof zero, cudaMemcpyHostToDevice,
+		                                x->stream)));
+		PAMHD_TRY(launch(*x, period_kernel, P));
+		PAMHD_TRY(launch(*x, reach_kernel, P));
+		PAMHD_TRY(read_plan(*x, p));
+	}
+	const double substep = from_bits(p.substep);
 	const int steps = int(p.max_period);
 	double total = 0;
 	for (int s = 1; s <= steps; s++) {
 		total += substep;
-		PAMHD_TRY(faces(*x, s, substep));
+		PAMHD_TRY(faces(*x, s));
 		PAMHD_TRY(launch(*x, update_kernel, P, s));
 	}
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
