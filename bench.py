@@ -737,6 +737,9 @@ def substep_section(local, n=128, steps=10, solver="hlld_athena", cpu=True):
         "updates_per_s": updates * steps / sec,
         "ms_per_step": ms,
         "substeps_per_step": subs / steps,
+        "gpu_launches": steps * 5 + 2 * subs,
+        "gpu_launches_what": "per step the plan's five kernels (one restriction pass: the exponents given satisfy "
+                             "the neighbour rule) and faces_kernel + update_kernel per substep",
         "timing": "host clock around synchronous steps (each step plans on the device and reads the plan back)",
         "roofline": section_roofline(n, "substep_step_hlld", 128, updates, ms, clocks.summary(),
                                      "whole step: the plan's kernels and faces_kernel + update_kernel per substep"),
