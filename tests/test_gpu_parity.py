@@ -268,6 +268,44 @@ def test_blast_positivity_failure_matches_oracle(port):
 
 # ---------------------------------------------------------------- the configured workloads
 
+def test_blast_256_configured(port):
+    """The headline workload at its size: the 256^3 magnetised blast, HLLD, CFL 0.4, periodic.
+    The priming step and two steps against the oracle (on every host thread) at the per-step bar;
+    then size-independent properties over 20 more steps: the conserved totals stay within
+    round-off, and a copy of the state shifted by whole cells stays the shifted solution bit for
+    bit."""
+    import os
+    n = 256
+    U0 = states.blast_wave(n)
+    gpu, _ = pair(port, (n, n, n), po.HLLD, (1 / n,) * 3, 5 / 3, 1.0, 0.4)
+    ora = port.grid(po.make_cfg((n, n, n), po.HLLD, (1 / n,) * 3, 5 / 3, 1.0, 0.4),
+                    threads=max(1, len(os.sched_getaffinity(0))))
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    for s in range(3):
+        cap = 0.0 if s == 0 else 1.0
+        do, flag, _, _ = ora.step(cap)
+        dg = gpu.step(cap)
+        assert flag == 0
+        assert abs(dg - do) <= 1e-13 * max(do, 1e-300)
+        assert field_err(gpu.get_state(), ora.get_state()) <= STEP_TOL, s
+    del ora
+    shift = (17, 5, 200)   # z, y, x
+    b = pg.Context(gpu.cfg)
+    U3 = gpu.get_state()
+    b.set_state(np.roll(U3, shift, axis=(1, 2, 3)))
+    gpu.set_state(U3)
+    t0 = gpu.totals()
+    gpu.steps(20, 1e9)
+    b.steps(20, 1e9)
+    t1 = gpu.totals()
+    Uf = gpu.get_state()
+    # round-off of 16.7 M cell updates a step (random signs): about sqrt(N) eps of the sum of |U|
+    absum = np.maximum(np.abs(U3).reshape(8, -1).sum(axis=1), np.abs(Uf).reshape(8, -1).sum(axis=1)) / n ** 3
+    assert np.all(np.abs(t1 - t0) <= 1e-11 * absum)
+    np.testing.assert_array_equal(np.roll(Uf, shift, axis=(1, 2, 3)), b.get_state())
+
+
 @pytest.mark.parametrize("solver", list(po.SOLVERS))
 def test_brio_wu_configured_every_solver(port, solver):
     """The shock-tube workload with each solver: 1000 cells on [0, 1], gamma 2, CFL 0.5, copy
