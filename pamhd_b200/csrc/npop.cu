@@ -71,6 +71,7 @@ struct Npop_Params {
 	double len[3];
 	double area[3];
 	double gamma, mu0, min_pressure;
+	double inv_mu0, half_inv_mu0;   // 1 / mu0 and 0.5 / mu0
 	Speed_Max* red;                 // [3] ring by step phase: max signal speed per axis
 	Clock* clock;                   // [3]
 	Status* status;
@@ -79,10 +80,26 @@ struct Npop_Params {
 	int kchunk;                     // z planes per face-solve block
 };
 
-// a total state: mass, momentum, energy, field
+/*
+A total state: mass, momentum, energy, field, with inv = 1 / rho and
+half = 0.5 / rho divided once per cell (the same IEEE divisions as the
+expressions they stand for, so the same bits).
+*/
 struct St {
 	double rho, m[3], e, b[3];
+	double inv, half;
 };
+
+// the run's constants, 1 / mu0 and 0.5 / mu0 divided once (on the host: IEEE division, the same bits)
+struct Gas_N {
+	double gamma, mu0, inv_mu0, half_inv_mu0;
+};
+
+__device__ __forceinline__ void set_reciprocals(St& s)
+{
+	s.inv = 1 / s.rho;
+	s.half = 0.5 / s.rho;
+}
 
 __device__ __forceinline__ double max_of(const double a, const double b)
 {
@@ -95,30 +112,29 @@ __device__ __forceinline__ double min_of(const double a, const double b)
 }
 
 // get_pressure (mhd/common.hpp:79-118); rho <= 0 is the reference's throw
-__device__ __forceinline__ double pressure(const St& s, const double gamma, const double mu0, uint32_t& flag)
+__device__ __forceinline__ double pressure(const St& s, const Gas_N& g, uint32_t& flag)
 {
 	if (s.rho <= 0 and flag == 0) flag = PAMHD_FLAG_DENSITY;
 	const double
-		kinetic = 0.5 / s.rho * (s.m[0] * s.m[0] + s.m[1] * s.m[1] + s.m[2] * s.m[2]),
-		magnetic = 0.5 / mu0 * (s.b[0] * s.b[0] + s.b[1] * s.b[1] + s.b[2] * s.b[2]);
-	return (s.e - kinetic - magnetic) * (gamma - 1);
+		kinetic = s.half * (s.m[0] * s.m[0] + s.m[1] * s.m[1] + s.m[2] * s.m[2]),
+		magnetic = g.half_inv_mu0 * (s.b[0] * s.b[0] + s.b[1] * s.b[1] + s.b[2] * s.b[2]);
+	return (s.e - kinetic - magnetic) * (g.gamma - 1);
 }
 
 // get_velocity (mhd/common.hpp:121-130)
-__device__ __forceinline__ void velocity(const double m[3], const double rho, double v[3])
+__device__ __forceinline__ void velocity(const St& s, double v[3])
 {
-	if (rho > 0) {
-		const double inv = 1 / rho;
-		v[0] = m[0] * inv;
-		v[1] = m[1] * inv;
-		v[2] = m[2] * inv;
+	if (s.rho > 0) {
+		v[0] = s.m[0] * s.inv;
+		v[1] = s.m[1] * s.inv;
+		v[2] = s.m[2] * s.inv;
 	} else {
 		v[0] = v[1] = v[2] = 0;
 	}
 }
 
 // get_fast_magnetosonic_speed without background field (mhd/common.hpp:418-491)
-__device__ double fast_speed(const St& s, const double gamma, const double mu0, uint32_t& flag)
+__device__ double fast_speed(const St& s, const Gas_N& g, uint32_t& flag)
 {
 	const double t0 = s.b[0] + 0.0, t1 = s.b[1] + 0.0, t2 = s.b[2] + 0.0;
 	if (not is_finite(t0)) {
@@ -131,16 +147,16 @@ __device__ double fast_speed(const St& s, const double gamma, const double mu0, 
 		if (flag == 0) flag = PAMHD_FLAG_DENSITY;
 		return 0;
 	}
-	const double p = pressure(s, gamma, mu0, flag);
+	const double p = pressure(s, g, flag);
 	if (not (is_normal(p) and not (p < 0))) {
 		if (flag == 0) flag = PAMHD_FLAG_PRESSURE;
 		return 0;
 	}
-	const double sound = sqrt(gamma * p / s.rho);
+	const double sound = sqrt(g.gamma * p / s.rho);
 	if (b <= 0) return sound;
 	// get_alfven_speed
 	const double bb = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
-	const double alfven = bb / sqrt(mu0 * s.rho);
+	const double alfven = bb / sqrt(g.mu0 * s.rho);
 	const double sound2 = sound * sound, alfven2 = alfven * alfven, sum2 = sound2 + alfven2;
 	if (not (is_normal(sum2) and not (sum2 < 0))) {
 		if (flag == 0) flag = PAMHD_FLAG_WAVE_SPEED;
@@ -156,7 +172,7 @@ __device__ double fast_speed(const St& s, const double gamma, const double mu0, 
 }
 
 // get_flux without background field (mhd/common.hpp:146-244), the physical flux along x
-__device__ void physical(const St& s, const double gamma, const double mu0, double F[8], uint32_t& flag)
+__device__ void physical(const St& s, const Gas_N& g, double F[8], uint32_t& flag)
 {
 	if (not (is_normal(s.rho) and s.rho > 0)) {
 		if (flag == 0) flag = PAMHD_FLAG_DENSITY;
@@ -169,13 +185,13 @@ __device__ void physical(const St& s, const double gamma, const double mu0, doub
 	const double bg = 0.0;
 	const double tot[3] = {s.b[0] + bg, s.b[1] + bg, s.b[2] + bg};
 	const double
-		inv_mu0 = 1.0 / mu0,
+		inv_mu0 = g.inv_mu0,
 		p_bg = 0.5 * inv_mu0 * (bg * bg + bg * bg + bg * bg),
 		p_b1 = 0.5 * inv_mu0 * (s.b[0] * s.b[0] + s.b[1] * s.b[1] + s.b[2] * s.b[2]),
 		p_tot = 0.5 * inv_mu0 * (tot[0] * tot[0] + tot[1] * tot[1] + tot[2] * tot[2]),
-		p_th = pressure(s, gamma, mu0, flag);
+		p_th = pressure(s, g, flag);
 	double v[3];
-	velocity(s.m, s.rho, v);
+	velocity(s, v);
 	F[0] = s.m[0];
 	if (not is_finite(F[0])) {
 		if (flag == 0) flag = PAMHD_FLAG_FLUX;
@@ -216,8 +232,7 @@ struct Fast {
 
 // get_flux_N_rusanov (mhd/N_rusanov.hpp:61-170)
 __device__ double split_rusanov(const St& L, const St& R, const Fast& fl, const Fast& fr, const double area,
-                                const double dt, const double gamma, const double mu0, double fn[8], double fp[8],
-                                uint32_t& flag)
+                                const double dt, const Gas_N& g, double fn[8], double fp[8], uint32_t& flag)
 {
 	if (not (is_normal(L.rho) and not (L.rho < 0)) or not (is_normal(R.rho) and not (R.rho < 0))) {
 		flag = PAMHD_FLAG_DENSITY;
@@ -231,13 +246,13 @@ __device__ double split_rusanov(const St& L, const St& R, const Fast& fl, const 
 	const double fast_pos = fr.speed;
 	const double max_fast = max_of(fast_neg, fast_pos);
 	double vl[3], vr[3];
-	velocity(L.m, L.rho, vl);
-	velocity(R.m, R.rho, vr);
+	velocity(L, vl);
+	velocity(R, vr);
 	const double s = max_of(fabs(vl[0]) + max_fast, fabs(vr[0]) + max_fast);
 	double FL[8], FR[8];
-	physical(L, gamma, mu0, FL, flag);
+	physical(L, g, FL, flag);
 	if (flag) return 0;
-	physical(R, gamma, mu0, FR, flag);
+	physical(R, g, FR, flag);
 	if (flag) return 0;
 	double uL[8], uR[8];
 	state_row(L, uL);
@@ -260,18 +275,17 @@ __device__ double split_rusanov(const St& L, const St& R, const Fast& fl, const 
 
 // get_flux_N_hll (mhd/N_hll_athena.hpp:47-231)
 __device__ double split_hll(const St& L, const St& R, const Fast& fl, const Fast& fr, const double area,
-                            const double dt, const double gamma, const double mu0, double fn[8], double fp[8],
-                            uint32_t& flag)
+                            const double dt, const Gas_N& g, double fn[8], double fp[8], uint32_t& flag)
 {
 	double vn[3], vp[3];
-	velocity(L.m, L.rho, vn);
-	velocity(R.m, R.rho, vp);
-	const double p_neg = pressure(L, gamma, mu0, flag);
-	const double p_pos = pressure(R, gamma, mu0, flag);
+	velocity(L, vn);
+	velocity(R, vp);
+	const double p_neg = pressure(L, g, flag);
+	const double p_pos = pressure(R, g, flag);
 	if (flag) return 0;
 	const double
-		pb_neg = (L.b[0] * L.b[0] + L.b[1] * L.b[1] + L.b[2] * L.b[2]) / (2 * mu0),
-		pb_pos = (R.b[0] * R.b[0] + R.b[1] * R.b[1] + R.b[2] * R.b[2]) / (2 * mu0);
+		pb_neg = (L.b[0] * L.b[0] + L.b[1] * L.b[1] + L.b[2] * L.b[2]) / (2 * g.mu0),
+		pb_pos = (R.b[0] * R.b[0] + R.b[1] * R.b[1] + R.b[2] * R.b[2]) / (2 * g.mu0);
 	flag = fl.flag;
 	if (flag) return 0;
 	const double fast_neg = fl.speed;
@@ -306,9 +320,9 @@ __device__ double split_hll(const St& L, const St& R, const Fast& fl, const Fast
 		return 0;
 	}
 	double FL[8], FR[8];
-	physical(L, gamma, mu0, FL, flag);
+	physical(L, g, FL, flag);
 	if (flag) return 0;
-	physical(R, gamma, mu0, FR, flag);
+	physical(R, g, FR, flag);
 	if (flag) return 0;
 	double uL[8], uR[8];
 	state_row(L, uL);
@@ -348,11 +362,14 @@ __device__ __forceinline__ void load13(const Npop_Params& P, const long long c, 
 	for (int v = 0; v < NV; v++) u[v] = P.U[v * P.N + c];
 }
 
-// the total state of a cell, rotated into the frame of axis A (get_rotated_vector, mhd/common.hpp:612-648)
+// the total state of a cell, rotated into the frame of axis A (get_rotated_vector, mhd/common.hpp:612-648),
+// with the reciprocals of its density given
 template <int A>
-__device__ __forceinline__ St total_rotated(const double u[NV])
+__device__ __forceinline__ St total_rotated(const double u[NV], const double inv, const double half)
 {
 	St s;
+	s.inv = inv;
+	s.half = half;
 	s.rho = u[0] + u[5];
 	const double m[3] = {u[1] + u[6], u[2] + u[7], u[3] + u[8]};
 	s.e = u[4] + u[9];
@@ -400,18 +417,24 @@ plane's stores apart from the reads of the plane two before it.
 constexpr int NTX = 32, NTY = 4;
 constexpr int NW = NTX + 1;                 // a record row: the -x halo at column 0
 constexpr int NCELLS = NW * (NTY + 1);      // record rows: the -y halo at row 0
-constexpr int NREC = NV + 3;                // state, fast speed along x, y, z
+constexpr int NREC = NV + 5;                // state, fast speed along x, y, z, 1 / rho, 0.5 / rho
+enum { N_CF = NV, N_INV = NV + 3, N_HALF = NV + 4 };
 constexpr int NSLOT = NREC * NCELLS;
 constexpr int NSLOTS = 3;
 constexpr size_t SMEM_FACES = NSLOTS * (NSLOT * sizeof(double) + NCELLS * sizeof(uint32_t));
 
+__device__ __forceinline__ Gas_N gas_of(const Npop_Params& P)
+{
+	return Gas_N{P.gamma, P.mu0, P.inv_mu0, P.half_inv_mu0};
+}
+
 template <int A>
-__device__ __forceinline__ void stage_fast(const Npop_Params& P, const double u[NV], double* rec, const int r,
-                                           uint32_t& flags)
+__device__ __forceinline__ void stage_fast(const Npop_Params& P, const double u[NV], const double inv,
+                                           const double half, double* rec, const int r, uint32_t& flags)
 {
 	if (not P.active[A]) return;
 	uint32_t f = 0;
-	rec[(NV + A) * NCELLS + r] = fast_speed(total_rotated<A>(u), P.gamma, P.mu0, f);
+	rec[(N_CF + A) * NCELLS + r] = fast_speed(total_rotated<A>(u, inv, half), gas_of(P), f);
 	flags |= f << (8 * A);
 }
 
@@ -424,10 +447,14 @@ __device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, ui
 	load13(P, c, u);
 	#pragma unroll
 	for (int v = 0; v < NV; v++) rec[v * NCELLS + r] = u[v];
+	const double rho = u[0] + u[5];
+	const double inv = 1 / rho, half = 0.5 / rho;
+	rec[N_INV * NCELLS + r] = inv;
+	rec[N_HALF * NCELLS + r] = half;
 	uint32_t flags = 0;
-	if (CX) stage_fast<0>(P, u, rec, r, flags);
-	if (CY) stage_fast<1>(P, u, rec, r, flags);
-	if (CZ) stage_fast<2>(P, u, rec, r, flags);
+	if (CX) stage_fast<0>(P, u, inv, half, rec, r, flags);
+	if (CY) stage_fast<1>(P, u, inv, half, rec, r, flags);
+	if (CZ) stage_fast<2>(P, u, inv, half, rec, r, flags);
 	flg[r] = flags;
 }
 
@@ -443,14 +470,15 @@ __device__ __forceinline__ void minus_face(const Npop_Params& P, const double* r
 		um[v] = recl[v * NCELLS + rl];
 		uc[v] = recr[v * NCELLS + rr];
 	}
-	const St L = total_rotated<A>(um), R = total_rotated<A>(uc);
-	const Fast fl{recl[(NV + A) * NCELLS + rl], (flgl[rl] >> (8 * A)) & 0xffu};
-	const Fast fr{recr[(NV + A) * NCELLS + rr], (flgr[rr] >> (8 * A)) & 0xffu};
+	const St L = total_rotated<A>(um, recl[N_INV * NCELLS + rl], recl[N_HALF * NCELLS + rl]);
+	const St R = total_rotated<A>(uc, recr[N_INV * NCELLS + rr], recr[N_HALF * NCELLS + rr]);
+	const Fast fl{recl[(N_CF + A) * NCELLS + rl], (flgl[rl] >> (8 * A)) & 0xffu};
+	const Fast fr{recr[(N_CF + A) * NCELLS + rr], (flgr[rr] >> (8 * A)) & 0xffu};
 	double fn[8], fp[8];
 	uint32_t flag = 0;
 	const double s = SOLVER == PAMHD_RUSANOV
-		? split_rusanov(L, R, fl, fr, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag)
-		: split_hll(L, R, fl, fr, P.area[A], dt, P.gamma, P.mu0, fn, fp, flag);
+		? split_rusanov(L, R, fl, fr, P.area[A], dt, gas_of(P), fn, fp, flag)
+		: split_hll(L, R, fl, fr, P.area[A], dt, gas_of(P), fn, fp, flag);
 	if (flag != 0) {
 		atomicOr(&P.status->flags, flag);
 		atomicMin(&P.status->first, ((unsigned long long)(m * 3 + A) << 8) | flag);
@@ -640,11 +668,12 @@ __global__ void __launch_bounds__(THREADS, 1) npop_update_kernel(const Npop_Para
 			t.b[0] = u[10];
 			t.b[1] = u[11];
 			t.b[2] = u[12];
+			set_reciprocals(t);
 			uint32_t flag = 0;
-			const double p = pressure(t, P.gamma, P.mu0, flag);
+			const double p = pressure(t, gas_of(P), flag);
 			if (not (p >= P.min_pressure)) {
 				double v[3];
-				velocity(t.m, t.rho, v);
+				velocity(t, v);
 				const double
 					kinetic = 0.5 * t.rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]),
 					magnetic = 0.5 / P.mu0 * (t.b[0] * t.b[0] + t.b[1] * t.b[1] + t.b[2] * t.b[2]);
@@ -787,6 +816,8 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	P.N = N;
 	P.gamma = gamma;
 	P.mu0 = mu0;
+	P.inv_mu0 = 1.0 / mu0;
+	P.half_inv_mu0 = 0.5 / mu0;
 	P.min_pressure = min_pressure;
 	P.X = x->X;
 	P.red = x->red;
