@@ -593,13 +593,12 @@ __global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) np
 
 __global__ void __launch_bounds__(THREADS, 1) npop_update_kernel(const Npop_Params P)
 {
-	__shared__ double s_dt;
+	// the contributions already hold area dt: dt is needed here only to advance the clock
 	__shared__ int s_skip;
 	if (threadIdx.x == 0) {
 		const Clock c = P.clock[P.phase];
 		const bool skip = P.status->flags != 0u or (P.control.dt < 0.0 and c.t >= P.control.t_end);
 		const double dt = skip ? 0.0 : step_dt(P);
-		s_dt = dt;
 		s_skip = skip ? 1 : 0;
 		if (blockIdx.x == 0) {
 			Clock& next = P.clock[(P.phase + 1) % 3];
