@@ -266,6 +266,23 @@ def test_blast_positivity_failure_matches_oracle(port):
     assert fail_g == fail_o
 
 
+@pytest.mark.parametrize("count", [0, 1, 33, 257])
+def test_face_flux_empty_and_ragged_batches(port, count):
+    """Batches of no face, one face and counts that leave partial blocks: the same results as
+    the oracle face by face (an empty batch is a valid call that does nothing)."""
+    rng = np.random.default_rng(12)
+    a, b = states.nearby_face_states(max(count, 1), rng)
+    a, b = a[:count], b[:count]
+    fo, so, go = port.face_flux(po.HLLD, a, b, None, 5 / 3, 1.0)
+    fg, sg, gg = pg.face_flux(po.HLLD, a, b, None, 5 / 3, 1.0)
+    assert fg.shape == (count, 8) and sg.shape == (count,) and gg.shape == (count,)
+    assert np.array_equal(gg, go)
+    if count:
+        row = np.maximum(np.abs(fo).max(axis=1, keepdims=True), 1e-300)
+        assert (np.abs(fg - fo) / row).max() <= STEP_TOL
+        assert (np.abs(sg - so) / np.maximum(so, 1e-300)).max() <= STEP_TOL
+
+
 # ---------------------------------------------------------------- the configured workloads
 
 def test_blast_256_configured(port):
