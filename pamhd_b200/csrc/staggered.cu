@@ -526,7 +526,8 @@ The cell update of update_mhd_state (mass, momentum, energy, volume field;
 x, then y, then z, each flux slot 0 + dt F as the reference accumulates it),
 then update_vol_B twice with the new faces.  Block 0 advances the clock ring.
 */
-__global__ void __launch_bounds__(THREADS, 1) cell_kernel(const Stag_Params P)
+// two blocks per SM (128 registers, a few spilled): 16 warps with their loads in flight
+__global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
