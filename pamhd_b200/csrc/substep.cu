@@ -314,7 +314,8 @@ __global__ void __launch_bounds__(128, 3) faces_kernel(const Sub_Params P, const
 	}
 }
 
-__global__ void update_kernel(const Sub_Params P, const int s)
+// two blocks per SM (128 registers, a few spilled): 16 warps with their loads in flight
+__global__ void __launch_bounds__(THREADS, 2) update_kernel(const Sub_Params P, const int s)
 {
 	if (P.status->flags != 0u) return;
 	const long long N = P.N;
