@@ -19,7 +19,8 @@ roofline achieved HBM GB/s at the algorithmic 128 B per cell-update (8 FP64
          measured copy bandwidth
 cpu_baseline  the reference's own solver code (oracle/_ref, compiled from
          the reference headers) on the host cores, on a bounded sample
---impl reference  that CPU path alone, timed per step on the sample
+--impl reference  that CPU path alone on the full configured grid, same steps,
+         warm-up and segments as the GPU arm, all host threads
 """
 from __future__ import annotations
 
@@ -222,9 +223,10 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_sample_run(U_full, n, planes, steps, threads):
-    """Times `steps` HLLD steps of the reference solver code (oracle/_ref) on a periodic slab of
-    `planes` z-planes of the workload's initial state, after one priming step."""
+def cpu_grid(U_full, n, world, threads):
+    """The reference's own solver code (oracle/_ref, compiled from the reference headers; the
+    restated port where that build is absent) in the restated Mode C driver on the host cores, on
+    the grid the GPU arm steps: n x n x (world n) cells, the blast cube repeated along z."""
     from oracle import pyoracle as po
     kind = "reference"
     try:
@@ -232,39 +234,72 @@ def cpu_sample_run(U_full, n, planes, steps, threads):
     except Exception:
         o = po.Oracle("port")
         kind = "port"
-    z0 = (n - planes) // 2
-    U = np.ascontiguousarray(U_full[:, z0:z0 + planes])
-    cfg = po.make_cfg((n, n, planes), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL)
+    U = np.ascontiguousarray(np.concatenate([U_full] * world, axis=1)) if world > 1 else U_full
+    cfg = po.make_cfg((n, n, n * world), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL)
     g = o.grid(cfg, threads=threads)
+    return g, U, kind
+
+
+def cpu_timed_steps(g, U, steps, warmup):
+    """The GPU arm's schedule on the CPU: priming step and warm-up steps, then `steps` timed steps
+    in segments of at most SEGMENT, each restarted from the initial state with its dt = 0 priming
+    step outside the clock.  Returns the seconds spent in the timed steps."""
     g.set_state(U)
-    g.step(1.0)  # priming
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        dt, flag, _, _ = g.step(T_END)
-        if flag:
-            raise RuntimeError("CPU sample failed")
-    el = time.perf_counter() - t0
-    return n * n * planes * steps / el, kind, el
+    g.step(T_END)  # priming
+    for _ in range(min(warmup, SEGMENT - 1)):
+        g.step(T_END)
+    el, left = 0.0, steps
+    while left > 0:
+        seg = min(SEGMENT, left)
+        g.set_state(U)
+        g.step(T_END)
+        t0 = time.perf_counter()
+        for _ in range(seg):
+            dt, flag, _, _ = g.step(T_END)
+            if flag:
+                raise RuntimeError("reference step failed")
+        el += time.perf_counter() - t0
+        left -= seg
+    return el
 
 
 def cpu_baseline(U_full, n):
+    """The CPU path on the full configured grid (all host threads), a bounded number of steps
+    (about 10 s of wall time); one core on a thin slab beside it (the reference runs one MPI rank
+    per core, so one core is its unit of scale)."""
     threads = cpu_threads()
-    planes = 16
-    rate, kind, el = cpu_sample_run(U_full, n, planes, 1, threads)
-    # aim at ~10 s of wall time (not more than 8 steps)
-    steps = int(max(1, min(8, 10.0 / max(el, 1e-3))))
-    rate, kind, el = cpu_sample_run(U_full, n, planes, steps, threads)
-    # one core: the reference's own model is one MPI rank per core
-    rate1, _, el1 = cpu_sample_run(U_full, n, 4, 2, 1)
+    g, U, kind = cpu_grid(U_full, n, 1, threads)
+    g.set_state(U)
+    g.step(T_END)  # priming
+    t0 = time.perf_counter()
+    g.step(T_END)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(8, 10.0 / max(one, 1e-3))))
+    el = cpu_timed_steps(g, U, steps, 0)
+    rate = n ** 3 * steps / el
+    del g
+    # one core: a periodic slab of 4 z-planes from the middle of the blast
+    from oracle import pyoracle as po
+    o = po.Oracle(kind)
+    z0 = (n - 4) // 2
+    Us = np.ascontiguousarray(U_full[:, z0:z0 + 4])
+    g1 = o.grid(po.make_cfg((n, n, 4), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL), threads=1)
+    g1.set_state(Us)
+    g1.step(1.0)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        g1.step(T_END)
+    el1 = time.perf_counter() - t0
     return {
         "value": rate,
         "unit": UNIT,
         "cores": threads,
         "kind": kind,
-        "sample": f"{steps} HLLD steps on a {n}x{n}x{planes} periodic slab of the blast initial state "
+        "sample": f"{steps} HLLD steps of the full {n}^3 periodic blast after its priming step "
                   f"({el:.1f} s wall on {threads} threads, std::thread over cells)",
-        "one_core": {"value": rate1, "unit": UNIT,
-                     "sample": f"2 HLLD steps on a {n}x{n}x4 periodic slab, 1 thread ({el1:.1f} s wall)"},
+        "one_core": {"value": n * n * 4 * 2 / el1, "unit": UNIT,
+                     "sample": f"2 HLLD steps on a {n}x{n}x4 periodic slab of the blast, 1 thread "
+                               f"({el1:.1f} s wall; a separate sample, not the configured grid)"},
         "cpu": cpu_model(),
     }
 
@@ -774,51 +809,40 @@ def dist_env():
     return rank, world, local
 
 
+def bench_config(n, world, steps):
+    """The `config` of the bench line, the same for the GPU arm and the reference arm."""
+    return dict(workload(n),
+                parallelism=(f"{world} z slabs of {n}^3 of one {n}x{n}x{n * world} grid "
+                             f"(the blast cube repeated along z), one per GPU; cut planes "
+                             f"and the speed reduction exchanged over NCCL every step"
+                             if world > 1 else f"one {n}^3 grid on one GPU"),
+                timing=f"{steps} steps in segments of <= {SEGMENT} from the initial state "
+                       f"(the blast fails positivity later in the reference scheme)")
+
+
 def run_reference(a):
+    """The reference arm: the reference's own HLLD solver code (compiled from its headers) in the
+    restated cell-centred driver, on every host thread, stepping the same grid as the GPU arm
+    (n^3, or n x n x (N n) for N ranks) with the same warm-up and segment schedule."""
     rank, world, local = dist_env()
     if rank != 0:
         return 0
     n = a.n
-    U = blast_state(n)
     threads = cpu_threads()
-    planes = 16
-    from oracle import pyoracle as po
-    kind = "reference"
-    try:
-        o = po.Oracle("reference")
-    except Exception:
-        o = po.Oracle("port")
-        kind = "port"
-    z0 = (n - planes) // 2
-    Us = np.ascontiguousarray(U[:, z0:z0 + planes])
-    cfg = po.make_cfg((n, n, planes), po.HLLD, (1 / n, 1 / n, 1 / n), 5 / 3, 1.0, CFL)
-    g = o.grid(cfg, threads=threads)
-    g.set_state(Us)
-    g.step(T_END)  # priming
-    for _ in range(min(a.warmup, SEGMENT - 1)):
-        g.step(T_END)
-    # segments restarted from the initial state, as the GPU arm (the blast loses positivity later)
-    el, left = 0.0, a.steps
-    while left > 0:
-        seg = min(SEGMENT, left)
-        g.set_state(Us)
-        g.step(T_END)
-        t0 = time.perf_counter()
-        for _ in range(seg):
-            dt, flag, _, _ = g.step(T_END)
-            if flag:
-                raise RuntimeError("reference step failed")
-        el += time.perf_counter() - t0
-        left -= seg
-    value = n * n * planes * a.steps / el
-    sample = f"each step: one HLLD step on a {n}x{n}x{planes} periodic slab of the blast initial state"
+    g, U, kind = cpu_grid(blast_state(n), n, world, threads)
+    el = cpu_timed_steps(g, U, a.steps, a.warmup)
+    cells = n ** 3 * world
+    value = cells * a.steps / el
+    sample = (f"{a.steps} timed HLLD steps of the full {n}x{n}x{n * world} grid, {threads} host threads "
+              f"(std::thread over cells), the reference's solver headers compiled from source")
     line = {
         "impl": "reference",
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": 1e3 * el / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": dict(workload(n), sample=sample),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+        "config": bench_config(n, world, a.steps),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+                         "cpu": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "gpu_launches": 0,
     }
@@ -949,12 +973,7 @@ def run_b200(a):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": dict(workload(n), parallelism=(f"{world} z slabs of {n}^3 of one {n}x{n}x{n * world} grid "
-                                                 f"(the blast cube repeated along z), one per GPU; cut planes "
-                                                 f"and the speed reduction exchanged over NCCL every step"
-                                                 if world > 1 else f"one {n}^3 grid on one GPU"),
-                       timing=f"{a.steps} steps in segments of <= {SEGMENT} from the initial state "
-                              f"(the blast fails positivity later in the reference scheme)"),
+        "config": bench_config(n, world, a.steps),
         "roofline": {
             "bound": "hbm",
             "achieved": achieved,

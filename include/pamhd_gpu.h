@@ -33,7 +33,7 @@ Conventions
 extern "C" {
 #endif
 
-#define PAMHD_GPU_ABI_VERSION 1
+#define PAMHD_GPU_ABI_VERSION 2
 
 /* Return codes. */
 enum {
@@ -165,10 +165,17 @@ One step of the lagged-CFL rule; replaces pamhd::mhd::timestep()
   ghost refresh.
 The first step after create/set_state is the reference's dt = 0 priming
 step whatever max_dt is (tests/mhd/test.cpp:462-470).
-Synchronises; *dt_taken receives the step length.
+Synchronises; *dt_taken receives the step length.  max_signal (NULL, or
+three doubles) receives the largest signal speed of this step's faces
+normal to x, y and z (0 for a dimension of one cell): the maxima of the
+per-face Max_v the reference's get_fluxes stores (mhd/solve.hpp:319-322)
+and its minimize_timestep reads (mhd/solve.hpp:1933-2014), so that a host
+caller can apply its own timestep rule: dt = min over dimensions d of
+CFL * dx_d / max_signal[d].  Faces between two ghost cells of a
+non-periodic side count, as in the reference.
 Returns PAMHD_ERR_PHYSICS if any face met an invalid state.
 */
-int pamhd_gpu_step(pamhd_ctx* ctx, double max_dt, double* dt_taken);
+int pamhd_gpu_step(pamhd_ctx* ctx, double max_dt, double* dt_taken, double* max_signal);
 
 /*
 Runs nsteps steps without host synchronisation (captured in a CUDA graph
@@ -276,20 +283,25 @@ int pamhd_gpu_face_flux(
 /*
 pamhd_gpu_face_flux without device memory allocation.  No reference
 counterpart: the reference evaluates its solvers on the host.  Same
-arguments, results and return codes as pamhd_gpu_face_flux, for callers
-that cannot allocate device memory once set up (device memory reserved by
-another allocator, or a loop that cannot take the device-wide
-synchronisation of cudaMalloc / cudaFree).  Faces are staged through a
-fixed 3.56 MiB scratch area of this library's device code instead of
-per-call buffers, so:
+arguments and results as pamhd_gpu_face_flux, for callers that cannot
+allocate device memory once set up (device memory reserved by another
+allocator, or a loop that cannot take the device-wide synchronisation of
+cudaMalloc / cudaFree).  Faces are staged through a fixed 3.56 MiB scratch
+area of this library's device code instead of per-call buffers, so:
   - n > PAMHD_NOALLOC_MAX_FACES is rejected with PAMHD_ERR_TOO_LARGE
     before any CUDA call: split the faces into calls of at most that many;
   - all calls on one device share the scratch, so calls that overlap in
     time (from several host threads) race: serialise them;
   - the first call on a device does the set-up (loads this scratch, which
     the CUDA driver places when it loads the library's device code, and
-    looks up its address): make it before any stream capture.
-Runs on the legacy default stream of `device`, synchronously.
+    looks up its address): make it before any stream capture;
+  - the address is kept for the life of the process: a cudaDeviceReset
+    between calls is not supported;
+  - devices 0..63 only (PAMHD_ERR_ARGUMENT for a higher ordinal that
+    exists; a device that does not exist gives PAMHD_ERR_CUDA, as
+    pamhd_gpu_face_flux does); n = 0 returns PAMHD_OK before any CUDA call.
+Runs on the legacy default stream of `device`, synchronously, and restores
+the caller's current device before it returns.
 */
 int pamhd_gpu_face_flux_noalloc(
 	int32_t device, int32_t solver, int64_t n,

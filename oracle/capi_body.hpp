@@ -152,6 +152,24 @@ int ORACLE_API(grid_step)(void* grid, double max_dt, double* dt_taken,
 }
 
 /*
+Largest face signal speed of the last step per dimension: the maximum of
+Max_v over the cells the step visited (mhd/solve.hpp:319-322 stores each
+face's speed in both cells' slots).
+*/
+int ORACLE_API(grid_max_signal)(void* grid, double out[3])
+{
+	const Grid& g = *static_cast<const Grid*>(grid);
+	for (int d = 0; d < 3; d++) out[d] = 0.0;
+	for (size_t idx = 0; idx < g.U.size(); idx++) {
+		if (g.CType[idx] < 0) continue;
+		for (int d = 0; d < 3; d++) {
+			out[d] = std::max(out[d], std::max(g.Max_v[idx][2 * d], g.Max_v[idx][2 * d + 1]));
+		}
+	}
+	return PAMHD_OK;
+}
+
+/*
 Time-stamped inflow of a VALUE side (see Mode_C_Grid::set_inflow): count
 timestamps and count + 1 states of 8 doubles.
 */

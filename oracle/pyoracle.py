@@ -47,6 +47,12 @@ class Cfg(ctypes.Structure):
     ]
 
 
+# Where the reference's source tree is read from, by the oracle's build and by the tests that pin
+# against its own files: the PAMHD_REFERENCE environment variable (the reference tree is absent
+# on machines that only run the built oracle; the pins that need it are skipped there).
+REFERENCE = os.environ.get("PAMHD_REFERENCE", "/root/reference")
+
+
 def make_cfg(n, solver, cell_length, gamma, mu0, cfl, bc_lo=(0, 0, 0), bc_hi=(0, 0, 0),
              value_lo=None, value_hi=None, device=0) -> Cfg:
     c = Cfg()
@@ -127,6 +133,8 @@ class Oracle:
         self._run = getattr(L, p + "grid_run")
         self._run.restype = ctypes.c_int64
         self._run.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int64, _DP, _DP]
+        self._max_signal = getattr(L, p + "grid_max_signal")
+        self._max_signal.argtypes = [ctypes.c_void_p, _DP]
         self._set_inflow = getattr(L, p + "grid_set_inflow")
         self._set_inflow.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
         self._screate = getattr(L, p + "sgrid_create")
@@ -296,6 +304,12 @@ class OracleGrid:
         if rc not in (0, 3):
             raise ValueError(self.o.last_error())
         return dt.value, flag.value, tuple(cell), d.value
+
+    def max_signal(self):
+        """Largest face signal speed of the last step along x, y, z (max of Max_v)."""
+        out = np.zeros(3)
+        self.o._max_signal(self.h, out.ctypes.data_as(_DP))
+        return out
 
     def step_dt(self, dt):
         """One step with a prescribed dt; returns the failure flag (0 when fine)."""

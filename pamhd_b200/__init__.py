@@ -126,7 +126,7 @@ def lib() -> ctypes.CDLL:
     for name in ("pamhd_gpu_set_state", "pamhd_gpu_get_state", "pamhd_gpu_set_state_device",
                  "pamhd_gpu_get_state_device"):
         getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_void_p]
-    L.pamhd_gpu_step.argtypes = [ctypes.c_void_p, _D, _DP]
+    L.pamhd_gpu_step.argtypes = [ctypes.c_void_p, _D, _DP, _DP]
     L.pamhd_gpu_steps.argtypes = [ctypes.c_void_p, ctypes.c_int32, _D]
     L.pamhd_gpu_sync.argtypes = [ctypes.c_void_p]
     L.pamhd_gpu_get_stream.argtypes = [ctypes.c_void_p, _P(ctypes.c_void_p)]
@@ -151,7 +151,7 @@ def lib() -> ctypes.CDLL:
     L.pamhd_gpu_batch_dt_history.argtypes = [V, ctypes.c_int32, _DP, ctypes.c_int32, _P(ctypes.c_int32)]
     L.pamhd_gpu_batch_status.argtypes = [V, ctypes.c_int32, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                          _P(ctypes.c_int32)]
-    if L.pamhd_gpu_abi_version() != 1:
+    if L.pamhd_gpu_abi_version() != 2:
         raise ImportError("libpamhd_gpu.so ABI version mismatch")
     _lib = L
     return L
@@ -227,8 +227,16 @@ class Context:
 
     def step(self, max_dt: float) -> float:
         dt = ctypes.c_double(0)
-        self._check(self.L.pamhd_gpu_step(self.h, max_dt, ctypes.byref(dt)), "pamhd_gpu_step")
+        self._check(self.L.pamhd_gpu_step(self.h, max_dt, ctypes.byref(dt), None), "pamhd_gpu_step")
         return dt.value
+
+    def step_signal(self, max_dt: float):
+        """One step as step(); returns (dt, max_signal): the step length and the largest face
+        signal speed of the step along x, y and z (the reference's Max_v, maximised per axis)."""
+        dt = ctypes.c_double(0)
+        sig = (ctypes.c_double * 3)()
+        self._check(self.L.pamhd_gpu_step(self.h, max_dt, ctypes.byref(dt), sig), "pamhd_gpu_step")
+        return dt.value, np.array(sig[:], dtype=np.float64)
 
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
@@ -648,12 +656,22 @@ class SubstepContext:
         return f.value, tuple(cell), d.value
 
 
+def _check_face_shapes(neg, pos, bg):
+    """The C entry points read n rows of every array: refuse arrays of other shapes before the
+    call (a shorter array would be read past its end)."""
+    if neg.ndim != 2 or neg.shape[1] != 8 or pos.shape != neg.shape:
+        raise ValueError(f"neg and pos must both be (n, 8); got {neg.shape} and {pos.shape}")
+    if bg is not None and np.shape(bg) != (neg.shape[0], 3):
+        raise ValueError(f"bg must be None or ({neg.shape[0]}, 3); got {np.shape(bg)}")
+
+
 def face_flux(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, device=0):
     """Solver-level entry point (pamhd_gpu_face_flux).  neg, pos: (n, 8); bg: (n, 3) or None.
     Returns flux (n, 8), speed (n,), flags (n,); failed faces have flags != 0 (no exception)."""
     L = lib()
     neg = np.ascontiguousarray(neg, dtype=np.float64)
     pos = np.ascontiguousarray(pos, dtype=np.float64)
+    _check_face_shapes(neg, pos, bg)
     n = neg.shape[0]
     flux = np.zeros((n, 8))
     speed = np.zeros(n)
@@ -680,6 +698,7 @@ def face_flux_noalloc(solver, neg, pos, bg=None, gamma=5.0 / 3.0, mu0=1.0, devic
                    _P(ctypes.c_uint32)]
     neg = np.ascontiguousarray(neg, dtype=np.float64)
     pos = np.ascontiguousarray(pos, dtype=np.float64)
+    _check_face_shapes(neg, pos, bg)
     n = neg.shape[0]
     flux = np.zeros((n, 8))
     speed = np.zeros(n)

@@ -307,7 +307,7 @@ int pamhd_gpu_get_state_device(pamhd_ctx* x, double* const soa[8])
 	return get_state_impl(x, soa, cudaMemcpyDeviceToDevice);
 }
 
-int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken)
+int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken, double* max_signal)
 {
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
 	if (not x->loaded) return PAMHD_ERR_STATE;
@@ -315,11 +315,22 @@ int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken)
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	PAMHD_TRY(set_control(*x, max_dt, 0.0));
 	PAMHD_TRY(issue_step(*x));
+	// the step's clock and speed reduction sit in ring slot (steps after it) mod 3
 	Clock c;
 	PAMHD_TRY(check(cudaMemcpyAsync(&c, x->clock + x->steps % 3, sizeof c, cudaMemcpyDeviceToHost, x->stream)));
+	Speed_Max r;
+	PAMHD_TRY(check(cudaMemcpyAsync(&r, x->red + x->steps % 3, sizeof r, cudaMemcpyDeviceToHost, x->stream)));
 	Status s;
 	PAMHD_TRY(read_status(*x, s));
 	if (dt_taken != nullptr) *dt_taken = c.dt;
+	if (max_signal != nullptr) {
+		// internal axis a holds the caller's axis map.perm[a]; the maxima are non-negative doubles
+		for (int a = 0; a < 3; a++) {
+			double v = 0.0;
+			if (x->base.active[a]) std::memcpy(&v, &r.smax[a], sizeof v);
+			max_signal[x->map.perm[a]] = v;
+		}
+	}
 	return s.flags != 0 ? PAMHD_ERR_PHYSICS : PAMHD_OK;
 }
 

@@ -6,7 +6,10 @@ pamhd_gpu_face_flux stages its host arrays through six device buffers that
 it allocates and frees on every call.  This variant stages them through one
 fixed scratch area, a file-scope __device__ array of
 PAMHD_NOALLOC_MAX_FACES faces (3.56 MiB), whose address is looked up once
-per device.  It is for callers that cannot allocate device memory between
+per device (and kept for the life of the process: a cudaDeviceReset between
+calls is not supported, since the driver may place the array elsewhere when
+it reloads the module).  The caller's current device is restored on every
+return.  It is for callers that cannot allocate device memory between
 set-up and tear-down: a process whose device memory is reserved by another
 allocator, or a loop that cannot accept the device-wide synchronisation of
 cudaMalloc / cudaFree.
@@ -50,6 +53,21 @@ int check(const cudaError_t e)
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
+// makes `device` current for the life of the guard, then restores the caller's current device
+struct Device_Guard {
+	int previous = -1;
+	int rc = PAMHD_OK;
+	explicit Device_Guard(const int device)
+	{
+		rc = check(cudaGetDevice(&previous));
+		if (rc == PAMHD_OK) rc = check(cudaSetDevice(device));
+	}
+	~Device_Guard()
+	{
+		if (previous >= 0) cudaSetDevice(previous);
+	}
+};
+
 // address of this device's scratch; the device must be current
 int scratch_address(const int device, unsigned char** out)
 {
@@ -81,10 +99,13 @@ int pamhd_gpu_face_flux_noalloc(const int32_t device, const int32_t solver, cons
 		return PAMHD_ERR_ARGUMENT;
 	}
 	if (not (adiabatic_index > 1.0) or not (vacuum_permeability > 0.0)) return PAMHD_ERR_ARGUMENT;
-	if (device < 0 or device >= MAX_DEVICES) return PAMHD_ERR_ARGUMENT;
 	if (n == 0) return PAMHD_OK;
-	int rc = check(cudaSetDevice(device));
-	if (rc != PAMHD_OK) return rc;
+	// the same code as pamhd_gpu_face_flux for a device that does not exist (the failed
+	// cudaSetDevice), then the limit of the per-device address table
+	const Device_Guard on(device);
+	if (on.rc != PAMHD_OK) return on.rc;
+	if (device >= MAX_DEVICES) return PAMHD_ERR_ARGUMENT;
+	int rc = PAMHD_OK;
 	unsigned char* s = nullptr;
 	rc = scratch_address(device, &s);
 	if (rc != PAMHD_OK) return rc;

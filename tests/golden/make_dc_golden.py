@@ -34,7 +34,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.pyoracle import REFERENCE as REF  # noqa: E402 (the PAMHD_REFERENCE environment variable)
 CASES = {
     "da_px": "tests/mhd/reference/hydrodynamic/density_advection/1d/+x/rusanov/mhd_000000917.dc",
     "da_mx": "tests/mhd/reference/hydrodynamic/density_advection/1d/-x/rusanov/mhd_000000917.dc",

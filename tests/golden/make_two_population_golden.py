@@ -28,7 +28,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 from oracle import pyoracle as po  # noqa: E402
 import states  # noqa: E402
 
-REF = "/root/reference"
+REF = po.REFERENCE  # the PAMHD_REFERENCE environment variable
 TWO_EXE = os.path.join(po.ORACLE_DIR, "_ref", "two_reference.exe")
 SEED = 20261207
 AREA, DT = 0.37, 0.013

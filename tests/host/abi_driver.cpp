@@ -8,8 +8,9 @@ time left as the cap, report the result and write it as a .dc file.
 
 The workload is the Brio-Wu shock tube: cells on [0, 1], gamma 2, mu0 1,
 CFL 0.5, copy boundaries, t = 0 .. 0.1; left rho 1, p 1, B (0.75, 1, 0),
-right rho 0.125, p 0.1, B (0.75, -1, 0).  Prints "steps time rho_sum" and
-exits 0, or prints the error and exits 1.
+right rho 0.125, p 0.1, B (0.75, -1, 0).  Every step's dt is checked against
+the one computed here from the previous step's max_signal output.  Prints
+"steps time rho_sum" and exits 0, or prints the error and exits 1.
 */
 #include <cstdio>
 #include <cstdlib>
@@ -76,12 +77,21 @@ int main(int argc, char** argv)
 	if (rc != PAMHD_OK) return fail("pamhd_gpu_set_state", rc);
 
 	// the priming step, then steps capped by the time left, as the reference's time loop
-	double t = 0.0, dt = 0.0;
-	rc = pamhd_gpu_step(ctx, 0.0, &dt);
+	double t = 0.0, dt = 0.0, signal[3] = {0.0, 0.0, 0.0};
+	rc = pamhd_gpu_step(ctx, 0.0, &dt, signal);
 	if (rc != PAMHD_OK) return fail("pamhd_gpu_step", rc);
 	uint64_t steps = 0;
 	while (t < t_end) {
-		rc = pamhd_gpu_step(ctx, t_end - t, &dt);
+		// the step's dt from the previous step's largest face speed, as a caller with its own
+		// timestep logic computes it (mhd/solve.hpp:1983-2003, capped as substepping.hpp:331-338)
+		double expect = signal[0] > 0.0 ? (cfg.time_step_factor * cfg.cell_length[0]) / signal[0] : 0.0;
+		if (t_end - t <= expect) expect = t_end - t;
+		rc = pamhd_gpu_step(ctx, t_end - t, &dt, signal);
+		if (rc == PAMHD_OK and dt != expect) {
+			std::fprintf(stderr, "step %llu: dt %.17g, from max_signal %.17g\n",
+			             static_cast<unsigned long long>(steps), dt, expect);
+			return 1;
+		}
 		if (rc == PAMHD_ERR_PHYSICS) {
 			uint32_t flags = 0;
 			int32_t cell[3], dir = 0;

@@ -41,7 +41,7 @@ def test_library_exports(lib, name):
 
 
 def test_abi_version_and_errstr(lib):
-    assert lib.pamhd_gpu_abi_version() == 1
+    assert lib.pamhd_gpu_abi_version() == 2
     assert lib.pamhd_gpu_errstr(pg.ERR_PHYSICS).decode().startswith("a face met")
 
 
@@ -73,7 +73,7 @@ def test_create_rejects_invalid_config(lib, change):
 
 def test_null_arguments_rejected(lib):
     assert lib.pamhd_gpu_create(None, None) == pg.ERR_ARGUMENT
-    assert lib.pamhd_gpu_step(None, 0.0, None) == pg.ERR_ARGUMENT
+    assert lib.pamhd_gpu_step(None, 0.0, None, None) == pg.ERR_ARGUMENT
     assert lib.pamhd_gpu_destroy(None) == pg.OK
 
 

@@ -9,8 +9,9 @@ import numpy as np
 import pytest
 
 import pamhd_b200 as pg
+from oracle import pyoracle as po
 
-REF = "/root/reference"
+REF = po.REFERENCE
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 SHIPPED = {
     "da_px": "tests/mhd/reference/hydrodynamic/density_advection/1d/+x/rusanov/mhd_000000917.dc",

@@ -132,6 +132,39 @@ def test_bounded_grid_matches_oracle(port, solver):
         assert field_err(gpu.get_state(), ora.get_state()) <= STEP_TOL * (1 + step)
 
 
+@pytest.mark.parametrize("solver", list(po.SOLVERS))
+@pytest.mark.parametrize("layout", ["bounded3d", "yz_plane"])
+def test_max_signal_matches_oracle(port, layout, solver):
+    """pamhd_gpu_step's max_signal output: per dimension the largest face speed of the step (the
+    maxima of the reference's Max_v, ghost-ghost faces of non-periodic sides included), equal to
+    the oracle's to round-off, and the next step's dt follows from it by the CFL rule."""
+    rng = np.random.default_rng(13)
+    if layout == "bounded3d":
+        n, lengths = (11, 9, 7), (0.09, 0.11, 0.13)
+        U0 = states.smooth_3d((7, 9, 11), rng, amp=0.1)
+        bc = dict(bc_lo=(po.BC_COPY, po.BC_COPY, po.BC_PERIODIC), bc_hi=(po.BC_COPY, po.BC_COPY, po.BC_PERIODIC))
+    else:  # a y-z grid: the context relabels its axes, max_signal stays in the caller's axes
+        n, lengths = (1, 16, 12), (1.0, 1 / 16, 1 / 12)
+        U0 = states.smooth_3d((12, 16, 1), rng, amp=0.1)
+        bc = {}
+    gpu, ora = pair(port, n, po.SOLVERS[solver], lengths, 5 / 3, 1.0, 0.4, **bc)
+    gpu.set_state(U0)
+    ora.set_state(U0)
+    prev = None
+    for step in range(4):
+        dg, sig = gpu.step_signal(1.0)
+        do, flag, _, _ = ora.step(1.0)
+        assert flag == 0
+        so = ora.max_signal()
+        assert np.all((sig == 0) == (so == 0))
+        assert np.abs(sig - so).max() <= 1e-12 * so.max()
+        if prev is not None:
+            # the lagged rule: dt = min over dimensions of CFL * dx_d / max_signal_d of the last step
+            expect = min(0.4 * lengths[d] / prev[d] for d in range(3) if prev[d] > 0)
+            assert dg == min(expect, 1.0)
+        prev = sig
+
+
 # ---------------------------------------------------------------- trajectories
 
 @pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena"])

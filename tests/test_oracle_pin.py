@@ -28,7 +28,7 @@ from oracle import pyoracle as po
 import states
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-REF_TESTS = "/root/reference/tests/mhd"
+REF_TESTS = os.path.join(po.REFERENCE, "tests", "mhd")
 
 
 def _load(name):
