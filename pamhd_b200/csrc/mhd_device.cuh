@@ -85,11 +85,38 @@ __device__ __forceinline__ double recip(const double x)
 }
 
 /*
+Reciprocal square root of a positive normal double: Newton-Raphson
+iteration for f(r) = 1/r^2 - x, r <- r + (r/2)(1 - x r^2) (quadratic
+convergence), from the hardware estimate of PTX rsqrt.approx.ftz.f64; two
+iterations.  sqrt(x) is then x * rsqrt(x), within a few units in the last
+place, which the 1e-12 parity bar leaves ample room for.
+*/
+__device__ __forceinline__ double rsqrt_nr(const double x)
+{
+	double r;
+	asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+	double e = __fma_rn(__dmul_rn(-x, r), r, 1.0);
+	r = __fma_rn(__dmul_rn(0.5, r), e, r);
+	e = __fma_rn(__dmul_rn(-x, r), r, 1.0);
+	return __fma_rn(__dmul_rn(0.5, r), e, r);
+}
+
+/*
+Square root of a non-negative double as x * rsqrt_nr(x) (0, +inf and NaN
+pass through as themselves).
+*/
+__device__ __forceinline__ double sqrt_nr(const double x)
+{
+	return (x > 0.0 and x <= 1.7976931348623157e308) ? __dmul_rn(x, rsqrt_nr(x)) : x;
+}
+
+
+/*
 Every operation below is an explicitly rounded intrinsic, so that every
 inlined copy of this function computes the same bits for the same cell
 (the halo of one tile is the interior of the next).
 */
-template <bool NEED_X, bool NEED_Y, bool NEED_Z>
+template <bool NEED_X, bool NEED_Y, bool NEED_Z, bool NR_SQRT = false>
 __device__ __forceinline__ Derived derive(
 	const double rho, const double mx, const double my, const double mz,
 	const double E, const double bx, const double by, const double bz, const Gas& g
@@ -129,11 +156,13 @@ __device__ __forceinline__ Derived derive(
 			const double cos2 = __dmul_rn(__dmul_rn(comp[a], comp[a]), inv_b2);
 			const double to_sqrt = __fma_rn(prod, __fma_rn(-2.0, cos2, 1.0), base);
 			wave_ok = wave_ok and to_sqrt > 0.0 and is_normal(to_sqrt);
-			d.cf[a] = __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(sum2, __dsqrt_rn(fmax(to_sqrt, 0.0)))));
+			d.cf[a] = NR_SQRT
+				? sqrt_nr(__dmul_rn(0.5, __dadd_rn(sum2, sqrt_nr(fmax(to_sqrt, 0.0)))))
+				: __dsqrt_rn(__dmul_rn(0.5, __dadd_rn(sum2, __dsqrt_rn(fmax(to_sqrt, 0.0)))));
 		}
 		if (d.bad == 0 and not wave_ok) d.bad = PAMHD_FLAG_WAVE_SPEED;
 	} else {
-		const double cs = __dsqrt_rn(fmax(cs2, 0.0));
+		const double cs = NR_SQRT ? sqrt_nr(fmax(cs2, 0.0)) : __dsqrt_rn(fmax(cs2, 0.0));
 		d.cf[0] = d.cf[1] = d.cf[2] = cs;
 		if (d.bad == 0 and not is_finite(b2)) d.bad = PAMHD_FLAG_WAVE_SPEED;
 	}
@@ -309,10 +338,38 @@ __device__ __forceinline__ double flux_hll(const Side& L, const Side& R, const G
 	return fmax(fabs(bp), fabs(bm));
 }
 
+// transverse velocity and field of one side's star state (Miyoshi & Kusano eqns 44-47); the
+// degeneracy test is a select, so the function is one basic block
+struct Star_T {
+	double w1, w2, b1, b2;
+};
+
+__device__ __forceinline__ Star_T star_transverse(const Side& X, const double rho_sd, const double sd,
+                                                  const double sm, const double s_mid, const double bx,
+                                                  const double bx2_mu, const double thr, const Gas& g)
+{
+	const double tmp = rho_sd * sm - bx2_mu;
+	const double it = recip(tmp);
+	const double t1 = bx * (s_mid - X.v0) * g.inv_mu0 * it;
+	const double t2 = (rho_sd * sd - bx2_mu) * it;
+	const bool keep = fabs(tmp) < thr;
+	Star_T t;
+	t.w1 = keep ? X.v1 : X.v1 - X.b1 * t1;
+	t.w2 = keep ? X.v2 : X.v2 - X.b2 * t1;
+	t.b1 = keep ? X.b1 : X.b1 * t2;
+	t.b2 = keep ? X.b2 : X.b2 * t2;
+	return t;
+}
+
 /*
 HLLD of Miyoshi & Kusano (J. Comput. Phys. 208, 2005), as
 mhd/hlld_athena.hpp:62-559; the background field is ignored there (:77)
-and here.
+and here.  Past the supersonic cases every region's ingredients are
+computed in one straight run (both sides' transverse star states, the
+double-star state) and the reference's region choice (:475-552) selects
+among them, so that the compiler can overlap the two sides' dependency
+chains; values of regions not taken are discarded by selects, never
+multiplied in.
 */
 __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const Gas& g, double F[8],
                                             uint32_t& /*flag*/)
@@ -331,130 +388,85 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 		physical_flux(R, pbR, g, F);
 		return fabs(s_neg);
 	}
+	const double speed = fmax(fabs(s_neg), fabs(s_pos));
 
 	const double bx = 0.5 * (L.b0 + R.b0);
 	const double bx2_mu = bx * bx * g.inv_mu0;
 	const double sdL = s_neg - L.v0, sdR = s_pos - R.v0;       // < 0 and > 0 here
 	const double ptL = L.p + pbL, ptR = R.p + pbR;
+	const double rsdL = L.rho * sdL, rsdR = R.rho * sdR;
 	// eqn 38; the denominator is sdR rho_R - sdL rho_L > 0
-	const double s_mid = (sdR * R.m0 - sdL * L.m0 - ptR + ptL) * recip(sdR * R.rho - sdL * L.rho);
+	const double s_mid = (sdR * R.m0 - sdL * L.m0 - ptR + ptL) * recip(rsdR - rsdL);
 	const double smL = s_neg - s_mid, smR = s_pos - s_mid;     // < 0 and > 0 for physical states
 	const double ismL = recip(smL), ismR = recip(smR);
-	// eqn 43
-	const double rsL = L.rho * sdL * ismL, rsR = R.rho * sdR * ismR;
-	const double sqL = sqrt(rsL), sqR = sqrt(rsR);
+	// eqn 43, and the square roots of the star densities with their reciprocals
+	const double rsL = rsdL * ismL, rsR = rsdR * ismR;
+	const double irL = rsqrt_nr(rsL), irR = rsqrt_nr(rsR);
+	const double sqL = rsL * irL, sqR = rsR * irR;
 	// eqn 51
 	const double abx = fabs(bx) * g.inv_sqrt_mu0;
-	const double ssL = s_mid - abx * recip(sqL), ssR = s_mid + abx * recip(sqR);
-	const double ptst = ptL + L.rho * sdL * (s_mid - L.v0);
+	const double ssL = s_mid - abx * irL, ssR = s_mid + abx * irR;
+	const double ptst = ptL + rsdL * (s_mid - L.v0);
 	const double thr = DBL_EPS * ptst;
-
-	/*
-	Star states, eqns 44-48.  The star velocity is (v - B t1) (non-degenerate)
-	or v (degenerate): computed directly instead of dividing the star
-	momentum by the star density.
-	*/
-	double uL[8], uR[8], wL1, wL2, wR1, wR2, vbL, vbR;
-	{
-		const double tmp = L.rho * sdL * smL - bx2_mu;
-		double b1 = L.b1, b2 = L.b2;
-		wL1 = L.v1;
-		wL2 = L.v2;
-		if (not (fabs(tmp) < thr)) {
-			const double it = recip(tmp);
-			const double t1 = bx * (s_mid - L.v0) * g.inv_mu0 * it;
-			const double t2 = (L.rho * sdL * sdL - bx2_mu) * it;
-			wL1 = L.v1 - L.b1 * t1;
-			wL2 = L.v2 - L.b2 * t1;
-			b1 = L.b1 * t2;
-			b2 = L.b2 * t2;
-		}
-		vbL = s_mid * bx + wL1 * b1 + wL2 * b2;
-		const double vb = L.v0 * L.b0 + L.v1 * L.b1 + L.v2 * L.b2;
-		uL[0] = rsL; uL[1] = rsL * s_mid; uL[2] = rsL * wL1; uL[3] = rsL * wL2;
-		uL[4] = (sdL * L.E - ptL * L.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vbL)) * ismL;
-		uL[5] = bx; uL[6] = b1; uL[7] = b2;
-	}
-	{
-		const double tmp = R.rho * sdR * smR - bx2_mu;
-		double b1 = R.b1, b2 = R.b2;
-		wR1 = R.v1;
-		wR2 = R.v2;
-		if (not (fabs(tmp) < thr)) {
-			const double it = recip(tmp);
-			const double t1 = bx * (s_mid - R.v0) * g.inv_mu0 * it;
-			const double t2 = (R.rho * sdR * sdR - bx2_mu) * it;
-			wR1 = R.v1 - R.b1 * t1;
-			wR2 = R.v2 - R.b2 * t1;
-			b1 = R.b1 * t2;
-			b2 = R.b2 * t2;
-		}
-		vbR = s_mid * bx + wR1 * b1 + wR2 * b2;
-		const double vb = R.v0 * R.b0 + R.v1 * R.b1 + R.v2 * R.b2;
-		uR[0] = rsR; uR[1] = rsR * s_mid; uR[2] = rsR * wR1; uR[3] = rsR * wR2;
-		uR[4] = (sdR * R.E - ptR * R.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vbR)) * ismR;
-		uR[5] = bx; uR[6] = b1; uR[7] = b2;
-	}
-
-	const double UL[8] = {L.rho, L.m0, L.m1, L.m2, L.E, L.b0, L.b1, L.b2};
-	const double UR[8] = {R.rho, R.m0, R.m1, R.m2, R.E, R.b0, R.b1, R.b2};
+	// transverse star velocity and field of both sides, eqns 44-47
+	const Star_T tl = star_transverse(L, rsdL, sdL, smL, s_mid, bx, bx2_mu, thr, g);
+	const Star_T tr = star_transverse(R, rsdR, sdR, smR, s_mid, bx, bx2_mu, thr, g);
 
 	// region order of hlld_athena.hpp:475-552: S*_L >= 0, S_M >= 0, S*_R > 0, else
-	if (ssL >= 0.0) {
-		physical_flux(L, pbL, g, F);
-		#pragma unroll
-		for (int v = 0; v < 8; v++) F[v] += s_neg * (uL[v] - UL[v]);
-		F[5] = 0.0;
-		return fmax(fabs(s_neg), fabs(s_pos));
-	}
 	const bool left = s_mid >= 0.0;
-	if (not left and not (ssR > 0.0)) {
-		physical_flux(R, pbR, g, F);
-		#pragma unroll
-		for (int v = 0; v < 8; v++) F[v] += s_pos * (uR[v] - UR[v]);
-		F[5] = 0.0;
-		return fmax(fabs(s_neg), fabs(s_pos));
-	}
+	const bool star_l = ssL >= 0.0;
+	const bool star_r = not star_l and not left and not (ssR > 0.0);
+	const bool dbl = not star_l and not star_r;
+	const bool useL = star_l or (dbl and left);   // the side the flux is taken from
+	const Side& S = useL ? L : R;
+	const Star_T& ts = useL ? tl : tr;
+	const double sd = useL ? sdL : sdR, ism = useL ? ismL : ismR, rs = useL ? rsL : rsR;
+	const double pt = useL ? ptL : ptR, s_out = useL ? s_neg : s_pos;
 
-	// double-star states, eqns 59-63 (identical to the star states when Bx ~ 0)
+	// that side's full star state, eqn 48 for the energy
+	const double vb_star = s_mid * bx + ts.w1 * ts.b1 + ts.w2 * ts.b2;
+	const double vb = S.v0 * S.b0 + S.v1 * S.b1 + S.v2 * S.b2;
+	double us[8];
+	us[0] = rs; us[1] = rs * s_mid; us[2] = rs * ts.w1; us[3] = rs * ts.w2;
+	us[4] = (sd * S.E - pt * S.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vb_star)) * ism;
+	us[5] = bx; us[6] = ts.b1; us[7] = ts.b2;
+	const double U0[8] = {S.rho, S.m0, S.m1, S.m2, S.E, S.b0, S.b1, S.b2};
+	physical_flux(S, useL ? pbL : pbR, g, F);
+
+	// double-star state, eqns 59-63 (the star state itself when Bx ~ 0)
+	const double inv_sum = recip(sqL + sqR);
+	const double sgn = (bx > 0.0) ? 1.0 : -1.0;
+	const double cv = sgn * g.inv_sqrt_mu0;
+	const double v1 = inv_sum * ((sqL * tl.w1 + sqR * tr.w1) + cv * (tr.b1 - tl.b1));
+	const double v2 = inv_sum * ((sqL * tl.w2 + sqR * tr.w2) + cv * (tr.b2 - tl.b2));
+	const double wb = sgn * sqL * sqR * g.sqrt_mu0;
+	const double b1 = inv_sum * ((sqL * tr.b1 + sqR * tl.b1) + wb * (tr.w1 - tl.w1));
+	const double b2 = inv_sum * ((sqL * tr.b2 + sqR * tl.b2) + wb * (tr.w2 - tl.w2));
+	const double vb2 = s_mid * bx + v1 * b1 + v2 * b2;
+	const double e2 = left
+		? us[4] - sqL * sgn * (vb_star - vb2) * g.inv_sqrt_mu0
+		: us[4] + sqR * sgn * (vb_star - vb2) * g.inv_sqrt_mu0;
+	const bool two = dbl and not (0.5 * bx * bx < thr);
 	double u2[8];
-	const double* us = left ? uL : uR;
-	if (0.5 * bx * bx < thr) {
-		#pragma unroll
-		for (int v = 0; v < 8; v++) u2[v] = us[v];
-	} else {
-		const double inv_sum = recip(sqL + sqR);
-		const double sgn = (bx > 0.0) ? 1.0 : -1.0;
-		const double cv = sgn * g.inv_sqrt_mu0;
-		const double v1 = inv_sum * ((sqL * wL1 + sqR * wR1) + cv * (uR[6] - uL[6]));
-		const double v2 = inv_sum * ((sqL * wL2 + sqR * wR2) + cv * (uR[7] - uL[7]));
-		const double wb = sgn * sqL * sqR * g.sqrt_mu0;
-		const double b1 = inv_sum * ((sqL * uR[6] + sqR * uL[6]) + wb * (wR1 - wL1));
-		const double b2 = inv_sum * ((sqL * uR[7] + sqR * uL[7]) + wb * (wR2 - wL2));
-		const double vb2 = s_mid * bx + v1 * b1 + v2 * b2;
-		const double rs = us[0];
-		u2[0] = rs;
-		u2[1] = us[1];
-		u2[2] = rs * v1;
-		u2[3] = rs * v2;
-		u2[4] = left
-			? uL[4] - sqL * sgn * (vbL - vb2) * g.inv_sqrt_mu0
-			: uR[4] + sqR * sgn * (vbR - vb2) * g.inv_sqrt_mu0;
-		u2[5] = bx;
-		u2[6] = b1;
-		u2[7] = b2;
-	}
-	const Side& S = left ? L : R;
-	const double s_out = left ? s_neg : s_pos;
+	u2[0] = us[0]; u2[1] = us[1];
+	u2[2] = two ? rs * v1 : us[2];
+	u2[3] = two ? rs * v2 : us[3];
+	u2[4] = two ? e2 : us[4];
+	u2[5] = us[5];
+	u2[6] = two ? b1 : us[6];
+	u2[7] = two ? b2 : us[7];
+
+	// single star: F + s_out (U* - U); double star: F + s_in U** - (s_in - s_out) U* - s_out U
 	const double s_in = left ? ssL : ssR;
-	const double* U0 = left ? UL : UR;
-	physical_flux(S, left ? pbL : pbR, g, F);
+	const double c2 = dbl ? s_in : 0.0;
+	const double c1 = dbl ? s_in - s_out : -s_out;
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
-		F[v] = F[v] + u2[v] * s_in - us[v] * (s_in - s_out) - U0[v] * s_out;
+		if (v == 5) continue;
+		F[v] = F[v] + u2[v] * c2 - us[v] * c1 - U0[v] * s_out;
 	}
 	F[5] = 0.0;
-	return fmax(fabs(s_neg), fabs(s_pos));
+	return speed;
 }
 
 /*

@@ -264,7 +264,7 @@ __device__ __forceinline__ void load_record(const Step_Params& P, double* rec, u
 	double U[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) U[v] = __ldg(P.in + v * P.L.var + off);
-	const Derived d = derive<CX, CY, CZ>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
+	const Derived d = derive<CX, CY, CZ, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
 	#pragma unroll
 	for (int v = 0; v < 8; v++) rec[v * cells + ri] = U[v];
 	rec[R_RINV * cells + ri] = d.rinv;
@@ -295,35 +295,80 @@ __device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, 
 }
 
 /*
-Solves one face normal to axis A, folds its speed into the running max and
-stores dt * F in the xyz frame.  Each kernel inlines this once per axis, so
-a face is computed by the same instructions wherever it lies in the tiling.
+Solves one z face, folds its speed into the running max and returns the
+unscaled flux in the xyz frame (the update multiplies by dt / dz once per
+cell).  Each kernel inlines this once, so a z face is computed by the same
+instructions wherever it lies in the tiling.
 */
-template <int SOLVER, int CELLS, int A>
-__device__ __forceinline__ void solve_axis(const Step_Params& P, const double* rec_l, const uint32_t* bad_l,
-                                           const int ri_l, const double* rec_r, const uint32_t* bad_r,
-                                           const int ri_r, const double dt, double d[8],
-                                           double& smax, bool& zero, const int i, const int j, const int k)
+template <int SOLVER, int CELLS>
+__device__ __forceinline__ void solve_z(const Step_Params& P, const double* rec_l, const uint32_t* bad_l,
+                                        const double* rec_r, const uint32_t* bad_r, const int ri, double d[8],
+                                        double& smax, bool& zero, const int i, const int j, const int k)
 {
-	const Side L = side_at<A>(rec_l, bad_l, CELLS, ri_l);
-	const Side R = side_at<A>(rec_r, bad_r, CELLS, ri_r);
+	const Side L = side_at<2>(rec_l, bad_l, CELLS, ri);
+	const Side R = side_at<2>(rec_r, bad_r, CELLS, ri);
 	double F[8];
 	uint32_t flag = 0;
 	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
-	if (flag != 0) record_failure(P, flag, i, j, k, A + 1);
+	if (flag != 0) record_failure(P, flag, i, j, k, 3);
 	smax = fmax(smax, s);
 	zero = zero or not (s > 0.0);
-	double m0, m1, m2, b0, b1, b2;
-	unrotate<A>(F[1], F[2], F[3], m0, m1, m2);
-	unrotate<A>(F[5], F[6], F[7], b0, b1, b2);
-	d[0] = dt * F[0];
-	d[1] = dt * m0;
-	d[2] = dt * m1;
-	d[3] = dt * m2;
-	d[4] = dt * F[4];
-	d[5] = dt * b0;
-	d[6] = dt * b1;
-	d[7] = dt * b2;
+	d[0] = F[0];
+	unrotate<2>(F[1], F[2], F[3], d[1], d[2], d[3]);
+	d[4] = F[4];
+	unrotate<2>(F[5], F[6], F[7], d[5], d[6], d[7]);
+}
+
+/*
+One x or y face (axis a, 0 or 1, known only at run time) between record
+positions rl and rr of one slot.  The x and y faces of a plane share this
+one inlined solver instance (half the code of one instance per axis, which
+the instruction cache rewards); the rotation into the face frame is a
+choice of record rows to read, and back a choice of rows of `out` to write.
+The unscaled flux goes to out[v][idx] in the xyz frame.
+*/
+template <int SOLVER, int CELLS>
+__device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec, const uint32_t* bad,
+                                         const int rl, const int rr, const int a, double* out, const int nout,
+                                         const int idx, double& s0, double& s1, bool& zero,
+                                         const int i, const int j, const int k)
+{
+	const int a1 = a + 1, a2 = a == 0 ? 2 : 0;  // the face frame's tangential axes
+	auto side = [&](const int r) {
+		Side s;
+		s.rho = rec[r];
+		s.m0 = rec[(1 + a) * CELLS + r];
+		s.m1 = rec[(1 + a1) * CELLS + r];
+		s.m2 = rec[(1 + a2) * CELLS + r];
+		s.E = rec[4 * CELLS + r];
+		s.b0 = rec[(5 + a) * CELLS + r];
+		s.b1 = rec[(5 + a1) * CELLS + r];
+		s.b2 = rec[(5 + a2) * CELLS + r];
+		s.rinv = rec[R_RINV * CELLS + r];
+		s.p = rec[R_P * CELLS + r];
+		s.cf = rec[(R_CF + a) * CELLS + r];
+		s.v0 = s.m0 * s.rinv;
+		s.v1 = s.m1 * s.rinv;
+		s.v2 = s.m2 * s.rinv;
+		s.bad = bad[r];
+		return s;
+	};
+	const Side L = side(rl);
+	const Side R = side(rr);
+	double F[8];
+	uint32_t flag = 0;
+	const double sp = solve_face<SOLVER>(L, R, P.gas, F, flag);
+	if (flag != 0) record_failure(P, flag, i, j, k, a + 1);
+	if (a == 0) s0 = fmax(s0, sp); else s1 = fmax(s1, sp);
+	zero = zero or not (sp > 0.0);
+	out[idx] = F[0];
+	out[(1 + a) * nout + idx] = F[1];
+	out[(1 + a1) * nout + idx] = F[2];
+	out[(1 + a2) * nout + idx] = F[3];
+	out[4 * nout + idx] = F[4];
+	out[(5 + a) * nout + idx] = F[5];
+	out[(5 + a1) * nout + idx] = F[6];
+	out[(5 + a2) * nout + idx] = F[7];
 }
 
 // ------------------------------------------------------------------ the step
@@ -333,6 +378,13 @@ One work item of a step: the tile (bx, by) of 32 x TY columns over the z
 chunk bz, marched plane by plane; the face speeds are folded into
 s0, s1, s2 and zero (flushed by the caller).  Shared by the single-grid
 and the batched kernels, so that both compute the same bits.
+
+Per plane k: (a) stage the plane's records (two slots alternate, so the
+z face between planes k - 1 and k can read both); (b) every x and y face
+of the plane into shared memory, and the z face below each own cell in
+registers, which completes the cell below: its new state is written; (c)
+each own cell's state plus its x and y flux differences, and the flux of
+its -z face, held in registers until the +z face of the next plane.
 */
 template <int SOLVER, int TY>
 __device__ __forceinline__ void tile_step(const Step_Params& P, double* const smem, const double dt,
@@ -366,10 +418,14 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 	const int kfirst = zact ? kb - 1 : kb;
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
+	// the flux terms are dt F / dx: dt / dx once per axis and cell
+	const double cx = dt * P.inv_len[0], cy = dt * P.inv_len[1], cz = dt * P.inv_len[2];
 
-	double Up[8], Fzm[8];
+	// the cell below the current plane: its state plus its x and y flux differences plus the
+	// flux of its -z face, all scaled; its +z face completes it
+	double Acc[8];
 	#pragma unroll
-	for (int v = 0; v < 8; v++) Up[v] = Fzm[v] = 0.0;
+	for (int v = 0; v < 8; v++) Acc[v] = 0.0;
 
 	for (int k = kfirst; k <= klast; k++) {
 		const int slot = (k - kfirst) & 1;
@@ -403,75 +459,77 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 		}
 		__syncthreads();
 
-		// (b) faces: every thread its -x, -y and -z face; the tile's last column and row also need
-		// their +x / +y faces, taken by the first TY + TX threads in a second pass of the same loop
+		// (b) x and y faces: every thread its -x and -y face; the tile's last column and row also
+		// need their +x / +y faces, taken by one warp each in a further pass of the same loop
 		if (inner) {
 			#pragma unroll 1
-			for (int pass = 0; pass < 2; pass++) {
-				const bool extra = pass == 1;
-				if (extra and warp != XFACE_WARP) break;
-				const int row = extra ? lane : ty;
-				const int col = extra ? TX : tx;
-				if ((extra ? lane < TY : true) and gx0 + col <= nx and gy0 + row < ny) {
-					const int r = (row + T::JO) * T::W + col;
-					double F[8];
-					solve_axis<SOLVER, T::CELLS, 0>(P, rec, bad, r, rec, bad, r + 1, dt, F, s0, zero,
-					                                gx0 + col - 1, gy0 + row, k);
-					#pragma unroll
-					for (int v = 0; v < 8; v++) fx[v * T::FXN + row * (TX + 1) + col] = F[v];
+			for (int task = 0; task < 4; task++) {
+				// 0: own -x face, 1: own -y face, 2: the tile's +x faces, 3: its +y faces
+				if (task == 1 and not YACT) continue;
+				if (task == 2 and warp != XFACE_WARP) continue;
+				if (task == 3 and (not YACT or warp != YFACE_WARP)) continue;
+				const int a = (task == 0 or task == 2) ? 0 : 1;
+				const int row = task == 2 ? lane : (task == 3 ? TY : ty);
+				const int col = task == 2 ? TX : tx;
+				// one call site: the x and y faces share one inlined solver instance
+				bool ok;
+				int rl, rr, idx, i, j;
+				if (a == 0) {
+					ok = (task == 2 ? lane < TY : true) and gx0 + col <= nx and gy0 + row < ny;
+					rl = (row + T::JO) * T::W + col;
+					rr = rl + 1;
+					idx = row * (TX + 1) + col;
+					i = gx0 + col - 1;
+					j = gy0 + row;
+				} else {
+					ok = gy0 + row <= ny and gx0 + col < nx;
+					rl = row * T::W + col + 1;
+					rr = rl + T::W;
+					idx = row * TX + col;
+					i = gx0 + col;
+					j = gy0 + row - 1;
 				}
-			}
-			if (YACT) {
-				#pragma unroll 1
-				for (int pass = 0; pass < 2; pass++) {
-					const bool extra = pass == 1;
-					if (extra and warp != YFACE_WARP) break;
-					const int row = extra ? TY : ty;
-					const int col = tx;
-					if (gy0 + row <= ny and gx0 + col < nx) {
-						const int r = row * T::W + col + 1;
-						double F[8];
-						solve_axis<SOLVER, T::CELLS, 1>(P, rec, bad, r, rec, bad, r + T::W, dt, F, s1, zero,
-						                                gx0 + col, gy0 + row - 1, k);
-						#pragma unroll
-						for (int v = 0; v < 8; v++) fy[v * T::FYN + row * TX + col] = F[v];
-					}
+				if (ok) {
+					solve_xy<SOLVER, T::CELLS>(P, rec, bad, rl, rr, a, a == 0 ? fx : fy, a == 0 ? T::FXN : T::FYN,
+					                           idx, s0, s1, zero, i, j, k);
 				}
 			}
 		}
-		double Fz[8];
+		// the z face between the previous plane and this one, by the column's owner; it completes
+		// the cell below (U += (F- - F+) dt/dx, then y, then z: solve.hpp:1551-1587)
 		if (zact and k > kfirst and own) {
-			solve_axis<SOLVER, T::CELLS, 2>(P, prev, prev_bad, ri, rec, bad, ri, dt, Fz, s2, zero, gx, gy, k - 1);
+			double Fz[8];
+			solve_z<SOLVER, T::CELLS>(P, prev, prev_bad, rec, bad, ri, Fz, s2, zero, gx, gy, k - 1);
+			if (k > kb) {
+				#pragma unroll
+				for (int v = 0; v < 8; v++) Acc[v] = Acc[v] - Fz[v] * cz;
+				write_cell(P, gx, gy, k - 1, Acc, dt);
+			}
+			#pragma unroll
+			for (int v = 0; v < 8; v++) Acc[v] = Fz[v] * cz;
 		}
 		__syncthreads();
 
-		// (c) update: U += (F- - F+)/dx, then y, then z (solve.hpp:1551-1587)
-		if (own) {
-			if (zact and k > kb) {
-				double Un[8];
-				#pragma unroll
-				for (int v = 0; v < 8; v++) Un[v] = Up[v] + (Fzm[v] - Fz[v]) * P.inv_len[2];
-				write_cell(P, gx, gy, k - 1, Un, dt);
+		// (c) the own cell: state plus x and y flux differences (plus its -z flux, held in Acc)
+		if (own and inner) {
+			double Un[8];
+			#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				const double* f = fx + v * T::FXN + ty * (TX + 1) + tx;
+				Un[v] = rec[v * T::CELLS + ri] + (f[0] - f[1]) * cx;
 			}
-			if (inner) {
+			if (YACT) {
 				#pragma unroll
 				for (int v = 0; v < 8; v++) {
-					const double* f = fx + v * T::FXN + ty * (TX + 1) + tx;
-					Up[v] = rec[v * T::CELLS + ri] + (f[0] - f[1]) * P.inv_len[0];
+					const double* f = fy + v * T::FYN + ty * TX + tx;
+					Un[v] += (f[0] - f[TX]) * cy;
 				}
-				if (YACT) {
-					#pragma unroll
-					for (int v = 0; v < 8; v++) {
-						const double* f = fy + v * T::FYN + ty * TX + tx;
-						Up[v] += (f[0] - f[TX]) * P.inv_len[1];
-					}
-				}
-				if (zact) {
-					#pragma unroll
-					for (int v = 0; v < 8; v++) Fzm[v] = Fz[v];
-				} else {
-					write_cell(P, gx, gy, k, Up, dt);
-				}
+			}
+			if (zact) {
+				#pragma unroll
+				for (int v = 0; v < 8; v++) Acc[v] = Un[v] + Acc[v];
+			} else {
+				write_cell(P, gx, gy, k, Un, dt);
 			}
 		}
 	}
