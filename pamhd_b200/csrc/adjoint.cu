@@ -13,9 +13,8 @@ linearisation).  With lambda = dJ/dU_{n+1}, one reverse step is
              COPY source) or, for VALUE sides, to the inflow-state gradient.
 
 Kernels: faces_vjp_kernel (one launch for every active axis: one thread
-per cell, extended by the low ghost layer, computes the faces whose lower
-cell it is and writes g_L and g_R as 16 arrays per axis, x fastest, so that
-reads and writes are coalesced), gather_kernel (one thread per cell, sums
+per face, one solver VJP instance for every axis; writes g_L and g_R as 16
+arrays per axis, x fastest, so that reads and writes are coalesced), gather_kernel (one thread per cell, sums
 its faces in a fixed order: deterministic), value_side_kernel (sums the
 ghost gradients of VALUE sides, one block per side, fixed order; launched
 only when the grid has a VALUE side).
@@ -81,69 +80,57 @@ __device__ __forceinline__ long long face_at(const Layout& L, const int c0, cons
 }
 
 /*
-g_L and g_R of the axis-D face whose lower cell is c (state UL and cotangent
-LL of that cell already loaded, in the state's variable order).
-*/
-template <int SOLVER, int D>
-__device__ __forceinline__ void face_vjp_at(const Adj_Params& A, const int* c, const double* UL, const double* LL)
-{
-	constexpr int E = (D + 1) % 3, F = (D + 2) % 3;
-	constexpr int perm[8] = {0, 1 + D, 1 + E, 1 + F, 4, 5 + D, 5 + E, 5 + F};
-	int r[3] = {c[0], c[1], c[2]};
-	r[D] += 1;
-	const long long oR = A.L.offset(r[0], r[1], r[2]);
-	const bool lam_r = r[D] <= A.L.n[D] - 1;
-	const double scale = A.dt * A.inv_len[D];
-	double uL[8], uR[8], phi[8];
-	#pragma unroll
-	for (int v = 0; v < 8; v++) {
-		uL[v] = UL[perm[v]];
-		uR[v] = A.U[perm[v] * A.L.var + oR];
-		const double lr = lam_r ? A.lam[perm[v] * A.L.var + oR] : 0.0;
-		phi[v] = scale * (lr - LL[perm[v]]);
-	}
-	double gL[8], gR[8];
-	pamhd_b200::adjoint::face_vjp<SOLVER>(uL, uR, A.gas, phi, gL, gR);
-	const long long idx = face_at<D>(A.L, c[0], c[1], c[2]);
-	double* G = A.G[D];
-	const long long nf = A.nf[D];
-	#pragma unroll
-	for (int v = 0; v < 8; v++) {
-		G[perm[v] * nf + idx] = gL[v];
-		G[(8 + perm[v]) * nf + idx] = gR[v];
-	}
-}
-
-/*
 Cotangents of every face of every active axis in one launch: one thread per
-cell of the interior extended by the ghost layer on the low side of each
-active axis; the thread computes the faces whose lower cell is its cell
-(a ghost-layer thread only the face into the interior).
+face.  The faces of axis d are numbered as face_at<d> numbers them (lower
+cell c with c_d from -1 to n_d - 1, the other coordinates interior, x
+fastest), one axis after another, so consecutive threads read consecutive
+cells and write consecutive entries of the 16 arrays of their axis.  The
+axis is a run-time value (the rotation into the face frame a permutation
+of the variables read and written), so the kernel holds one instance of
+the solver's VJP.  A ghost cell has lambda 0; its g goes to the cell it is
+made from in gather_kernel.
 */
 template <int SOLVER>
-__global__ void faces_vjp_kernel(const Adj_Params A)
+__global__ void __launch_bounds__(128) faces_vjp_kernel(const Adj_Params A)
 {
-	const int a0 = A.active[0], a1 = A.active[1], a2 = A.active[2];
-	const int E0 = A.L.n[0] + a0, E1 = A.L.n[1] + a1, E2 = A.L.n[2] + a2;
-	const long long count = (long long)E0 * E1 * E2;
+	const long long n0 = A.active[0] ? A.nf[0] : 0, n1 = A.active[1] ? A.nf[1] : 0;
+	const long long n2 = A.active[2] ? A.nf[2] : 0;
+	const long long count = n0 + n1 + n2;
 	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
 	     t += (long long)gridDim.x * blockDim.x) {
+		const int D = t < n0 ? 0 : (t < n0 + n1 ? 1 : 2);
+		const long long idx = t - (D == 0 ? 0 : (D == 1 ? n0 : n0 + n1));
+		const int E = D == 2 ? 0 : D + 1, F = D == 0 ? 2 : D - 1;
+		const long long N0 = A.L.n[0] + (D == 0), N1 = A.L.n[1] + (D == 1);
 		int c[3];
-		c[0] = int(t % E0) - a0;
-		c[1] = int((t / E0) % E1) - a1;
-		c[2] = int(t / ((long long)E0 * E1)) - a2;
-		const int ghosts = (c[0] < 0) + (c[1] < 0) + (c[2] < 0);
-		if (ghosts > 1) continue;
-		const long long oL = A.L.offset(c[0], c[1], c[2]);
-		double UL[8], LL[8];
+		c[0] = int(idx % N0) - (D == 0);
+		c[1] = int((idx / N0) % N1) - (D == 1);
+		c[2] = int(idx / (N0 * N1)) - (D == 2);
+		int r[3] = {c[0], c[1], c[2]};
+		r[D] += 1;
+		const long long oL = A.L.offset(c[0], c[1], c[2]), oR = A.L.offset(r[0], r[1], r[2]);
+		const bool lam_l = c[D] >= 0, lam_r = r[D] <= A.L.n[D] - 1;
+		const double scale = A.dt * A.inv_len[D];
+		const int perm[8] = {0, 1 + D, 1 + E, 1 + F, 4, 5 + D, 5 + E, 5 + F};
+		double uL[8], uR[8], phi[8];
 		#pragma unroll
 		for (int v = 0; v < 8; v++) {
-			UL[v] = A.U[v * A.L.var + oL];
-			LL[v] = ghosts == 0 ? A.lam[v * A.L.var + oL] : 0.0;
+			const long long o = perm[v] * A.L.var;
+			uL[v] = A.U[o + oL];
+			uR[v] = A.U[o + oR];
+			const double ll = lam_l ? A.lam[o + oL] : 0.0;
+			const double lr = lam_r ? A.lam[o + oR] : 0.0;
+			phi[v] = scale * (lr - ll);
 		}
-		if (a0 and (ghosts == 0 or c[0] < 0)) face_vjp_at<SOLVER, 0>(A, c, UL, LL);
-		if (a1 and (ghosts == 0 or c[1] < 0)) face_vjp_at<SOLVER, 1>(A, c, UL, LL);
-		if (a2 and (ghosts == 0 or c[2] < 0)) face_vjp_at<SOLVER, 2>(A, c, UL, LL);
+		double gL[8], gR[8];
+		pamhd_b200::adjoint::face_vjp<SOLVER>(uL, uR, A.gas, phi, gL, gR);
+		double* G = A.G[D];
+		const long long nf = A.nf[D];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) {
+			G[perm[v] * nf + idx] = gL[v];
+			G[(8 + perm[v]) * nf + idx] = gR[v];
+		}
 	}
 }
 
@@ -257,8 +244,8 @@ int check(const cudaError_t e)
 
 int launch_vjp(const Adj_Params& A, const int solver, cudaStream_t stream)
 {
-	const long long count = (long long)(A.L.n[0] + A.active[0]) * (A.L.n[1] + A.active[1])
-	                        * (A.L.n[2] + A.active[2]);
+	long long count = 0;
+	for (int d = 0; d < 3; d++) count += A.active[d] ? A.nf[d] : 0;
 	const int blocks = int(std::min<long long>(65535, (count + 127) / 128));
 	switch (solver) {
 	case PAMHD_RUSANOV: faces_vjp_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(A); break;

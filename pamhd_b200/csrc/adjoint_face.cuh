@@ -41,10 +41,31 @@ struct Gas_Adj {
 	double gamma, inv_mu0, inv_sqrt_mu0, sqrt_mu0;
 };
 
+/*
+1 / x.  On the device: Newton-Raphson iteration r <- r + r (1 - x r) from
+the estimate of PTX rcp.approx.ftz.f64, two iterations (within one unit in
+the last place for normal non-zero x); on the host, IEEE division.  Each
+denominator of the products below is inverted once and multiplied in.
+*/
+__host__ __device__ __forceinline__ double rcp(const double x)
+{
+#ifdef __CUDA_ARCH__
+	double r;
+	asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+	double e = fma(-x, r, 1.0);
+	r = fma(r, e, r);
+	e = fma(-x, r, 1.0);
+	return fma(r, e, r);
+#else
+	return 1.0 / x;
+#endif
+}
+
 // forward intermediates of one cell seen from a face
 struct Side_Fwd {
 	double rho, m0, m1, m2, E, b0, b1, b2;
 	double r, v0, v1, v2, b2s, m2s, ke, pb, p, cs2, va2, sum2, cos2, base, prod, ts, q, h, cf;
+	double ib2s, iq, icf;  // 1 / b2s, 1 / q (0 when q is 0), 1 / cf
 	bool has_field;
 };
 
@@ -57,7 +78,7 @@ struct Side_Adj {
 __host__ __device__ __forceinline__ void side_forward(const double* U, const Gas_Adj& g, Side_Fwd& s)
 {
 	s.rho = U[0]; s.m0 = U[1]; s.m1 = U[2]; s.m2 = U[3]; s.E = U[4]; s.b0 = U[5]; s.b1 = U[6]; s.b2 = U[7];
-	s.r = 1.0 / s.rho;
+	s.r = rcp(s.rho);
 	s.v0 = s.m0 * s.r;
 	s.v1 = s.m1 * s.r;
 	s.v2 = s.m2 * s.r;
@@ -71,18 +92,21 @@ __host__ __device__ __forceinline__ void side_forward(const double* U, const Gas
 	if (s.has_field) {
 		s.va2 = s.b2s * g.inv_mu0 * s.r;
 		s.sum2 = s.cs2 + s.va2;
-		s.cos2 = s.b0 * s.b0 / s.b2s;
+		s.ib2s = rcp(s.b2s);
+		s.cos2 = s.b0 * s.b0 * s.ib2s;
 		s.base = s.cs2 * s.cs2 + s.va2 * s.va2;
 		s.prod = 2.0 * s.cs2 * s.va2;
 		s.ts = s.base + s.prod * (1.0 - 2.0 * s.cos2);
 		s.q = sqrt(fmax(s.ts, 0.0));
+		s.iq = s.q > 0.0 ? rcp(s.q) : 0.0;
 		s.h = 0.5 * (s.sum2 + s.q);
 		s.cf = sqrt(s.h);
 	} else {
-		s.va2 = s.sum2 = s.cos2 = s.base = s.prod = s.ts = s.q = 0.0;
+		s.va2 = s.sum2 = s.cos2 = s.base = s.prod = s.ts = s.q = s.ib2s = s.iq = 0.0;
 		s.h = s.cs2;
 		s.cf = sqrt(fmax(s.cs2, 0.0));
 	}
+	s.icf = s.cf > 0.0 ? rcp(s.cf) : 0.0;
 }
 
 __host__ __device__ __forceinline__ void side_adj_zero(Side_Adj& a)
@@ -100,10 +124,10 @@ __host__ __device__ __forceinline__ void side_reverse(const Side_Fwd& s, const S
 	double a_p = a.p, a_pb = a.pb, a_r = 0.0, a_b2s = 0.0, a_cs2 = 0.0;
 	if (s.has_field) {
 		// cf = sqrt(h), h = (sum2 + q)/2, q = sqrt(ts), ts = base + prod (1 - 2 cos2)
-		const double a_h = a.cf * 0.5 / s.cf;
+		const double a_h = a.cf * 0.5 * s.icf;
 		const double a_sum2 = 0.5 * a_h;
 		const double a_q = 0.5 * a_h;
-		const double a_ts = s.q > 0.0 ? a_q * 0.5 / s.q : 0.0;
+		const double a_ts = a_q * 0.5 * s.iq;
 		const double a_base = a_ts;
 		const double a_prod = a_ts * (1.0 - 2.0 * s.cos2);
 		const double a_cos2 = -2.0 * s.prod * a_ts;
@@ -111,13 +135,13 @@ __host__ __device__ __forceinline__ void side_reverse(const Side_Fwd& s, const S
 		a_cs2 += 2.0 * s.va2 * a_prod + 2.0 * s.cs2 * a_base + a_sum2;
 		const double a_va2 = 2.0 * s.cs2 * a_prod + 2.0 * s.va2 * a_base + a_sum2;
 		// cos2 = b0^2 / b2s
-		a_b0 += 2.0 * s.b0 / s.b2s * a_cos2;
-		a_b2s += -s.cos2 / s.b2s * a_cos2;
+		a_b0 += 2.0 * s.b0 * s.ib2s * a_cos2;
+		a_b2s += -s.cos2 * s.ib2s * a_cos2;
 		// va2 = b2s / mu0 * r
 		a_b2s += g.inv_mu0 * s.r * a_va2;
 		a_r += s.b2s * g.inv_mu0 * a_va2;
 	} else {
-		a_cs2 += s.cs2 > 0.0 ? a.cf * 0.5 / s.cf : 0.0;
+		a_cs2 += s.cs2 > 0.0 ? a.cf * 0.5 * s.icf : 0.0;
 	}
 	// cs2 = gamma p r
 	a_p += g.gamma * s.r * a_cs2;
@@ -317,7 +341,8 @@ __host__ __device__ __forceinline__ void hll_vjp(const double* UL, const double*
 	double FL[8], FR[8];
 	phys_forward(L, g, FL);
 	phys_forward(R, g, FR);
-	const double w = 0.5 * (bp + bm) / width;
+	const double iwidth = rcp(width);
+	const double w = 0.5 * (bp + bm) * iwidth;
 	double a[8], b[8];
 	for (int v = 0; v < 8; v++) {
 		a[v] = v == 5 ? 0.0 : FL[v] - bm * UL[v];
@@ -333,9 +358,9 @@ __host__ __device__ __forceinline__ void hll_vjp(const double* UL, const double*
 	}
 	aa[5] = ab[5] = 0.0;
 	// w = (bp + bm) / (2 width), width = bp - bm
-	const double a_width = -w / width * a_w;
-	double a_bp = 0.5 / width * a_w + a_width;
-	double a_bm = 0.5 / width * a_w - a_width;
+	const double a_width = -w * iwidth * a_w;
+	double a_bp = 0.5 * iwidth * a_w + a_width;
+	double a_bm = 0.5 * iwidth * a_w - a_width;
 	double dUL[8], dUR[8];
 	for (int v = 0; v < 8; v++) {
 		a_bm += -UL[v] * aa[v];
@@ -363,6 +388,7 @@ __host__ __device__ __forceinline__ void hll_vjp(const double* UL, const double*
 // one side's star state (eqns 44-48) and everything its reverse needs
 struct Star {
 	double sd, sm, rs, tmp, t1, t2, w1, w2, sb1, sb2, vb, vb_old, num_e, Es;
+	double ism, itmp;  // 1 / sm, 1 / tmp (0 when degenerate)
 	bool degenerate;
 };
 
@@ -403,14 +429,18 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 	sR.sd = s_pos - R.v0;
 	const double num = sR.sd * R.m0 - sL.sd * L.m0 - ptR + ptL;
 	const double den = sR.sd * R.rho - sL.sd * L.rho;
-	const double s_mid = num / den;
+	const double iden = rcp(den);
+	const double s_mid = num * iden;
 	sL.sm = s_neg - s_mid;
 	sR.sm = s_pos - s_mid;
-	sL.rs = L.rho * sL.sd / sL.sm;
-	sR.rs = R.rho * sR.sd / sR.sm;
+	sL.ism = rcp(sL.sm);
+	sR.ism = rcp(sR.sm);
+	sL.rs = L.rho * sL.sd * sL.ism;
+	sR.rs = R.rho * sR.sd * sR.ism;
 	const double sqL = sqrt(sL.rs), sqR = sqrt(sR.rs);
+	const double isqL = rcp(sqL), isqR = rcp(sqR);
 	const double abx = fabs(bx) * g.inv_sqrt_mu0;
-	const double ssL = s_mid - abx / sqL, ssR = s_mid + abx / sqR;
+	const double ssL = s_mid - abx * isqL, ssR = s_mid + abx * isqR;
 	const double ptst = ptL + L.rho * sL.sd * (s_mid - L.v0);
 	const double thr = eps * ptst;
 
@@ -418,11 +448,12 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 		st.tmp = S.rho * st.sd * st.sm - bx2m;
 		st.degenerate = fabs(st.tmp) < thr;
 		if (st.degenerate) {
-			st.t1 = st.t2 = 0.0;
+			st.t1 = st.t2 = st.itmp = 0.0;
 			st.w1 = S.v1; st.w2 = S.v2; st.sb1 = S.b1; st.sb2 = S.b2;
 		} else {
-			st.t1 = bx * (s_mid - S.v0) * im / st.tmp;
-			st.t2 = (S.rho * st.sd * st.sd - bx2m) / st.tmp;
+			st.itmp = rcp(st.tmp);
+			st.t1 = bx * (s_mid - S.v0) * im * st.itmp;
+			st.t2 = (S.rho * st.sd * st.sd - bx2m) * st.itmp;
 			st.w1 = S.v1 - S.b1 * st.t1;
 			st.w2 = S.v2 - S.b2 * st.t1;
 			st.sb1 = S.b1 * st.t2;
@@ -431,7 +462,7 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 		st.vb = s_mid * bx + st.w1 * st.sb1 + st.w2 * st.sb2;
 		st.vb_old = S.v0 * S.b0 + S.v1 * S.b1 + S.v2 * S.b2;
 		st.num_e = st.sd * S.E - pt * S.v0 + ptst * s_mid + bx * im * (st.vb_old - st.vb);
-		st.Es = st.num_e / st.sm;
+		st.Es = st.num_e * st.ism;
 	};
 	star_fwd(L, sL, ptL);
 	star_fwd(R, sR, ptR);
@@ -489,7 +520,7 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 		if (not dstar) {
 			for (int v = 0; v < 8; v++) u2[v] = us[v];
 		} else {
-			isum = 1.0 / (sqL + sqR);
+			isum = rcp(sqL + sqR);
 			sgn = bx > 0.0 ? 1.0 : -1.0;
 			cv = sgn * g.inv_sqrt_mu0;
 			n1 = (sqL * sL.w1 + sqR * sR.w1) + cv * (sR.sb1 - sL.sb1);
@@ -608,8 +639,8 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 		a_sb1 += a_u[6];
 		a_sb2 += a_u[7];
 		// E* = num_e / sm
-		const double a_num_e = a_u[4] / st.sm;
-		a_sm += -st.Es / st.sm * a_u[4];
+		const double a_num_e = a_u[4] * st.ism;
+		a_sm += -st.Es * st.ism * a_u[4];
 		// num_e = sd E - pt v0 + ptst s_mid + bx/mu0 (vb_old - vb)
 		a_sd += S.E * a_num_e;
 		A.E += st.sd * a_num_e;
@@ -640,13 +671,14 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 			const double a_t1 = -S.b1 * a_w1 - S.b2 * a_w2;
 			const double a_t2 = S.b1 * a_sb1 + S.b2 * a_sb2;
 			// t1 = bx (s_mid - v0) / mu0 / tmp, t2 = (rho sd^2 - bx2m) / tmp
-			const double a_tmp = -(st.t1 * a_t1 + st.t2 * a_t2) / st.tmp;
-			a_bx += (s_mid - S.v0) * im / st.tmp * a_t1;
-			a_smid += bx * im / st.tmp * a_t1;
-			A.v0 += -bx * im / st.tmp * a_t1;
-			A.rho += st.sd * st.sd / st.tmp * a_t2;
-			a_sd += 2.0 * S.rho * st.sd / st.tmp * a_t2;
-			double a_bx2m = -a_t2 / st.tmp;
+			const double a_tmp = -(st.t1 * a_t1 + st.t2 * a_t2) * st.itmp;
+			const double c1 = im * st.itmp * a_t1, c2 = st.itmp * a_t2;
+			a_bx += (s_mid - S.v0) * c1;
+			a_smid += bx * c1;
+			A.v0 += -bx * c1;
+			A.rho += st.sd * st.sd * c2;
+			a_sd += 2.0 * S.rho * st.sd * c2;
+			double a_bx2m = -c2;
 			// tmp = rho sd sm - bx2m
 			A.rho += st.sd * st.sm * a_tmp;
 			a_sd += S.rho * st.sm * a_tmp;
@@ -668,27 +700,27 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 	AL.v0 += -L.rho * sL.sd * a_ptst;
 	// ssL = s_mid - abx / sqL, ssR = s_mid + abx / sqR, abx = |bx| / sqrt(mu0)
 	a_smid += a_ssL + a_ssR;
-	const double a_abx = -a_ssL / sqL + a_ssR / sqR;
-	a_sqL += abx / (sqL * sqL) * a_ssL;
-	a_sqR += -abx / (sqR * sqR) * a_ssR;
+	const double a_abx = -a_ssL * isqL + a_ssR * isqR;
+	a_sqL += abx * isqL * isqL * a_ssL;
+	a_sqR += -abx * isqR * isqR * a_ssR;
 	a_bx += abs_rev(bx, g.inv_sqrt_mu0 * a_abx);
 	// sq = sqrt(rs)
-	a_rsL += 0.5 / sqL * a_sqL;
-	a_rsR += 0.5 / sqR * a_sqR;
+	a_rsL += 0.5 * isqL * a_sqL;
+	a_rsR += 0.5 * isqR * a_sqR;
 	// rs = rho sd / sm
-	AL.rho += sL.sd / sL.sm * a_rsL;
-	a_sdL += L.rho / sL.sm * a_rsL;
-	a_smL += -sL.rs / sL.sm * a_rsL;
-	AR.rho += sR.sd / sR.sm * a_rsR;
-	a_sdR += R.rho / sR.sm * a_rsR;
-	a_smR += -sR.rs / sR.sm * a_rsR;
+	AL.rho += sL.sd * sL.ism * a_rsL;
+	a_sdL += L.rho * sL.ism * a_rsL;
+	a_smL += -sL.rs * sL.ism * a_rsL;
+	AR.rho += sR.sd * sR.ism * a_rsR;
+	a_sdR += R.rho * sR.ism * a_rsR;
+	a_smR += -sR.rs * sR.ism * a_rsR;
 	// sm = s - s_mid
 	a_sneg += a_smL;
 	a_spos += a_smR;
 	a_smid += -a_smL - a_smR;
 	// s_mid = num / den
-	const double a_num = a_smid / den;
-	const double a_den = -s_mid / den * a_smid;
+	const double a_num = a_smid * iden;
+	const double a_den = -s_mid * iden * a_smid;
 	// num = sdR mR0 - sdL mL0 - ptR + ptL, den = sdR rhoR - sdL rhoL
 	a_sdR += R.m0 * a_num + R.rho * a_den;
 	a_sdL += -L.m0 * a_num - L.rho * a_den;
