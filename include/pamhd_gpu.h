@@ -326,7 +326,7 @@ segment from its checkpoint, on the forward run's dt schedule held fixed.
 seed and grad: eight host arrays each (the layout of set_state).
 grad_value (NULL or 48 doubles): the gradient with respect to the state
 of each VALUE side, [dimension][lo, hi][8].  dt_out (NULL or nsteps
-doubles) receives the schedule.  Solvers: Rusanov, HLL, HLLD.  The
+doubles) receives the schedule.  Solvers: Rusanov, HLL, HLLD, Roe.  The
 device memory (ceil(nsteps/every) checkpoints, two buffers of every - 1
 recompute states, cotangents) stays with the context after the first call
 and is reused by later calls; it grows when a call needs more and is freed

@@ -251,6 +251,7 @@ int launch_vjp(const Adj_Params& A, const int solver, cudaStream_t stream)
 	case PAMHD_RUSANOV: faces_vjp_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(A); break;
 	case PAMHD_HLL_ATHENA: faces_vjp_kernel<PAMHD_HLL_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
 	case PAMHD_HLLD_ATHENA: faces_vjp_kernel<PAMHD_HLLD_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
+	case PAMHD_ROE_ATHENA: faces_vjp_kernel<PAMHD_ROE_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 	return check(cudaGetLastError());
@@ -362,7 +363,6 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 		seed[v] = user_seed[x->map.user_var(v)];
 		grad[v] = user_grad[x->map.user_var(v)];
 	}
-	if (x->cfg.solver == PAMHD_ROE_ATHENA) return PAMHD_ERR_ARGUMENT;  // no Roe adjoint
 	if (x->cfg.bc_lo[2] == PAMHD_BC_EXTERNAL or x->cfg.bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
 	// the inflow-state gradient is of one constant state per side
 	if (x->base.inflow != nullptr) return PAMHD_ERR_ARGUMENT;

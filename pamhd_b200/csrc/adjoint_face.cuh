@@ -749,13 +749,626 @@ __host__ __device__ __forceinline__ void hlld_vjp(const double* UL, const double
 	side_reverse(R, AR, g, gR);
 }
 
+// ---------------------------------------------------------------- Roe
+
+/*
+Roe solver for adiabatic MHD (flux_roe of mhd_device.cuh: Athena's
+esys_roe_adb_mhd and fluxes, mhd/roe_athena.hpp:56-559, the eigensystem of
+eqns B17-B29 of Stone et al., ApJS 178, 2008), in units where the field is
+B / sqrt(mu0).  Forward, then reverse: through the flux of the upwind side
+(supersonic fans) or through F = (F_L + F_R)/2 - sum_m a_m |ev_m| R_m / 2,
+a = L (U_R - U_L), back through the 7 x 7 right and left eigenvectors, the
+eigenvalues and the Roe averages to the two states.  Kinks: |ev_m| at 0
+(abs_rev), the floor of twid_asq (max_rev), the branches of alpha_f and
+alpha_s and of the transverse field direction (bt = 0) taken as evaluated.
+The positivity check of the intermediate states only raises flags: it has
+no derivative.
+*/
+__host__ __device__ __forceinline__ void roe_vjp(const double* UL, const double* UR, const Gas_Adj& g,
+                                                 const double* phi, double* gL, double* gR, double* F = nullptr)
+{
+	constexpr double eps = 2.220446049250313080847e-16;
+	Side_Fwd L, R;
+	side_forward(UL, g, L);
+	side_forward(UR, g, R);
+	Side_Adj AL, AR;
+	side_adj_zero(AL);
+	side_adj_zero(AR);
+	const double gm1 = g.gamma - 1.0, gm2 = g.gamma - 2.0, igm1 = rcp(gm1);
+	const double ism = g.inv_sqrt_mu0;
+
+	// ---- forward: Roe averages (roe_athena.hpp:575-760)
+	const double bxi = 0.5 * (L.b0 + R.b0) * ism;
+	const double byl = L.b1 * ism, bzl = L.b2 * ism, byr = R.b1 * ism, bzr = R.b2 * ism;
+	// pressure with mu0 = 1, as the reference's get_primitive call
+	const double pl = (L.E - 0.5 * L.r * L.m2s - 0.5 * L.b2s) * gm1;
+	const double pr = (R.E - 0.5 * R.r * R.m2s - 0.5 * R.b2s) * gm1;
+	const double sdl = sqrt(L.rho), sdr = sqrt(R.rho);
+	const double isdl = rcp(sdl), isdr = rcp(sdr);
+	const double isd = rcp(sdl + sdr);
+	const double droe = sdl * sdr;
+	const double di = rcp(droe);
+	const double v1 = (sdl * L.v0 + sdr * R.v0) * isd;
+	const double v2 = (sdl * L.v1 + sdr * R.v1) * isd;
+	const double v3 = (sdl * L.v2 + sdr * R.v2) * isd;
+	const double b2 = (sdr * byl + sdl * byr) * isd;
+	const double b3 = (sdr * bzl + sdl * bzr) * isd;
+	const double dby = byl - byr, dbz = bzl - bzr;
+	const double x = 0.5 * (dby * dby + dbz * dbz) * (isd * isd);
+	const double y = 0.5 * (L.rho + R.rho) * di;
+	const double pbl = 0.5 * (bxi * bxi + byl * byl + bzl * bzl);
+	const double pbr = 0.5 * (bxi * bxi + byr * byr + bzr * bzr);
+	const double hl = (L.E + pl + pbl) * isdl, hr = (R.E + pr + pbr) * isdr;
+	const double h = (hl + hr) * isd;
+	const double b1 = bxi;
+	// eigensystem (B17-B29)
+	const double vsq = v1 * v1 + v2 * v2 + v3 * v3;
+	const double btsq = b2 * b2 + b3 * b3;
+	const double ystar = gm1 - gm2 * y;
+	const double bt_starsq = ystar * btsq;
+	const double vaxsq = b1 * b1 * di;
+	const double hp = h - (vaxsq + btsq * di);
+	const double twid_raw = gm1 * (hp - 0.5 * vsq) - gm2 * x;
+	const double twid_asq = fmax(twid_raw, eps);
+	const double ct2 = bt_starsq * di;
+	const double tsum = vaxsq + ct2 + twid_asq;
+	const double tdif = vaxsq + ct2 - twid_asq;
+	const double cf2_cs2 = sqrt(tdif * tdif + 4.0 * twid_asq * ct2);
+	const double cfsq = 0.5 * (tsum + cf2_cs2);
+	const double cf = sqrt(cfsq);
+	const double icfsq = rcp(cfsq);
+	const double cssq = twid_asq * vaxsq * icfsq;
+	const double cs = sqrt(cssq);
+	const double bt = sqrt(btsq);
+	const double bt_star = sqrt(bt_starsq);
+	const bool has_bt = bt != 0.0;
+	const double ibt = has_bt ? rcp(bt) : 0.0;
+	const double bet2 = has_bt ? b2 * ibt : 1.0, bet3 = has_bt ? b3 * ibt : 0.0;
+	const double iys = rcp(sqrt(ystar));
+	const double bet2_star = bet2 * iys, bet3_star = bet3 * iys;
+	const double bet_starsq = bet2_star * bet2_star + bet3_star * bet3_star;
+	const double vbet = v2 * bet2_star + v3 * bet3_star;
+	int acase;
+	double alpha_f, alpha_s, aid = 0.0, ra = 0.0, rb = 0.0;
+	if ((cfsq - cssq) == 0.0) {
+		acase = 0; alpha_f = 1.0; alpha_s = 0.0;
+	} else if ((twid_asq - cssq) <= 0.0) {
+		acase = 1; alpha_f = 0.0; alpha_s = 1.0;
+	} else if ((cfsq - twid_asq) <= 0.0) {
+		acase = 2; alpha_f = 1.0; alpha_s = 0.0;
+	} else {
+		acase = 3;
+		aid = rcp(cfsq - cssq);
+		ra = (twid_asq - cssq) * aid;
+		rb = (cfsq - twid_asq) * aid;
+		alpha_f = sqrt(ra);
+		alpha_s = sqrt(rb);
+	}
+	const double sqrtd = sqrt(droe);
+	const double isqrtd = rcp(sqrtd);
+	const double sg = (b1 > 0.0) ? 1.0 : -1.0;
+	const double twid_a = sqrt(twid_asq);
+	const double qf = cf * alpha_f * sg, qs = cs * alpha_s * sg;
+	const double af_prime = twid_a * alpha_f * isqrtd, as_prime = twid_a * alpha_s * isqrtd;
+	const double afpbb = af_prime * bt_star * bet_starsq, aspbb = as_prime * bt_star * bet_starsq;
+	const double vax = sqrt(vaxsq);
+	const double ev[7] = {v1 - cf, v1 - vax, v1 - cs, v1, v1 + cs, v1 + vax, v1 + cf};
+
+	// both states and their fluxes in units B / sqrt(mu0)
+	const double Ul[7] = {L.rho, L.m0, L.m1, L.m2, L.E, byl, bzl};
+	const double Ur[7] = {R.rho, R.m0, R.m1, R.m2, R.E, byr, bzr};
+	auto flux7 = [&](const Side_Fwd& S, const double p, const double pb, const double by, const double bz,
+	                 double* Fs) {
+		Fs[0] = S.m0;
+		Fs[1] = S.m0 * S.v0 + p - 0.5 * (bxi * bxi - by * by - bz * bz);
+		Fs[2] = S.m0 * S.v1 - bxi * by;
+		Fs[3] = S.m0 * S.v2 - bxi * bz;
+		Fs[4] = (S.E + p) * S.v0 + pb * S.v0 - bxi * (bxi * S.v0 + by * S.v1 + bz * S.v2);
+		Fs[5] = by * S.v0 - bxi * S.v1;
+		Fs[6] = bz * S.v0 - bxi * S.v2;
+	};
+	double Fl[7], Fr[7];
+	flux7(L, pl, pbl, byl, bzl, Fl);
+	flux7(R, pr, pbr, byr, bzr, Fr);
+
+	// adjoint of the 7-component flux
+	const double aFo[7] = {phi[0], phi[1], phi[2], phi[3], phi[4], phi[6] * g.sqrt_mu0, phi[7] * g.sqrt_mu0};
+	double aFl[7] = {0, 0, 0, 0, 0, 0, 0}, aFr[7] = {0, 0, 0, 0, 0, 0, 0};
+	double aUl[7] = {0, 0, 0, 0, 0, 0, 0}, aUr[7] = {0, 0, 0, 0, 0, 0, 0};
+	// adjoints of the averages and of the eigensystem's scalars
+	double a_v1 = 0, a_v2 = 0, a_v3 = 0, a_b2 = 0, a_b3 = 0, a_x = 0, a_hp = 0, a_vsq = 0, a_cf = 0, a_cs = 0;
+	double a_af = 0, a_as = 0, a_qf = 0, a_qs = 0, a_bet2 = 0, a_bet3 = 0, a_b2s = 0, a_b3s = 0, a_vbet = 0;
+	double a_afp = 0, a_asp = 0, a_afpbb = 0, a_aspbb = 0, a_isqrtd = 0, a_sqrtd = 0, a_droe = 0, a_vax = 0;
+	double a_bt_star = 0, a_bsq = 0, a_twid = 0;
+	double Fo[7];
+
+	if (ev[0] >= 0.0) {
+		for (int r = 0; r < 7; r++) { Fo[r] = Fl[r]; aFl[r] = aFo[r]; }
+	} else if (ev[6] <= 0.0) {
+		for (int r = 0; r < 7; r++) { Fo[r] = Fr[r]; aFr[r] = aFo[r]; }
+	} else {
+		// right eigenvectors as columns, R[row][wave]
+		double Rm[7][7];
+		Rm[0][0] = alpha_f; Rm[0][1] = 0.0; Rm[0][2] = alpha_s; Rm[0][3] = 1.0;
+		Rm[0][4] = alpha_s; Rm[0][5] = 0.0; Rm[0][6] = alpha_f;
+		Rm[1][0] = alpha_f * ev[0]; Rm[1][1] = 0.0; Rm[1][2] = alpha_s * ev[2]; Rm[1][3] = v1;
+		Rm[1][4] = alpha_s * ev[4]; Rm[1][5] = 0.0; Rm[1][6] = alpha_f * ev[6];
+		{
+			const double qa = alpha_f * v2, qb = alpha_s * v2, qc = qs * bet2_star, qd = qf * bet2_star;
+			Rm[2][0] = qa + qc; Rm[2][1] = -bet3; Rm[2][2] = qb - qd; Rm[2][3] = v2;
+			Rm[2][4] = qb + qd; Rm[2][5] = bet3; Rm[2][6] = qa - qc;
+		}
+		{
+			const double qa = alpha_f * v3, qb = alpha_s * v3, qc = qs * bet3_star, qd = qf * bet3_star;
+			Rm[3][0] = qa + qc; Rm[3][1] = bet2; Rm[3][2] = qb - qd; Rm[3][3] = v3;
+			Rm[3][4] = qb + qd; Rm[3][5] = -bet2; Rm[3][6] = qa - qc;
+		}
+		const double wv = v2 * bet3 - v3 * bet2;
+		Rm[4][0] = alpha_f * (hp - v1 * cf) + qs * vbet + aspbb;
+		Rm[4][1] = -wv;
+		Rm[4][2] = alpha_s * (hp - v1 * cs) - qf * vbet - afpbb;
+		Rm[4][3] = 0.5 * vsq + gm2 * x * igm1;
+		Rm[4][4] = alpha_s * (hp + v1 * cs) + qf * vbet - afpbb;
+		Rm[4][5] = wv;
+		Rm[4][6] = alpha_f * (hp + v1 * cf) - qs * vbet + aspbb;
+		Rm[5][0] = as_prime * bet2_star; Rm[5][1] = -bet3 * sg * isqrtd; Rm[5][2] = -af_prime * bet2_star;
+		Rm[5][3] = 0.0; Rm[5][4] = Rm[5][2]; Rm[5][5] = Rm[5][1]; Rm[5][6] = Rm[5][0];
+		Rm[6][0] = as_prime * bet3_star; Rm[6][1] = bet2 * sg * isqrtd; Rm[6][2] = -af_prime * bet3_star;
+		Rm[6][3] = 0.0; Rm[6][4] = Rm[6][2]; Rm[6][5] = Rm[6][1]; Rm[6][6] = Rm[6][0];
+
+		// left eigenvectors as rows
+		const double itw = rcp(twid_asq);
+		const double norm0 = 0.5 * itw;
+		const double cff = norm0 * alpha_f * cf, css = norm0 * alpha_s * cs;
+		const double qfn = qf * norm0, qsn = qs * norm0;
+		const double afd = norm0 * af_prime * droe, asd = norm0 * as_prime * droe;
+		const double afpb = norm0 * af_prime * bt_star, aspb = norm0 * as_prime * bt_star;
+		const double norm1 = norm0 * gm1;
+		const double af_n = alpha_f * norm1, as_n = alpha_s * norm1;
+		const double ibs = rcp(bet_starsq);
+		const double q2s = bet2_star * ibs, q3s = bet3_star * ibs;
+		const double vqstr = v2 * q2s + v3 * q3s;
+		const double norm2 = norm1 * 2.0;
+		double Lm[7][7];
+		Lm[0][0] = af_n * (vsq - hp) + cff * (cf + v1) - qsn * vqstr - aspb;
+		Lm[0][1] = -af_n * v1 - cff;
+		Lm[0][2] = -af_n * v2 + qsn * q2s;
+		Lm[0][3] = -af_n * v3 + qsn * q3s;
+		Lm[0][4] = af_n;
+		Lm[0][5] = asd * q2s - af_n * b2;
+		Lm[0][6] = asd * q3s - af_n * b3;
+		Lm[1][0] = 0.5 * wv; Lm[1][1] = 0.0; Lm[1][2] = -0.5 * bet3;
+		Lm[1][3] = 0.5 * bet2; Lm[1][4] = 0.0; Lm[1][5] = -0.5 * sqrtd * bet3 * sg;
+		Lm[1][6] = 0.5 * sqrtd * bet2 * sg;
+		Lm[2][0] = as_n * (vsq - hp) + css * (cs + v1) + qfn * vqstr + afpb;
+		Lm[2][1] = -as_n * v1 - css;
+		Lm[2][2] = -as_n * v2 - qfn * q2s;
+		Lm[2][3] = -as_n * v3 - qfn * q3s;
+		Lm[2][4] = as_n;
+		Lm[2][5] = -afd * q2s - as_n * b2;
+		Lm[2][6] = -afd * q3s - as_n * b3;
+		Lm[3][0] = 1.0 - norm2 * (0.5 * vsq - gm2 * x * igm1);
+		Lm[3][1] = norm2 * v1; Lm[3][2] = norm2 * v2; Lm[3][3] = norm2 * v3;
+		Lm[3][4] = -norm2; Lm[3][5] = norm2 * b2; Lm[3][6] = norm2 * b3;
+		Lm[4][0] = as_n * (vsq - hp) + css * (cs - v1) - qfn * vqstr + afpb;
+		Lm[4][1] = -as_n * v1 + css;
+		Lm[4][2] = -as_n * v2 + qfn * q2s;
+		Lm[4][3] = -as_n * v3 + qfn * q3s;
+		Lm[4][4] = as_n;
+		Lm[4][5] = Lm[2][5];
+		Lm[4][6] = Lm[2][6];
+		Lm[5][0] = -Lm[1][0]; Lm[5][1] = 0.0; Lm[5][2] = -Lm[1][2]; Lm[5][3] = -Lm[1][3];
+		Lm[5][4] = 0.0; Lm[5][5] = Lm[1][5]; Lm[5][6] = Lm[1][6];
+		Lm[6][0] = af_n * (vsq - hp) + cff * (cf - v1) + qsn * vqstr - aspb;
+		Lm[6][1] = -af_n * v1 + cff;
+		Lm[6][2] = -af_n * v2 - qsn * q2s;
+		Lm[6][3] = -af_n * v3 - qsn * q3s;
+		Lm[6][4] = af_n;
+		Lm[6][5] = Lm[0][5];
+		Lm[6][6] = Lm[0][6];
+
+		double a[7], dU[7];
+		for (int m = 0; m < 7; m++) dU[m] = Ur[m] - Ul[m];
+		for (int n = 0; n < 7; n++) {
+			double t = 0.0;
+			for (int m = 0; m < 7; m++) t += Lm[n][m] * dU[m];
+			a[n] = t;
+		}
+		double c[7];
+		for (int r = 0; r < 7; r++) Fo[r] = 0.5 * (Fl[r] + Fr[r]);
+		for (int m = 0; m < 7; m++) {
+			c[m] = 0.5 * a[m] * fabs(ev[m]);
+			for (int r = 0; r < 7; r++) Fo[r] -= c[m] * Rm[r][m];
+		}
+
+		// ---- reverse of the projection: Fo = (Fl + Fr)/2 - sum_m c_m R[:, m], c_m = a_m |ev_m| / 2
+		double aR[7][7], aL[7][7], a_a[7], a_ev[7];
+		for (int r = 0; r < 7; r++) {
+			aFl[r] += 0.5 * aFo[r];
+			aFr[r] += 0.5 * aFo[r];
+		}
+		for (int m = 0; m < 7; m++) {
+			double a_c = 0.0;
+			for (int r = 0; r < 7; r++) {
+				a_c -= aFo[r] * Rm[r][m];
+				aR[r][m] = -c[m] * aFo[r];
+			}
+			a_a[m] = 0.5 * fabs(ev[m]) * a_c;
+			a_ev[m] = abs_rev(ev[m], 0.5 * a[m] * a_c);
+		}
+		// a = L dU
+		for (int m = 0; m < 7; m++) {
+			double t = 0.0;
+			for (int n = 0; n < 7; n++) {
+				aL[n][m] = a_a[n] * dU[m];
+				t += Lm[n][m] * a_a[n];
+			}
+			aUr[m] += t;
+			aUl[m] -= t;
+		}
+		// entries of L defined as others
+		aL[2][5] += aL[4][5]; aL[2][6] += aL[4][6];
+		aL[0][5] += aL[6][5]; aL[0][6] += aL[6][6];
+		aL[1][0] -= aL[5][0]; aL[1][2] -= aL[5][2]; aL[1][3] -= aL[5][3];
+		aL[1][5] += aL[5][5]; aL[1][6] += aL[5][6];
+		double a_af_n = 0, a_as_n = 0, a_cff = 0, a_css = 0, a_qsn = 0, a_qfn = 0, a_vqstr = 0;
+		double a_aspb = 0, a_afpb = 0, a_asd = 0, a_afd = 0, a_q2s = 0, a_q3s = 0, a_norm2 = 0, a_wv = 0;
+		// rows 0 and 6 (fast waves), 2 and 4 (slow waves): X (vsq - hp) + Y (c +/- v1) +/- Q vqstr +/- P
+		auto wave_row0 = [&](const double* A, const double sgn_c, const double sgn_q, const double sgn_p,
+		                     const double n_, const double cc, const double c_, const double qn, const double* row,
+		                     double& a_n_, double& a_cc, double& a_c_, double& a_qn, double& a_p) {
+			a_n_ += (vsq - hp) * A[0];
+			a_vsq += n_ * A[0];
+			a_hp -= n_ * A[0];
+			a_cc += (c_ + sgn_c * v1) * A[0];
+			a_c_ += cc * A[0];
+			a_v1 += sgn_c * cc * A[0];
+			a_qn += sgn_q * vqstr * A[0];
+			a_vqstr += sgn_q * qn * A[0];
+			a_p += sgn_p * A[0];
+			(void)row;
+		};
+		// row 0: af_n (vsq - hp) + cff (cf + v1) - qsn vqstr - aspb
+		wave_row0(aL[0], 1.0, -1.0, -1.0, af_n, cff, cf, qsn, Lm[0], a_af_n, a_cff, a_cf, a_qsn, a_aspb);
+		// row 6: af_n (vsq - hp) + cff (cf - v1) + qsn vqstr - aspb
+		wave_row0(aL[6], -1.0, 1.0, -1.0, af_n, cff, cf, qsn, Lm[6], a_af_n, a_cff, a_cf, a_qsn, a_aspb);
+		// row 2: as_n (vsq - hp) + css (cs + v1) + qfn vqstr + afpb
+		wave_row0(aL[2], 1.0, 1.0, 1.0, as_n, css, cs, qfn, Lm[2], a_as_n, a_css, a_cs, a_qfn, a_afpb);
+		// row 4: as_n (vsq - hp) + css (cs - v1) - qfn vqstr + afpb
+		wave_row0(aL[4], -1.0, -1.0, 1.0, as_n, css, cs, qfn, Lm[4], a_as_n, a_css, a_cs, a_qfn, a_afpb);
+		// columns 1..4 of rows 0, 6: -af_n v -/+ ..., row 0: -cff, +qsn q; row 6: +cff, -qsn q
+		a_af_n += -v1 * aL[0][1] - v2 * aL[0][2] - v3 * aL[0][3] + aL[0][4];
+		a_af_n += -v1 * aL[6][1] - v2 * aL[6][2] - v3 * aL[6][3] + aL[6][4];
+		a_v1 += -af_n * (aL[0][1] + aL[6][1]);
+		a_v2 += -af_n * (aL[0][2] + aL[6][2]);
+		a_v3 += -af_n * (aL[0][3] + aL[6][3]);
+		a_cff += -aL[0][1] + aL[6][1];
+		a_qsn += q2s * (aL[0][2] - aL[6][2]) + q3s * (aL[0][3] - aL[6][3]);
+		a_q2s += qsn * (aL[0][2] - aL[6][2]);
+		a_q3s += qsn * (aL[0][3] - aL[6][3]);
+		// rows 2, 4: -as_n v -/+ ..., row 2: -css, -qfn q; row 4: +css, +qfn q
+		a_as_n += -v1 * aL[2][1] - v2 * aL[2][2] - v3 * aL[2][3] + aL[2][4];
+		a_as_n += -v1 * aL[4][1] - v2 * aL[4][2] - v3 * aL[4][3] + aL[4][4];
+		a_v1 += -as_n * (aL[2][1] + aL[4][1]);
+		a_v2 += -as_n * (aL[2][2] + aL[4][2]);
+		a_v3 += -as_n * (aL[2][3] + aL[4][3]);
+		a_css += -aL[2][1] + aL[4][1];
+		a_qfn += q2s * (-aL[2][2] + aL[4][2]) + q3s * (-aL[2][3] + aL[4][3]);
+		a_q2s += qfn * (-aL[2][2] + aL[4][2]);
+		a_q3s += qfn * (-aL[2][3] + aL[4][3]);
+		// columns 5, 6: row 0 asd q - af_n b, row 2 -afd q - as_n b
+		a_asd += q2s * aL[0][5] + q3s * aL[0][6];
+		a_q2s += asd * aL[0][5] - afd * aL[2][5];
+		a_q3s += asd * aL[0][6] - afd * aL[2][6];
+		a_af_n += -b2 * aL[0][5] - b3 * aL[0][6];
+		a_b2 += -af_n * aL[0][5] - as_n * aL[2][5];
+		a_b3 += -af_n * aL[0][6] - as_n * aL[2][6];
+		a_afd += -q2s * aL[2][5] - q3s * aL[2][6];
+		a_as_n += -b2 * aL[2][5] - b3 * aL[2][6];
+		// row 1: 0.5 wv, -0.5 bet3, 0.5 bet2, -0.5 sqrtd bet3 sg, 0.5 sqrtd bet2 sg
+		a_wv += 0.5 * aL[1][0];
+		a_bet3 += -0.5 * aL[1][2] - 0.5 * sqrtd * sg * aL[1][5];
+		a_bet2 += 0.5 * aL[1][3] + 0.5 * sqrtd * sg * aL[1][6];
+		a_sqrtd += 0.5 * sg * (-bet3 * aL[1][5] + bet2 * aL[1][6]);
+		// row 3: 1 - norm2 (vsq / 2 - gm2 x / gm1), norm2 (v1, v2, v3, -1, b2, b3)
+		a_norm2 += -(0.5 * vsq - gm2 * x * igm1) * aL[3][0]
+		           + v1 * aL[3][1] + v2 * aL[3][2] + v3 * aL[3][3] - aL[3][4] + b2 * aL[3][5] + b3 * aL[3][6];
+		a_vsq += -0.5 * norm2 * aL[3][0];
+		a_x += norm2 * gm2 * igm1 * aL[3][0];
+		a_v1 += norm2 * aL[3][1];
+		a_v2 += norm2 * aL[3][2];
+		a_v3 += norm2 * aL[3][3];
+		a_b2 += norm2 * aL[3][5];
+		a_b3 += norm2 * aL[3][6];
+		// the left eigenvectors' scalars
+		double a_norm1 = 2.0 * a_norm2, a_norm0 = 0.0;
+		a_v2 += q2s * a_vqstr;
+		a_v3 += q3s * a_vqstr;
+		a_q2s += v2 * a_vqstr;
+		a_q3s += v3 * a_vqstr;
+		const double a_ibs = bet2_star * a_q2s + bet3_star * a_q3s;
+		a_b2s += ibs * a_q2s;
+		a_b3s += ibs * a_q3s;
+		a_bsq += -ibs * ibs * a_ibs;
+		a_af += norm1 * a_af_n;
+		a_as += norm1 * a_as_n;
+		a_norm1 += alpha_f * a_af_n + alpha_s * a_as_n;
+		a_norm0 += gm1 * a_norm1;
+		a_norm0 += af_prime * bt_star * a_afpb + as_prime * bt_star * a_aspb;
+		a_afp += norm0 * bt_star * a_afpb;
+		a_asp += norm0 * bt_star * a_aspb;
+		a_bt_star += norm0 * (af_prime * a_afpb + as_prime * a_aspb);
+		a_norm0 += af_prime * droe * a_afd + as_prime * droe * a_asd;
+		a_afp += norm0 * droe * a_afd;
+		a_asp += norm0 * droe * a_asd;
+		a_droe += norm0 * (af_prime * a_afd + as_prime * a_asd);
+		a_qf += norm0 * a_qfn;
+		a_qs += norm0 * a_qsn;
+		a_norm0 += qf * a_qfn + qs * a_qsn;
+		a_norm0 += alpha_f * cf * a_cff + alpha_s * cs * a_css;
+		a_af += norm0 * cf * a_cff;
+		a_cf += norm0 * alpha_f * a_cff;
+		a_as += norm0 * cs * a_css;
+		a_cs += norm0 * alpha_s * a_css;
+		a_twid += -0.5 * itw * itw * a_norm0;
+
+		// ---- reverse of the right eigenvectors
+		a_af += aR[0][0] + aR[0][6];
+		a_as += aR[0][2] + aR[0][4];
+		a_af += ev[0] * aR[1][0] + ev[6] * aR[1][6];
+		a_as += ev[2] * aR[1][2] + ev[4] * aR[1][4];
+		a_ev[0] += alpha_f * aR[1][0];
+		a_ev[6] += alpha_f * aR[1][6];
+		a_ev[2] += alpha_s * aR[1][2];
+		a_ev[4] += alpha_s * aR[1][4];
+		a_v1 += aR[1][3];
+		{
+			// row 2: qa + qc, -bet3, qb - qd, v2, qb + qd, bet3, qa - qc
+			const double a_qa = aR[2][0] + aR[2][6], a_qc = aR[2][0] - aR[2][6];
+			const double a_qb = aR[2][2] + aR[2][4], a_qd = -aR[2][2] + aR[2][4];
+			a_bet3 += -aR[2][1] + aR[2][5];
+			a_v2 += aR[2][3] + alpha_f * a_qa + alpha_s * a_qb;
+			a_af += v2 * a_qa;
+			a_as += v2 * a_qb;
+			a_qs += bet2_star * a_qc;
+			a_qf += bet2_star * a_qd;
+			a_b2s += qs * a_qc + qf * a_qd;
+		}
+		{
+			// row 3: qa + qc, bet2, qb - qd, v3, qb + qd, -bet2, qa - qc
+			const double a_qa = aR[3][0] + aR[3][6], a_qc = aR[3][0] - aR[3][6];
+			const double a_qb = aR[3][2] + aR[3][4], a_qd = -aR[3][2] + aR[3][4];
+			a_bet2 += aR[3][1] - aR[3][5];
+			a_v3 += aR[3][3] + alpha_f * a_qa + alpha_s * a_qb;
+			a_af += v3 * a_qa;
+			a_as += v3 * a_qb;
+			a_qs += bet3_star * a_qc;
+			a_qf += bet3_star * a_qd;
+			a_b3s += qs * a_qc + qf * a_qd;
+		}
+		// row 4
+		a_af += (hp - v1 * cf) * aR[4][0] + (hp + v1 * cf) * aR[4][6];
+		a_as += (hp - v1 * cs) * aR[4][2] + (hp + v1 * cs) * aR[4][4];
+		a_hp += alpha_f * (aR[4][0] + aR[4][6]) + alpha_s * (aR[4][2] + aR[4][4]);
+		a_v1 += alpha_f * cf * (-aR[4][0] + aR[4][6]) + alpha_s * cs * (-aR[4][2] + aR[4][4]);
+		a_cf += alpha_f * v1 * (-aR[4][0] + aR[4][6]);
+		a_cs += alpha_s * v1 * (-aR[4][2] + aR[4][4]);
+		a_qs += vbet * (aR[4][0] - aR[4][6]);
+		a_qf += vbet * (-aR[4][2] + aR[4][4]);
+		a_vbet += qs * (aR[4][0] - aR[4][6]) + qf * (-aR[4][2] + aR[4][4]);
+		a_aspbb += aR[4][0] + aR[4][6];
+		a_afpbb += -aR[4][2] - aR[4][4];
+		a_wv += -aR[4][1] + aR[4][5];
+		a_vsq += 0.5 * aR[4][3];
+		a_x += gm2 * igm1 * aR[4][3];
+		// rows 5 and 6
+		a_asp += bet2_star * (aR[5][0] + aR[5][6]) + bet3_star * (aR[6][0] + aR[6][6]);
+		a_afp += -bet2_star * (aR[5][2] + aR[5][4]) - bet3_star * (aR[6][2] + aR[6][4]);
+		a_b2s += as_prime * (aR[5][0] + aR[5][6]) - af_prime * (aR[5][2] + aR[5][4]);
+		a_b3s += as_prime * (aR[6][0] + aR[6][6]) - af_prime * (aR[6][2] + aR[6][4]);
+		a_bet3 += -sg * isqrtd * (aR[5][1] + aR[5][5]);
+		a_bet2 += sg * isqrtd * (aR[6][1] + aR[6][5]);
+		a_isqrtd += sg * (-bet3 * (aR[5][1] + aR[5][5]) + bet2 * (aR[6][1] + aR[6][5]));
+		// wv = v2 bet3 - v3 bet2
+		a_v2 += bet3 * a_wv;
+		a_v3 += -bet2 * a_wv;
+		a_bet3 += v2 * a_wv;
+		a_bet2 += -v3 * a_wv;
+		// eigenvalues
+		for (int m = 0; m < 7; m++) a_v1 += a_ev[m];
+		a_cf += -a_ev[0] + a_ev[6];
+		a_vax += -a_ev[1] + a_ev[5];
+		a_cs += -a_ev[2] + a_ev[4];
+	}
+	if (F != nullptr) {
+		F[0] = Fo[0]; F[1] = Fo[1]; F[2] = Fo[2]; F[3] = Fo[3]; F[4] = Fo[4];
+		F[5] = 0.0;
+		F[6] = Fo[5] * g.sqrt_mu0;
+		F[7] = Fo[6] * g.sqrt_mu0;
+	}
+
+	// ---- reverse of the eigensystem's scalars (zero outside the middle branch)
+	double a_vaxsq = vax > 0.0 ? 0.5 * rcp(vax) * a_vax : 0.0;
+	a_afp += bt_star * bet_starsq * a_afpbb;
+	a_asp += bt_star * bet_starsq * a_aspbb;
+	a_bt_star += bet_starsq * (af_prime * a_afpbb + as_prime * a_aspbb);
+	a_bsq += bt_star * (af_prime * a_afpbb + as_prime * a_aspbb);
+	double a_twid_a = alpha_f * isqrtd * a_afp + alpha_s * isqrtd * a_asp;
+	a_af += twid_a * isqrtd * a_afp;
+	a_as += twid_a * isqrtd * a_asp;
+	a_isqrtd += twid_a * (alpha_f * a_afp + alpha_s * a_asp);
+	a_cf += alpha_f * sg * a_qf;
+	a_af += cf * sg * a_qf;
+	a_cs += alpha_s * sg * a_qs;
+	a_as += cs * sg * a_qs;
+	a_twid += twid_a > 0.0 ? 0.5 * rcp(twid_a) * a_twid_a : 0.0;
+	a_sqrtd += -isqrtd * isqrtd * a_isqrtd;
+	a_droe += 0.5 * isqrtd * a_sqrtd;
+	double a_cfsq = 0.0, a_cssq = 0.0;
+	if (acase == 3) {
+		const double a_ra = alpha_f > 0.0 ? 0.5 * rcp(alpha_f) * a_af : 0.0;
+		const double a_rb = alpha_s > 0.0 ? 0.5 * rcp(alpha_s) * a_as : 0.0;
+		a_twid += aid * (a_ra - a_rb);
+		a_cssq += -aid * a_ra;
+		a_cfsq += aid * a_rb;
+		const double a_aid = (twid_asq - cssq) * a_ra + (cfsq - twid_asq) * a_rb;
+		a_cfsq += -aid * aid * a_aid;
+		a_cssq += aid * aid * a_aid;
+	}
+	// vbet = v2 bet2* + v3 bet3*, bet_starsq = bet2*^2 + bet3*^2, bet* = bet iys
+	a_v2 += bet2_star * a_vbet;
+	a_v3 += bet3_star * a_vbet;
+	a_b2s += v2 * a_vbet + 2.0 * bet2_star * a_bsq;
+	a_b3s += v3 * a_vbet + 2.0 * bet3_star * a_bsq;
+	a_bet2 += iys * a_b2s;
+	a_bet3 += iys * a_b3s;
+	const double a_iys = bet2 * a_b2s + bet3 * a_b3s;
+	double a_ystar = -0.5 * iys * iys * iys * a_iys;
+	double a_btsq = 0.0;
+	if (has_bt) {
+		a_b2 += ibt * a_bet2;
+		a_b3 += ibt * a_bet3;
+		const double a_bt = -ibt * ibt * (b2 * a_bet2 + b3 * a_bet3);
+		a_btsq += 0.5 * ibt * a_bt;
+	}
+	double a_bt_starsq = bt_star > 0.0 ? 0.5 * rcp(bt_star) * a_bt_star : 0.0;
+	a_cssq += cs > 0.0 ? 0.5 * rcp(cs) * a_cs : 0.0;
+	a_twid += vaxsq * icfsq * a_cssq;
+	a_vaxsq += twid_asq * icfsq * a_cssq;
+	a_cfsq += -cssq * icfsq * a_cssq;
+	a_cfsq += cf > 0.0 ? 0.5 * rcp(cf) * a_cf : 0.0;
+	const double a_tsum = 0.5 * a_cfsq, a_cf2 = 0.5 * a_cfsq;
+	const double a_q = cf2_cs2 > 0.0 ? 0.5 * rcp(cf2_cs2) * a_cf2 : 0.0;
+	const double a_tdif = 2.0 * tdif * a_q;
+	a_twid += 4.0 * ct2 * a_q + a_tsum - a_tdif;
+	double a_ct2 = 4.0 * twid_asq * a_q + a_tsum + a_tdif;
+	a_vaxsq += a_tsum + a_tdif;
+	a_bt_starsq += di * a_ct2;
+	double a_di = bt_starsq * a_ct2;
+	// twid_asq = max(twid_raw, eps)
+	double a_raw = 0.0, a_floor = 0.0;
+	max_rev(twid_raw, eps, a_twid, a_raw, a_floor);
+	a_hp += gm1 * a_raw;
+	a_vsq += -0.5 * gm1 * a_raw;
+	a_x += -gm2 * a_raw;
+	// hp = h - (vaxsq + btsq di)
+	double a_h = a_hp;
+	a_vaxsq += -a_hp;
+	a_btsq += -di * a_hp;
+	a_di += -btsq * a_hp;
+	// vaxsq = b1^2 di
+	double a_bxi = 2.0 * b1 * di * a_vaxsq;
+	a_di += b1 * b1 * a_vaxsq;
+	// bt_starsq = ystar btsq, ystar = gm1 - gm2 y
+	a_ystar += btsq * a_bt_starsq;
+	a_btsq += ystar * a_bt_starsq;
+	const double a_y = -gm2 * a_ystar;
+	a_b2 += 2.0 * b2 * a_btsq;
+	a_b3 += 2.0 * b3 * a_btsq;
+	a_v1 += 2.0 * v1 * a_vsq;
+	a_v2 += 2.0 * v2 * a_vsq;
+	a_v3 += 2.0 * v3 * a_vsq;
+
+	// ---- reverse of the Roe averages
+	double a_sdl = 0.0, a_sdr = 0.0, a_isd = 0.0;
+	double a_byl = 0.0, a_bzl = 0.0, a_byr = 0.0, a_bzr = 0.0, a_pl = 0.0, a_pr = 0.0, a_pbl = 0.0, a_pbr = 0.0;
+	// h = (hl + hr) isd, hl = (E + p + pb) / sd
+	const double a_hl = isd * a_h, a_hr = isd * a_h;
+	a_isd += (hl + hr) * a_h;
+	AL.E += isdl * a_hl; a_pl += isdl * a_hl; a_pbl += isdl * a_hl;
+	AR.E += isdr * a_hr; a_pr += isdr * a_hr; a_pbr += isdr * a_hr;
+	a_sdl += -isdl * isdl * (L.E + pl + pbl) * a_hl;
+	a_sdr += -isdr * isdr * (R.E + pr + pbr) * a_hr;
+	// y = (rhoL + rhoR) di / 2
+	AL.rho += 0.5 * di * a_y;
+	AR.rho += 0.5 * di * a_y;
+	a_di += 0.5 * (L.rho + R.rho) * a_y;
+	// x = (dby^2 + dbz^2) isd^2 / 2
+	const double a_dby = dby * isd * isd * a_x, a_dbz = dbz * isd * isd * a_x;
+	a_isd += (dby * dby + dbz * dbz) * isd * a_x;
+	a_byl += a_dby; a_byr -= a_dby;
+	a_bzl += a_dbz; a_bzr -= a_dbz;
+	// b2 = (sdr byl + sdl byr) isd, b3 likewise
+	a_sdr += (byl * a_b2 + bzl * a_b3) * isd;
+	a_sdl += (byr * a_b2 + bzr * a_b3) * isd;
+	a_byl += sdr * isd * a_b2;
+	a_byr += sdl * isd * a_b2;
+	a_bzl += sdr * isd * a_b3;
+	a_bzr += sdl * isd * a_b3;
+	a_isd += (sdr * byl + sdl * byr) * a_b2 + (sdr * bzl + sdl * bzr) * a_b3;
+	// v = (sdl vL + sdr vR) isd
+	a_sdl += (L.v0 * a_v1 + L.v1 * a_v2 + L.v2 * a_v3) * isd;
+	a_sdr += (R.v0 * a_v1 + R.v1 * a_v2 + R.v2 * a_v3) * isd;
+	AL.v0 += sdl * isd * a_v1; AL.v1 += sdl * isd * a_v2; AL.v2 += sdl * isd * a_v3;
+	AR.v0 += sdr * isd * a_v1; AR.v1 += sdr * isd * a_v2; AR.v2 += sdr * isd * a_v3;
+	a_isd += (sdl * L.v0 + sdr * R.v0) * a_v1 + (sdl * L.v1 + sdr * R.v1) * a_v2 + (sdl * L.v2 + sdr * R.v2) * a_v3;
+	// di = 1 / droe, droe = sdl sdr, isd = 1 / (sdl + sdr)
+	a_droe += -di * di * a_di;
+	a_sdl += sdr * a_droe;
+	a_sdr += sdl * a_droe;
+	const double a_sum = -isd * isd * a_isd;
+	a_sdl += a_sum;
+	a_sdr += a_sum;
+
+	// ---- reverse of both fluxes and states
+	auto flux7_rev = [&](const Side_Fwd& S, Side_Adj& A, const double p, const double pb, const double by,
+	                     const double bz, const double* aFs, const double* aUs, double& a_p, double& a_pb,
+	                     double& a_by, double& a_bz) {
+		const double vbx = bxi * S.v0 + by * S.v1 + bz * S.v2;
+		A.m0 += aFs[0] + S.v0 * aFs[1] + S.v1 * aFs[2] + S.v2 * aFs[3];
+		A.v0 += S.m0 * aFs[1] + (S.E + p + pb) * aFs[4] - bxi * bxi * aFs[4] + by * aFs[5] + bz * aFs[6];
+		A.v1 += S.m0 * aFs[2] - bxi * by * aFs[4] - bxi * aFs[5];
+		A.v2 += S.m0 * aFs[3] - bxi * bz * aFs[4] - bxi * aFs[6];
+		a_p += aFs[1] + S.v0 * aFs[4];
+		a_pb += S.v0 * aFs[4];
+		A.E += S.v0 * aFs[4];
+		a_bxi += -bxi * aFs[1] - by * aFs[2] - bz * aFs[3] - (vbx + bxi * S.v0) * aFs[4] - S.v1 * aFs[5] - S.v2 * aFs[6];
+		a_by += by * aFs[1] - bxi * aFs[2] - bxi * S.v1 * aFs[4] + S.v0 * aFs[5];
+		a_bz += bz * aFs[1] - bxi * aFs[3] - bxi * S.v2 * aFs[4] + S.v0 * aFs[6];
+		// the state [rho, m, E, by, bz]
+		A.rho += aUs[0];
+		A.m0 += aUs[1]; A.m1 += aUs[2]; A.m2 += aUs[3];
+		A.E += aUs[4];
+		a_by += aUs[5];
+		a_bz += aUs[6];
+	};
+	flux7_rev(L, AL, pl, pbl, byl, bzl, aFl, aUl, a_pl, a_pbl, a_byl, a_bzl);
+	flux7_rev(R, AR, pr, pbr, byr, bzr, aFr, aUr, a_pr, a_pbr, a_byr, a_bzr);
+	// pb = (bxi^2 + by^2 + bz^2) / 2
+	a_bxi += bxi * (a_pbl + a_pbr);
+	a_byl += byl * a_pbl; a_bzl += bzl * a_pbl;
+	a_byr += byr * a_pbr; a_bzr += bzr * a_pbr;
+	// sd = sqrt(rho)
+	AL.rho += 0.5 * isdl * a_sdl;
+	AR.rho += 0.5 * isdr * a_sdr;
+	// p = (E - r m2s / 2 - b2s / 2)(gamma - 1), with r = 1 / rho
+	auto pres_rev = [&](const Side_Fwd& S, Side_Adj& A, const double a_p) {
+		A.E += gm1 * a_p;
+		A.rho += 0.5 * S.m2s * gm1 * S.r * S.r * a_p;
+		const double c = -S.r * gm1 * a_p;
+		A.m0 += c * S.m0; A.m1 += c * S.m1; A.m2 += c * S.m2;
+		const double d = -gm1 * a_p;
+		A.b0 += d * S.b0; A.b1 += d * S.b1; A.b2 += d * S.b2;
+	};
+	pres_rev(L, AL, a_pl);
+	pres_rev(R, AR, a_pr);
+	// bxi = (bL0 + bR0) / (2 sqrt(mu0)), by = b1 / sqrt(mu0), bz = b2 / sqrt(mu0)
+	AL.b0 += 0.5 * ism * a_bxi;
+	AR.b0 += 0.5 * ism * a_bxi;
+	AL.b1 += ism * a_byl; AL.b2 += ism * a_bzl;
+	AR.b1 += ism * a_byr; AR.b2 += ism * a_bzr;
+	side_reverse(L, AL, g, gL);
+	side_reverse(R, AR, g, gR);
+}
+
 template <int SOLVER>
 __host__ __device__ __forceinline__ void face_vjp(const double* UL, const double* UR, const Gas_Adj& g,
                                                   const double* phi, double* gL, double* gR, double* F = nullptr)
 {
 	if (SOLVER == 0) rusanov_vjp(UL, UR, g, phi, gL, gR, F);
 	else if (SOLVER == 2) hll_vjp(UL, UR, g, phi, gL, gR, F);
-	else hlld_vjp(UL, UR, g, phi, gL, gR, F);
+	else if (SOLVER == 3) hlld_vjp(UL, UR, g, phi, gL, gR, F);
+	else roe_vjp(UL, UR, g, phi, gL, gR, F);
 }
 
 }} // namespaces

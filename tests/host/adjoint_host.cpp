@@ -26,7 +26,8 @@ extern "C" void adj_face_vjp(int32_t solver, int64_t n, const double* UL, const 
 		switch (solver) {
 		case 0: pamhd_b200::adjoint::face_vjp<0>(a, b, g, p, x, y, f); break;
 		case 2: pamhd_b200::adjoint::face_vjp<2>(a, b, g, p, x, y, f); break;
-		default: pamhd_b200::adjoint::face_vjp<3>(a, b, g, p, x, y, f); break;
+		case 3: pamhd_b200::adjoint::face_vjp<3>(a, b, g, p, x, y, f); break;
+		default: pamhd_b200::adjoint::face_vjp<4>(a, b, g, p, x, y, f); break;
 		}
 	}
 }

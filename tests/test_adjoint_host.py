@@ -42,7 +42,7 @@ def vjp(L, solver, UL, UR, phi, gamma=5 / 3, mu0=1.0):
     return gL, gR, F
 
 
-@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena"])
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena", "roe_athena"])
 @pytest.mark.parametrize("mu0", [1.0, 4e-7 * np.pi])
 def test_face_vjp_matches_oracle_finite_differences(adj, port, solver, mu0):
     sid = po.SOLVERS[solver]

@@ -60,10 +60,17 @@ def grad_primitive(g, U0):
     return g_rho, g_v
 
 
-@pytest.mark.parametrize("solver", [pg.RUSANOV, pg.HLL, pg.HLLD])
-def test_small_grid_against_gpu_and_oracle_perturbed_runs(port, solver):
+# Roe on a smooth state with no symmetry: on the Orszag-Tang vortex whole lines of faces hold a
+# Roe-averaged transverse field of exactly zero, where the Roe flux is not differentiable (the
+# Alfven waves' direction bet2, bet3 is then arbitrary, mhd/roe_athena.hpp:97-105) and a finite
+# difference straddles the jump; the other solvers are differentiable there up to kinks the
+# adjoint resolves as a central difference does
+@pytest.mark.parametrize("solver,case", [(pg.RUSANOV, "ot"), (pg.HLL, "ot"), (pg.HLLD, "ot"), (pg.ROE, "smooth")])
+def test_small_grid_against_gpu_and_oracle_perturbed_runs(port, solver, case):
     n, steps, every = 32, 24, 5
     U0, cfg, mask = ot_case(n, solver)
+    if case == "smooth":
+        U0 = states.smooth_3d((1, n, n), np.random.default_rng(41), amp=0.1)
     vol = 1 / n ** 2
     ctx = pg.Context(cfg)
     ctx.set_state(U0)
