@@ -362,6 +362,41 @@ int pamhd_gpu_batch_get_state(pamhd_batch* batch, int32_t box, double* const soa
 int pamhd_gpu_batch_steps(pamhd_batch* batch, int32_t nsteps, double t_end);
 
 /*
+nsteps steps of every box in ONE persistent kernel launch (the time loop of
+each box, tests/mhd/solar_wind_box.cpp:466-527, for the whole ensemble):
+a cooperative launch of the SMs' resident capacity hands out the (step,
+work item) pairs in order (a box's tiles, and chunks of the ghost-ghost
+faces whose speeds enter its timestep); an item of step s of a box waits
+until the box's items of step s - 1 are done, so each box advances at its
+own pace with its own lagged CFL dt from its own reduction ring, capped so
+that its time does not pass t_end.  The launch is captured in a CUDA graph
+and replayed (captured again for another nsteps, state parity or step
+phase).  Each wait is bounded (pamhd_gpu_batch_set_wait_limit polls, about
+a second by default): when one runs out, the launch winds down, every box's
+status gets PAMHD_FLAG_TIMEOUT and pamhd_gpu_batch_sync returns
+PAMHD_ERR_TIMEOUT; the state is then mid-step (set it again).  Results
+equal pamhd_gpu_batch_steps bit for bit.  Does not wait for the GPU.
+*/
+int pamhd_gpu_batch_run(pamhd_batch* batch, int32_t nsteps, double t_end);
+
+/* Polls a wait of pamhd_gpu_batch_run makes before it gives up (>= 0; 0: no wait at all). */
+int pamhd_gpu_batch_set_wait_limit(pamhd_batch* batch, int64_t polls);
+
+/*
+The persistent run's launch: blocks (the resident capacity for the current
+tiling), work items per step, and whether the last run was replayed from a
+CUDA graph (1) or launched directly (0).
+*/
+int pamhd_gpu_batch_run_info(pamhd_batch* batch, int32_t* grid, int32_t* items, int32_t* graphed);
+
+/*
+Autotuner of the persistent run: times trial_steps steps of the loaded
+ensemble for each tile shape (32 x 4, 32 x 8) and z planes per work item
+(8, 16, 32, 64), keeps the fastest and restores the state it started from.
+*/
+int pamhd_gpu_batch_tune_run(pamhd_batch* batch, int32_t trial_steps, int32_t* tile_rows, int32_t* planes);
+
+/*
 Autotuner: times trial_steps steps of the loaded ensemble for each
 candidate tile shape (32 x 4 or 32 x 8 cells per block, 32 x 1 when y is
 inactive), number of z planes per work item (8, 16, 32, 64) and resident

@@ -854,6 +854,34 @@ class Batch:
                     "pamhd_gpu_batch_tune")
         return planes.value, grid.value
 
+    def run(self, n: int, t_end: float = 1e300):
+        """n steps of every box in one persistent launch, graph-replayed (pamhd_gpu_batch_run)."""
+        fn = self.L.pamhd_gpu_batch_run
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, _D]
+        self._check(fn(self.h, int(n), float(t_end)), "pamhd_gpu_batch_run")
+
+    def set_wait_limit(self, polls: int):
+        """Polls a wait of the persistent run makes before it gives up (pamhd_gpu_batch_set_wait_limit)."""
+        fn = self.L.pamhd_gpu_batch_set_wait_limit
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        self._check(fn(self.h, int(polls)), "pamhd_gpu_batch_set_wait_limit")
+
+    def run_info(self):
+        """(blocks, work items per step, graph-replayed) of the persistent run (pamhd_gpu_batch_run_info)."""
+        fn = self.L.pamhd_gpu_batch_run_info
+        fn.argtypes = [ctypes.c_void_p, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        g, i, r = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        self._check(fn(self.h, ctypes.byref(g), ctypes.byref(i), ctypes.byref(r)), "pamhd_gpu_batch_run_info")
+        return g.value, i.value, bool(r.value)
+
+    def tune_run(self, trial_steps: int = 3):
+        """Autotuner of the persistent run (pamhd_gpu_batch_tune_run): (tile rows, z planes per item)."""
+        fn = self.L.pamhd_gpu_batch_tune_run
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, _P(ctypes.c_int32), _P(ctypes.c_int32)]
+        t, p = ctypes.c_int32(0), ctypes.c_int32(0)
+        self._check(fn(self.h, trial_steps, ctypes.byref(t), ctypes.byref(p)), "pamhd_gpu_batch_tune_run")
+        return t.value, p.value
+
     def sync(self):
         self._check(self.L.pamhd_gpu_batch_sync(self.h), "pamhd_gpu_batch_sync")
 

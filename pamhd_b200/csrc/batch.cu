@@ -53,7 +53,8 @@ struct pamhd_batch {
 	std::vector<Step_Params> params[2];
 	Step_Params* d_params[2] = {nullptr, nullptr};
 	int4* d_items = nullptr;
-	int nitems = 0;
+	int nitems = 0;                  // work items of the boxes' tiles (the per-step kernel's table)
+	int nitems_run = 0;              // the same plus the boundary-face chunks (the persistent run's table)
 	int grid = 0;
 	int planes_per_item = 32;
 	int ty = 1;                      // tile rows of the work items (autotuned when y is active)
@@ -64,6 +65,16 @@ struct pamhd_batch {
 	int cur = 0;
 	bool loaded = false;
 	cudaGraphExec_t graph = nullptr;
+	// the persistent run (pamhd_gpu_batch_run): scheduler state, per-box items per step and items
+	// done, poll limit, resident grid, its graph
+	Run_Sync* sync = nullptr;
+	int* d_box_items = nullptr;
+	unsigned int* d_done = nullptr;
+	long long wait_limit = 10000000;
+	int run_grid = 0;
+	cudaGraphExec_t run_graph = nullptr;
+	long long run_key = -1;          // nsteps, state parity and step phase the run graph was captured for
+	bool run_graphed = false;        // whether the last run was replayed from a graph
 	Axis_Map map{{0, 1, 2}};        // the boxes' axes as the kernels see them
 	// time-stamped inflow of VALUE sides, per box and side (index 6 box + 2 dimension + side)
 	std::vector<Inflow_Table> inflow;
@@ -168,6 +179,31 @@ int build_work(pamhd_batch& b, const int planes)
 		}
 	}
 	b.nitems = int(items.size());
+	// the persistent run also solves the ghost-ghost faces of non-periodic sides (for their speeds),
+	// in chunks: (box, combination, chunk, 1), the combinations numbered as boundary_combos does
+	for (const int i: order) {
+		const Step_Params& P = b.params[0][i];
+		int combo = 0;
+		for (int d = 0; d < 3; d++) {
+			if (not P.active[d] or P.periodic[d]) continue;
+			for (int side = 0; side < 2; side++) {
+				if ((side ? P.bc_hi[d] : P.bc_lo[d]) == PAMHD_BC_EXTERNAL) continue;
+				for (int e = 0; e < 3; e++) {
+					if (e == d or not P.active[e]) continue;
+					const int f = 3 - d - e;
+					const int ne = (P.periodic[e] or P.bc_hi[e] == PAMHD_BC_EXTERNAL) ? P.L.n[e] : P.L.n[e] - 1;
+					const long long count = (long long)ne * P.L.n[f];
+					const int chunks = int((count + BOUNDARY_CHUNK - 1) / BOUNDARY_CHUNK);
+					for (int k = 0; k < chunks; k++) items.push_back(make_int4(i, combo, k, 1));
+					combo++;
+				}
+			}
+		}
+	}
+	b.nitems_run = int(items.size());
+	std::vector<int> per_box(b.nboxes, 0);
+	for (const int4& w: items) per_box[w.x]++;
+	PAMHD_TRY(check(cudaMemcpy(b.d_box_items, per_box.data(), b.nboxes * sizeof(int), cudaMemcpyHostToDevice)));
 	cudaFree(b.d_items);
 	b.d_items = nullptr;
 	PAMHD_TRY(check(cudaMalloc(&b.d_items, items.size() * sizeof(int4))));
@@ -179,6 +215,11 @@ int build_work(pamhd_batch& b, const int planes)
 	if (b.graph != nullptr) {
 		cudaGraphExecDestroy(b.graph);
 		b.graph = nullptr;
+	}
+	if (b.run_graph != nullptr) {
+		cudaGraphExecDestroy(b.run_graph);
+		b.run_graph = nullptr;
+		b.run_key = -1;
 	}
 	return PAMHD_OK;
 }
@@ -265,6 +306,69 @@ int run_steps(pamhd_batch& b, int left)
 	return PAMHD_OK;
 }
 
+// the resident grid of the persistent run for the current tile shape (one wave: a cooperative launch)
+int set_run_grid(pamhd_batch& b)
+{
+	int per_sm = 0, sms = 0;
+	PAMHD_TRY(batch_run_blocks_per_sm(b.solver, b.ty, &per_sm));
+	PAMHD_TRY(check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b.device)));
+	if (per_sm < 1) return PAMHD_ERR_CUDA;
+	b.run_grid = std::max(1, std::min(b.nitems_run, sms * per_sm));
+	return PAMHD_OK;
+}
+
+int issue_run(pamhd_batch& b, const int nsteps)
+{
+	if ((long long)nsteps * b.nitems_run >= (1ll << 31)) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaMemsetAsync(b.sync, 0, sizeof(Run_Sync), b.stream)));
+	PAMHD_TRY(check(cudaMemsetAsync(b.d_done, 0, b.nboxes * sizeof(unsigned int), b.stream)));
+	return launch_batch_run(b.d_params[b.cur], b.d_params[b.cur ^ 1], b.d_items, b.nitems_run, b.d_box_items,
+	                        b.d_done, b.nboxes, b.steps, nsteps, b.sync, b.wait_limit, b.run_grid, b.solver, b.ty,
+	                        b.stream);
+}
+
+/*
+nsteps steps in one persistent launch, replayed from a CUDA graph of that one launch (captured
+again when nsteps, the state parity or the step phase differ from the captured ones); launched
+directly when the capture is refused.
+*/
+int run_persistent(pamhd_batch& b, const int nsteps)
+{
+	if (nsteps <= 0) return PAMHD_OK;
+	PAMHD_TRY(set_run_grid(b));
+	const long long key = (long long)nsteps * 6 + b.cur * 3 + b.steps % 3;
+	if (b.run_graph == nullptr or b.run_key != key) {
+		if (b.run_graph != nullptr) {
+			cudaGraphExecDestroy(b.run_graph);
+			b.run_graph = nullptr;
+		}
+		b.run_key = -1;
+		cudaGraph_t g = nullptr;
+		bool ok = cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+		const int rc = ok ? issue_run(b, nsteps) : PAMHD_ERR_CUDA;
+		if (ok) ok = cudaStreamEndCapture(b.stream, &g) == cudaSuccess and rc == PAMHD_OK;
+		if (ok) ok = cudaGraphInstantiate(&b.run_graph, g, 0) == cudaSuccess;
+		if (g != nullptr) cudaGraphDestroy(g);
+		cudaGetLastError();  // a refused capture leaves no error behind
+		if (ok) {
+			b.run_key = key;
+		} else if (b.run_graph != nullptr) {
+			cudaGraphExecDestroy(b.run_graph);
+			b.run_graph = nullptr;
+		}
+	}
+	if (b.run_graph != nullptr) {
+		PAMHD_TRY(check(cudaGraphLaunch(b.run_graph, b.stream)));
+		b.run_graphed = true;
+	} else {
+		PAMHD_TRY(issue_run(b, nsteps));
+		b.run_graphed = false;
+	}
+	b.steps += nsteps;
+	b.cur ^= nsteps & 1;
+	return PAMHD_OK;
+}
+
 int box_ok(const pamhd_batch* b, const int box)
 {
 	return (b != nullptr and box >= 0 and box < b->nboxes) ? PAMHD_OK : PAMHD_ERR_ARGUMENT;
@@ -323,7 +427,10 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 		or cudaMalloc(&b->dt_hist, size_t(b->hist_len) * nboxes * sizeof(double)) != cudaSuccess
 		or cudaMalloc(&b->d_params[0], nboxes * sizeof(Step_Params)) != cudaSuccess
 		or cudaMalloc(&b->d_params[1], nboxes * sizeof(Step_Params)) != cudaSuccess
-		or cudaMalloc(&b->staging, largest_cells * sizeof(double)) != cudaSuccess) {
+		or cudaMalloc(&b->staging, largest_cells * sizeof(double)) != cudaSuccess
+		or cudaMalloc(&b->sync, sizeof(Run_Sync)) != cudaSuccess
+		or cudaMalloc(&b->d_box_items, nboxes * sizeof(int)) != cudaSuccess
+		or cudaMalloc(&b->d_done, nboxes * sizeof(unsigned int)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
 	if (cudaMemset(b->state[0], 0, bytes) != cudaSuccess or cudaMemset(b->state[1], 0, bytes) != cudaSuccess
@@ -333,6 +440,7 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 	b->ty = b->yact ? step_tile_rows() : 1;
 	for (const int ty: tile_choices(*b)) {
 		if (prepare_batch_kernels(b->solver, ty) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+		if (prepare_batch_run_kernels(b->solver, ty) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
 	}
 	int per_sm = 0;
 	if (batch_blocks_per_sm(b->solver, b->ty, &per_sm) != PAMHD_OK or per_sm < 1) return fail(PAMHD_ERR_CUDA);
@@ -351,6 +459,10 @@ int pamhd_gpu_batch_destroy(pamhd_batch* b)
 	cudaSetDevice(b->device);
 	if (b->stream != nullptr) cudaStreamSynchronize(b->stream);
 	if (b->graph != nullptr) cudaGraphExecDestroy(b->graph);
+	if (b->run_graph != nullptr) cudaGraphExecDestroy(b->run_graph);
+	cudaFree(b->sync);
+	cudaFree(b->d_box_items);
+	cudaFree(b->d_done);
 	cudaFree(b->state[0]);
 	cudaFree(b->state[1]);
 	cudaFree(b->red);
@@ -488,6 +600,41 @@ int pamhd_gpu_batch_steps(pamhd_batch* b, const int32_t nsteps, const double t_e
 	return run_steps(*b, nsteps);
 }
 
+int pamhd_gpu_batch_run(pamhd_batch* b, const int32_t nsteps, const double t_end)
+{
+	if (b == nullptr or nsteps < 0) return PAMHD_ERR_ARGUMENT;
+	if (not b->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(b->device)));
+	PAMHD_TRY(set_control(*b, -1.0, t_end));
+	return run_persistent(*b, nsteps);
+}
+
+int pamhd_gpu_batch_set_wait_limit(pamhd_batch* b, const int64_t polls)
+{
+	if (b == nullptr or polls < 0) return PAMHD_ERR_ARGUMENT;
+	b->wait_limit = polls;
+	// the limit is a launch argument: a graph captured with the old one is captured again
+	if (b->run_graph != nullptr) {
+		PAMHD_TRY(check(cudaSetDevice(b->device)));
+		PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+		cudaGraphExecDestroy(b->run_graph);
+		b->run_graph = nullptr;
+		b->run_key = -1;
+	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_batch_run_info(pamhd_batch* b, int32_t* grid, int32_t* items, int32_t* graphed)
+{
+	if (b == nullptr) return PAMHD_ERR_ARGUMENT;
+	PAMHD_TRY(check(cudaSetDevice(b->device)));
+	PAMHD_TRY(set_run_grid(*b));
+	if (grid != nullptr) *grid = b->run_grid;
+	if (items != nullptr) *items = b->nitems_run;
+	if (graphed != nullptr) *graphed = b->run_graphed ? 1 : 0;
+	return PAMHD_OK;
+}
+
 int pamhd_gpu_batch_tune(pamhd_batch* b, const int32_t trial_steps, int32_t* planes_chosen, int32_t* grid_chosen)
 {
 	if (b == nullptr or trial_steps < 1) return PAMHD_ERR_ARGUMENT;
@@ -570,6 +717,64 @@ int pamhd_gpu_batch_set_tiling(pamhd_batch* b, const int32_t tile_rows, const in
 	return PAMHD_OK;
 }
 
+int pamhd_gpu_batch_tune_run(pamhd_batch* b, const int32_t trial_steps, int32_t* tile_rows_chosen,
+                             int32_t* planes_chosen)
+{
+	if (b == nullptr or trial_steps < 1) return PAMHD_ERR_ARGUMENT;
+	if (not b->loaded) return PAMHD_ERR_STATE;
+	PAMHD_TRY(check(cudaSetDevice(b->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+	// keep the state the trials start from
+	double* backup = nullptr;
+	PAMHD_TRY(check(cudaMalloc(&backup, size_t(b->total) * sizeof(double))));
+	int rc = check(cudaMemcpyAsync(backup, b->state[b->cur], size_t(b->total) * sizeof(double),
+	                               cudaMemcpyDeviceToDevice, b->stream));
+	float best = 3.0e38f;
+	int best_planes = b->planes_per_item, best_ty = b->ty;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	if (rc == PAMHD_OK) rc = set_control(*b, -1.0, 1.0e300);
+	for (const int ty: tile_choices(*b))
+	for (const int planes: {8, 16, 32, 64}) {
+		if (rc != PAMHD_OK) break;
+		b->ty = ty;
+		rc = build_work(*b, planes);
+		if (rc == PAMHD_OK) rc = set_run_grid(*b);
+		if (rc == PAMHD_OK) {
+			rc = check(cudaMemcpyAsync(b->state[0], backup, size_t(b->total) * sizeof(double),
+			                           cudaMemcpyDeviceToDevice, b->stream));
+		}
+		b->cur = 0;
+		if (rc == PAMHD_OK) rc = reset_run_state(*b);
+		if (rc == PAMHD_OK) rc = check(cudaEventRecord(e0, b->stream));
+		if (rc == PAMHD_OK) rc = issue_run(*b, trial_steps + 1);  // the priming step and the trial steps
+		if (rc == PAMHD_OK) rc = check(cudaEventRecord(e1, b->stream));
+		if (rc == PAMHD_OK) rc = check(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		if (rc == PAMHD_OK) rc = check(cudaEventElapsedTime(&ms, e0, e1));
+		if (rc == PAMHD_OK and ms < best) {
+			best = ms;
+			best_planes = planes;
+			best_ty = ty;
+		}
+	}
+	b->ty = best_ty;
+	if (rc == PAMHD_OK) rc = build_work(*b, best_planes);
+	if (rc == PAMHD_OK) {
+		rc = check(cudaMemcpyAsync(b->state[0], backup, size_t(b->total) * sizeof(double), cudaMemcpyDeviceToDevice,
+		                           b->stream));
+	}
+	b->cur = 0;
+	if (rc == PAMHD_OK) rc = reset_run_state(*b);
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaFree(backup);
+	if (tile_rows_chosen != nullptr) *tile_rows_chosen = best_ty;
+	if (planes_chosen != nullptr) *planes_chosen = best_planes;
+	return rc;
+}
+
 int pamhd_gpu_batch_tiling(pamhd_batch* b, int32_t* tile_rows, int32_t* planes, int32_t* grid)
 {
 	if (b == nullptr) return PAMHD_ERR_ARGUMENT;
@@ -587,6 +792,9 @@ int pamhd_gpu_batch_sync(pamhd_batch* b)
 	PAMHD_TRY(check(cudaMemcpyAsync(s.data(), b->status, s.size() * sizeof(Status), cudaMemcpyDeviceToHost,
 	                                b->stream)));
 	PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
+	for (const auto& x: s) {
+		if (x.flags & PAMHD_FLAG_TIMEOUT) return PAMHD_ERR_TIMEOUT;
+	}
 	for (const auto& x: s) {
 		if (x.flags != 0) return PAMHD_ERR_PHYSICS;
 	}

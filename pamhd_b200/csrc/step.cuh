@@ -74,6 +74,16 @@ struct Inflow_Table {
 	int count;
 };
 
+/*
+Scheduler state of the persistent batched run: the next (step, work item)
+to hand out, and an error word set by a block whose bounded wait ran out.
+*/
+struct Run_Sync {
+	unsigned int next;
+	unsigned int error;
+	unsigned int pad[2];
+};
+
 struct Step_Params {
 	const double* __restrict__ in;
 	double* __restrict__ out;
@@ -119,6 +129,13 @@ int launch_batch_step(const Step_Params* boxes, const int4* items, int nitems, i
                       int tile_rows, cudaStream_t stream);
 int launch_batch_boundary_speeds(const Step_Params* boxes, int nboxes, int largest, int phase, int solver,
                                  cudaStream_t stream);
+// the persistent batched run: nsteps steps of every box in one cooperative launch (see batch_run_kernel)
+int prepare_batch_run_kernels(int solver, int tile_rows);
+int batch_run_blocks_per_sm(int solver, int tile_rows, int* blocks);
+int launch_batch_run(const Step_Params* boxes_even, const Step_Params* boxes_odd, const int4* items, int nitems,
+                     const int* box_items, unsigned int* done, int nboxes, long long step0, int nsteps,
+                     Run_Sync* sync, long long wait_limit, int grid, int solver, int tile_rows, cudaStream_t stream);
+constexpr int BOUNDARY_CHUNK = 4096;  // ghost-ghost faces per boundary work item of the persistent run
 
 } // namespace pamhd_b200
 

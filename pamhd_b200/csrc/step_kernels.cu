@@ -82,13 +82,14 @@ face speed was <= 0; replaced by the cap when cap <= that minimum
 __device__ __forceinline__ double step_dt(const Step_Params& P)
 {
 	if (P.forced_dt >= 0.0) return P.forced_dt;
+	// read at L2 (ld.global.cg): a persistent launch reads what other blocks wrote a step before
 	const Speed_Max& r = P.red[P.phase];
-	bool zero = r.zero != 0;
+	bool zero = __ldcg(&r.zero) != 0;
 	double smallest = 1.7976931348623157e308;
 	#pragma unroll
 	for (int d = 0; d < 3; d++) {
 		if (not P.active[d]) continue;
-		const double s = __longlong_as_double((long long)r.smax[d]);
+		const double s = __longlong_as_double((long long)__ldcg(&r.smax[d]));
 		if (not (s > 0.0)) {
 			zero = true;
 		} else {
@@ -96,7 +97,7 @@ __device__ __forceinline__ double step_dt(const Step_Params& P)
 		}
 	}
 	if (zero) smallest = 0.0;
-	const double t = P.clock[P.phase].t;
+	const double t = __ldcg(&P.clock[P.phase].t);
 	const double cap = P.control->max_dt >= 0.0 ? P.control->max_dt : P.control->t_end - t;
 	return (cap <= smallest) ? cap : smallest;
 }
@@ -108,7 +109,9 @@ __device__ __forceinline__ double begin_step(const Step_Params& P, double* s_dt,
 		const double dt = step_dt(P);
 		*s_dt = dt;
 		if (first_block) {
-			const Clock c = P.clock[P.phase];
+			Clock c;
+			c.t = __ldcg(&P.clock[P.phase].t);
+			c.steps = __ldcg(&P.clock[P.phase].steps);
 			Clock& next = P.clock[(P.phase + 1) % 3];
 			next.t = c.t + dt;
 			next.dt = dt;
@@ -234,7 +237,7 @@ __device__ void write_cell(const Step_Params& P, const int i, const int j, const
 				store_cell(P.out, P.L, t[0], t[1], t[2], C);
 			} else if (P.bc_lo[d] == PAMHD_BC_VALUE and P.inflow != nullptr and P.inflow[2 * d].states != nullptr) {
 				t[d] = -1;
-				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d], P.clock[P.phase].t + dt));
+				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d], __ldcg(&P.clock[P.phase].t) + dt));
 			}
 		}
 		if (c[d] == n - 1) {
@@ -249,21 +252,26 @@ __device__ void write_cell(const Step_Params& P, const int i, const int j, const
 				store_cell(P.out, P.L, t[0], t[1], t[2], C);
 			} else if (P.bc_hi[d] == PAMHD_BC_VALUE and P.inflow != nullptr and P.inflow[2 * d + 1].states != nullptr) {
 				t[d] = n;
-				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d + 1], P.clock[P.phase].t + dt));
+				store_cell(P.out, P.L, t[0], t[1], t[2], inflow_at(P.inflow[2 * d + 1], __ldcg(&P.clock[P.phase].t) + dt));
 			}
 		}
 	}
 }
 
-// read a cell from HBM, derive its per-cell quantities into a record slot
-template <bool CX, bool CY, bool CZ>
+/*
+Read a cell from HBM, derive its per-cell quantities into a record slot.
+CO: loads at L2 (ld.global.cg) instead of through the read-only cache, for a
+persistent launch whose later steps read what other blocks wrote (the
+non-coherent L1 could hold a line of the same buffer from two steps before).
+*/
+template <bool CX, bool CY, bool CZ, bool CO>
 __device__ __forceinline__ void load_record(const Step_Params& P, double* rec, uint32_t* bad, const int cells,
                                             const int ri, const int i, const int j, const int k)
 {
 	const long long off = P.L.offset(i, j, k);
 	double U[8];
 	#pragma unroll
-	for (int v = 0; v < 8; v++) U[v] = __ldg(P.in + v * P.L.var + off);
+	for (int v = 0; v < 8; v++) U[v] = CO ? __ldcg(P.in + v * P.L.var + off) : __ldg(P.in + v * P.L.var + off);
 	const Derived d = derive<CX, CY, CZ, true>(U[0], U[1], U[2], U[3], U[4], U[5], U[6], U[7], P.gas);
 	#pragma unroll
 	for (int v = 0; v < 8; v++) rec[v * cells + ri] = U[v];
@@ -386,7 +394,7 @@ registers, which completes the cell below: its new state is written; (c)
 each own cell's state plus its x and y flux differences, and the flux of
 its -z face, held in registers until the +z face of the next plane.
 */
-template <int SOLVER, int TY>
+template <int SOLVER, int TY, bool CO = false>
 __device__ __forceinline__ void tile_step(const Step_Params& P, double* const smem, const double dt,
                                           const int bx, const int by, const int bz,
                                           double& s0, double& s1, double& s2, bool& zero)
@@ -436,7 +444,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 		const bool inner = k >= kb and k < ke;
 
 		// (a) stage the plane: own cells, and the halo for planes with x / y faces
-		if (stage) load_record<true, YACT, true>(P, rec, bad, T::CELLS, ri, gx, gy, k);
+		if (stage) load_record<true, YACT, true, CO>(P, rec, bad, T::CELLS, ri, gx, gy, k);
 		// halo, spread over warps: the rows below / above the tile on warps 0 and 1, the columns
 		// left / right of it on warp 2 (warp 0 when y is inactive)
 		if (inner) {
@@ -445,7 +453,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 				const int hy = top ? gy0 + TY : gy0 - 1;
 				if (gx0 + lane < nx and hy <= ny) {
 					const int hri = (top ? TY + 1 : 0) * T::W + lane + 1;
-					load_record<false, true, false>(P, rec, bad, T::CELLS, hri, gx0 + lane, hy, k);
+					load_record<false, true, false, CO>(P, rec, bad, T::CELLS, hri, gx0 + lane, hy, k);
 				}
 			} else if (warp == XHALO_WARP and lane < 2 * TY) {
 				const int row = lane % TY;
@@ -453,7 +461,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 				const int hx = right ? gx0 + TX : gx0 - 1;
 				if (gy0 + row < ny and hx <= nx) {
 					const int hri = (row + T::JO) * T::W + (right ? TX + 1 : 0);
-					load_record<true, false, false>(P, rec, bad, T::CELLS, hri, hx, gy0 + row, k);
+					load_record<true, false, false, CO>(P, rec, bad, T::CELLS, hri, hx, gy0 + row, k);
 				}
 			}
 		}
@@ -584,17 +592,9 @@ __global__ void __launch_bounds__(TX * TY, MINB) batch_step_kernel(const Step_Pa
 	}
 }
 
-/*
-Speeds of the faces between two boundary ghosts of a non-periodic side
-(cells of class 0 on both sides).  The reference solves those faces too
-(mhd/solve.hpp:254-311 visits every cell of class >= 0) and their speeds
-enter the timestep (:1965-2005); their fluxes change nothing.
-blockIdx.y enumerates (ghost dimension d, side, tangential axis e).
-*/
-template <int SOLVER>
-__device__ __forceinline__ void boundary_speeds(const Step_Params& P)
+// the (ghost dimension d, side, tangential axis e) combinations with ghost-ghost faces
+__device__ __forceinline__ int boundary_combos(const Step_Params& P, int combos[12][3])
 {
-	int combos[12][3];
 	int nc = 0;
 	for (int d = 0; d < 3; d++) {
 		if (not P.active[d] or P.periodic[d]) continue;
@@ -608,54 +608,83 @@ __device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 			}
 		}
 	}
+	return nc;
+}
+
+// faces of one combination: along a slab cut at the high side, the face into the ghost plane is
+// this slab's (the one into the low ghost plane is the lower neighbour's)
+__device__ __forceinline__ long long boundary_count(const Step_Params& P, const int d, const int e)
+{
+	const int f = 3 - d - e;
+	const int ne = (P.periodic[e] or P.bc_hi[e] == PAMHD_BC_EXTERNAL) ? P.L.n[e] : P.L.n[e] - 1;
+	return (long long)ne * P.L.n[f];
+}
+
+// face t of combination (d, side, e): solved for its speed only (CO: loads at L2, see load_record)
+template <int SOLVER, bool CO>
+__device__ __forceinline__ void boundary_face(const Step_Params& P, const int d, const int side, const int e,
+                                              const long long t, double smax[3], bool& zero)
+{
+	const int f = 3 - d - e;
+	const int ne = (P.periodic[e] or P.bc_hi[e] == PAMHD_BC_EXTERNAL) ? P.L.n[e] : P.L.n[e] - 1;
+	int a[3], b[3];
+	a[d] = b[d] = side ? P.L.n[d] : -1;
+	a[e] = int(t % ne);
+	b[e] = (a[e] + 1 == P.L.n[e] and P.periodic[e]) ? 0 : a[e] + 1;
+	a[f] = b[f] = int(t / ne);
+	double UA[8], UB[8];
+	const long long oa = P.L.offset(a[0], a[1], a[2]), ob = P.L.offset(b[0], b[1], b[2]);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) {
+		UA[v] = CO ? __ldcg(P.in + v * P.L.var + oa) : P.in[v * P.L.var + oa];
+		UB[v] = CO ? __ldcg(P.in + v * P.L.var + ob) : P.in[v * P.L.var + ob];
+	}
+	const Derived da = derive<true, true, true>(UA[0], UA[1], UA[2], UA[3], UA[4], UA[5], UA[6], UA[7], P.gas);
+	const Derived db = derive<true, true, true>(UB[0], UB[1], UB[2], UB[3], UB[4], UB[5], UB[6], UB[7], P.gas);
+	Side L, R;
+	auto fill = [e](Side& s, const double U[8], const Derived& dd) {
+		s.rho = U[0];
+		s.E = U[4];
+		double m[3] = {U[1], U[2], U[3]}, B[3] = {U[5], U[6], U[7]};
+		const int i0 = e, i1 = (e + 1) % 3, i2 = (e + 2) % 3;
+		s.m0 = m[i0]; s.m1 = m[i1]; s.m2 = m[i2];
+		s.b0 = B[i0]; s.b1 = B[i1]; s.b2 = B[i2];
+		s.rinv = dd.rinv;
+		s.v0 = s.m0 * s.rinv; s.v1 = s.m1 * s.rinv; s.v2 = s.m2 * s.rinv;
+		s.p = dd.p;
+		s.cf = dd.cf[e];
+		s.bad = dd.bad;
+	};
+	fill(L, UA, da);
+	fill(R, UB, db);
+	double F[8];
+	uint32_t flag = 0;
+	const double sp = solve_face<SOLVER>(L, R, P.gas, F, flag);
+	if (flag != 0) record_failure(P, flag, a[0], a[1], a[2], e + 1);
+	smax[e] = fmax(smax[e], sp);
+	zero = zero or not (sp > 0.0);
+}
+
+/*
+Speeds of the faces between two boundary ghosts of a non-periodic side
+(cells of class 0 on both sides).  The reference solves those faces too
+(mhd/solve.hpp:254-311 visits every cell of class >= 0) and their speeds
+enter the timestep (:1965-2005); their fluxes change nothing.
+blockIdx.y enumerates (ghost dimension d, side, tangential axis e).
+*/
+template <int SOLVER>
+__device__ __forceinline__ void boundary_speeds(const Step_Params& P)
+{
+	int combos[12][3];
+	const int nc = boundary_combos(P, combos);
 	double smax[3] = {0.0, 0.0, 0.0};
 	bool zero = false;
 	if ((int)blockIdx.y < nc) {
 		const int d = combos[blockIdx.y][0], side = combos[blockIdx.y][1], e = combos[blockIdx.y][2];
-		const int f = 3 - d - e;
-		// along a slab cut at the high side, the face into the ghost plane is this slab's
-		// (the one into the low ghost plane is the lower neighbour's)
-		const int ne = (P.periodic[e] or P.bc_hi[e] == PAMHD_BC_EXTERNAL) ? P.L.n[e] : P.L.n[e] - 1;
-		const int nf = P.L.n[f];
-		const long long count = (long long)ne * nf;
+		const long long count = boundary_count(P, d, e);
 		for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count;
 		     t += (long long)gridDim.x * blockDim.x) {
-			int a[3], b[3];
-			a[d] = b[d] = side ? P.L.n[d] : -1;
-			a[e] = int(t % ne);
-			b[e] = (a[e] + 1 == P.L.n[e] and P.periodic[e]) ? 0 : a[e] + 1;
-			a[f] = b[f] = int(t / ne);
-			double UA[8], UB[8];
-			const long long oa = P.L.offset(a[0], a[1], a[2]), ob = P.L.offset(b[0], b[1], b[2]);
-			#pragma unroll
-			for (int v = 0; v < 8; v++) {
-				UA[v] = P.in[v * P.L.var + oa];
-				UB[v] = P.in[v * P.L.var + ob];
-			}
-			const Derived da = derive<true, true, true>(UA[0], UA[1], UA[2], UA[3], UA[4], UA[5], UA[6], UA[7], P.gas);
-			const Derived db = derive<true, true, true>(UB[0], UB[1], UB[2], UB[3], UB[4], UB[5], UB[6], UB[7], P.gas);
-			Side L, R;
-			auto fill = [e](Side& s, const double U[8], const Derived& dd) {
-				s.rho = U[0];
-				s.E = U[4];
-				double m[3] = {U[1], U[2], U[3]}, B[3] = {U[5], U[6], U[7]};
-				const int i0 = e, i1 = (e + 1) % 3, i2 = (e + 2) % 3;
-				s.m0 = m[i0]; s.m1 = m[i1]; s.m2 = m[i2];
-				s.b0 = B[i0]; s.b1 = B[i1]; s.b2 = B[i2];
-				s.rinv = dd.rinv;
-				s.v0 = s.m0 * s.rinv; s.v1 = s.m1 * s.rinv; s.v2 = s.m2 * s.rinv;
-				s.p = dd.p;
-				s.cf = dd.cf[e];
-				s.bad = dd.bad;
-			};
-			fill(L, UA, da);
-			fill(R, UB, db);
-			double F[8];
-			uint32_t flag = 0;
-			const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
-			if (flag != 0) record_failure(P, flag, a[0], a[1], a[2], e + 1);
-			smax[e] = fmax(smax[e], s);
-			zero = zero or not (s > 0.0);
+			boundary_face<SOLVER, false>(P, d, side, e, t, smax, zero);
 		}
 	}
 	flush_speeds(P, smax, zero);
@@ -747,6 +776,118 @@ __global__ void fill_ghosts_kernel(const Step_Params P, double* state, const Gho
 			}
 			store_cell(state, P.L, c[0], c[1], c[2], U);
 		}
+	}
+}
+
+// ------------------------------------------------------------------ the persistent batched run
+
+// marks every box's status with PAMHD_FLAG_TIMEOUT, once per launch
+__device__ void run_timeout(Run_Sync* sync, const Step_Params* boxes, const int nboxes)
+{
+	if (atomicExch(&sync->error, 1u) == 0u) {
+		for (int b = 0; b < nboxes; b++) atomicOr(&boxes[b].status->flags, (unsigned int)PAMHD_FLAG_TIMEOUT);
+	}
+}
+
+/*
+The batched ensemble advanced nsteps steps in one launch.  The grid is the
+resident capacity of the SMs (a cooperative launch, so that every block
+runs at once).  The work is the sequence of (step, work item) pairs, the
+items of a step being the boxes' tiles as in batch_step_kernel, largest
+boxes first, then, for boxes with non-periodic sides, chunks of their
+ghost-ghost faces, whose speeds enter the timestep.  Blocks take the pairs
+one at a time from a shared counter.  An item of step s of box b first
+waits until all items of step s - 1 of box b are done (done[b] counts the
+box's finished items): the only dependency of a box's step, since each box
+has its own state, reduction ring and clock.  Boxes therefore advance at
+their own pace, without a grid-wide barrier, and a block that finishes
+early takes the next item, of this step or the next.  The pairs are handed
+out in order and all blocks are resident, so the earliest unfinished item
+has its dependency met: the run always progresses.  A wait gives up after
+wait_limit polls: it sets the error word and PAMHD_FLAG_TIMEOUT on every
+box, and every block stops at its next item.  boxes_even / boxes_odd are
+the boxes' parameters of the two state parities, the first used by step
+step0.  Loads that read what another block wrote before go through L2 (CO).
+*/
+template <int SOLVER, int TY, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB) batch_run_kernel(
+	const Step_Params* __restrict__ boxes_even, const Step_Params* __restrict__ boxes_odd,
+	const int4* __restrict__ items, const int nitems, const int* __restrict__ box_items, unsigned int* done,
+	const int nboxes, const long long step0, const int nsteps, Run_Sync* sync, const long long wait_limit)
+{
+	extern __shared__ __align__(16) double smem[];
+	__shared__ Step_Params sp;
+	__shared__ double s_dt;
+	__shared__ unsigned int s_q;
+	__shared__ int s_go;
+	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+	const int nthreads = blockDim.x * blockDim.y;
+	const unsigned int total = (unsigned int)nsteps * (unsigned int)nitems;
+	for (;;) {
+		__syncthreads();  // the previous item is done with sp and the shared words
+		if (tid == 0) {
+			volatile unsigned int* verr = &sync->error;
+			s_q = *verr != 0u ? total : atomicAdd(&sync->next, 1u);
+		}
+		__syncthreads();
+		const unsigned int q = s_q;
+		if (q >= total) return;
+		const int s = int(q / (unsigned int)nitems);
+		const int4 w = items[q % (unsigned int)nitems];
+		const Step_Params* boxes = (s & 1) ? boxes_odd : boxes_even;
+		if (tid == 0) {
+			// the box's previous step: all its items done
+			const unsigned int need = (unsigned int)s * (unsigned int)box_items[w.x];
+			volatile unsigned int* vdone = done + w.x;
+			volatile unsigned int* verr = &sync->error;
+			long long polls = 0;
+			int go = 1;
+			while (*vdone < need) {
+				if (*verr != 0u) {
+					go = 0;
+					break;
+				}
+				if (polls >= wait_limit) {
+					run_timeout(sync, boxes, nboxes);
+					go = 0;
+					break;
+				}
+				polls++;
+				__nanosleep(100);
+			}
+			__threadfence();
+			s_go = go;
+			sp = boxes[w.x];
+			sp.phase = int((step0 + s) % 3);
+		}
+		__syncthreads();
+		if (not s_go) return;
+		double smax[3] = {0.0, 0.0, 0.0};
+		bool zero = false;
+		if (w.w == 0) {
+			const bool first = w.y == 0 and w.z == 0;
+			const double dt = begin_step(sp, &s_dt, first);
+			const int tiles_x = (sp.L.n[0] + TX - 1) / TX;
+			tile_step<SOLVER, TY, true>(sp, smem, dt, w.y % tiles_x, w.y / tiles_x, w.z, smax[0], smax[1],
+			                            smax[2], zero);
+		} else {
+			// ghost-ghost faces: combination w.y, faces [w.z BOUNDARY_CHUNK, (w.z + 1) BOUNDARY_CHUNK)
+			int combos[12][3];
+			const int nc = boundary_combos(sp, combos);
+			if (w.y < nc) {
+				const int d = combos[w.y][0], side = combos[w.y][1], e = combos[w.y][2];
+				const long long count = boundary_count(sp, d, e);
+				const long long t1 = min(count, (long long)(w.z + 1) * BOUNDARY_CHUNK);
+				for (long long t = (long long)w.z * BOUNDARY_CHUNK + tid; t < t1; t += nthreads) {
+					boundary_face<SOLVER, true>(sp, d, side, e, t, smax, zero);
+				}
+			}
+		}
+		flush_speeds(sp, smax, zero);
+		// publish the item's writes (every thread's), then count it done
+		__threadfence();
+		__syncthreads();
+		if (tid == 0) atomicAdd(done + w.x, 1u);
 	}
 }
 
@@ -959,6 +1100,116 @@ int batch_blocks_per_sm(const int solver, const int ty, int* blocks)
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+template <int SOLVER, int TY>
+static int prepare_run_t()
+{
+	const cudaError_t e = cudaFuncSetAttribute(batch_run_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
+	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tile<TY>::BYTES));
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+template <int SOLVER, int TY>
+static cudaError_t run_occupancy_t(int* blocks)
+{
+	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_run_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
+	                                                     TX * TY, Tile<TY>::BYTES);
+}
+
+template <int SOLVER, int TY>
+static int launch_run_t(const Step_Params* even, const Step_Params* odd, const int4* items, const int nitems,
+                        const int* box_items, unsigned int* done, const int nboxes, const long long step0,
+                        const int nsteps, Run_Sync* sync, const long long wait_limit, const int grid,
+                        cudaStream_t stream)
+{
+	cudaLaunchConfig_t c = {};
+	c.gridDim = dim3(grid);
+	c.blockDim = dim3(TX, TY);
+	c.dynamicSmemBytes = Tile<TY>::BYTES;
+	c.stream = stream;
+	cudaLaunchAttribute a[1];
+	a[0].id = cudaLaunchAttributeCooperative;
+	a[0].val.cooperative = 1;
+	c.attrs = a;
+	c.numAttrs = 1;
+	const cudaError_t e = cudaLaunchKernelEx(&c, batch_run_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>, even, odd,
+	                                         items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit);
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+template <int SOLVER>
+static int prepare_run_s(const int ty)
+{
+	switch (ty) {
+	case 1: return prepare_run_t<SOLVER, 1>();
+	case TY_3D: return prepare_run_t<SOLVER, TY_3D>();
+	case TY_WIDE: return prepare_run_t<SOLVER, TY_WIDE>();
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+template <int SOLVER>
+static cudaError_t run_occupancy_s(const int ty, int* blocks)
+{
+	switch (ty) {
+	case 1: return run_occupancy_t<SOLVER, 1>(blocks);
+	case TY_3D: return run_occupancy_t<SOLVER, TY_3D>(blocks);
+	case TY_WIDE: return run_occupancy_t<SOLVER, TY_WIDE>(blocks);
+	default: return cudaErrorInvalidValue;
+	}
+}
+
+template <int SOLVER>
+static int launch_run_s(const Step_Params* even, const Step_Params* odd, const int4* items, const int nitems,
+                        const int* box_items, unsigned int* done, const int nboxes, const long long step0,
+                        const int nsteps, Run_Sync* sync, const long long wait_limit, const int grid, const int ty,
+                        cudaStream_t stream)
+{
+	switch (ty) {
+	case 1: return launch_run_t<SOLVER, 1>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, stream);
+	case TY_3D: return launch_run_t<SOLVER, TY_3D>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, stream);
+	case TY_WIDE: return launch_run_t<SOLVER, TY_WIDE>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, stream);
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+int prepare_batch_run_kernels(const int solver, const int ty)
+{
+	switch (solver) {
+	case PAMHD_RUSANOV: return prepare_run_s<PAMHD_RUSANOV>(ty);
+	case PAMHD_HLL_ATHENA: return prepare_run_s<PAMHD_HLL_ATHENA>(ty);
+	case PAMHD_HLLD_ATHENA: return prepare_run_s<PAMHD_HLLD_ATHENA>(ty);
+	case PAMHD_ROE_ATHENA: return prepare_run_s<PAMHD_ROE_ATHENA>(ty);
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+}
+
+int batch_run_blocks_per_sm(const int solver, const int ty, int* blocks)
+{
+	cudaError_t e = cudaErrorInvalidValue;
+	switch (solver) {
+	case PAMHD_RUSANOV: e = run_occupancy_s<PAMHD_RUSANOV>(ty, blocks); break;
+	case PAMHD_HLL_ATHENA: e = run_occupancy_s<PAMHD_HLL_ATHENA>(ty, blocks); break;
+	case PAMHD_HLLD_ATHENA: e = run_occupancy_s<PAMHD_HLLD_ATHENA>(ty, blocks); break;
+	case PAMHD_ROE_ATHENA: e = run_occupancy_s<PAMHD_ROE_ATHENA>(ty, blocks); break;
+	default: return PAMHD_ERR_ARGUMENT;
+	}
+	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
+int launch_batch_run(const Step_Params* even, const Step_Params* odd, const int4* items, const int nitems,
+                     const int* box_items, unsigned int* done, const int nboxes, const long long step0,
+                     const int nsteps, Run_Sync* sync, const long long wait_limit, const int grid, const int solver,
+                     const int ty, cudaStream_t stream)
+{
+	switch (solver) {
+	case PAMHD_RUSANOV: return launch_run_s<PAMHD_RUSANOV>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, ty, stream);
+	case PAMHD_HLL_ATHENA: return launch_run_s<PAMHD_HLL_ATHENA>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, ty, stream);
+	case PAMHD_HLLD_ATHENA: return launch_run_s<PAMHD_HLLD_ATHENA>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, ty, stream);
+	case PAMHD_ROE_ATHENA: return launch_run_s<PAMHD_ROE_ATHENA>(even, odd, items, nitems, box_items, done, nboxes, step0, nsteps, sync, wait_limit, grid, ty, stream);
+	default: return PAMHD_ERR_ARGUMENT;
+	}
 }
 
 template <int SOLVER, int TY>

@@ -139,3 +139,76 @@ def test_batch_reports_failing_box():
     assert "box 2" in str(e.value) and e.value.flags == pg.FLAG_PRESSURE
     for i in (0, 1, 3, 4):
         assert batch.status(i)[0] == 0
+
+
+# ---------------------------------------------------------------- the persistent run
+
+
+@pytest.mark.parametrize("tile_rows,planes", [(4, 8), (8, 32)])
+def test_persistent_run_equals_per_step_launches_bitwise(tile_rows, planes):
+    """pamhd_gpu_batch_run (every step in one launch, each box's step waiting for its previous
+    one) against pamhd_gpu_batch_steps (one launch per step): the same bits, box by box, including
+    the boundary-face speeds that set each box's timestep; run twice in a row (graph replay, and the
+    parity and phase of the second run differ from the first's)."""
+    cfgs, U0s = small_ensemble()
+    a, b = pg.Batch(cfgs), pg.Batch(cfgs)
+    for batch in (a, b):
+        batch.set_tiling(tile_rows, planes, 1)
+        for i, U in enumerate(U0s):
+            batch.set_state(i, U)
+    a.steps(11)
+    a.steps(8)
+    a.sync()
+    b.run(11)
+    b.run(8)
+    b.sync()
+    grid, items, graphed = b.run_info()
+    assert grid > 1 and items > 0
+    for i in range(len(cfgs)):
+        np.testing.assert_array_equal(b.get_state(i), a.get_state(i))
+        np.testing.assert_array_equal(b.dt_history(i, 19), a.dt_history(i, 19))
+        assert b.time(i) == a.time(i)
+
+
+def test_persistent_run_tuner_restores_state():
+    cfgs, U0s = small_ensemble()
+    a, b = pg.Batch(cfgs), pg.Batch(cfgs)
+    for batch in (a, b):
+        for i, U in enumerate(U0s):
+            batch.set_state(i, U)
+    rows, planes = b.tune_run(2)
+    assert rows in (4, 8) and planes in (8, 16, 32, 64)
+    a.set_tiling(rows, planes, 1)
+    a.steps(6)
+    b.run(6)
+    for i in range(len(cfgs)):
+        np.testing.assert_array_equal(b.get_state(i), a.get_state(i))
+
+
+def test_persistent_run_wait_timeout_is_reported():
+    """A wait that runs out (a limit of 0 polls: the first block to take an item of step 1 before
+    its box's step 0 is done gives up at once) ends the launch with PAMHD_FLAG_TIMEOUT on every
+    box and PAMHD_ERR_TIMEOUT from sync, without a fault; the batch is usable again after
+    set_state."""
+    cfgs, U0s = small_ensemble()
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.set_wait_limit(0)
+    batch.run(5)
+    with pytest.raises(pg.PamhdError) as e:
+        batch.sync()
+    assert e.value.code == pg.ERR_TIMEOUT
+    for i in range(len(cfgs)):
+        assert batch.status(i)[0] & pg.FLAG_TIMEOUT
+    batch.set_wait_limit(10_000_000)
+    ref = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+        ref.set_state(i, U)
+    batch.run(4)
+    batch.sync()
+    ref.steps(4)
+    ref.sync()
+    for i in range(len(cfgs)):
+        np.testing.assert_array_equal(batch.get_state(i), ref.get_state(i))
