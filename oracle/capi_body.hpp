@@ -444,6 +444,28 @@ int ORACLE_API(lgrid_set_exponents)(void* grid, const int32_t* mins, const int32
 	return PAMHD_OK;
 }
 
+/*
+The substep plan from given per-cell CFL limits (x fastest) on the grid's
+exponent bounds (lgrid_set_exponents first): every cell's period, the
+substep length and the largest period.  Returns PAMHD_OK, or
+PAMHD_ERR_PHYSICS where the reference aborts on unexpected substeps.
+*/
+int ORACLE_API(lgrid_plan)(void* grid, const double* limits, double max_dt, int32_t* periods, double* substep,
+                           int32_t* max_period)
+{
+	LGrid& g = *static_cast<LGrid*>(grid);
+	try {
+		g.plan_from_limits(limits, max_dt);
+	} catch (const std::exception& e) {
+		last_error = e.what();
+		return PAMHD_ERR_PHYSICS;
+	}
+	for (size_t c = 0; c < g.U.size(); c++) periods[c] = g.period[c];
+	*substep = g.substep;
+	*max_period = g.max_substep;
+	return PAMHD_OK;
+}
+
 // one step with substeps; *dt_taken its length, *substeps their number, periods[c] each cell's period
 int ORACLE_API(lgrid_step)(void* grid, double max_dt, double* dt_taken, int32_t* substeps, int32_t* periods,
                            uint32_t* flag)

@@ -21,6 +21,8 @@ import numpy as np
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
 REF_LIB = os.path.join(ORACLE_DIR, "_ref", "libpamhd_ref.so")
+# the reference's substepping.hpp on a single-rank uniform-grid stand-in (ref_substep_bridge.cpp)
+REF_SUBSTEP_LIB = os.path.join(ORACLE_DIR, "_ref", "libsubstep_ref.so")
 REF_EXE = os.path.join(ORACLE_DIR, "_ref", "reference.exe")
 
 RUSANOV, RUSANOV_STAGGERED, HLL, HLLD, ROE = 0, 1, 2, 3, 4
@@ -184,6 +186,8 @@ class Oracle:
         self._lstep = getattr(L, p + "lgrid_step")
         self._lstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_int32), _P(ctypes.c_int32),
                                 _P(ctypes.c_uint32)]
+        self._lplan = getattr(L, p + "lgrid_plan")
+        self._lplan.argtypes = [ctypes.c_void_p, _DP, _D, _P(ctypes.c_int32), _DP, _P(ctypes.c_int32)]
         self._last_error = getattr(L, p + "last_error")
         self._last_error.restype = ctypes.c_char_p
         if kind == "port":
@@ -472,6 +476,20 @@ class OracleSubstepGrid:
         b = np.ascontiguousarray(maxs, dtype=np.int32).reshape(-1)
         if self.o._lexp(self.h, a.ctypes.data_as(_P(ctypes.c_int32)), b.ctypes.data_as(_P(ctypes.c_int32))) != 0:
             raise ValueError(self.o.last_error())
+
+    def plan(self, limits, max_dt):
+        """The substep plan from given CFL limits (nz, ny, nx) on the exponent bounds set before:
+        (periods (nz, ny, nx), substep length, largest period), or None where the reference would
+        abort on unexpected substeps."""
+        lim = np.ascontiguousarray(limits, dtype=np.float64).reshape(-1)
+        periods = np.zeros(self.shape, dtype=np.int32)
+        sub = ctypes.c_double(0)
+        top = ctypes.c_int32(0)
+        rc = self.o._lplan(self.h, lim.ctypes.data_as(_DP), max_dt, periods.ctypes.data_as(_P(ctypes.c_int32)),
+                           ctypes.byref(sub), ctypes.byref(top))
+        if rc != 0:
+            return None
+        return periods, sub.value, top.value
 
     def step(self, max_dt):
         """Returns (dt, substeps, periods (nz, ny, nx), flag)."""

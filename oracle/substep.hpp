@@ -116,6 +116,20 @@ public:
 	// the exponents and the substep of a step capped by max_dt (substepping.hpp:195-394)
 	void plan(const double max_dt)
 	{
+		this->timestep(std::numeric_limits<double>::max());  // fills Timestep[] (minimize_timestep)
+		plan_from_limits(max_dt);
+	}
+
+	// the same from given CFL limits, one per cell (the reference functions' pin)
+	void plan_from_limits(const double* limits, const double max_dt)
+	{
+		for (size_t c = 0; c < U.size(); c++) Timestep[c] = limits[c];
+		plan_from_limits(max_dt);
+	}
+
+	// the plan from the limits in Timestep[]
+	void plan_from_limits(const double max_dt)
+	{
 		const size_t N = U.size();
 		std::vector<int> smin(user_min), smax(user_max);
 		int lowest = std::numeric_limits<int>::max();
@@ -123,7 +137,6 @@ public:
 		if (lowest > 0) {
 			for (size_t c = 0; c < N; c++) smin[c] -= lowest;
 		}
-		this->timestep(std::numeric_limits<double>::max());  // fills Timestep[] (minimize_timestep)
 		double smallest = std::numeric_limits<double>::max();
 		for (size_t c = 0; c < N; c++) smallest = std::min(Timestep[c], smallest);
 		if (max_dt <= smallest) {
