@@ -116,6 +116,18 @@ def ncu_traffic(n):
     return ncu_count(n, "step_kernel_hlld")
 
 
+def ncu_source(key):
+    """The commit whose kernel source the committed count of `key` was captured from."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "traffic.txt")):
+            parts = line.split()
+            if len(parts) >= 4 and parts[0] == key:
+                return parts[3]
+    except OSError:
+        pass
+    return None
+
+
 def fp64_roof(n, kernel_ms, clocks):
     """The second roof: FP64 flops of one step (ncu count per cell-update x cells) per second
     against the chip's FP64 rate, 148 SMs x 64 FMA lanes x 2 flops at the median SM clock sampled
@@ -152,6 +164,7 @@ def section_roofline(n, key, alg_bytes, updates, ms, clk, scope):
     achieved = alg_bytes * updates / (ms / 1e3) / 1e9
     out = {"bound": "hbm", "scope": scope, "achieved": achieved, "peak": peak, "unit": "GB/s",
            "frac": achieved / peak, "traffic": ncu_count(n, key), "traffic_scope": "one step, all its kernels",
+           "traffic_source_commit": ncu_source(key),
            "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
            "algorithmic_bytes_per_cell_update": alg_bytes, "step_ms": ms}
     flops = ncu_count(n, key + "_fp64")
@@ -1012,6 +1025,9 @@ def run_b200(a):
             "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": traffic,
+            "traffic_source": f"ncu DRAM bytes of one launch at 160^3 scaled to {n}^3 by cell count, captured from "
+                              f"the kernel source of commit {ncu_source('step_kernel_hlld')} "
+                              f"(profiles/step_kernel_hlld_blast160.md)",
             "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_cell_update": BYTES_PER_CELL_UPDATE,
             "kernel_ms": kernel_ms,
