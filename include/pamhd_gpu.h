@@ -187,6 +187,22 @@ pamhd_gpu_time() to collect the result.
 int pamhd_gpu_steps(pamhd_ctx* ctx, int32_t nsteps, double t_end);
 
 /*
+One step in two launches, for a z slab that overlaps its halo exchange with
+the step's interior: part 1 computes the new state of the first and last z
+planes (and the speeds of ghost-ghost faces), part 2 the planes between them
+and ends the step.  Between the two, pamhd_gpu_halo returns the planes of the
+state being written, so the caller can send the new cut planes to its
+neighbours (and receive theirs into the new ghost planes) while part 2 runs.
+Both parts read the same state and fold into the same speed reduction: the
+result equals pamhd_gpu_steps(ctx, 1, t_end) bit for bit.  Parts must
+alternate, starting with 1; needs active z.  No host synchronisation (the
+time cap t_end is written to the device only when it changes).  The
+reference overlaps its remote-neighbour update with the inner cells the same
+way (mhd/solve.hpp:1767-1802).
+*/
+int pamhd_gpu_step_part(pamhd_ctx* ctx, int32_t part, double t_end);
+
+/*
 The CUDA stream (a cudaStream_t) every kernel of the context runs on, so
 that callers can order their own work with it or time it with CUDA events.
 No reference counterpart (the reference has no device streams).
@@ -216,9 +232,10 @@ each slab into its neighbours' ghost planes.
 side: 0 = low z, 1 = high z; ghost: 0 = the interior plane next to that
 side (to send), 1 = the ghost plane of that side (to receive).
 planes[v] receives the device address of variable v's plane in the
-current state, *count the plane's length in doubles (padded rows; a plane
-of one variable is contiguous).  The addresses alternate between two
-buffers from step to step: ask again after every step.
+current state (between the parts of a step split by pamhd_gpu_step_part:
+the state that step writes), *count the plane's length in doubles (padded
+rows; a plane of one variable is contiguous).  The addresses alternate
+between two buffers from step to step: ask again after every step.
 */
 int pamhd_gpu_halo(pamhd_ctx* ctx, int32_t side, int32_t ghost, double* planes[8], int64_t* count);
 

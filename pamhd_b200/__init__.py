@@ -241,6 +241,13 @@ class Context:
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_steps(self.h, int(n), float(t_end)), "pamhd_gpu_steps")
 
+    def step_part(self, part: int, t_end: float):
+        """Half of a step (pamhd_gpu_step_part): part 1 the first and last z planes, part 2 the others
+        and the step's end."""
+        fn = self.L.pamhd_gpu_step_part
+        fn.argtypes = [ctypes.c_void_p, ctypes.c_int32, _D]
+        self._check(fn(self.h, int(part), float(t_end)), "pamhd_gpu_step_part")
+
     def set_inflow(self, dim: int, side: int, times, states):
         """Time-stamped inflow of a VALUE side (pamhd_gpu_set_inflow): states[i] (8 conservative
         values) holds while i of the increasing timestamps are <= the simulation time."""

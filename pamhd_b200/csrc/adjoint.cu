@@ -342,7 +342,7 @@ extern "C" {
 int pamhd_gpu_steps_dt(pamhd_ctx* x, const int32_t nsteps, const double* dts)
 {
 	if (x == nullptr or nsteps < 0 or (nsteps > 0 and dts == nullptr)) return PAMHD_ERR_ARGUMENT;
-	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (not x->loaded or x->half) return PAMHD_ERR_STATE;
 	for (int n = 0; n < nsteps; n++) {
 		if (not (dts[n] >= 0.0)) return PAMHD_ERR_ARGUMENT;
 	}
@@ -366,7 +366,7 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 	if (x->cfg.bc_lo[2] == PAMHD_BC_EXTERNAL or x->cfg.bc_hi[2] == PAMHD_BC_EXTERNAL) return PAMHD_ERR_ARGUMENT;
 	// the inflow-state gradient is of one constant state per side
 	if (x->base.inflow != nullptr) return PAMHD_ERR_ARGUMENT;
-	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (not x->loaded or x->half) return PAMHD_ERR_STATE;
 	if (dt_in != nullptr) {
 		for (int n = 0; n < nsteps; n++) if (not (dt_in[n] >= 0.0)) return PAMHD_ERR_ARGUMENT;
 	}
@@ -423,6 +423,8 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 		c.max_dt = -1.0;
 		c.t_end = 1.0e300;
 		PAMHD_TRY(check(cudaMemcpyAsync(x->control, &c, sizeof c, cudaMemcpyHostToDevice, x->stream)));
+		x->control_max_dt = c.max_dt;
+		x->control_t_end = c.t_end;
 	}
 	// VALUE ghosts are constant and the step kernel never writes them: fill each recompute state once
 	for (int b = 0; b < 2; b++) {

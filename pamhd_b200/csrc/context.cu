@@ -63,6 +63,21 @@ int issue_step(pamhd_ctx& x)
 	return PAMHD_OK;
 }
 
+// one part of a step: 1 the first and last z planes (and the boundary speeds), 2 the rest and the
+// step's end; the two launches read the same state and fold into the same reduction slot
+int issue_step_part(pamhd_ctx& x, const int part)
+{
+	Step_Params P = params_for(x, x.steps, x.cur);
+	P.kpart = part;
+	if (part == 1 and x.needs_boundary_speeds) PAMHD_TRY(launch_boundary_speeds(P, x.cfg.solver, x.stream));
+	PAMHD_TRY(launch_step(P, x.cfg.solver, x.stream));
+	if (part == 2) {
+		x.cur ^= 1;
+		x.steps++;
+	}
+	return PAMHD_OK;
+}
+
 } // namespace
 
 int pamhd_b200::context_issue_step(pamhd_ctx& x)
@@ -83,6 +98,7 @@ int reset_run_state(pamhd_ctx& x)
 	PAMHD_TRY(check(cudaMemcpyAsync(x.status, &s, sizeof s, cudaMemcpyHostToDevice, x.stream)));
 	x.steps = 0;
 	x.cur = 0;
+	x.half = 0;
 	return PAMHD_OK;
 }
 
@@ -94,6 +110,8 @@ int read_status(pamhd_ctx& x, Status& s)
 
 int set_control(pamhd_ctx& x, const double max_dt, const double t_end)
 {
+	x.control_max_dt = max_dt;
+	x.control_t_end = t_end;
 	Control c;
 	c.max_dt = max_dt;
 	c.t_end = t_end;
@@ -310,7 +328,7 @@ int pamhd_gpu_get_state_device(pamhd_ctx* x, double* const soa[8])
 int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken, double* max_signal)
 {
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
-	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (not x->loaded or x->half) return PAMHD_ERR_STATE;
 	if (not (max_dt >= 0.0)) return PAMHD_ERR_ARGUMENT;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	PAMHD_TRY(set_control(*x, max_dt, 0.0));
@@ -337,7 +355,7 @@ int pamhd_gpu_step(pamhd_ctx* x, const double max_dt, double* dt_taken, double* 
 int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
 {
 	if (x == nullptr or nsteps < 0) return PAMHD_ERR_ARGUMENT;
-	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (not x->loaded or x->half) return PAMHD_ERR_STATE;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	PAMHD_TRY(set_control(*x, -1.0, t_end));
 	int left = nsteps;
@@ -357,6 +375,21 @@ int pamhd_gpu_steps(pamhd_ctx* x, const int32_t nsteps, const double t_end)
 		PAMHD_TRY(issue_step(*x));
 		left--;
 	}
+	return PAMHD_OK;
+}
+
+int pamhd_gpu_step_part(pamhd_ctx* x, const int32_t part, const double t_end)
+{
+	if (x == nullptr or (part != 1 and part != 2)) return PAMHD_ERR_ARGUMENT;
+	if (not x->loaded) return PAMHD_ERR_STATE;
+	if (x->base.active[2] == 0) return PAMHD_ERR_ARGUMENT;  // needs z planes
+	if ((part == 1) == (x->half != 0)) return PAMHD_ERR_STATE;  // parts 1 and 2 alternate
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	if (part == 1 and (x->control_max_dt != -1.0 or x->control_t_end != t_end)) {
+		PAMHD_TRY(set_control(*x, -1.0, t_end));
+	}
+	PAMHD_TRY(issue_step_part(*x, part));
+	x->half = part == 1 ? 1 : 0;
 	return PAMHD_OK;
 }
 
@@ -431,7 +464,9 @@ int pamhd_gpu_halo(pamhd_ctx* x, const int32_t side, const int32_t ghost, double
 	if (L.g[2] == 0) return PAMHD_ERR_ARGUMENT;  // no z ghosts: not a slab
 	const int k = side == 0 ? (ghost ? -1 : 0) : (ghost ? L.n[2] : L.n[2] - 1);
 	const long long first = (long long)(k + L.g[2]) * L.plane;
-	for (int v = 0; v < 8; v++) planes[v] = x->state[x->cur] + v * L.var + first;
+	// between the two parts of a split step: the state that step writes
+	const double* base = x->state[x->half ? x->cur ^ 1 : x->cur];
+	for (int v = 0; v < 8; v++) planes[v] = const_cast<double*>(base) + v * L.var + first;
 	*count = L.plane;
 	return PAMHD_OK;
 }

@@ -32,6 +32,8 @@ struct pamhd_ctx {
 	double* dt_hist = nullptr;
 	int hist_len = 1 << 16;
 	long long steps = 0;
+	int half = 0;         // 1 between the two parts of a step split by pamhd_gpu_step_part
+	double control_max_dt = -2.0, control_t_end = -2.0;  // the device Control last written
 	double* staging = nullptr;
 	double* partial = nullptr;
 	int partial_blocks = 296;

@@ -106,6 +106,7 @@ struct Step_Params {
 	int phase;           // step index mod 3
 	int kchunk;          // z planes per block
 	double forced_dt;    // >= 0: the step's dt (a prescribed schedule); < 0: the CFL rule
+	int kpart;           // z planes a launch computes: 0 all, 1 the first and last only, 2 the others
 	const Inflow_Table* inflow;  // [3][2] by dimension and side (lo, hi) in device memory, or nullptr
 };
 

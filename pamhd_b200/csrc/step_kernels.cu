@@ -421,8 +421,12 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 	const bool own = gx < nx and gy < ny;
 	// the +x / +y ghost of a partial tile lies inside the tile's own columns / rows
 	const bool stage = gx <= nx and (TY == 1 ? gy == 0 : gy <= ny);
-	const int kb = bz * P.kchunk;
-	const int ke = min(P.L.n[2], kb + P.kchunk);
+	// the planes of this block: a z chunk, or with kpart 1 the first (bz 0) or the last (bz 1)
+	// plane alone, or with kpart 2 a chunk of the planes between them
+	const int nz = P.L.n[2];
+	const int kbase = P.kpart == 2 ? 1 : 0, ktop = P.kpart == 2 ? nz - 1 : nz;
+	const int kb = P.kpart == 1 ? (bz == 0 ? 0 : nz - 1) : kbase + bz * P.kchunk;
+	const int ke = P.kpart == 1 ? kb + 1 : min(ktop, kb + P.kchunk);
 	const int kfirst = zact ? kb - 1 : kb;
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
@@ -1016,8 +1020,12 @@ static int launch_step_t(const Step_Params& P, cudaStream_t stream)
 {
 	const size_t smem = Tile<TY>::BYTES;
 	const dim3 block(TX, TY);
-	const dim3 grid((P.L.n[0] + TX - 1) / TX, (P.L.n[1] + TY - 1) / TY,
-	                (P.L.n[2] + P.kchunk - 1) / P.kchunk);
+	const int nz = P.L.n[2];
+	const int chunks = P.kpart == 1 ? (nz > 1 ? 2 : 1)
+	                 : P.kpart == 2 ? (nz - 2 + P.kchunk - 1) / P.kchunk
+	                 : (nz + P.kchunk - 1) / P.kchunk;
+	if (chunks < 1) return PAMHD_OK;  // no planes between the first and the last
+	const dim3 grid((P.L.n[0] + TX - 1) / TX, (P.L.n[1] + TY - 1) / TY, chunks);
 	step_kernel<SOLVER, TY, MINB><<<grid, block, smem, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }

@@ -9,10 +9,15 @@ along z into contiguous slabs:
   * each slab is an ordinary context whose cut z sides are BC_EXTERNAL:
     the step kernel computes the faces between the ghost plane and the
     slab like any other face, but never writes the ghost plane;
-  * after every step (and after set_state) each slab sends its first and
-    last interior planes to the neighbouring slabs' ghost planes
-    (exchange_halos: one batch of point-to-point sends / receives over
-    torch.distributed, NCCL on GPUs);
+  * every step is split in two launches (pamhd_gpu_step_part): first the
+    new state of the slab's first and last planes, then the planes between;
+    as soon as the first launch is done each slab sends its new first and
+    last planes to the neighbouring slabs' new ghost planes (exchange_halos:
+    one batch of point-to-point sends / receives over torch.distributed,
+    NCCL on GPUs, on a stream of its own) while the second launch computes
+    the interior, as the reference posts its remote-neighbour copies, solves
+    the inner cells and then waits for the copies (mhd/solve.hpp:1767-1802);
+    after set_state the current planes are exchanged once;
   * the speed reduction the next step takes its dt from is combined by an
     element-wise max over all slabs (merge_speeds: one all-reduce of four
     64-bit words), so every slab takes the grid's dt.  The dt rule is
@@ -125,6 +130,19 @@ def device_tensor(ptr: int, count: int, dtype, device):
     return t
 
 
+def overlapped_steps(n: int, boundary, exchange_new, interior, finish) -> None:
+    """The order of n split steps: boundary() computes the new first and last planes,
+    exchange_new() starts sending them and receiving the neighbours' into the new ghost planes
+    (returning what finish needs to wait for), interior() computes the planes between while the
+    exchange is in flight, finish(pending) waits for the exchange and merges the speed
+    reductions.  Shared by SlabGrid and its CPU tests."""
+    for _ in range(int(n)):
+        boundary()
+        pending = exchange_new()
+        interior()
+        finish(pending)
+
+
 class SlabGrid:
     """This rank's slab of a grid cut along z, on this rank's GPU (cfg.device), exchanging with
     the other ranks of `comm` (a torch.distributed group; None = the default group)."""
@@ -143,6 +161,7 @@ class SlabGrid:
         self.ctx = Context(self.cfg)
         self.device = torch.device("cuda", cfg.device)
         self.stream = torch.cuda.ExternalStream(self.ctx.stream(), device=self.device)
+        self.comm_stream = torch.cuda.Stream(device=self.device) if world > 1 else None
         self._halos = {}   # address of the current state's first plane -> the four plane lists
         self._slots = {}   # address of a reduction slot -> tensor
 
@@ -174,6 +193,26 @@ class SlabGrid:
         with torch.cuda.stream(self.stream):
             exchange_halos(self.comm, self.lo, self.hi, send_lo, send_hi, recv_lo, recv_hi)
 
+    def exchange_async(self):
+        """Between the two parts of a split step: sends the new first and last planes and receives
+        the neighbours' into the new ghost planes, on the communication stream once the first part
+        is done; returns the event that marks the exchange complete."""
+        import torch
+        ready = torch.cuda.Event()
+        ready.record(self.stream)
+        self.comm_stream.wait_event(ready)
+        send_lo, send_hi, recv_lo, recv_hi = self.halo_tensors()
+        with torch.cuda.stream(self.comm_stream):
+            exchange_halos(self.comm, self.lo, self.hi, send_lo, send_hi, recv_lo, recv_hi)
+        done = torch.cuda.Event()
+        done.record(self.comm_stream)
+        return done
+
+    def finish_step(self, exchanged):
+        """The step's end: the context's stream waits for the exchange, then the speed merge."""
+        self.stream.wait_event(exchanged)
+        self.merge()
+
     def merge(self):
         if self.world == 1:
             return
@@ -198,15 +237,14 @@ class SlabGrid:
         self.ctx.get_state_device(ptrs)
 
     def steps(self, n: int, t_end: float):
-        """n steps (the first after set_state is the dt = 0 priming step), each followed by the
-        halo exchange and the speed merge; nothing here waits for the GPU."""
+        """n steps (the first after set_state is the dt = 0 priming step), each split so that the
+        halo exchange of its new cut planes overlaps the computation of its interior, then the
+        speed merge; nothing here waits for the GPU."""
         if self.world == 1:
             self.ctx.steps(n, t_end)
             return
-        for _ in range(int(n)):
-            self.ctx.steps(1, t_end)
-            self.exchange()
-            self.merge()
+        overlapped_steps(n, lambda: self.ctx.step_part(1, t_end), self.exchange_async,
+                         lambda: self.ctx.step_part(2, t_end), self.finish_step)
 
     def sync(self):
         self.ctx.sync()
