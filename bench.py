@@ -57,6 +57,8 @@ def args_():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-configs", action="store_true", help="skip the other configured workloads")
+    p.add_argument("--configs-solver", default=None,
+                   help="with --only configs: the Orszag-Tang run of this solver alone (rusanov, hll_athena, hlld_athena, roe_athena)")
     p.add_argument("--only", choices=["batched", "adjoint", "configs", "staggered", "two_population", "substep"],
                    help="run one section alone and print it (for profiling)")
     p.add_argument("--boxes", type=int, default=64, help="boxes of the batched section")
@@ -329,10 +331,11 @@ def cpu_model():
     return "unknown"
 
 
-def configs_section(local, cpu=True):
+def configs_section(local, cpu=True, solver=None):
     """The other configured workloads, GPU beside the reference's solver headers on the host cores
     (a bounded sample each): cell-updates/s of the shock tube run to its end time and of 100
-    Orszag-Tang 512^2 steps with each solver (the reference scheme keeps positivity that long)."""
+    Orszag-Tang 512^2 steps with each solver (the reference scheme keeps positivity that long).
+    solver: the Orszag-Tang run of that solver alone (no shock tube)."""
     import torch
     import pamhd_b200 as pg
     import states
@@ -380,22 +383,27 @@ def configs_section(local, cpu=True):
         return (time.perf_counter() - t0) * 1e3, done
 
     out = {}
+    if solver is not None and solver not in po.SOLVERS:
+        raise ValueError(f"--configs-solver: one of {sorted(po.SOLVERS)}")
     # shock tube: 1000 cells, gamma 2, HLLD, CFL 0.5, copy boundaries, to t = 0.1
-    U = states.brio_wu(1000)
-    cfg = pg.Config(n=(1000, 1, 1), solver=pg.HLLD, cell_length=(1e-3, 1.0, 1.0), adiabatic_index=2.0,
-                    time_step_factor=0.5, bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0), device=local)
-    ms, steps = gpu_rate(cfg, U, 2000, 0.1)
-    entry = {"workload": "Brio-Wu 1000 cells, HLLD, CFL 0.5, to t = 0.1", "steps": steps,
-             "gpu": 1000 * steps / (ms / 1e3), "gpu_ms": ms, "unit": UNIT}
-    if cpu:
-        ocfg = po.make_cfg((1000, 1, 1), po.HLLD, (1e-3, 1.0, 1.0), 2.0, 1.0, 0.5, (1, 0, 0), (1, 0, 0))
-        cms, csteps = cpu_rate(ocfg, U, 2000, 0.1, 1)
-        entry.update(cpu_one_core=1000 * csteps / (cms / 1e3), cpu_sample=f"{csteps} steps, 1 thread")
-    out["brio_wu"] = entry
+    if solver is None:
+        U = states.brio_wu(1000)
+        cfg = pg.Config(n=(1000, 1, 1), solver=pg.HLLD, cell_length=(1e-3, 1.0, 1.0), adiabatic_index=2.0,
+                        time_step_factor=0.5, bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0), device=local)
+        ms, steps = gpu_rate(cfg, U, 2000, 0.1)
+        entry = {"workload": "Brio-Wu 1000 cells, HLLD, CFL 0.5, to t = 0.1", "steps": steps,
+                 "gpu": 1000 * steps / (ms / 1e3), "gpu_ms": ms, "unit": UNIT}
+        if cpu:
+            ocfg = po.make_cfg((1000, 1, 1), po.HLLD, (1e-3, 1.0, 1.0), 2.0, 1.0, 0.5, (1, 0, 0), (1, 0, 0))
+            cms, csteps = cpu_rate(ocfg, U, 2000, 0.1, 1)
+            entry.update(cpu_one_core=1000 * csteps / (cms / 1e3), cpu_sample=f"{csteps} steps, 1 thread")
+        out["brio_wu"] = entry
     # Orszag-Tang 512^2, each solver, 100 steps
     n = 512
     U = states.orszag_tang(n)
     for name, sid in po.SOLVERS.items():
+        if solver is not None and name != solver:
+            continue
         cfg = pg.Config(n=(n, n, 1), solver=sid, cell_length=(1 / n, 1 / n, 1.0), adiabatic_index=5 / 3,
                         time_step_factor=0.4, device=local)
         ms, steps = gpu_rate(cfg, U, 100, 10.0)
@@ -1092,7 +1100,7 @@ def run_only(a):
     elif a.only == "substep":
         out = substep_section(local, cpu=not a.no_cpu_baseline)
     else:
-        out = configs_section(local, cpu=not a.no_cpu_baseline)
+        out = configs_section(local, cpu=not a.no_cpu_baseline, solver=a.configs_solver)
     print(json.dumps({a.only: out}), flush=True)
     return 0
 
