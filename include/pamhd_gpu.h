@@ -6,7 +6,7 @@ on uniform Cartesian grids: the conservative state (mass density, momentum
 density, total energy density, magnetic field), the Rusanov / HLL / HLLD /
 Roe face fluxes, flux application and the lagged CFL timestep rule; and for
 its staggered-field step (face magnetic field by constrained transport,
-pamhd_gpu_staggered_*) on uniform periodic grids.
+pamhd_gpu_staggered_*) on uniform grids, periodic or bounded.
 Host code (C or C++) calls these entry points with plain pointers and
 sizes; no C++ types, exceptions or torch types cross this boundary.
 
@@ -477,19 +477,39 @@ Staggered-field step: the reference's timestep() with the normal magnetic
 field of every face (Face_B) advanced by constrained transport
 (mhd/solve.hpp:1837-1924: get_fluxes with assign_face_dBs_f{x,y,z},
 update_mhd_state, update_vol_B with constant thermal pressure before and
-after sync_magnetic_field), on a uniform grid periodic in every dimension.
-A dimension of one cell is its own neighbour, as in the reference's
-emulated 1-D and 2-D runs.  Solvers: Rusanov, HLL, HLLD, Roe.
+after sync_magnetic_field), on a uniform grid.  A periodic dimension of
+one cell is its own neighbour, as in the reference's emulated 1-D and 2-D
+runs.  Solvers: Rusanov, HLL, HLLD, Roe.
 
-  - create: cfg as pamhd_gpu_create, every side PAMHD_BC_PERIODIC and
-    n[1] at most 262140 (else PAMHD_ERR_ARGUMENT); replaces the state a PAMHD program keeps in
+A dimension of two cells or more may be bounded (PAMHD_BC_COPY or
+PAMHD_BC_VALUE on both sides, at most one VALUE side in the grid), as the
+reference's solar-wind box (tests/mhd/solar_wind_box.cpp:527-553), the
+driver of its staggered runs with open sides: a layer of boundary cells
+lies outside the walls (faces, edges and vertices of the box alike,
+grid/solar_wind_box.hpp:268-376); its faces are solved and enter the
+timestep; the step updates interior cells and faces only, a wall face's
+two copies meeting about half way in sync_magnetic_field
+(common_functions.hpp:216-251); after the step the layer is refilled from
+the interior cell each layer cell touches, faces mirrored across the walls
+(apply_boundaries_sw_box, mhd/solar_wind_box.hpp:386-537), and the VALUE
+plane takes its state with the inner cells' shared faces
+(apply_solar_wind_boundaries, :227-306).
+
+  - create: cfg as pamhd_gpu_create, each dimension periodic on both sides
+    or on neither (a dimension of one cell periodic), n[1] at most 262140
+    (else PAMHD_ERR_ARGUMENT); replaces the state a PAMHD program keeps in
     Mas, Mom, Nrj, Vol_B and Face_B (tests/mhd/test.cpp:422-456).
   - set_state / get_state: cells as pamhd_gpu_set_state (eight arrays, x
     fastest; cells[5..7] is the volume field Vol_B) and faces[d] the normal
     field of every cell's -d face (Face_B(-d); a cell's +d face is the -d
-    face of its +d neighbour).  set_state resets the clock; the first step
-    after it is the reference's dt = 0 priming step when called with
-    max_dt = 0.  get_state may be given faces == NULL.
+    face of its +d neighbour), x fastest; along a bounded dimension d,
+    faces[d] holds n[d] + 1 faces per row, the high wall last.  set_state
+    resets the clock and fills the boundary layer; the first step after it
+    is the reference's dt = 0 priming step when called with max_dt = 0.
+    get_state may be given faces == NULL.
+  - set_inflow: time-stamped states of the VALUE side (count timestamps,
+    count + 1 states of 8 conservative values, as pamhd_gpu_set_inflow;
+    the configured value until then); refills the plane at once.
   - step: one step with dt = min(lagged CFL dt, max_dt) as pamhd_gpu_step;
     PAMHD_ERR_PHYSICS when a face failed (the state is left as it was).
   - steps: nsteps steps launched on the context's stream, each capped by
@@ -502,11 +522,14 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** ctx);
 int pamhd_gpu_staggered_destroy(pamhd_stag* ctx);
 int pamhd_gpu_staggered_set_state(pamhd_stag* ctx, const double* const cells[8], const double* const faces[3]);
 int pamhd_gpu_staggered_get_state(pamhd_stag* ctx, double* const cells[8], double* const faces[3]);
+int pamhd_gpu_staggered_set_inflow(pamhd_stag* ctx, int32_t dim, int32_t side, int32_t count, const double* times,
+                                   const double* states);
 /*
 Background magnetic field of every face (the reference's Bg_B, mhd/solve.hpp:120-121):
 bg[3 d + c][cell] is component c at the cell's -d face; NULL removes it.  Rusanov and HLL
 use it in the flux and the fast speeds, HLLD and Roe ignore it (as the reference's solvers,
 mhd/hlld_athena.hpp:77).  The cell state and the faces hold the field without it.
+Periodic grids only (PAMHD_ERR_ARGUMENT on a bounded one).
 */
 int pamhd_gpu_staggered_set_background(pamhd_stag* ctx, const double* const bg[9]);
 int pamhd_gpu_staggered_step(pamhd_stag* ctx, double max_dt, double* dt_taken);

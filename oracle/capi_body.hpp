@@ -229,7 +229,7 @@ int64_t ORACLE_API(grid_run)(void* grid, double t_start, double t_end, int64_t m
 	return steps;
 }
 
-// a staggered-field grid (periodic in every dimension); NULL on an invalid configuration
+// a staggered-field grid (periodic, COPY or VALUE sides); NULL on an invalid configuration
 void* ORACLE_API(sgrid_create)(const pamhd_cfg* cfg)
 {
 	try {
@@ -245,7 +245,8 @@ void ORACLE_API(sgrid_destroy)(void* grid)
 	delete static_cast<SGrid*>(grid);
 }
 
-// cell state (8 arrays) and the normal field of every cell's -x, -y, -z face (3 arrays)
+// cell state (8 arrays) and the normal field of every cell's -x, -y, -z face (3 arrays; along a
+// bounded dimension n + 1 faces, the high wall included)
 int ORACLE_API(sgrid_set_state)(void* grid, const double* const soa[8], const double* const faces[3])
 {
 	try {
@@ -266,6 +267,24 @@ int ORACLE_API(sgrid_set_background)(void* grid, const double* const bg[9])
 int ORACLE_API(sgrid_get_state)(void* grid, double* const soa[8], double* const faces[3])
 {
 	static_cast<SGrid*>(grid)->get_state(soa, faces);
+	return PAMHD_OK;
+}
+
+// time-stamped states of the staggered grid's VALUE side, as grid_set_inflow
+int ORACLE_API(sgrid_set_inflow)(void* grid, int32_t dim, int32_t side, int32_t count, const double* times,
+                                 const double* states)
+{
+	if (count < 0 or (count > 0 and times == nullptr) or states == nullptr) return fail_with("inflow arguments");
+	std::vector<double> t(times, times + count);
+	std::vector<std::array<double, 8>> u(size_t(count) + 1);
+	for (size_t i = 0; i < u.size(); i++) {
+		for (int v = 0; v < 8; v++) u[i][v] = states[8 * i + v];
+	}
+	try {
+		static_cast<SGrid*>(grid)->set_inflow(dim, side, t, u);
+	} catch (const std::exception& e) {
+		return fail_with(e.what());
+	}
 	return PAMHD_OK;
 }
 

@@ -254,8 +254,11 @@ public:
 			if (CType[idx] != 0) continue;
 			int c[3];
 			coords(idx, c);
-			int d = 0;
+			int d = 0, outside = 0;
 			while (c[d] >= 0 and c[d] < n[d]) d++;
+			for (int e = 0; e < 3; e++) outside += (c[e] < 0 or c[e] >= n[e]) ? 1 : 0;
+			// edge and vertex cells of the staggered grid's layer (class 0 there) are its own to fill
+			if (outside > 1) continue;
 			const bool lo = c[d] < 0;
 			const int kind = lo ? cfg.bc_lo[d] : cfg.bc_hi[d];
 			if (kind == PAMHD_BC_VALUE) {

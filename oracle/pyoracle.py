@@ -150,6 +150,8 @@ class Oracle:
         self._sget.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         self._sbg = getattr(L, p + "sgrid_set_background")
         self._sbg.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        self._sinflow = getattr(L, p + "sgrid_set_inflow")
+        self._sinflow.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
         self._sstep = getattr(L, p + "sgrid_step")
         self._sstep.argtypes = [ctypes.c_void_p, _D, _DP, _P(ctypes.c_uint32), _P(ctypes.c_int32),
                                 _P(ctypes.c_int32)]
@@ -332,18 +334,41 @@ class OracleGrid:
         return t.value, hist[:steps]
 
 
+def staggered_face_shapes(n, bc_lo, bc_hi):
+    """Shapes (z, y, x) of the three face arrays of a staggered grid: the -d face of every cell, and
+    along a bounded dimension (not periodic, two cells or more) the high wall too."""
+    shapes = []
+    for d in range(3):
+        ext = [int(n[2]), int(n[1]), int(n[0])]
+        if int(n[d]) > 1 and not (bc_lo[d] == BC_PERIODIC and bc_hi[d] == BC_PERIODIC):
+            ext[2 - d] += 1
+        shapes.append(tuple(ext))
+    return shapes
+
+
 class OracleStaggeredGrid:
-    """A staggered-field grid in the oracle (periodic in every dimension).  Cell state arrays are
-    (8, nz, ny, nx); face field arrays (3, nz, ny, nx): the normal field of every cell's -x, -y
-    and -z face."""
+    """A staggered-field grid in the oracle (periodic, COPY or VALUE sides).  Cell state arrays are
+    (8, nz, ny, nx); face field arrays: the normal field of every cell's -x, -y and -z face, shapes
+    from staggered_face_shapes (n + 1 along a bounded dimension); on a periodic grid the three
+    come as one (3, nz, ny, nx) array."""
 
     def __init__(self, oracle: Oracle, cfg: Cfg):
         self.o = oracle
         self.cfg = cfg
         self.shape = (cfg.n[2], cfg.n[1], cfg.n[0])
+        self.face_shapes = staggered_face_shapes(list(cfg.n), list(cfg.bc_lo), list(cfg.bc_hi))
+        self.periodic = all(s == self.shape for s in self.face_shapes)
         self.h = oracle._screate(ctypes.byref(cfg))
         if not self.h:
             raise ValueError(oracle.last_error())
+
+    def set_inflow(self, dim, side, times, states):
+        """Time-stamped states of the VALUE side, as OracleGrid.set_inflow."""
+        times = np.ascontiguousarray(times, dtype=np.float64).reshape(-1)
+        states = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+        rc = self.o._sinflow(self.h, dim, side, len(times), times.ctypes.data_as(_DP), states.ctypes.data_as(_DP))
+        if rc != 0:
+            raise ValueError(self.o.last_error())
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -356,9 +381,11 @@ class OracleStaggeredGrid:
         fptrs = (ctypes.c_void_p * 3)()
         fkeep = []
         for d in range(3):
-            a = np.ascontiguousarray(faces[d], dtype=np.float64).reshape(-1)
-            fkeep.append(a)
-            fptrs[d] = a.ctypes.data
+            a = np.ascontiguousarray(faces[d], dtype=np.float64)
+            if a.size != int(np.prod(self.face_shapes[d])):
+                raise ValueError(f"faces[{d}]: {self.face_shapes[d]} expected, {a.shape} given")
+            fkeep.append(a.reshape(-1))
+            fptrs[d] = fkeep[-1].ctypes.data
         rc = self.o._sset(self.h, ptrs, fptrs)
         if rc != 0:
             raise ValueError(self.o.last_error())
@@ -376,7 +403,7 @@ class OracleStaggeredGrid:
 
     def get_state(self):
         U = np.zeros((8,) + self.shape)
-        faces = np.zeros((3,) + self.shape)
+        faces = np.zeros((3,) + self.shape) if self.periodic else [np.zeros(s) for s in self.face_shapes]
         ptrs = (ctypes.c_void_p * 8)()
         for k in range(8):
             ptrs[k] = U[k].ctypes.data

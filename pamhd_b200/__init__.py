@@ -354,10 +354,24 @@ class Context:
         return out
 
 
+def staggered_face_shapes(cfg: Config):
+    """Shapes (z, y, x) of the three face arrays of a staggered grid: the -d face of every cell,
+    and along a bounded dimension (not periodic, two cells or more) the high wall as well."""
+    shapes = []
+    for d in range(3):
+        ext = [int(cfg.n[2]), int(cfg.n[1]), int(cfg.n[0])]
+        if int(cfg.n[d]) > 1 and not (cfg.bc_lo[d] == BC_PERIODIC and cfg.bc_hi[d] == BC_PERIODIC):
+            ext[2 - d] += 1
+        shapes.append(tuple(ext))
+    return shapes
+
+
 class StaggeredContext:
     """A pamhd_stag: the staggered-field step (face magnetic field by constrained transport) on
-    one uniform grid periodic in every dimension.  Cell arrays are (8, nz, ny, nx) as Context;
-    face arrays (3, nz, ny, nx): the normal field of every cell's -x, -y and -z face."""
+    one uniform grid, periodic or bounded (COPY / VALUE sides, a layer of boundary cells as the
+    reference's solar-wind box).  Cell arrays are (8, nz, ny, nx) as Context; face arrays: the
+    normal field of every cell's -x, -y and -z face, n + 1 along a bounded dimension
+    (staggered_face_shapes); on a periodic grid the three come as one (3, nz, ny, nx) array."""
 
     def __init__(self, cfg: Config):
         self.cfg = cfg
@@ -375,7 +389,10 @@ class StaggeredContext:
         L.pamhd_gpu_staggered_time.argtypes = [V, _DP, _P(ctypes.c_int64), _DP]
         L.pamhd_gpu_staggered_status.argtypes = [V, _P(ctypes.c_uint32), _P(ctypes.c_int32), _P(ctypes.c_int32)]
         L.pamhd_gpu_staggered_get_stream.argtypes = [V, _P(V)]
+        L.pamhd_gpu_staggered_set_inflow.argtypes = [V, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _DP, _DP]
         self.shape = (int(cfg.n[2]), int(cfg.n[1]), int(cfg.n[0]))
+        self.face_shapes = staggered_face_shapes(cfg)
+        self.periodic = all(f == self.shape for f in self.face_shapes)
         self._c = cfg.to_c()
         h = ctypes.c_void_p()
         rc = L.pamhd_gpu_staggered_create(ctypes.byref(self._c), ctypes.byref(h))
@@ -404,12 +421,28 @@ class StaggeredContext:
         if rc != OK:
             raise PamhdError(rc, what)
 
-    def set_state(self, U: np.ndarray, faces: np.ndarray):
+    def set_state(self, U: np.ndarray, faces):
         U = np.ascontiguousarray(U, dtype=np.float64).reshape((8,) + self.shape)
-        faces = np.ascontiguousarray(faces, dtype=np.float64).reshape((3,) + self.shape)
-        fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
+        arrays = []
+        for d in range(3):
+            a = np.ascontiguousarray(faces[d], dtype=np.float64)
+            if a.shape != self.face_shapes[d]:
+                raise ValueError(f"set_state: faces[{d}] of shape {self.face_shapes[d]} expected, {a.shape} given")
+            arrays.append(a)
+        fp = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in arrays])
         self._check(self.L.pamhd_gpu_staggered_set_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
                     "pamhd_gpu_staggered_set_state")
+
+    def set_inflow(self, dim: int, side: int, times, states):
+        """Time-stamped states of the VALUE side (pamhd_gpu_staggered_set_inflow): states[i] (8
+        conservative values) holds while i of the increasing timestamps are <= the time."""
+        times = np.ascontiguousarray(times, dtype=np.float64).reshape(-1)
+        states = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 8)
+        if len(states) != len(times) + 1:
+            raise ValueError("set_inflow: one more state than timestamps")
+        self._check(self.L.pamhd_gpu_staggered_set_inflow(self.h, int(dim), int(side), len(times),
+                                                          times.ctypes.data_as(_DP), states.ctypes.data_as(_DP)),
+                    "pamhd_gpu_staggered_set_inflow")
 
     def set_background(self, bg):
         """bg: (3, 3, nz, ny, nx), bg[d, c] = component c of the background field at every cell's
@@ -423,10 +456,15 @@ class StaggeredContext:
 
     def get_state(self, out=None):
         """Returns (U, faces); out: an optional pair of C-contiguous float64 arrays of those shapes to
-        fill (pinned host memory makes the copy run at full speed)."""
-        U, faces = out if out is not None else (np.empty((8,) + self.shape), np.empty((3,) + self.shape))
-        for a, rows in ((U, 8), (faces, 3)):
-            if a.shape != (rows,) + self.shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+        fill (pinned host memory makes the copy run at full speed).  faces is one (3, nz, ny, nx)
+        array on a periodic grid, a list of the three face arrays on a bounded one."""
+        if out is None:
+            out = (np.empty((8,) + self.shape),
+                   np.empty((3,) + self.shape) if self.periodic else [np.empty(f) for f in self.face_shapes])
+        U, faces = out
+        checks = [(U, (8,) + self.shape)] + [(faces[d], self.face_shapes[d]) for d in range(3)]
+        for a, shape in checks:
+            if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
                 raise ValueError("get_state: out arrays must be C-contiguous float64 of the state's shapes")
         fp = (ctypes.c_void_p * 3)(*[faces[d].ctypes.data for d in range(3)])
         self._check(self.L.pamhd_gpu_staggered_get_state(self.h, _pointers([U[k].ctypes.data for k in range(8)]), fp),
@@ -442,9 +480,10 @@ class StaggeredContext:
         """Writes the cell state (mass, momentum, energy, volume field) as a reference .dc file,
         the variable the reference's MHD program saves (mhd/save.hpp:75-375)."""
         c = self.cfg
+        periodic = tuple(c.bc_lo[d] == BC_PERIODIC and c.bc_hi[d] == BC_PERIODIC for d in range(3))
         write_dc(path, self.get_state()[0], step=step, time=time, adiabatic_index=c.adiabatic_index,
                  proton_mass=proton_mass, vacuum_permeability=c.vacuum_permeability, cell_length=c.cell_length,
-                 periodic=(True, True, True), start=start)
+                 periodic=periodic, start=start)
 
     def steps(self, n: int, t_end: float):
         self._check(self.L.pamhd_gpu_staggered_steps(self.h, int(n), float(t_end)), "pamhd_gpu_staggered_steps")

@@ -1,7 +1,9 @@
 /*
 The staggered-field MHD step (the reference's timestep() with face magnetic
-field, mhd/solve.hpp:1837-1924) on uniform grids periodic in every
-dimension, behind pamhd_gpu_staggered_* of include/pamhd_gpu.h.
+field, mhd/solve.hpp:1837-1924) on uniform grids, behind
+pamhd_gpu_staggered_* of include/pamhd_gpu.h.  Periodic grids take the
+tiled kernels described here; bounded grids (a layer of boundary cells
+outside the walls) the plain kernels described further down.
 
 Data in HBM, every array x fastest over the n0 x n1 x n2 cells, no ghosts
 (neighbours wrap around):
@@ -73,6 +75,11 @@ struct Stag_Params {
 	double t_end;
 	int kchunk;                      // z planes per face-solve block
 	int fchunk;                      // z planes per face-field block
+	// bounded grids (one layer of boundary cells outside a bounded dimension's walls)
+	int ext[3];                      // 1 along a bounded dimension, 0 along a periodic one
+	int E[3];                        // cells along each dimension, the layer included (N = E0 E1 E2)
+	int value_dim, value_side;       // the VALUE side (value_dim -1: none)
+	const Inflow_Table* inflow;      // its time-stamped states, in device memory
 };
 
 __device__ __forceinline__ long long wrap_index(const Stag_Params& P, int i, int j, int k)
@@ -600,6 +607,418 @@ __global__ void __launch_bounds__(THREADS, 2) cell_kernel(const Stag_Params P)
 	}
 }
 
+/*
+Bounded grids.  The arrays hold the grid with its layer of boundary cells
+(E = n + 2 ext cells per dimension, x fastest); periodic dimensions wrap as
+above.  The layer follows the reference's solar-wind box (every layer cell a
+boundary cell, faces, edges and vertices alike; grid/solar_wind_box.hpp:
+268-376): its faces are solved and their speeds enter the timestep, its
+cells are refilled from the interior after each step
+(apply_boundaries_sw_box, mhd/solar_wind_box.hpp:386-537) and the VALUE
+side's plane from its table (apply_solar_wind_boundaries, :227-306).  One
+step is five launches, each a grid-stride loop of one thread per cell:
+  bounded_faces_kernel  every cell's -d faces that have a cell on both sides;
+  bounded_field_kernel  the new normal field of the interior cells' faces,
+                        the walls of bounded dimensions included;
+  bounded_cell_kernel   the interior cells' update, then update_vol_B, the
+                        walls' copy sync (sync_magnetic_field: the boundary
+                        cell's copy of a wall face is not updated, and the
+                        two copies meet about half way), update_vol_B again;
+  layer_fill_kernel     the layer from the interior;
+  value_fill_kernel     the VALUE plane and the cells on its inner side.
+*/
+__device__ __forceinline__ int wrap_or_keep(const Stag_Params& P, const int d, const int c)
+{
+	if (P.ext[d]) return c;
+	return c < 0 ? c + P.n[d] : (c >= P.n[d] ? c - P.n[d] : c);
+}
+
+// linear index of cell (i, j, k), layer coordinates -1 .. n (periodic dimensions wrap)
+__device__ __forceinline__ long long ext_index(const Stag_Params& P, const int i, const int j, const int k)
+{
+	return (long long)(wrap_or_keep(P, 0, i) + P.ext[0])
+		+ (long long)P.E[0] * ((long long)(wrap_or_keep(P, 1, j) + P.ext[1])
+		                       + (long long)P.E[1] * (wrap_or_keep(P, 2, k) + P.ext[2]));
+}
+
+__device__ __forceinline__ void ext_coords(const Stag_Params& P, const long long c, int x[3])
+{
+	x[0] = int(c % P.E[0]) - P.ext[0];
+	x[1] = int((c / P.E[0]) % P.E[1]) - P.ext[1];
+	x[2] = int(c / ((long long)P.E[0] * P.E[1])) - P.ext[2];
+}
+
+// total energy density from thermal pressure (get_total_energy_density, mhd/common.hpp:258-311)
+__device__ __forceinline__ double energy(const double u[8], const double p, const Gas& g)
+{
+	const double inv = 1 / u[0];
+	const double v0 = u[1] * inv, v1 = u[2] * inv, v2 = u[3] * inv;
+	const double kinetic = 0.5 * u[0] * (v0 * v0 + v1 * v1 + v2 * v2);
+	const double magnetic = 0.5 / g.mu0 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
+	return p / (g.gamma - 1) + kinetic + magnetic;
+}
+
+// the -A face of cell c (coordinates x) against its -A neighbour, both derived along A only
+template <int SOLVER, int A>
+__device__ __forceinline__ void bounded_minus_face(const Stag_Params& P, const long long c, const int x[3],
+                                                   const double Uc[8], double& smax, bool& zero)
+{
+	int m[3] = {x[0], x[1], x[2]};
+	m[A] -= 1;
+	const long long mi = ext_index(P, m[0], m[1], m[2]);
+	double Um[8];
+	#pragma unroll
+	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + mi);
+	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7], P.gas);
+	const Derived dc = derive<A == 0, A == 1, A == 2>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
+	double G[8];
+	uint32_t flag = 0;
+	const double s = solve_face<SOLVER>(side_of<A>(Um, dm), side_of<A>(Uc, dc), P.gas, G, flag);
+	if (flag != 0) record_failure(P, flag, mi, A);
+	smax = fmax(smax, s);
+	zero = zero or not (s > 0.0);
+	double out[8];
+	out[0] = G[0];
+	unrotate<A>(G[1], G[2], G[3], out[1], out[2], out[3]);
+	out[4] = G[4];
+	unrotate<A>(G[5], G[6], G[7], out[5], out[6], out[7]);
+	#pragma unroll
+	for (int v = 0; v < 8; v++) P.F[(A * 8 + v) * P.N + c] = out[v];
+}
+
+template <int SOLVER>
+__global__ void __launch_bounds__(THREADS) bounded_faces_kernel(const Stag_Params P)
+{
+	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+	bool zero = false;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		int x[3];
+		ext_coords(P, c, x);
+		double Uc[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) Uc[v] = __ldg(P.U + v * P.N + c);
+		// a layer cell's -d face past the low wall has no cell on its other side
+		if (not (P.ext[0] and x[0] < 0)) bounded_minus_face<SOLVER, 0>(P, c, x, Uc, s0, zero);
+		if (not (P.ext[1] and x[1] < 0)) bounded_minus_face<SOLVER, 1>(P, c, x, Uc, s1, zero);
+		if (not (P.ext[2] and x[2] < 0)) bounded_minus_face<SOLVER, 2>(P, c, x, Uc, s2, zero);
+	}
+	s0 = warp_max(s0);
+	s1 = warp_max(s1);
+	s2 = warp_max(s2);
+	const bool any_zero = __any_sync(0xffffffffu, zero);
+	if ((threadIdx.x & 31) == 0) {
+		Speed_Max& r = P.red[(P.phase + 1) % 3];
+		atomicMax(&r.smax[0], (unsigned long long)__double_as_longlong(s0));
+		atomicMax(&r.smax[1], (unsigned long long)__double_as_longlong(s1));
+		atomicMax(&r.smax[2], (unsigned long long)__double_as_longlong(s2));
+		if (any_zero) atomicOr(&r.zero, 1u);
+	}
+}
+
+// whether the -D face of cell x is one the step updates: an interior cell's, or a high wall's
+template <int D>
+__device__ __forceinline__ bool updated_face(const Stag_Params& P, const int x[3])
+{
+	#pragma unroll
+	for (int e = 0; e < 3; e++) {
+		const int top = P.n[e] + ((e == D and P.ext[e]) ? 1 : 0);
+		if (x[e] < 0 or x[e] >= top) return false;
+	}
+	return true;
+}
+
+template <int D>
+__device__ __forceinline__ void bounded_face_update(const Stag_Params& P, const long long c, const int x[3],
+                                                    const double dt)
+{
+	if (not updated_face<D>(P, x)) {
+		P.Bo[D * P.N + c] = P.B[D * P.N + c];
+		return;
+	}
+	auto get = [&](const int axis, const int comp, const int ox, const int oy, const int oz) {
+		return P.F[(axis * 8 + 5 + comp) * P.N + ext_index(P, x[0] + ox, x[1] + oy, x[2] + oz)];
+	};
+	P.Bo[D * P.N + c] = P.B[D * P.N + c] + face_dB<D>(P, get, dt) / P.area[D];
+}
+
+__global__ void __launch_bounds__(THREADS) bounded_field_kernel(const Stag_Params P)
+{
+	__shared__ double s_dt;
+	__shared__ int s_skip;
+	if (threadIdx.x == 0) {
+		bool skip;
+		s_dt = step_start(P, skip);
+		s_skip = skip ? 1 : 0;
+	}
+	__syncthreads();
+	const double dt = s_dt;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
+		if (s_skip != 0) {
+			#pragma unroll
+			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
+			continue;
+		}
+		int x[3];
+		ext_coords(P, c, x);
+		bounded_face_update<0>(P, c, x, dt);
+		bounded_face_update<1>(P, c, x, dt);
+		bounded_face_update<2>(P, c, x, dt);
+	}
+}
+
+/*
+sync_magnetic_field on a wall face (common_functions.hpp:216-251): the
+boundary cell's copy `old`, the interior cell's `updated`; the cells in
+index order, each visit moving the visitor's copy down by half the
+difference and the other's up by as much.  Returns the interior copy.
+*/
+__device__ __forceinline__ double wall_sync(const double old, const double updated, const bool lo_wall)
+{
+	if (lo_wall) {
+		const double diff1 = old - updated;
+		const double g1 = old - diff1 / 2, p1 = updated + diff1 / 2;
+		const double diff2 = p1 - g1;
+		return p1 - diff2 / 2;
+	}
+	const double diff1 = updated - old;
+	const double p1 = updated - diff1 / 2, g1 = old + diff1 / 2;
+	const double diff2 = g1 - p1;
+	return p1 + diff2 / 2;
+}
+
+__global__ void __launch_bounds__(THREADS) bounded_cell_kernel(const Stag_Params P)
+{
+	__shared__ double s_dt;
+	__shared__ int s_skip;
+	if (threadIdx.x == 0) {
+		bool skip;
+		const double dt = step_start(P, skip);
+		s_dt = dt;
+		s_skip = skip ? 1 : 0;
+		if (blockIdx.x == 0) {
+			const Clock c = P.clock[P.phase];
+			Clock& next = P.clock[(P.phase + 1) % 3];
+			next.t = skip ? c.t : c.t + dt;
+			next.dt = skip ? c.dt : dt;
+			next.steps = skip ? c.steps : c.steps + 1;
+			Speed_Max& z = P.red[(P.phase + 2) % 3];
+			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
+			z.zero = 0u;
+		}
+	}
+	__syncthreads();
+	const double dt = s_dt;
+	const bool skip = s_skip != 0;
+	const long long N = P.N;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
+		int x[3];
+		ext_coords(P, c, x);
+		const bool inside = x[0] >= 0 and x[0] < P.n[0] and x[1] >= 0 and x[1] < P.n[1] and x[2] >= 0
+			and x[2] < P.n[2];
+		if (skip or not inside) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) P.Uo[v * N + c] = P.U[v * N + c];
+			continue;
+		}
+		const long long up[3] = {ext_index(P, x[0] + 1, x[1], x[2]), ext_index(P, x[0], x[1] + 1, x[2]),
+		                         ext_index(P, x[0], x[1], x[2] + 1)};
+		double Fm[3][8], Fp[3][8], bm[3], bp[3];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int v = 0; v < 8; v++) {
+				Fm[d][v] = P.F[(d * 8 + v) * N + c];
+				Fp[d][v] = P.F[(d * 8 + v) * N + up[d]];
+			}
+			bm[d] = P.Bo[d * N + c];
+			bp[d] = P.Bo[d * N + up[d]];
+		}
+		auto fm = [&](const int d, const int v) { return 0 + dt * Fm[d][v]; };
+		auto fp = [&](const int d, const int v) { return 0 + dt * Fp[d][v]; };
+		double u[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) u[v] = P.U[v * N + c];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) u[0] += (fm(d, 0) - fp(d, 0)) / P.len[d];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int e = 1; e <= 3; e++) u[e] = u[e] + P.inv_len[d] * (fm(d, e) + (-fp(d, e)));
+		}
+		#pragma unroll
+		for (int d = 0; d < 3; d++) u[4] += (fm(d, 4) - fp(d, 4)) / P.len[d];
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			#pragma unroll
+			for (int e = 5; e <= 7; e++) u[e] = u[e] + P.inv_len[d] * (fm(d, e) + (-fp(d, e)));
+		}
+		const double mean1[3] = {0.5 * (bm[0] + bp[0]), 0.5 * (bm[1] + bp[1]), 0.5 * (bm[2] + bp[2])};
+		vol_B_constant_pressure(u, mean1, P.gas);
+		// the walls' copies (this cell is the only interior cell on each of its walls)
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			if (not P.ext[d]) continue;
+			if (x[d] == 0) {
+				bm[d] = wall_sync(P.B[d * N + c], bm[d], true);
+				P.Bo[d * N + c] = bm[d];
+			}
+			if (x[d] == P.n[d] - 1) {
+				bp[d] = wall_sync(P.B[d * N + up[d]], bp[d], false);
+				P.Bo[d * N + up[d]] = bp[d];
+			}
+		}
+		const double mean2[3] = {0.5 * (bm[0] + bp[0]), 0.5 * (bm[1] + bp[1]), 0.5 * (bm[2] + bp[2])};
+		vol_B_constant_pressure(u, mean2, P.gas);
+		#pragma unroll
+		for (int v = 0; v < 8; v++) P.Uo[v * N + c] = u[v];
+	}
+}
+
+/*
+The layer from the interior (apply_boundaries_sw_box, mhd/solar_wind_box.hpp:
+386-537), into the arrays U, B: each layer cell from the interior cell it
+touches through a face, an edge or a vertex; its faces from that cell's,
+mirrored across the walls it lies behind; volume field the face means;
+total energy from the source cell's thermal pressure.  Reads interior cells
+and the faces they hold only, writes layer cells and the faces they hold, so
+the threads never meet.  check: skip when the step was skipped.
+*/
+__global__ void __launch_bounds__(THREADS) layer_fill_kernel(const Stag_Params P, double* U, double* B,
+                                                             const bool check)
+{
+	if (check) {
+		bool skip;
+		step_start(P, skip);
+		if (skip) return;
+	}
+	const long long N = P.N;
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
+		int x[3], s[3];
+		ext_coords(P, c, x);
+		bool shell[3], any = false;
+		#pragma unroll
+		for (int d = 0; d < 3; d++) {
+			shell[d] = x[d] < 0 or x[d] >= P.n[d];
+			any = any or shell[d];
+			s[d] = x[d] < 0 ? 0 : (x[d] >= P.n[d] ? P.n[d] - 1 : x[d]);
+		}
+		if (not any) continue;
+		const long long src = ext_index(P, s[0], s[1], s[2]);
+		double u[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) u[v] = U[v * N + src];
+		const double p = pressure(u, P.gas);
+		#pragma unroll
+		for (int e = 0; e < 3; e++) {
+			int o[3] = {s[0], s[1], s[2]};
+			o[e] += 1;
+			const double lo = B[e * N + src], hi = B[e * N + ext_index(P, o[0], o[1], o[2])];
+			int f[3] = {s[0], s[1], s[2]};
+			f[e] = (shell[e] and x[e] < 0) ? 1 : x[e];
+			const long long fi = ext_index(P, f[0], f[1], f[2]);
+			if (fi != c) B[e * N + c] = B[e * N + fi];
+			u[5 + e] = shell[e] ? 0.5 * (hi + lo) : 0.5 * (lo + hi);
+		}
+		u[4] = energy(u, p, P.gas);
+		#pragma unroll
+		for (int v = 0; v < 8; v++) U[v * N + c] = u[v];
+	}
+}
+
+__device__ __forceinline__ const double* table_state(const Inflow_Table& T, const double t)
+{
+	int i = 0;
+	while (i < T.count and t >= T.times[i]) i++;
+	return T.states + 8 * i;
+}
+
+/*
+The VALUE plane (apply_solar_wind_boundaries, mhd/solar_wind_box.hpp:227-306)
+at the time in clock slot tslot: its cells take the table's state, every
+face of theirs its field; each cell on the plane's inner side gets the
+state's normal field on the face it shares with the plane, half of each of
+its two faces along that dimension as its volume field component, and its
+total energy from its thermal pressure before the change.  One thread per
+plane cell.
+*/
+__global__ void __launch_bounds__(THREADS) value_fill_kernel(const Stag_Params P, double* U, double* B,
+                                                             const int tslot, const bool check)
+{
+	if (check) {
+		bool skip;
+		step_start(P, skip);
+		if (skip) return;
+	}
+	const int d = P.value_dim, a = (d + 1) % 3, b = (d + 2) % 3;
+	const bool lo = P.value_side == 0;
+	const double* v = table_state(*P.inflow, P.clock[tslot].t);
+	const long long N = P.N, count = (long long)P.E[a] * P.E[b];
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += stride) {
+		int x[3];
+		x[d] = lo ? -1 : P.n[d];
+		x[a] = int(t % P.E[a]) - P.ext[a];
+		x[b] = int(t / P.E[a]) - P.ext[b];
+		const long long c = ext_index(P, x[0], x[1], x[2]);
+		#pragma unroll
+		for (int k = 0; k < 8; k++) U[k * N + c] = v[k];
+		#pragma unroll
+		for (int e = 0; e < 3; e++) B[e * N + c] = v[5 + e];
+		int q[3] = {x[0], x[1], x[2]};
+		q[d] = lo ? 0 : P.n[d] - 1;
+		const long long qi = ext_index(P, q[0], q[1], q[2]);
+		q[d] += 1;
+		const long long qu = ext_index(P, q[0], q[1], q[2]);
+		const long long shared = lo ? qi : qu, other = lo ? qu : qi;
+		double u[8];
+		#pragma unroll
+		for (int k = 0; k < 8; k++) u[k] = U[k * N + qi];
+		const double p = pressure(u, P.gas);
+		B[d * N + shared] = v[5 + d];
+		u[5 + d] = B[d * N + shared] / 2 + B[d * N + other] / 2;
+		u[4] = energy(u, p, P.gas);
+		#pragma unroll
+		for (int k = 0; k < 8; k++) U[k * N + qi] = u[k];
+	}
+}
+
+// interior cells and faces between the packed arrays of the ABI and the layered ones
+__global__ void __launch_bounds__(THREADS) bounded_pack_kernel(const Stag_Params P, double* U, double* B,
+                                                               double* packed, const bool to_packed)
+{
+	const long long cells = (long long)P.n[0] * P.n[1] * P.n[2];
+	long long fcount[3], total = 8 * cells;
+	#pragma unroll
+	for (int d = 0; d < 3; d++) {
+		fcount[d] = cells / P.n[d] * (P.n[d] + P.ext[d]);
+		total += fcount[d];
+	}
+	const long long stride = (long long)gridDim.x * blockDim.x;
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
+		double* dev;
+		if (t < 8 * cells) {
+			const int v = int(t / cells);
+			const long long r = t - v * cells;
+			const int i = int(r % P.n[0]), j = int((r / P.n[0]) % P.n[1]), k = int(r / ((long long)P.n[0] * P.n[1]));
+			dev = U + v * P.N + ext_index(P, i, j, k);
+		} else {
+			long long r = t - 8 * cells;
+			int d = 0;
+			while (r >= fcount[d]) r -= fcount[d++];
+			int ext[3] = {P.n[0], P.n[1], P.n[2]};
+			ext[d] += P.ext[d];
+			const int i = int(r % ext[0]), j = int((r / ext[0]) % ext[1]), k = int(r / ((long long)ext[0] * ext[1]));
+			dev = B + d * P.N + ext_index(P, i, j, k);
+		}
+		if (to_packed) packed[t] = *dev;
+		else *dev = packed[t];
+	}
+}
+
 // the face kernels' shared memory above the default 48 KB, once per kernel
 template <int SOLVER>
 int allow_face_smem()
@@ -635,6 +1054,22 @@ int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
+// the five launches of a step on a bounded grid
+template <int SOLVER>
+int launch_bounded(const Stag_Params& P, const int grid, cudaStream_t stream)
+{
+	bounded_faces_kernel<SOLVER><<<grid, THREADS, 0, stream>>>(P);
+	bounded_field_kernel<<<grid, THREADS, 0, stream>>>(P);
+	bounded_cell_kernel<<<grid, THREADS, 0, stream>>>(P);
+	layer_fill_kernel<<<grid, THREADS, 0, stream>>>(P, P.Uo, P.Bo, true);
+	if (P.value_dim >= 0) {
+		const long long count = (long long)P.E[(P.value_dim + 1) % 3] * P.E[(P.value_dim + 2) % 3];
+		value_fill_kernel<<<int((count + THREADS - 1) / THREADS), THREADS, 0, stream>>>(
+			P, P.Uo, P.Bo, (P.phase + 1) % 3, true);
+	}
+	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
+}
+
 int check(const cudaError_t e)
 {
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
@@ -660,6 +1095,11 @@ struct pamhd_stag {
 	long long steps = 0;         // launched steps since set_state (the ring phase)
 	int grid = 0;
 	bool loaded = false;
+	bool bounded = false;        // a layer of boundary cells outside some walls
+	long long packed = 0;        // doubles of the ABI's state arrays (cells and faces)
+	double* stage = nullptr;     // device staging of those arrays (bounded grids)
+	Inflow_Table* table = nullptr;   // the VALUE side's table in device memory
+	double* table_data = nullptr;    // its timestamps and states
 	Stag_Params base;
 };
 
@@ -682,12 +1122,22 @@ int issue(pamhd_stag& x, const double max_dt, const double t_end)
 {
 	const Stag_Params P = params_of(x, max_dt, t_end);
 	int rc = PAMHD_ERR_ARGUMENT;
-	switch (x.cfg.solver) {
-	case PAMHD_RUSANOV: rc = launch_pair<PAMHD_RUSANOV>(P, x.grid, x.stream); break;
-	case PAMHD_HLL_ATHENA: rc = launch_pair<PAMHD_HLL_ATHENA>(P, x.grid, x.stream); break;
-	case PAMHD_HLLD_ATHENA: rc = launch_pair<PAMHD_HLLD_ATHENA>(P, x.grid, x.stream); break;
-	case PAMHD_ROE_ATHENA: rc = launch_pair<PAMHD_ROE_ATHENA>(P, x.grid, x.stream); break;
-	default: break;
+	if (x.bounded) {
+		switch (x.cfg.solver) {
+		case PAMHD_RUSANOV: rc = launch_bounded<PAMHD_RUSANOV>(P, x.grid, x.stream); break;
+		case PAMHD_HLL_ATHENA: rc = launch_bounded<PAMHD_HLL_ATHENA>(P, x.grid, x.stream); break;
+		case PAMHD_HLLD_ATHENA: rc = launch_bounded<PAMHD_HLLD_ATHENA>(P, x.grid, x.stream); break;
+		case PAMHD_ROE_ATHENA: rc = launch_bounded<PAMHD_ROE_ATHENA>(P, x.grid, x.stream); break;
+		default: break;
+		}
+	} else {
+		switch (x.cfg.solver) {
+		case PAMHD_RUSANOV: rc = launch_pair<PAMHD_RUSANOV>(P, x.grid, x.stream); break;
+		case PAMHD_HLL_ATHENA: rc = launch_pair<PAMHD_HLL_ATHENA>(P, x.grid, x.stream); break;
+		case PAMHD_HLLD_ATHENA: rc = launch_pair<PAMHD_HLLD_ATHENA>(P, x.grid, x.stream); break;
+		case PAMHD_ROE_ATHENA: rc = launch_pair<PAMHD_ROE_ATHENA>(P, x.grid, x.stream); break;
+		default: break;
+		}
 	}
 	if (rc != PAMHD_OK) return rc;
 	x.cur ^= 1;
@@ -708,23 +1158,83 @@ int reset_ring(pamhd_stag& x)
 	return check(cudaStreamSynchronize(x.stream));
 }
 
+// a dimension with a layer of boundary cells: not periodic, two cells or more
+bool bounded_dim(const pamhd_cfg& c, const int d)
+{
+	return c.n[d] > 1 and not (c.bc_lo[d] == PAMHD_BC_PERIODIC and c.bc_hi[d] == PAMHD_BC_PERIODIC);
+}
+
 int validate_stag(const pamhd_cfg& c)
 {
 	if (c.solver != PAMHD_RUSANOV and c.solver != PAMHD_HLL_ATHENA and c.solver != PAMHD_HLLD_ATHENA
 		and c.solver != PAMHD_ROE_ATHENA) {
 		return PAMHD_ERR_ARGUMENT;
 	}
+	int values = 0;
+	long long N = 1;
 	for (int d = 0; d < 3; d++) {
 		if (c.n[d] < 1 or not (c.cell_length[d] > 0.0)) return PAMHD_ERR_ARGUMENT;
-		if (c.bc_lo[d] != PAMHD_BC_PERIODIC or c.bc_hi[d] != PAMHD_BC_PERIODIC) return PAMHD_ERR_ARGUMENT;
+		const int kinds[2] = {c.bc_lo[d], c.bc_hi[d]};
+		for (const int k: kinds) {
+			if (k != PAMHD_BC_PERIODIC and k != PAMHD_BC_COPY and k != PAMHD_BC_VALUE) return PAMHD_ERR_ARGUMENT;
+			if (k == PAMHD_BC_VALUE) values++;
+		}
+		// periodic on both sides or on neither; a dimension of one cell is its own (periodic) neighbour
+		if ((kinds[0] == PAMHD_BC_PERIODIC) != (kinds[1] == PAMHD_BC_PERIODIC)) return PAMHD_ERR_ARGUMENT;
+		if (c.n[d] == 1 and kinds[0] != PAMHD_BC_PERIODIC) return PAMHD_ERR_ARGUMENT;
+		N *= c.n[d] + (bounded_dim(c, d) ? 2 : 0);
 	}
+	if (values > 1) return PAMHD_ERR_ARGUMENT;   // one inflow side, as the solar-wind box's
 	if (not (c.adiabatic_index > 1.0) or not (c.vacuum_permeability > 0.0) or not (c.time_step_factor > 0.0)) {
 		return PAMHD_ERR_ARGUMENT;
 	}
-	const long long N = (long long)c.n[0] * c.n[1] * c.n[2];
 	if (N > (1ll << 31)) return PAMHD_ERR_ARGUMENT;
 	if ((c.n[1] + STY - 1) / STY > 65535) return PAMHD_ERR_ARGUMENT;   // rows of face tiles: the grid's y extent
 	return PAMHD_OK;
+}
+
+// the VALUE side's table: count timestamps, count + 1 states of 8 doubles (host memory)
+int upload_table(pamhd_stag& x, const int32_t count, const double* times, const double* states)
+{
+	const size_t nt = size_t(count), ns = 8 * (size_t(count) + 1);
+	double* data = nullptr;
+	PAMHD_TRY(check(cudaMalloc(&data, (nt + ns) * sizeof(double))));
+	Inflow_Table t;
+	t.times = data;
+	t.states = data + nt;
+	t.count = count;
+	if ((nt > 0 and cudaMemcpy(data, times, nt * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+		or cudaMemcpy(data + nt, states, ns * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess
+		or cudaMemcpy(x.table, &t, sizeof t, cudaMemcpyHostToDevice) != cudaSuccess) {
+		cudaFree(data);
+		return PAMHD_ERR_CUDA;
+	}
+	cudaFree(x.table_data);
+	x.table_data = data;
+	return PAMHD_OK;
+}
+
+// the layer (and the VALUE plane) of the current state from its interior, at the current time
+int fill_layer(pamhd_stag& x)
+{
+	Stag_Params P = params_of(x, -1.0, 0.0);
+	double* U = x.U[x.cur];
+	double* B = x.B[x.cur];
+	layer_fill_kernel<<<x.grid, THREADS, 0, x.stream>>>(P, U, B, false);
+	if (P.value_dim >= 0) {
+		const long long count = (long long)P.E[(P.value_dim + 1) % 3] * P.E[(P.value_dim + 2) % 3];
+		value_fill_kernel<<<int((count + THREADS - 1) / THREADS), THREADS, 0, x.stream>>>(P, U, B, P.phase, false);
+	}
+	return check(cudaGetLastError());
+}
+
+// doubles of one array of the ABI: cell variable v (face < 0) or the faces normal to axis `face`
+size_t packed_length(const pamhd_cfg& c, const int v, const int face)
+{
+	(void)v;
+	size_t len = 1;
+	for (int d = 0; d < 3; d++) len *= size_t(c.n[d] + ((d == face and bounded_dim(c, d)) ? 1 : 0));
+	return len;
 }
 
 } // namespace
@@ -740,7 +1250,15 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
 	x->cfg = *cfg;
 	x->device = cfg->device;
-	x->N = (long long)cfg->n[0] * cfg->n[1] * cfg->n[2];
+	int ext[3];
+	x->N = 1;
+	x->packed = 8ll * cfg->n[0] * cfg->n[1] * cfg->n[2];
+	for (int d = 0; d < 3; d++) {
+		ext[d] = bounded_dim(*cfg, d) ? 1 : 0;
+		x->bounded = x->bounded or ext[d] != 0;
+		x->N *= cfg->n[d] + 2 * ext[d];
+		x->packed += (long long)cfg->n[0] * cfg->n[1] * cfg->n[2] / cfg->n[d] * (cfg->n[d] + ext[d]);
+	}
 	auto fail = [&](const int rc) {
 		pamhd_gpu_staggered_destroy(x);
 		return rc;
@@ -756,6 +1274,9 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
 		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
 		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess) {
+		return fail(PAMHD_ERR_CUDA);
+	}
+	if (x->bounded and cudaMalloc(&x->stage, size_t(x->packed) * sizeof(double)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
 	int sms = 0;
@@ -805,6 +1326,22 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 	P.red = x->red;
 	P.clock = x->clock;
 	P.status = x->status;
+	P.value_dim = -1;
+	for (int d = 0; d < 3; d++) {
+		P.ext[d] = ext[d];
+		P.E[d] = cfg->n[d] + 2 * ext[d];
+		if (ext[d] and (cfg->bc_lo[d] == PAMHD_BC_VALUE or cfg->bc_hi[d] == PAMHD_BC_VALUE)) {
+			P.value_dim = d;
+			P.value_side = cfg->bc_lo[d] == PAMHD_BC_VALUE ? 0 : 1;
+		}
+	}
+	if (P.value_dim >= 0) {
+		// a constant table: the configured state until pamhd_gpu_staggered_set_inflow gives one
+		if (cudaMalloc(&x->table, sizeof(Inflow_Table)) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
+		const double* v = P.value_side == 0 ? cfg->value_lo[P.value_dim] : cfg->value_hi[P.value_dim];
+		if (upload_table(*x, 0, nullptr, v) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
+		P.inflow = x->table;
+	}
 	if (cudaMemsetAsync(x->U[0], 0, 8 * n * sizeof(double), x->stream) != cudaSuccess
 		or cudaMemsetAsync(x->B[0], 0, 3 * n * sizeof(double), x->stream) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
@@ -828,6 +1365,9 @@ int pamhd_gpu_staggered_destroy(pamhd_stag* x)
 	cudaFree(x->red);
 	cudaFree(x->clock);
 	cudaFree(x->status);
+	cudaFree(x->stage);
+	cudaFree(x->table);
+	cudaFree(x->table_data);
 	if (x->stream != nullptr) cudaStreamDestroy(x->stream);
 	delete x;
 	return PAMHD_OK;
@@ -842,6 +1382,31 @@ int pamhd_gpu_staggered_set_state(pamhd_stag* x, const double* const cells[8], c
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
 	const size_t n = size_t(x->N);
 	x->cur = 0;
+	if (x->bounded) {
+		// the caller's arrays into the staging buffer, from there into the layered arrays; then the
+		// layer from the interior at time 0
+		size_t at = 0;
+		for (int v = 0; v < 8; v++) {
+			const size_t len = packed_length(x->cfg, v, -1);
+			PAMHD_TRY(check(cudaMemcpyAsync(x->stage + at, cells[v], len * sizeof(double), cudaMemcpyHostToDevice,
+			                                x->stream)));
+			at += len;
+		}
+		for (int d = 0; d < 3; d++) {
+			const size_t len = packed_length(x->cfg, 0, d);
+			PAMHD_TRY(check(cudaMemcpyAsync(x->stage + at, faces[d], len * sizeof(double), cudaMemcpyHostToDevice,
+			                                x->stream)));
+			at += len;
+		}
+		PAMHD_TRY(reset_ring(*x));
+		const Stag_Params P = params_of(*x, -1.0, 0.0);
+		bounded_pack_kernel<<<x->grid, THREADS, 0, x->stream>>>(P, x->U[0], x->B[0], x->stage, false);
+		PAMHD_TRY(check(cudaGetLastError()));
+		PAMHD_TRY(fill_layer(*x));
+		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+		x->loaded = true;
+		return PAMHD_OK;
+	}
 	// one copy per array straight from the caller's memory (at full speed when it is pinned)
 	for (int v = 0; v < 8; v++) {
 		PAMHD_TRY(check(cudaMemcpyAsync(x->U[0] + v * n, cells[v], n * sizeof(double), cudaMemcpyHostToDevice,
@@ -856,6 +1421,26 @@ int pamhd_gpu_staggered_set_state(pamhd_stag* x, const double* const cells[8], c
 	return PAMHD_OK;
 }
 
+int pamhd_gpu_staggered_set_inflow(pamhd_stag* x, const int32_t dim, const int32_t side, const int32_t count,
+                                   const double* times, const double* states)
+{
+	if (x == nullptr or dim < 0 or dim > 2 or (side != 0 and side != 1) or count < 0) return PAMHD_ERR_ARGUMENT;
+	if ((count > 0 and times == nullptr) or states == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x->base.value_dim != dim or x->base.value_side != side) return PAMHD_ERR_ARGUMENT;
+	for (int i = 0; i < count; i++) {
+		if (not std::isfinite(times[i]) or (i > 0 and not (times[i] > times[i - 1]))) return PAMHD_ERR_ARGUMENT;
+	}
+	PAMHD_TRY(check(cudaSetDevice(x->device)));
+	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	PAMHD_TRY(upload_table(*x, count, times, states));
+	// the plane of the current state at the current time
+	if (x->loaded) {
+		PAMHD_TRY(fill_layer(*x));
+		PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
+	}
+	return PAMHD_OK;
+}
+
 int pamhd_gpu_staggered_set_background(pamhd_stag* x, const double* const bg[9])
 {
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
@@ -866,6 +1451,7 @@ int pamhd_gpu_staggered_set_background(pamhd_stag* x, const double* const bg[9])
 		return PAMHD_OK;
 	}
 	for (int k = 0; k < 9; k++) if (bg[k] == nullptr) return PAMHD_ERR_ARGUMENT;
+	if (x->bounded) return PAMHD_ERR_ARGUMENT;   // a background field on periodic grids only
 	const size_t n = size_t(x->N);
 	if (x->bg == nullptr) PAMHD_TRY(check(cudaMalloc(&x->bg, 9 * n * sizeof(double))));
 	for (int k = 0; k < 9; k++) {
@@ -885,6 +1471,25 @@ int pamhd_gpu_staggered_get_state(pamhd_stag* x, double* const cells[8], double*
 	if (not x->loaded) return PAMHD_ERR_STATE;
 	PAMHD_TRY(check(cudaSetDevice(x->device)));
 	const size_t n = size_t(x->N);
+	if (x->bounded) {
+		const Stag_Params P = params_of(*x, -1.0, 0.0);
+		bounded_pack_kernel<<<x->grid, THREADS, 0, x->stream>>>(P, x->U[x->cur], x->B[x->cur], x->stage, true);
+		PAMHD_TRY(check(cudaGetLastError()));
+		size_t at = 0;
+		for (int v = 0; v < 8; v++) {
+			const size_t len = packed_length(x->cfg, v, -1);
+			PAMHD_TRY(check(cudaMemcpyAsync(cells[v], x->stage + at, len * sizeof(double), cudaMemcpyDeviceToHost,
+			                                x->stream)));
+			at += len;
+		}
+		for (int d = 0; faces != nullptr and d < 3; d++) {
+			const size_t len = packed_length(x->cfg, 0, d);
+			PAMHD_TRY(check(cudaMemcpyAsync(faces[d], x->stage + at, len * sizeof(double), cudaMemcpyDeviceToHost,
+			                                x->stream)));
+			at += len;
+		}
+		return check(cudaStreamSynchronize(x->stream));
+	}
 	for (int v = 0; v < 8; v++) {
 		PAMHD_TRY(check(cudaMemcpyAsync(cells[v], x->U[x->cur] + v * n, n * sizeof(double), cudaMemcpyDeviceToHost,
 		                                x->stream)));
@@ -956,10 +1561,13 @@ int pamhd_gpu_staggered_status(pamhd_stag* x, uint32_t* flags, int32_t cell[3], 
 	if (s.flags != 0u and s.first != ~0ull) {
 		const long long key = (long long)(s.first >> 8);
 		const long long c = key / 3;
+		// the face's negative cell, in layer coordinates (-1 .. n along a bounded dimension)
+		const int* E = x->base.E;
+		const int* ext = x->base.ext;
 		if (cell != nullptr) {
-			cell[0] = int32_t(c % x->cfg.n[0]);
-			cell[1] = int32_t((c / x->cfg.n[0]) % x->cfg.n[1]);
-			cell[2] = int32_t(c / ((long long)x->cfg.n[0] * x->cfg.n[1]));
+			cell[0] = int32_t(c % E[0]) - ext[0];
+			cell[1] = int32_t((c / E[0]) % E[1]) - ext[1];
+			cell[2] = int32_t(c / ((long long)E[0] * E[1])) - ext[2];
 		}
 		if (dir != nullptr) *dir = int32_t(key % 3) + 1;
 	} else {

@@ -90,8 +90,11 @@ def test_any_active_dimensions_pass_the_checks(lib, n):
 
 
 @pytest.mark.parametrize("change", [
-    dict(bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0)),   # the staggered step is periodic only
+    dict(bc_lo=(pg.BC_COPY, 0, 0)),                 # periodic on one side only
     dict(bc_lo=(0, 0, pg.BC_VALUE)),
+    dict(bc_lo=(pg.BC_VALUE, pg.BC_VALUE, 0), bc_hi=(pg.BC_COPY, pg.BC_COPY, 0)),   # two inflow sides
+    dict(n=(4, 4, 1), bc_lo=(0, 0, pg.BC_COPY), bc_hi=(0, 0, pg.BC_COPY)),         # one cell, bounded
+    dict(bc_lo=(pg.BC_EXTERNAL, 0, 0), bc_hi=(pg.BC_EXTERNAL, 0, 0)),              # no slab cuts
     dict(solver=1),
     dict(n=(0, 4, 4)),
     dict(cell_length=(0.1, -0.1, 0.1)),

@@ -1,5 +1,6 @@
 """Parity of the staggered-field step on the GPU (pamhd_gpu_staggered_*, through the C ABI) with
-the CPU oracle (oracle/mode_s.hpp) and with the reference program's own outputs.
+the CPU oracle (oracle/mode_s.hpp) and with the reference program's own outputs, periodic grids
+(bounded ones: test_gpu_staggered_bounded.py).
 
 Tolerance: the GPU solves faces with FMA contraction and Newton reciprocals, the oracle in the
 reference's operation order; the cell and face updates are written in the oracle's order without
@@ -209,8 +210,22 @@ def test_failure_reports_oracle_face_and_keeps_state(port):
     assert np.array_equal(Ug, U) and np.array_equal(Fg, faces)
 
 
-def test_rejects_non_periodic_grid():
-    cfg = pg.Config(n=(8, 8, 1), solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1), bc_lo=(pg.BC_COPY, 0, 0),
-                    bc_hi=(pg.BC_COPY, 0, 0))
-    with pytest.raises(pg.PamhdError):
-        pg.StaggeredContext(cfg)
+def test_rejects_invalid_sides():
+    """Periodic on one side only, a bounded dimension of one cell, two VALUE sides, and a background
+    field on a bounded grid are refused."""
+    C, V = pg.BC_COPY, pg.BC_VALUE
+    v = [1.0, 0, 0, 0, 2.0, 0, 0, 0]
+    bad = [
+        dict(n=(8, 8, 4), bc_lo=(C, 0, 0), bc_hi=(0, 0, 0)),
+        dict(n=(8, 8, 1), bc_lo=(C, 0, C), bc_hi=(C, 0, C)),
+        dict(n=(8, 8, 4), bc_lo=(V, V, 0), bc_hi=(C, C, 0), value_lo=[v, v, None]),
+    ]
+    for kw in bad:
+        with pytest.raises(pg.PamhdError) as e:
+            pg.StaggeredContext(pg.Config(solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1), **kw))
+        assert e.value.code == pg.ERR_ARGUMENT
+    cfg = pg.Config(n=(8, 8, 1), solver=pg.HLL, cell_length=(0.1, 0.1, 0.1), bc_lo=(C, 0, 0), bc_hi=(C, 0, 0))
+    with pg.StaggeredContext(cfg) as ctx:
+        with pytest.raises(pg.PamhdError) as e:
+            ctx.set_background(np.zeros((3, 3, 1, 8, 8)))
+        assert e.value.code == pg.ERR_ARGUMENT
