@@ -8,7 +8,8 @@ TEST INFRASTRUCTURE ONLY: it is used by the oracle build recipe
 
 A cell is a tuple of tagged variables; cell[Tag()] returns a reference to
 the value of type Tag::data_type.  Storage and indexing only: there is no
-arithmetic, no MPI transfer logic and no I/O.
+arithmetic, no MPI transfer logic (set_transfer_all does nothing) and no
+I/O.
 */
 #ifndef ORACLE_GENSIMCELL_STANDIN_HPP
 #define ORACLE_GENSIMCELL_STANDIN_HPP
@@ -36,6 +37,9 @@ template <class Transfer_Policy, class... Tags> class Cell {
 	std::tuple<typename Tags::data_type...> values{};
 
 public:
+	// which variables MPI would transfer: nothing to transfer on one rank
+	template <class... Variables> static void set_transfer_all(const bool, const Variables&...) {}
+
 	template <class Tag> typename Tag::data_type& operator[](const Tag&)
 	{
 		return std::get<standin::position<Tag, Tags...>::value>(values);

@@ -182,3 +182,26 @@ def test_failure_in_the_layer_reports_the_oracle_face(port):
     Ug, Fg = gpu.get_state()
     assert np.array_equal(Ug, U0) and all(np.array_equal(x, y) for x, y in zip(Fg, F0))
     gpu.close()
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena", "roe_athena"])
+@pytest.mark.parametrize("name", ["periodic_3d", "copy_box", "wind_minus_x", "wind_plus_y_2d"])
+def test_matches_reference_step(name, solver):
+    """The GPU against the reference's own staggered step (the solar-wind box's loop, compiled
+    unchanged; committed outputs, see test_staggered_ref_pin.py): the priming step and five steps,
+    state and faces within 1e-12, dt within 1e-13."""
+    import test_staggered_ref_pin as R
+    U, F, dts, value = R.golden(name, solver)
+    n, bc_lo, bc_hi = R.CASES[name]
+    vlo = [list(value) if k == V else None for k in bc_lo]
+    vhi = [list(value) if k == V else None for k in bc_hi]
+    cfg = pg.Config(n=n, solver=R.SOLVERS[solver], cell_length=R.LENGTHS, time_step_factor=0.4, bc_lo=bc_lo,
+                    bc_hi=bc_hi, value_lo=vlo, value_hi=vhi)
+    U0, F0 = R.case_input(name)
+    with pg.StaggeredContext(cfg) as ctx:
+        ctx.set_state(U0, F0)
+        got = [ctx.step(0.0 if s == 0 else 1e300) for s in range(R.STEPS)]
+        Ug, Fg = ctx.get_state()
+    assert np.abs(np.array(got) - dts).max() <= 1e-13 * dts.max()
+    assert state_err(Ug, U) <= STEP_TOL
+    assert faces_err(list(Fg), F) <= STEP_TOL
