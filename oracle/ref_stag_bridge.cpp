@@ -1,5 +1,6 @@
 /*
-libstag_ref.so: the reference's OWN staggered-field step, compiled
+libstag_ref.so: the reference's OWN staggered-field step (and, below, its
+cell-centred subset), compiled
 unchanged from the reference tree by oracle/Makefile on a one-rank box
 stand-in for dccrg (ref_shim/box_grid.hpp): timestep() of mhd/solve.hpp
 (get_fluxes with assign_face_dBs_f{x,y,z}, update_mhd_state, update_vol_B,
@@ -310,3 +311,74 @@ extern "C" int ref_stag_run(const int32_t n[3], const double cell_length[3], con
 		return 1;
 	}
 }
+
+/*
+The cell-centred step on a periodic box (a dimension of one cell not
+periodic: it has no faces, as the reference's 2-D grids with periodic
+{true, true, false}), from the reference's own functions
+in timestep()'s order without its face-field parts (mhd/solve.hpp:1865-1902:
+set_minmax_substepping_period, minimize_timestep, the substep plan,
+get_all_fluxes, update_mhd_state; no update_vol_B and no sync, so the cell's
+volume field keeps the flux update): nsteps steps, the first the dt = 0
+priming step.  cells as ref_stag_run; writes the state after the steps and
+every step's dt.  Returns 0, or 1 with the message of a thrown exception.
+*/
+extern "C" int ref_cell_centred_run(const int32_t n[3], const double cell_length[3], const int32_t solver_id,
+                                    const double gamma, const double mu0, const double cfl, const double* cells,
+                                    const int32_t nsteps, double* cells_out, double* dts)
+{
+	try {
+		const std::array<int, 3> N{n[0], n[1], n[2]};
+		Grid grid(N, {cell_length[0], cell_length[1], cell_length[2]}, {n[0] > 1, n[1] > 1, n[2] > 1});
+		const size_t count = size_t(n[0]) * n[1] * n[2];
+		for (size_t i = 0; i < count; i++) {
+			Cell& c = grid.data[i];
+			Mas.data(c) = cells[i];
+			Mom.data(c) = {cells[count + i], cells[2 * count + i], cells[3 * count + i]};
+			Nrj.data(c) = cells[4 * count + i];
+			Vol_B.data(c) = {cells[5 * count + i], cells[6 * count + i], cells[7 * count + i]};
+			CType.data(c) = 1;
+			Substep.data(c) = Substep_Min.data(c) = Substep_Max.data(c) = 1;
+			Max_v.data(c) = {-1, -1, -1, -1, -1, -1};
+			for (int dir: {-3, -2, -1, +1, +2, +3}) {
+				Bg_B.data(c)(dir) = {0, 0, 0};
+				Face_B.data(c)(dir) = 0;
+			}
+		}
+		Sim_Options options;
+		const pamhd::mhd::Solver solver = solver_id == 0 ? pamhd::mhd::Solver::rusanov
+			: solver_id == 2 ? pamhd::mhd::Solver::hll_athena
+			: solver_id == 3 ? pamhd::mhd::Solver::hlld_athena
+			: pamhd::mhd::Solver::roe_athena;
+		double t = 0;
+		for (int s = 0; s < nsteps; s++) {
+			const double cap = s == 0 ? 0.0 : std::numeric_limits<double>::max();
+			pamhd::set_minmax_substepping_period(t, grid, options, Substep_Min, Substep_Max);
+			pamhd::mhd::minimize_timestep(grid, cfl, CType, Timestep, Max_v);
+			const double sub_dt = pamhd::set_minmax_substepping_period(grid, cap, CType, Timestep, Substep_Min,
+			                                                           Substep_Max);
+			pamhd::restrict_substepping_period(grid, Substep, Substep_Max, CType);
+			const int max_substep = pamhd::update_substeps(grid, CType, Substep);
+			for (int substep = 1; substep <= max_substep; substep++) {
+				pamhd::mhd::get_all_fluxes(sub_dt, solver, grid, substep, gamma, mu0, Mas, Mom, Nrj, Vol_B, Face_B,
+				                           Face_dB, Bg_B, Mas_f, Mom_f, Nrj_f, Mag_f, CType, Substep, Max_v);
+				pamhd::mhd::update_mhd_state(grid.local_cells(), grid, substep, Face_B, Face_dB, CType, Substep,
+				                             Mas, Mom, Nrj, Vol_B, Mas_f, Mom_f, Nrj_f, Mag_f);
+			}
+			dts[s] = sub_dt * max_substep;
+			t += dts[s];
+		}
+		for (size_t i = 0; i < count; i++) {
+			Cell& c = grid.data[i];
+			cells_out[i] = Mas.data(c);
+			for (int e = 0; e < 3; e++) cells_out[(1 + e) * count + i] = Mom.data(c)[e];
+			cells_out[4 * count + i] = Nrj.data(c);
+			for (int e = 0; e < 3; e++) cells_out[(5 + e) * count + i] = Vol_B.data(c)[e];
+		}
+		return 0;
+	} catch (const std::exception& e) {
+		std::cerr << e.what() << std::endl;
+		return 1;
+	}
+}
+
