@@ -136,13 +136,24 @@ const auto Mag_f = [](Cell& cell_data, const int dir)->auto& {
 	return MHDF.data(cell_data)(dir)[pamhd::Magnetic_Field()];
 };
 
-// substepping options: every cell's period 2^0 (no substeps)
-struct Constant_Exponent {
-	double evaluate(double, double, double, double, double, double, double) const { return 0; }
+// substepping options: every cell's exponent bounds from a per-cell table (x fastest) looked up at
+// the cell's centre, as the options' expressions are evaluated there (substepping.hpp:213-228), or
+// 0 everywhere (no substeps) without a table
+struct Per_Cell_Exponent {
+	const Grid* grid = nullptr;
+	const int32_t* values = nullptr;
+	double evaluate(double, const double x, const double y, const double z, double, double, double) const
+	{
+		if (values == nullptr) return 0;
+		const auto& g = grid->geometry;
+		const int i = int(std::floor(x / g.len[0])), j = int(std::floor(y / g.len[1])),
+			k = int(std::floor(z / g.len[2]));
+		return values[i + size_t(g.n[0]) * (j + size_t(g.n[1]) * k)];
+	}
 };
 struct Sim_Options {
 	int substep_min_i = 0, substep_max_i = 0;
-	Constant_Exponent substep_min_e, substep_max_e;
+	Per_Cell_Exponent substep_min_e, substep_max_e;
 };
 
 using Cell_List = std::vector<Grid::Cell>;
@@ -323,9 +334,31 @@ volume field keeps the flux update): nsteps steps, the first the dt = 0
 priming step.  cells as ref_stag_run; writes the state after the steps and
 every step's dt.  Returns 0, or 1 with the message of a thrown exception.
 */
+extern "C" int ref_cell_centred_substep_run(const int32_t n[3], const double cell_length[3],
+                                            const int32_t solver_id, const double gamma, const double mu0,
+                                            const double cfl, const double* cells, const int32_t* smin,
+                                            const int32_t* smax, const int32_t nsteps, double* cells_out,
+                                            double* dts, int32_t* max_periods);
+
 extern "C" int ref_cell_centred_run(const int32_t n[3], const double cell_length[3], const int32_t solver_id,
                                     const double gamma, const double mu0, const double cfl, const double* cells,
                                     const int32_t nsteps, double* cells_out, double* dts)
+{
+	return ref_cell_centred_substep_run(n, cell_length, solver_id, gamma, mu0, cfl, cells, nullptr, nullptr,
+	                                    nsteps, cells_out, dts, nullptr);
+}
+
+/*
+As ref_cell_centred_run with local time stepping: smin, smax the smallest
+and largest substep exponent of every cell (the options' substep-min and
+substep-max, x fastest), or nullptr for 0.  Writes each step's largest
+period too (max_periods, or nullptr).
+*/
+extern "C" int ref_cell_centred_substep_run(const int32_t n[3], const double cell_length[3],
+                                            const int32_t solver_id, const double gamma, const double mu0,
+                                            const double cfl, const double* cells, const int32_t* smin,
+                                            const int32_t* smax, const int32_t nsteps, double* cells_out,
+                                            double* dts, int32_t* max_periods)
 {
 	try {
 		const std::array<int, 3> N{n[0], n[1], n[2]};
@@ -346,6 +379,11 @@ extern "C" int ref_cell_centred_run(const int32_t n[3], const double cell_length
 			}
 		}
 		Sim_Options options;
+		if (smin != nullptr and smax != nullptr) {
+			options.substep_min_i = options.substep_max_i = -1;
+			options.substep_min_e = {&grid, smin};
+			options.substep_max_e = {&grid, smax};
+		}
 		const pamhd::mhd::Solver solver = solver_id == 0 ? pamhd::mhd::Solver::rusanov
 			: solver_id == 2 ? pamhd::mhd::Solver::hll_athena
 			: solver_id == 3 ? pamhd::mhd::Solver::hlld_athena
@@ -359,14 +397,17 @@ extern "C" int ref_cell_centred_run(const int32_t n[3], const double cell_length
 			                                                           Substep_Max);
 			pamhd::restrict_substepping_period(grid, Substep, Substep_Max, CType);
 			const int max_substep = pamhd::update_substeps(grid, CType, Substep);
+			double total_dt = 0;
 			for (int substep = 1; substep <= max_substep; substep++) {
+				total_dt += sub_dt;
 				pamhd::mhd::get_all_fluxes(sub_dt, solver, grid, substep, gamma, mu0, Mas, Mom, Nrj, Vol_B, Face_B,
 				                           Face_dB, Bg_B, Mas_f, Mom_f, Nrj_f, Mag_f, CType, Substep, Max_v);
 				pamhd::mhd::update_mhd_state(grid.local_cells(), grid, substep, Face_B, Face_dB, CType, Substep,
 				                             Mas, Mom, Nrj, Vol_B, Mas_f, Mom_f, Nrj_f, Mag_f);
 			}
-			dts[s] = sub_dt * max_substep;
-			t += dts[s];
+			dts[s] = total_dt;
+			if (max_periods != nullptr) max_periods[s] = max_substep;
+			t += total_dt;
 		}
 		for (size_t i = 0; i < count; i++) {
 			Cell& c = grid.data[i];

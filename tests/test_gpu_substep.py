@@ -78,3 +78,26 @@ def test_failure_is_reported():
     with pytest.raises(pg.PhysicsError) as e:
         ctx.step(0.0)
     assert e.value.flags != 0
+
+
+@pytest.mark.parametrize("solver", ["rusanov", "hll_athena", "hlld_athena", "roe_athena"])
+@pytest.mark.parametrize("name", ["forced_periods_3d", "slow_half_2d"])
+def test_matches_reference_substep_loop(name, solver):
+    """The GPU's substepped step against the reference's own substep loop (the options' exponent
+    bounds per cell, the plan and the substeps of timestep(), compiled unchanged; committed
+    outputs, see test_cell_centred_ref_pin.py): eight steps, step lengths within 1e-13, largest
+    periods equal, state within 1e-12."""
+    import test_cell_centred_ref_pin as R
+    U, dts, top = R.sub_golden(name, solver)
+    n, lengths = R.SUB_CASES[name]
+    U0, smin, smax = R.sub_case(name)
+    cfg = pg.Config(n=n, solver=R.SOLVERS[solver], cell_length=lengths, adiabatic_index=states.GAMMA_53,
+                    time_step_factor=0.4)
+    with pg.SubstepContext(cfg) as gpu:
+        gpu.set_state(U0)
+        gpu.set_exponents(smin, smax)
+        got = [gpu.step(0.0 if s == 0 else 1e300) for s in range(R.SUB_STEPS)]
+        Ug = gpu.get_state()
+    assert np.abs(np.array([g[0] for g in got]) - dts).max() <= 1e-13 * dts.max()
+    assert np.array_equal(np.array([g[1] for g in got]), top)
+    assert err(Ug, U) <= STEP_TOL
