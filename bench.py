@@ -666,6 +666,38 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
         ctx.get_state(out=(hUo, hFo))
         e2e_sec = time.perf_counter() - t0
     moved = (U.nbytes + faces.nbytes) / (steps + 1)
+    # the same state in a bounded box: inflow on -x (the state of the first cell, denser), COPY on
+    # every other side; the box's layer of boundary cells and the plain (untiled) kernels
+    bc_lo, bc_hi = (pg.BC_VALUE, pg.BC_COPY, pg.BC_COPY), (pg.BC_COPY,) * 3
+    inflow = U[:, 0, 0, 0].copy()
+    inflow[0:4] *= 1.3
+    bcfg = pg.Config(n=(n, n, n), solver=sid, cell_length=L, adiabatic_index=5 / 3, vacuum_permeability=1.0,
+                     time_step_factor=0.4, bc_lo=bc_lo, bc_hi=bc_hi, value_lo=[list(inflow), None, None],
+                     device=local)
+    bfaces = []
+    for d, shape in enumerate(pg.staggered_face_shapes(bcfg)):
+        f = faces[d]
+        if shape != f.shape:
+            f = np.concatenate([f, np.take(f, [0], axis=2 - d)], axis=2 - d)
+        bfaces.append(np.ascontiguousarray(f))
+    with pg.StaggeredContext(bcfg) as ctx:
+        ctx.set_state(U, bfaces)
+        ctx.step(0.0)
+        ctx.steps(3, T_END)
+        ctx.sync()
+        st = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        ctx.steps(steps, T_END)
+        e1.record(st)
+        ctx.sync()
+        torch.cuda.synchronize()
+        bms = e0.elapsed_time(e1) / steps
+    bounded = {"workload": f"{n}^3 bounded box: inflow on -x, COPY elsewhere, {solver}, the same state",
+               "value": n ** 3 / (bms * 1e-3), "unit": UNIT, "ms_per_step": bms, "steps": steps,
+               "gpu_launches": 5 * steps,
+               "what": "one thread per cell: face solves, face field, cell update, layer fill, inflow plane"}
     out = {
         "workload": f"{n}^3 periodic, {solver}, smooth state with a divergence-free face field, CFL 0.4",
         "value": n ** 3 / (ms * 1e-3),
@@ -680,6 +712,7 @@ def staggered_section(local, n=256, steps=20, solver="hlld_athena", cpu=True):
                 "what": f"StaggeredContext.set_state from pinned host arrays + the priming step + {steps} "
                         f"steps + get_state to pinned host arrays, host clock"},
         "clocks": clocks.summary(),
+        "bounded": bounded,
     }
     if cpu:
         from oracle import pyoracle as po

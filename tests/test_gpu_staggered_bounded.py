@@ -205,3 +205,29 @@ def test_matches_reference_step(name, solver):
     assert np.abs(np.array(got) - dts).max() <= 1e-13 * dts.max()
     assert state_err(Ug, U) <= STEP_TOL
     assert faces_err(list(Fg), F) <= STEP_TOL
+
+
+@pytest.mark.parametrize("solver", ["hll_athena", "hlld_athena"])
+def test_many_blocks_match_oracle(port, solver):
+    """A 44 x 38 x 30 box (about 55,000 cells with the layer: every kernel's grid-stride loop over
+    many blocks, and a 40 x 32 inflow plane over several blocks) with inflow on +z and COPY
+    elsewhere: the priming step and three steps against the oracle."""
+    n, bc_lo, bc_hi = (44, 38, 30), (C, C, C), (C, C, V)
+    L = (0.1, 0.12, 0.09)
+    U, faces, _ = states.staggered_random((n[2], n[1], n[0]), L, np.random.default_rng(13))
+    value = inflow_of(U)
+    cfg, gpu, ora = make_pair(port, n, po.SOLVERS[solver], L, bc_lo, bc_hi, value)
+    F = bounded_faces(faces, cfg)
+    gpu.set_state(U, F)
+    ora.set_state(U, F)
+    for s in range(4):
+        cap = 0.0 if s == 0 else 1.0
+        dg = gpu.step(cap)
+        do, flag, _, _ = ora.step(cap)
+        assert flag == 0
+        assert abs(dg - do) <= 1e-13 * max(do, 1e-300), s
+        Ug, Fg = gpu.get_state()
+        Uo, Fo = ora.get_state()
+        assert state_err(Ug, Uo) <= STEP_TOL, s
+        assert faces_err(Fg, Fo) <= STEP_TOL, s
+    gpu.close()
