@@ -15,23 +15,19 @@ the two sides' (mhd/N_solve.hpp:354-437).  Dimensions of one cell have no
 faces.
 
 Data in HBM: 13 arrays (rho1, mom1 xyz, E1, rho2, mom2 xyz, E2, B xyz) of
-n0 n1 n2 doubles, x fastest, no ghosts (neighbours wrap), ping-pong; the
-13 contributions of every cell's -d face, 3 x 13 arrays.
+n0 n1 n2 doubles, x fastest, no ghosts (neighbours wrap), ping-pong.
 
-One step, two launches:
-  npop_faces_kernel   dt (given, or min(CFL max_dt, t_end - t) from the
-                      previous step's face speeds, the loop of
-                      tests/mhd/two_reference.cpp:936-960); every cell solves
-                      its -d faces from per-cell records staged in shared
-                      memory by z-marching tiles (the fast speed of a cell
-                      along each axis computed once, not once per face side),
-                      stores their contributions and max-reduces the signal
-                      speeds per axis into a three-slot ring;
-  npop_update_kernel  the same dt; every cell sums its faces' contributions
-                      in the order -x, +x, -y, +y, -z, +z, applies them times
-                      1/volume (apply_fluxes_N, mhd/N_solve.hpp:505-546) and
-                      raises the total pressure to min_pressure where it is
-                      below (:553-583); advances the clock.
+One step, one fused launch (npop_fused_kernel, described below) and a
+one-flag check (restore_kernel):
+  dt (given, or min(CFL max_dt, t_end - t) from the previous step's face
+  speeds, the loop of tests/mhd/two_reference.cpp:936-960); every face
+  solved once from per-cell records staged in shared memory by z-marching
+  tiles (the fast speed of a cell along each axis computed once, not once
+  per face side), its contributions summed by the cells on both sides in
+  the order -x, +x, -y, +y, -z, +z, applied times 1/volume (apply_fluxes_N,
+  mhd/N_solve.hpp:505-546) with the total pressure raised to min_pressure
+  where it is below (:553-583); the signal speeds max-reduced per axis into
+  a three-slot ring; the clock advanced.
 The next step's limit is min over axes of d_len / max signal speed
 (mhd/N_solve.hpp:345).  Every operation is written in the order of the CPU
 oracle's restatement (oracle/n_solve.hpp) and the file is compiled without
@@ -64,7 +60,6 @@ struct Npop_Control {
 struct Npop_Params {
 	const double* __restrict__ U;   // 13 x N
 	double* __restrict__ Uo;
-	double* __restrict__ X;         // (3 x 13) x N
 	int n[3];
 	int active[3];
 	long long N;
@@ -405,40 +400,62 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 /*
-The face solves as tiles: a block of NTX x NTY threads owns a column of cells
-and marches it in z through a chunk of planes.  Each plane's cells, with the
--x column and -y row next to the tile, are read once into a shared-memory
-record (the 13 state values and, per active axis, the fast speed of the
-rotated total state with its check flag); every cell then solves its -d
-faces from the records, the -z face against the previous plane's record.
-Three record slots rotate over the planes, so one barrier per plane keeps a
-plane's stores apart from the reads of the plane two before it.
+One fused launch per step: a block of NTX x NTY threads owns a column of
+cells and marches it in z through a chunk of planes.  Per plane k:
+  (a) the plane's cells, with the columns left and right of the tile and the
+      rows below and above it, are read once into a shared-memory record (the
+      13 state values, the two density reciprocals and, per active axis, the
+      fast speed of the rotated total state with its check flag);
+  (b) every cell solves its -x and -y faces from the records (the last
+      column its +x face too, the last row its +y face) and its -z face
+      against its own record of plane k - 1, kept in registers;
+  (c) the x and y contributions go through shared memory to the cells on
+      their other side, and every cell sums its faces' contributions in the
+      order -x, +x, -y, +y, -z (the +z one arrives with plane k + 1);
+  (d) the cell of plane k - 1 takes its +z contribution and is updated as
+      apply_fluxes_N does (mhd/N_solve.hpp:505-583) and written out.
+The contributions never reach HBM.  A face that fails sets the status; the
+step's state is then restored by restore_kernel after the launch, as the
+reference stops before applying any flux of that step.  Partial tiles read
+wrapped cells in their unused positions (computed, not written), so that
+every owned cell's neighbours are the right ones.
 */
 constexpr int NTX = 32, NTY = 4;
-constexpr int NW = NTX + 1;                 // a record row: the -x halo at column 0
-constexpr int NCELLS = NW * (NTY + 1);      // record rows: the -y halo at row 0
+constexpr int NW = NTX + 2;                 // a record row: halo columns at 0 and NTX + 1
+constexpr int NH = NTY + 2;                 // record rows: halo rows at 0 and NTY + 1
+constexpr int NCELLS = NW * NH;
 constexpr int NREC = NV + 5;                // state, fast speed along x, y, z, 1 / rho, 0.5 / rho
 enum { N_CF = NV, N_INV = NV + 3, N_HALF = NV + 4 };
-constexpr int NSLOT = NREC * NCELLS;
-constexpr int NSLOTS = 3;
-constexpr size_t SMEM_FACES = NSLOTS * (NSLOT * sizeof(double) + NCELLS * sizeof(uint32_t));
+constexpr int NXF = (NTX + 1) * NTY;        // x faces of the tile: the -x face of every column and the last +x
+constexpr int NYF = NTX * (NTY + 1);        // y faces: the -y face of every row and the last +y
+constexpr size_t SMEM_RECORDS = size_t(NREC) * NCELLS * sizeof(double) + NCELLS * sizeof(uint32_t);
+constexpr size_t SMEM_EXCHANGE = size_t(NV) * (NXF + NYF) * sizeof(double);
+constexpr size_t SMEM_PENDING = size_t(NV) * NTX * NTY * sizeof(double);   // the sums waiting for +z
+constexpr size_t SMEM_FUSED = SMEM_RECORDS + SMEM_EXCHANGE + SMEM_PENDING;
 
 __device__ __forceinline__ Gas_N gas_of(const Npop_Params& P)
 {
 	return Gas_N{P.gamma, P.mu0, P.inv_mu0, P.half_inv_mu0};
 }
 
-template <int A>
-__device__ __forceinline__ void stage_fast(const Npop_Params& P, const double u[NV], const double inv,
-                                           const double half, double* rec, const int r, uint32_t& flags)
+__device__ __forceinline__ int wrap_any(const int i, const int n)
 {
-	if (not P.active[A]) return;
-	uint32_t f = 0;
-	rec[(N_CF + A) * NCELLS + r] = fast_speed(total_rotated<A>(u, inv, half), gas_of(P), f);
-	flags |= f << (8 * A);
+	const int r = i % n;
+	return r < 0 ? r + n : r;
 }
 
-// read cell c into slot position r, with its fast speeds along the axes its faces in the tile need
+// the fast speed of a cell's rotated total state along axis A, with its flag in byte A of flags
+template <int A>
+__device__ __forceinline__ double fast_of(const Npop_Params& P, const double u[NV], const double inv,
+                                          const double half, uint32_t& flags)
+{
+	uint32_t f = 0;
+	const double cf = fast_speed(total_rotated<A>(u, inv, half), gas_of(P), f);
+	flags |= f << (8 * A);
+	return cf;
+}
+
+// read cell c into record position r, with its fast speeds along the axes its faces in the tile need
 template <bool CX, bool CY, bool CZ>
 __device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, uint32_t* flg, const int r,
                                            const long long c)
@@ -452,28 +469,36 @@ __device__ __forceinline__ void stage_cell(const Npop_Params& P, double* rec, ui
 	rec[N_INV * NCELLS + r] = inv;
 	rec[N_HALF * NCELLS + r] = half;
 	uint32_t flags = 0;
-	if (CX) stage_fast<0>(P, u, inv, half, rec, r, flags);
-	if (CY) stage_fast<1>(P, u, inv, half, rec, r, flags);
-	if (CZ) stage_fast<2>(P, u, inv, half, rec, r, flags);
+	if (CX and P.active[0]) rec[N_CF * NCELLS + r] = fast_of<0>(P, u, inv, half, flags);
+	if (CY and P.active[1]) rec[(N_CF + 1) * NCELLS + r] = fast_of<1>(P, u, inv, half, flags);
+	if (CZ and P.active[2]) rec[(N_CF + 2) * NCELLS + r] = fast_of<2>(P, u, inv, half, flags);
 	flg[r] = flags;
 }
 
-// the -A face of cell c between its -A neighbour m (record rl) and c (record rr)
+// a cell as the -z side of a face, kept in registers from one plane to the next
+struct Zrec {
+	double u[NV];
+	double inv, half, cf;
+	uint32_t flag;
+};
+
+/*
+The contribution x of the -A face between the cells with states um (left,
+reciprocals iml / hml, fast speed fl) and uc (right): the split solver's two
+fluxes, shared among the populations by each side's mass fractions, the
+field flux the sum of the two sides' (mhd/N_solve.hpp:354-437), written to
+x[v * stride].  Returns the failure flag (0: none); m names the face's
+negative cell.
+*/
 template <int SOLVER, int A>
-__device__ __forceinline__ void minus_face(const Npop_Params& P, const double* recl, const uint32_t* flgl,
-                                           const int rl, const double* recr, const uint32_t* flgr, const int rr,
-                                           const long long c, const long long m, const double dt, double& smax)
+__device__ __forceinline__ uint32_t face_contribution(const Npop_Params& P, const double um[NV], const double iml,
+                                                      const double hml, const Fast& fl, const double uc[NV],
+                                                      const double imr, const double hmr, const Fast& fr,
+                                                      const double dt, const long long m, double& smax,
+                                                      double* x, const int stride)
 {
-	double um[NV], uc[NV];
-	#pragma unroll
-	for (int v = 0; v < NV; v++) {
-		um[v] = recl[v * NCELLS + rl];
-		uc[v] = recr[v * NCELLS + rr];
-	}
-	const St L = total_rotated<A>(um, recl[N_INV * NCELLS + rl], recl[N_HALF * NCELLS + rl]);
-	const St R = total_rotated<A>(uc, recr[N_INV * NCELLS + rr], recr[N_HALF * NCELLS + rr]);
-	const Fast fl{recl[(N_CF + A) * NCELLS + rl], (flgl[rl] >> (8 * A)) & 0xffu};
-	const Fast fr{recr[(N_CF + A) * NCELLS + rr], (flgr[rr] >> (8 * A)) & 0xffu};
+	const St L = total_rotated<A>(um, iml, hml);
+	const St R = total_rotated<A>(uc, imr, hmr);
 	double fn[8], fp[8];
 	uint32_t flag = 0;
 	const double s = SOLVER == PAMHD_RUSANOV
@@ -482,7 +507,9 @@ __device__ __forceinline__ void minus_face(const Npop_Params& P, const double* r
 	if (flag != 0) {
 		atomicOr(&P.status->flags, flag);
 		atomicMin(&P.status->first, ((unsigned long long)(m * 3 + A) << 8) | flag);
-		return;
+		#pragma unroll
+		for (int v = 0; v < NV; v++) x[v * stride] = 0.0;
+		return flag;
 	}
 	smax = fmax(smax, s);
 	double gn[8], gp[8];
@@ -491,92 +518,275 @@ __device__ __forceinline__ void minus_face(const Npop_Params& P, const double* r
 	unrotate<A>(fp[1], fp[2], fp[3], gp[1], gp[2], gp[3]);
 	unrotate<A>(fn[5], fn[6], fn[7], gn[5], gn[6], gn[7]);
 	unrotate<A>(fp[5], fp[6], fp[7], gp[5], gp[6], gp[7]);
-	// shares of the populations (mass fractions of the face's two cells) and of the field
 	const double
 		f1n = um[0] / (um[0] + um[5]), f2n = um[5] / (um[0] + um[5]),
 		f1p = uc[0] / (uc[0] + uc[5]), f2p = uc[5] / (uc[0] + uc[5]);
-	double x[NV];
 	x[0] = f1n * gn[0] + f1p * gp[0];
-	x[5] = f2n * gn[0] + f2p * gp[0];
-	x[4] = f1n * gn[4] + f1p * gp[4];
-	x[9] = f2n * gn[4] + f2p * gp[4];
+	x[5 * stride] = f2n * gn[0] + f2p * gp[0];
+	x[4 * stride] = f1n * gn[4] + f1p * gp[4];
+	x[9 * stride] = f2n * gn[4] + f2p * gp[4];
 	#pragma unroll
 	for (int v = 0; v < 3; v++) {
-		x[1 + v] = f1n * gn[1 + v] + f1p * gp[1 + v];
-		x[6 + v] = f2n * gn[1 + v] + f2p * gp[1 + v];
-		x[10 + v] = gn[5 + v] + gp[5 + v];
+		x[(1 + v) * stride] = f1n * gn[1 + v] + f1p * gp[1 + v];
+		x[(6 + v) * stride] = f2n * gn[1 + v] + f2p * gp[1 + v];
+		x[(10 + v) * stride] = gn[5 + v] + gp[5 + v];
 	}
+	return 0;
+}
+
+// the -A face between record positions rl and rr, its contribution to x[v * stride]
+template <int SOLVER, int A>
+__device__ __forceinline__ void record_face(const Npop_Params& P, const double* rec, const uint32_t* flg,
+                                            const int rl, const int rr, const double dt, const long long m,
+                                            double& smax, double* x, const int stride)
+{
+	double um[NV], uc[NV];
 	#pragma unroll
-	for (int v = 0; v < NV; v++) P.X[(A * NV + v) * P.N + c] = x[v];
+	for (int v = 0; v < NV; v++) {
+		um[v] = rec[v * NCELLS + rl];
+		uc[v] = rec[v * NCELLS + rr];
+	}
+	const Fast fl{rec[(N_CF + A) * NCELLS + rl], (flg[rl] >> (8 * A)) & 0xffu};
+	const Fast fr{rec[(N_CF + A) * NCELLS + rr], (flg[rr] >> (8 * A)) & 0xffu};
+	face_contribution<SOLVER, A>(P, um, rec[N_INV * NCELLS + rl], rec[N_HALF * NCELLS + rl], fl, uc,
+	                             rec[N_INV * NCELLS + rr], rec[N_HALF * NCELLS + rr], fr, dt, m, smax, x, stride);
+}
+
+// apply_fluxes_N for one cell (mhd/N_solve.hpp:505-583): the summed contributions f times 1 / volume,
+// then the minimum total pressure
+__device__ __forceinline__ void apply_cell(const Npop_Params& P, double u[NV], const double f[NV],
+                                           const double inverse_volume)
+{
+	u[0] += f[0] * inverse_volume;
+	u[5] += f[5] * inverse_volume;
+	#pragma unroll
+	for (int v = 1; v <= 3; v++) u[v] += f[v] * inverse_volume;
+	#pragma unroll
+	for (int v = 6; v <= 8; v++) u[v] += f[v] * inverse_volume;
+	u[4] += f[4] * inverse_volume;
+	u[9] += f[9] * inverse_volume;
+	#pragma unroll
+	for (int v = 10; v <= 12; v++) u[v] += f[v] * inverse_volume;
+	St t;
+	t.rho = u[0] + u[5];
+	t.e = u[4] + u[9];
+	t.m[0] = u[1] + u[6];
+	t.m[1] = u[2] + u[7];
+	t.m[2] = u[3] + u[8];
+	t.b[0] = u[10];
+	t.b[1] = u[11];
+	t.b[2] = u[12];
+	set_reciprocals(t);
+	uint32_t flag = 0;
+	const double p = pressure(t, gas_of(P), flag);
+	if (not (p >= P.min_pressure)) {
+		double v[3];
+		velocity(t, v);
+		const double
+			kinetic = 0.5 * t.rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]),
+			magnetic = 0.5 / P.mu0 * (t.b[0] * t.b[0] + t.b[1] * t.b[1] + t.b[2] * t.b[2]);
+		const double e = P.min_pressure / (P.gamma - 1) + kinetic + magnetic;
+		u[4] = u[0] / t.rho * e;
+		u[9] = u[5] / t.rho * e;
+	}
 }
 
 template <int SOLVER>
-__global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) npop_faces_kernel(const Npop_Params P)
+__global__ void __launch_bounds__(NTX * NTY, 3) npop_fused_kernel(const Npop_Params P)
 {
 	extern __shared__ __align__(16) double smem[];
-	uint32_t* const flg_base = reinterpret_cast<uint32_t*>(smem + NSLOTS * NSLOT);
+	double* const rec = smem;
+	uint32_t* const flg = reinterpret_cast<uint32_t*>(smem + NREC * NCELLS);
+	double* const xch = reinterpret_cast<double*>(reinterpret_cast<char*>(smem) + SMEM_RECORDS);
+	double* const ych = xch + NV * NXF;
+	double* const pend = ych + NV * NYF;
 	__shared__ double s_dt;
 	__shared__ int s_skip;
 	const int tx = threadIdx.x, ty = threadIdx.y;
+	const int tid = ty * NTX + tx;
 	if (tx == 0 and ty == 0) {
 		const Clock c = P.clock[P.phase];
-		const bool skip = P.control.dt < 0.0 and c.t >= P.control.t_end;
+		// a failure in an earlier step leaves every later one as it is, as a run past t_end
+		const bool skip = P.status->flags != 0u or (P.control.dt < 0.0 and c.t >= P.control.t_end);
+		const double dt = skip ? 0.0 : step_dt(P);
 		s_skip = skip ? 1 : 0;
-		s_dt = skip ? 0.0 : step_dt(P);
+		s_dt = dt;
+		if (blockIdx.x == 0 and blockIdx.y == 0 and blockIdx.z == 0) {
+			Clock& next = P.clock[(P.phase + 1) % 3];
+			next.t = skip ? c.t : c.t + dt;
+			next.dt = skip ? c.dt : dt;
+			next.steps = skip ? c.steps : c.steps + 1;
+			Speed_Max& z = P.red[(P.phase + 2) % 3];
+			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
+			z.zero = 0u;
+		}
 	}
 	__syncthreads();
 	const double dt = s_dt;
+	const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+	const int gx0 = blockIdx.x * NTX, gy0 = blockIdx.y * NTY;
+	const int gx = gx0 + tx, gy = gy0 + ty;
+	const bool own = gx < nx and gy < ny;
+	const int kb = blockIdx.z * P.kchunk;
+	const int ke = min(nz, kb + P.kchunk);
+	const long long plane = (long long)nx * ny;
+	const long long N = P.N;
+	if (s_skip != 0) {
+		if (own) {
+			for (int k = kb; k < ke; k++) {
+				const long long c = gx + (long long)nx * gy + plane * k;
+				#pragma unroll
+				for (int v = 0; v < NV; v++) P.Uo[v * N + c] = P.U[v * N + c];
+			}
+		}
+		return;
+	}
+	const bool ax = P.active[0] != 0, ay = P.active[1] != 0, az = P.active[2] != 0;
+	const int ri = (ty + 1) * NW + tx + 1;
+	const int xi = ty * (NTX + 1) + tx;   // this cell's -x face in the exchange; +1 its +x face
+	const int yi = ty * NTX + tx;         // this cell's -y face; + NTX its +y face
+	// this position's cell (wrapped in a partial tile) and its halo cell, if any: warp 0 the row below
+	// the tile, warp 1 the row above (their y speeds), warp 2 the columns left and right (x speeds)
+	const int wx = wrap_any(gx, nx), wy = wrap_any(gy, ny);
+	const long long col = wx + (long long)nx * wy;
+	int hr = -1, haxis = 0;
+	long long hcol = 0;
+	if (ty == 0) {
+		hr = tx + 1;
+		hcol = wx + (long long)nx * wrap_any(gy0 - 1, ny);
+		haxis = 1;
+	} else if (ty == 1) {
+		hr = (NTY + 1) * NW + tx + 1;
+		hcol = wx + (long long)nx * wrap_any(gy0 + NTY, ny);
+		haxis = 1;
+	} else if (ty == 2 and tx < 2 * NTY) {
+		const int row = tx % NTY;
+		const bool left = tx < NTY;
+		hr = (row + 1) * NW + (left ? 0 : NTX + 1);
+		hcol = wrap_any(left ? gx0 - 1 : gx0 + NTX, nx) + (long long)nx * wrap_any(gy0 + row, ny);
+		haxis = 0;
+	}
+	// the faces' negative cells (failure reports name them)
+	const long long col_mx = wrap_any(gx - 1, nx) + (long long)nx * wy;
+	const long long col_my = wx + (long long)nx * wrap_any(gy - 1, ny);
+	const double inverse_volume = 1.0 / (P.len[0] * P.len[1] * P.len[2]);
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-	if (s_skip == 0) {
-		const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
-		const int gx0 = blockIdx.x * NTX, gy0 = blockIdx.y * NTY;
-		const int gx = gx0 + tx, gy = gy0 + ty;
-		const bool own = gx < nx and gy < ny;
-		const int kb = blockIdx.z * P.kchunk;
-		const int ke = min(nz, kb + P.kchunk);
-		const int ri = (ty + 1) * NW + tx + 1;
-		const long long plane = (long long)nx * ny;
-		const long long col = gx + (long long)nx * gy;
-		// this thread's halo cell, if any: warp 0 the row below the tile (its y speed), warp 1 the
-		// column left of it (its x speed)
-		int hr = -1;
-		long long hcol = 0;
-		if (ty == 0 and gx < nx) {
-			hr = tx + 1;
-			hcol = gx + (long long)nx * (gy0 == 0 ? ny - 1 : gy0 - 1);
-		} else if (ty == 1 and tx < NTY and gy0 + tx < ny) {
-			hr = (tx + 1) * NW;
-			hcol = (gx0 == 0 ? nx - 1 : gx0 - 1) + (long long)nx * (gy0 + tx);
-		}
-		// the -d neighbours' columns (failure reports name the face's negative cell)
-		const long long col_mx = (gx == 0 ? nx - 1 : gx - 1) + (long long)nx * gy;
-		const long long col_my = gx + (long long)nx * (gy == 0 ? ny - 1 : gy - 1);
-		// the plane before the chunk, own cells only: the left sides of the first plane's -z faces
-		if (own and P.active[2]) {
-			stage_cell<false, false, true>(P, smem, flg_base, ri, col + plane * (kb == 0 ? nz - 1 : kb - 1));
-		}
-		for (int k = kb; k < ke; k++) {
-			const int t = k - kb + 1;
-			double* const rec = smem + (t % NSLOTS) * NSLOT;
-			uint32_t* const flg = flg_base + (t % NSLOTS) * NCELLS;
-			const double* const prv = smem + ((t - 1) % NSLOTS) * NSLOT;
-			const uint32_t* const pflg = flg_base + ((t - 1) % NSLOTS) * NCELLS;
-			const long long kofs = plane * k;
-			if (own) stage_cell<true, true, true>(P, rec, flg, ri, col + kofs);
-			if (ty == 0) {
-				if (hr >= 0) stage_cell<false, true, false>(P, rec, flg, hr, hcol + kofs);
-			} else if (hr >= 0) {
-				stage_cell<true, false, false>(P, rec, flg, hr, hcol + kofs);
+	// the own cell of the plane before the chunk: the -z side of the first plane's -z faces
+	Zrec zr;
+	if (az) {
+		load13(P, col + plane * wrap_any(kb - 1, nz), zr.u);
+		const double rho = zr.u[0] + zr.u[5];
+		zr.inv = 1 / rho;
+		zr.half = 0.5 / rho;
+		uint32_t f = 0;
+		zr.cf = fast_of<2>(P, zr.u, zr.inv, zr.half, f);
+		zr.flag = (f >> 16) & 0xffu;
+	}
+	for (int k = kb; k <= ke; k++) {
+		const long long kofs = plane * wrap_any(k, nz);
+		if (k < ke) {
+			// (a) records
+			stage_cell<true, true, true>(P, rec, flg, ri, col + kofs);
+			if (hr >= 0) {
+				if (haxis == 1) stage_cell<false, true, false>(P, rec, flg, hr, hcol + kofs);
+				else stage_cell<true, false, false>(P, rec, flg, hr, hcol + kofs);
 			}
 			__syncthreads();
-			if (own) {
-				const long long c = col + kofs;
-				if (P.active[0]) minus_face<SOLVER, 0>(P, rec, flg, ri - 1, rec, flg, ri, c, col_mx + kofs, dt, s0);
-				if (P.active[1]) minus_face<SOLVER, 1>(P, rec, flg, ri - NW, rec, flg, ri, c, col_my + kofs, dt, s1);
-				if (P.active[2]) {
-					minus_face<SOLVER, 2>(P, prv, pflg, ri, rec, flg, ri, c, col + plane * (k == 0 ? nz - 1 : k - 1),
-					                      dt, s2);
+			// (b) the faces, straight into the exchange: own -x (and the last column's +x), own -y
+			// (and the last row's +y)
+			if (ax) {
+				record_face<SOLVER, 0>(P, rec, flg, ri - 1, ri, dt, col_mx + kofs, s0, xch + xi, NXF);
+				if (tx == NTX - 1) record_face<SOLVER, 0>(P, rec, flg, ri, ri + 1, dt, col + kofs, s0, xch + xi + 1, NXF);
+			}
+			if (ay) {
+				record_face<SOLVER, 1>(P, rec, flg, ri - NW, ri, dt, col_my + kofs, s1, ych + yi, NYF);
+				if (ty == NTY - 1) record_face<SOLVER, 1>(P, rec, flg, ri, ri + NW, dt, col + kofs, s1, ych + yi + NTX, NYF);
+			}
+			// the -z face of this cell: its contribution closes the cell below and opens this one
+			double xz[NV];
+			if (az) {
+				double uc[NV];
+				#pragma unroll
+				for (int v = 0; v < NV; v++) uc[v] = rec[v * NCELLS + ri];
+				const Fast fl{zr.cf, zr.flag};
+				const Fast fr{rec[(N_CF + 2) * NCELLS + ri], (flg[ri] >> 16) & 0xffu};
+				face_contribution<SOLVER, 2>(P, zr.u, zr.inv, zr.half, fl, uc, rec[N_INV * NCELLS + ri],
+				                             rec[N_HALF * NCELLS + ri], fr, dt, col + plane * wrap_any(k - 1, nz),
+				                             s2, xz, 1);
+				#pragma unroll
+				for (int v = 0; v < NV; v++) zr.u[v] = uc[v];
+				zr.inv = rec[N_INV * NCELLS + ri];
+				zr.half = rec[N_HALF * NCELLS + ri];
+				zr.cf = fr.speed;
+				zr.flag = fr.flag;
+			}
+			__syncthreads();
+			// (c) this cell's sum in the reference's order: -x, +x, -y, +y, -z
+			double f[NV];
+			#pragma unroll
+			for (int v = 0; v < NV; v++) f[v] = 0;
+			if (ax) {
+				#pragma unroll
+				for (int v = 0; v < NV; v++) {
+					f[v] += xch[v * NXF + xi];
+					f[v] -= xch[v * NXF + xi + 1];
 				}
+			}
+			if (ay) {
+				#pragma unroll
+				for (int v = 0; v < NV; v++) {
+					f[v] += ych[v * NYF + yi];
+					f[v] -= ych[v * NYF + yi + NTX];
+				}
+			}
+			if (az) {
+				#pragma unroll
+				for (int v = 0; v < NV; v++) f[v] += xz[v];
+				// (d) the cell below takes its +z contribution and is updated
+				if (k > kb and own) {
+					const long long c = col + plane * (k - 1);
+					double u[NV], g[NV];
+					load13(P, c, u);
+					#pragma unroll
+					for (int v = 0; v < NV; v++) g[v] = pend[v * (NTX * NTY) + tid] - xz[v];
+					apply_cell(P, u, g, inverse_volume);
+					#pragma unroll
+					for (int v = 0; v < NV; v++) P.Uo[v * N + c] = u[v];
+				}
+				#pragma unroll
+				for (int v = 0; v < NV; v++) pend[v * (NTX * NTY) + tid] = f[v];
+			} else if (own) {
+				// no z faces: this plane's cells are complete
+				const long long c = col + kofs;
+				double u[NV];
+				load13(P, c, u);
+				apply_cell(P, u, f, inverse_volume);
+				#pragma unroll
+				for (int v = 0; v < NV; v++) P.Uo[v * N + c] = u[v];
+			}
+			// the records and the exchange are written again only after this barrier
+			__syncthreads();
+		} else if (az) {
+			// the plane above the chunk: the last plane's +z faces
+			double uc[NV], xz[NV];
+			load13(P, col + kofs, uc);
+			const double rho = uc[0] + uc[5];
+			const double inv = 1 / rho, half = 0.5 / rho;
+			uint32_t fflag = 0;
+			const double cf = fast_of<2>(P, uc, inv, half, fflag);
+			const Fast fl{zr.cf, zr.flag};
+			const Fast fr{cf, (fflag >> 16) & 0xffu};
+			face_contribution<SOLVER, 2>(P, zr.u, zr.inv, zr.half, fl, uc, inv, half, fr, dt,
+			                             col + plane * (ke - 1), s2, xz, 1);
+			if (own and ke > kb) {
+				const long long c = col + plane * (ke - 1);
+				double u[NV], g[NV];
+				load13(P, c, u);
+				#pragma unroll
+				for (int v = 0; v < NV; v++) g[v] = pend[v * (NTX * NTY) + tid] - xz[v];
+				apply_cell(P, u, g, inverse_volume);
+				#pragma unroll
+				for (int v = 0; v < NV; v++) P.Uo[v * N + c] = u[v];
 			}
 		}
 	}
@@ -591,108 +801,28 @@ __global__ void __launch_bounds__(NTX * NTY, SOLVER == PAMHD_RUSANOV ? 3 : 2) np
 	}
 }
 
-__global__ void __launch_bounds__(THREADS, 1) npop_update_kernel(const Npop_Params P)
+/*
+After the fused launch: if a face has failed (in this step, or in an earlier
+one, which the fused launch skipped), the step leaves the state and the
+clock as they were: the reference stops before applying any flux of the
+step.  One flag read per block otherwise.
+*/
+__global__ void __launch_bounds__(THREADS) restore_kernel(const Npop_Params P)
 {
-	// the contributions already hold area dt: dt is needed here only to advance the clock
-	__shared__ int s_skip;
-	if (threadIdx.x == 0) {
-		const Clock c = P.clock[P.phase];
-		const bool skip = P.status->flags != 0u or (P.control.dt < 0.0 and c.t >= P.control.t_end);
-		const double dt = skip ? 0.0 : step_dt(P);
-		s_skip = skip ? 1 : 0;
-		if (blockIdx.x == 0) {
-			Clock& next = P.clock[(P.phase + 1) % 3];
-			next.t = skip ? c.t : c.t + dt;
-			next.dt = skip ? c.dt : dt;
-			next.steps = skip ? c.steps : c.steps + 1;
-			Speed_Max& z = P.red[(P.phase + 2) % 3];
-			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
-			z.zero = 0u;
-		}
-	}
-	__syncthreads();
-	const bool skip = s_skip != 0;
-	const double inverse_volume = 1.0 / (P.len[0] * P.len[1] * P.len[2]);
-	const long long N = P.N;
+	if (P.status->flags == 0u) return;
+	if (blockIdx.x == 0 and threadIdx.x == 0) P.clock[(P.phase + 1) % 3] = P.clock[P.phase];
+	const long long total = (long long)NV * P.N;
 	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
-		double u[NV];
-		load13(P, c, u);
-		if (not skip) {
-			const int i = int(c % P.n[0]);
-			const int j = int((c / P.n[0]) % P.n[1]);
-			const int k = int(c / ((long long)P.n[0] * P.n[1]));
-			// every contribution read first: 78 independent loads in flight
-			double xm[3][NV], xp[3][NV];
-			#pragma unroll
-			for (int d = 0; d < 3; d++) {
-				if (not P.active[d]) continue;
-				const long long hi = wrap(P, i + (d == 0), j + (d == 1), k + (d == 2));
-				#pragma unroll
-				for (int v = 0; v < NV; v++) {
-					xm[d][v] = P.X[(d * NV + v) * N + c];
-					xp[d][v] = P.X[(d * NV + v) * N + hi];
-				}
-			}
-			double f[NV];
-			#pragma unroll
-			for (int v = 0; v < NV; v++) f[v] = 0;
-			#pragma unroll
-			for (int d = 0; d < 3; d++) {
-				if (not P.active[d]) continue;
-				#pragma unroll
-				for (int v = 0; v < NV; v++) {
-					f[v] += xm[d][v];
-					f[v] -= xp[d][v];
-				}
-			}
-			// apply_fluxes_N: rho1, rho2, mom1, mom2, E1, E2, B
-			u[0] += f[0] * inverse_volume;
-			u[5] += f[5] * inverse_volume;
-			#pragma unroll
-			for (int v = 1; v <= 3; v++) u[v] += f[v] * inverse_volume;
-			#pragma unroll
-			for (int v = 6; v <= 8; v++) u[v] += f[v] * inverse_volume;
-			u[4] += f[4] * inverse_volume;
-			u[9] += f[9] * inverse_volume;
-			#pragma unroll
-			for (int v = 10; v <= 12; v++) u[v] += f[v] * inverse_volume;
-			// minimum total pressure
-			St t;
-			t.rho = u[0] + u[5];
-			t.e = u[4] + u[9];
-			t.m[0] = u[1] + u[6];
-			t.m[1] = u[2] + u[7];
-			t.m[2] = u[3] + u[8];
-			t.b[0] = u[10];
-			t.b[1] = u[11];
-			t.b[2] = u[12];
-			set_reciprocals(t);
-			uint32_t flag = 0;
-			const double p = pressure(t, gas_of(P), flag);
-			if (not (p >= P.min_pressure)) {
-				double v[3];
-				velocity(t, v);
-				const double
-					kinetic = 0.5 * t.rho * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]),
-					magnetic = 0.5 / P.mu0 * (t.b[0] * t.b[0] + t.b[1] * t.b[1] + t.b[2] * t.b[2]);
-				const double e = P.min_pressure / (P.gamma - 1) + kinetic + magnetic;
-				u[4] = u[0] / t.rho * e;
-				u[9] = u[5] / t.rho * e;
-			}
-		}
-		#pragma unroll
-		for (int v = 0; v < NV; v++) P.Uo[v * N + c] = u[v];
-	}
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) P.Uo[t] = P.U[t];
 }
 
 template <int SOLVER>
 int launch_pair(const Npop_Params& P, const int grid, cudaStream_t stream)
 {
 	const dim3 tiles((P.n[0] + NTX - 1) / NTX, (P.n[1] + NTY - 1) / NTY, (P.n[2] + P.kchunk - 1) / P.kchunk);
-	npop_faces_kernel<SOLVER><<<tiles, dim3(NTX, NTY), SMEM_FACES, stream>>>(P);
+	npop_fused_kernel<SOLVER><<<tiles, dim3(NTX, NTY), SMEM_FUSED, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
-	npop_update_kernel<<<grid, THREADS, 0, stream>>>(P);
+	restore_kernel<<<grid, THREADS, 0, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -711,7 +841,6 @@ struct pamhd_npop {
 	cudaStream_t stream = nullptr;
 	long long N = 0;
 	double* U[2] = {nullptr, nullptr};
-	double* X = nullptr;
 	Speed_Max* red = nullptr;
 	Clock* clock = nullptr;
 	Status* status = nullptr;
@@ -782,7 +911,6 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(PAMHD_ERR_CUDA);
 	const size_t bytes = size_t(NV) * size_t(N) * sizeof(double);
 	if (cudaMalloc(&x->U[0], bytes) != cudaSuccess or cudaMalloc(&x->U[1], bytes) != cudaSuccess
-		or cudaMalloc(&x->X, 3 * bytes) != cudaSuccess
 		or cudaMalloc(&x->red, 3 * sizeof(Speed_Max)) != cudaSuccess
 		or cudaMalloc(&x->clock, 3 * sizeof(Clock)) != cudaSuccess
 		or cudaMalloc(&x->status, sizeof(Status)) != cudaSuccess) {
@@ -793,10 +921,10 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	const long long blocks = (N + THREADS - 1) / THREADS;
 	x->grid = int(blocks < 8ll * sms ? blocks : 8ll * sms);
 	const cudaError_t attr = solver == PAMHD_RUSANOV
-		? cudaFuncSetAttribute(npop_faces_kernel<PAMHD_RUSANOV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                       int(SMEM_FACES))
-		: cudaFuncSetAttribute(npop_faces_kernel<PAMHD_HLL_ATHENA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                       int(SMEM_FACES));
+		? cudaFuncSetAttribute(npop_fused_kernel<PAMHD_RUSANOV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                       int(SMEM_FUSED))
+		: cudaFuncSetAttribute(npop_fused_kernel<PAMHD_HLL_ATHENA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+		                       int(SMEM_FUSED));
 	if (attr != cudaSuccess) return fail(PAMHD_ERR_CUDA);
 	Npop_Params& P = x->base;
 	std::memset(&P, 0, sizeof P);
@@ -818,7 +946,6 @@ int pamhd_gpu_npop_create(const int32_t n[3], const double cell_length[3], const
 	P.inv_mu0 = 1.0 / mu0;
 	P.half_inv_mu0 = 0.5 / mu0;
 	P.min_pressure = min_pressure;
-	P.X = x->X;
 	P.red = x->red;
 	P.clock = x->clock;
 	P.status = x->status;
@@ -835,7 +962,6 @@ int pamhd_gpu_npop_destroy(pamhd_npop* x)
 	if (x->stream != nullptr) cudaStreamSynchronize(x->stream);
 	cudaFree(x->U[0]);
 	cudaFree(x->U[1]);
-	cudaFree(x->X);
 	cudaFree(x->red);
 	cudaFree(x->clock);
 	cudaFree(x->status);
