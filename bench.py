@@ -775,7 +775,7 @@ def two_population_section(local, n=256, steps=20, cpu=True):
         "steps": steps,
         "gpu_launches": 2 * steps,
         "roofline": section_roofline(n, "two_population_step_rusanov", 208, n ** 3, ms, clocks.summary(),
-                                     "whole step: npop_faces_kernel + npop_update_kernel"),
+                                     "whole step: npop_fused_kernel + restore_kernel"),
         "e2e": {"value": n ** 3 * steps / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": U.nbytes / steps,
                 "d2h_bytes_per_step": U.nbytes / steps,
                 "what": f"TwoPopulationContext.set_state from a pinned host array + {steps} steps + "
