@@ -245,13 +245,16 @@ __global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3)
 	extern __shared__ __align__(16) double smem[];
 	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(smem + SSLOTS * SSLOT);
 	const int tx = threadIdx.x, ty = threadIdx.y;
-	const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+	// the grid with its boundary layer on a bounded grid (E = n on a periodic one)
+	const int nx = P.E[0], ny = P.E[1], nz = P.E[2];
 	const int gx0 = blockIdx.x * STX, gy0 = blockIdx.y * STY;
 	const int gx = gx0 + tx, gy = gy0 + ty;
 	const bool own = gx < nx and gy < ny;
 	const int kb = blockIdx.z * P.kchunk;
 	const int ke = min(nz, kb + P.kchunk);
 	const int ri = (ty + 1) * SW + tx + 1;
+	// a layer cell's -d face past the low wall has no cell on its other side
+	const bool has_x = not (P.ext[0] and gx == 0), has_y = not (P.ext[1] and gy == 0);
 	const long long plane = (long long)nx * ny;
 	const long long col = gx + (long long)nx * gy;
 	// this thread's halo cell, if any: warp 0 the row below the tile (its y speed), warp 1 the column
@@ -290,12 +293,18 @@ __global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3)
 		if (own) {
 			const long long c = col + kofs;
 			const long long mz = col + plane * (k == 0 ? nz - 1 : k - 1);
-			solve_minus_face<SOLVER, 0, BG>(P, side_rec<0>(rec, bad, ri - 1), side_rec<0>(rec, bad, ri), c,
-			                                col_mx + kofs, s0, zero);
-			solve_minus_face<SOLVER, 1, BG>(P, side_rec<1>(rec, bad, ri - SW), side_rec<1>(rec, bad, ri), c,
-			                                col_my + kofs, s1, zero);
-			solve_minus_face<SOLVER, 2, BG>(P, side_rec<2>(prv, pbad, ri), side_rec<2>(rec, bad, ri), c, mz,
-			                                s2, zero);
+			if (has_x) {
+				solve_minus_face<SOLVER, 0, BG>(P, side_rec<0>(rec, bad, ri - 1), side_rec<0>(rec, bad, ri), c,
+				                                col_mx + kofs, s0, zero);
+			}
+			if (has_y) {
+				solve_minus_face<SOLVER, 1, BG>(P, side_rec<1>(rec, bad, ri - SW), side_rec<1>(rec, bad, ri), c,
+				                                col_my + kofs, s1, zero);
+			}
+			if (not (P.ext[2] and k == 0)) {
+				solve_minus_face<SOLVER, 2, BG>(P, side_rec<2>(prv, pbad, ri), side_rec<2>(rec, bad, ri), c, mz,
+				                                s2, zero);
+			}
 		}
 	}
 	// per-axis maxima of the non-negative speeds, as bit patterns
@@ -404,6 +413,18 @@ __device__ __forceinline__ double step_start(const Stag_Params& P, bool& skip)
 	return skip ? 0.0 : step_dt(P);
 }
 
+// whether the -D face of cell x is one the step updates: an interior cell's, or a high wall's
+template <int D>
+__device__ __forceinline__ bool updated_face(const Stag_Params& P, const int x[3])
+{
+	#pragma unroll
+	for (int e = 0; e < 3; e++) {
+		const int top = P.n[e] + ((e == D and P.ext[e]) ? 1 : 0);
+		if (x[e] < 0 or x[e] >= top) return false;
+	}
+	return true;
+}
+
 /*
 Face_B += Face_dB / area for the three -d faces of every cell, as a z-marching
 stencil: a block of FTX x FTY threads owns a column of cells; the six
@@ -429,7 +450,7 @@ this thread's i-th element (-1 past the plane's end).
 */
 __device__ __forceinline__ void plane_offsets(const Stag_Params& P, const int gx0, const int gy0, long long off[FPER])
 {
-	const int nx = P.n[0], ny = P.n[1];
+	const int nx = P.E[0], ny = P.E[1];
 	const int tid = threadIdx.y * FTX + threadIdx.x;
 	#pragma unroll
 	for (int i = 0; i < FPER; i++) {
@@ -449,8 +470,8 @@ __device__ __forceinline__ void plane_offsets(const Stag_Params& P, const int gx
 
 __device__ __forceinline__ void load_plane(const Stag_Params& P, const long long off[FPER], const int pz, double v[FPER])
 {
-	const int nz = P.n[2];
-	const long long z = (long long)P.n[0] * P.n[1] * (((pz % nz) + nz) % nz);
+	const int nz = P.E[2];
+	const long long z = (long long)P.E[0] * P.E[1] * (((pz % nz) + nz) % nz);
 	#pragma unroll
 	for (int i = 0; i < FPER; i++) v[i] = off[i] >= 0 ? P.F[off[i] + z] : 0.0;
 }
@@ -478,7 +499,7 @@ __global__ void __launch_bounds__(FTX * FTY, 3) field_kernel(const Stag_Params P
 	}
 	__syncthreads();
 	const double dt = s_dt;
-	const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+	const int nx = P.E[0], ny = P.E[1], nz = P.E[2];
 	const int gx0 = blockIdx.x * FTX, gy0 = blockIdx.y * FTY;
 	const int gx = gx0 + tx, gy = gy0 + ty;
 	const bool own = gx < nx and gy < ny;
@@ -517,9 +538,12 @@ __global__ void __launch_bounds__(FTX * FTY, 3) field_kernel(const Stag_Params P
 			const long long c = col + plane * k;
 			const double d0 = face_dB<0>(P, get, dt), d1 = face_dB<1>(P, get, dt), d2 = face_dB<2>(P, get, dt);
 			const double b0 = P.B[c], b1 = P.B[P.N + c], b2 = P.B[2 * P.N + c];
-			P.Bo[c] = b0 + d0 / P.area[0];
-			P.Bo[P.N + c] = b1 + d1 / P.area[1];
-			P.Bo[2 * P.N + c] = b2 + d2 / P.area[2];
+			// on a bounded grid only the interior cells' faces (the high walls included) change; the
+			// layer's are refilled after the step
+			const int x[3] = {gx - P.ext[0], gy - P.ext[1], k - P.ext[2]};
+			P.Bo[c] = updated_face<0>(P, x) ? b0 + d0 / P.area[0] : b0;
+			P.Bo[P.N + c] = updated_face<1>(P, x) ? b1 + d1 / P.area[1] : b1;
+			P.Bo[2 * P.N + c] = updated_face<2>(P, x) ? b2 + d2 / P.area[2] : b2;
 		}
 		// plane k + 2 into its slot (not one of the three the slowest thread may still read), then
 		// the loads of plane k + 3
@@ -616,10 +640,15 @@ boundary cell, faces, edges and vertices alike; grid/solar_wind_box.hpp:
 cells are refilled from the interior after each step
 (apply_boundaries_sw_box, mhd/solar_wind_box.hpp:386-537) and the VALUE
 side's plane from its table (apply_solar_wind_boundaries, :227-306).  One
-step is five launches, each a grid-stride loop of one thread per cell:
-  bounded_faces_kernel  every cell's -d faces that have a cell on both sides;
-  bounded_field_kernel  the new normal field of the interior cells' faces,
-                        the walls of bounded dimensions included;
+step is five launches:
+  faces_kernel          the tiled face solves above over the grid with its
+                        layer: every cell's -d faces that have a cell on
+                        both sides;
+  field_kernel          the tiled face-field stencil above: the new normal
+                        field of the interior cells' faces, the walls of
+                        bounded dimensions included (the layer's faces are
+                        copied and refilled after the step);
+and, each a grid-stride loop of one thread per cell,
   bounded_cell_kernel   the interior cells' update, then update_vol_B, the
                         walls' copy sync (sync_magnetic_field: the boundary
                         cell's copy of a wall face is not updated, and the
@@ -641,11 +670,14 @@ __device__ __forceinline__ long long ext_index(const Stag_Params& P, const int i
 		                       + (long long)P.E[1] * (wrap_or_keep(P, 2, k) + P.ext[2]));
 }
 
+// coordinates of cell c in 32-bit arithmetic (create keeps N below 2^31)
 __device__ __forceinline__ void ext_coords(const Stag_Params& P, const long long c, int x[3])
 {
-	x[0] = int(c % P.E[0]) - P.ext[0];
-	x[1] = int((c / P.E[0]) % P.E[1]) - P.ext[1];
-	x[2] = int(c / ((long long)P.E[0] * P.E[1])) - P.ext[2];
+	const unsigned int u = (unsigned int)c, e0 = (unsigned int)P.E[0], e1 = (unsigned int)P.E[1];
+	const unsigned int q = u / e0;
+	x[0] = int(u - q * e0) - P.ext[0];
+	x[1] = int(q % e1) - P.ext[1];
+	x[2] = int(q / e1) - P.ext[2];
 }
 
 // total energy density from thermal pressure (get_total_energy_density, mhd/common.hpp:258-311)
@@ -656,116 +688,6 @@ __device__ __forceinline__ double energy(const double u[8], const double p, cons
 	const double kinetic = 0.5 * u[0] * (v0 * v0 + v1 * v1 + v2 * v2);
 	const double magnetic = 0.5 / g.mu0 * (u[5] * u[5] + u[6] * u[6] + u[7] * u[7]);
 	return p / (g.gamma - 1) + kinetic + magnetic;
-}
-
-// the -A face of cell c (coordinates x) against its -A neighbour, both derived along A only
-template <int SOLVER, int A>
-__device__ __forceinline__ void bounded_minus_face(const Stag_Params& P, const long long c, const int x[3],
-                                                   const double Uc[8], double& smax, bool& zero)
-{
-	int m[3] = {x[0], x[1], x[2]};
-	m[A] -= 1;
-	const long long mi = ext_index(P, m[0], m[1], m[2]);
-	double Um[8];
-	#pragma unroll
-	for (int v = 0; v < 8; v++) Um[v] = __ldg(P.U + v * P.N + mi);
-	const Derived dm = derive<A == 0, A == 1, A == 2>(Um[0], Um[1], Um[2], Um[3], Um[4], Um[5], Um[6], Um[7], P.gas);
-	const Derived dc = derive<A == 0, A == 1, A == 2>(Uc[0], Uc[1], Uc[2], Uc[3], Uc[4], Uc[5], Uc[6], Uc[7], P.gas);
-	double G[8];
-	uint32_t flag = 0;
-	const double s = solve_face<SOLVER>(side_of<A>(Um, dm), side_of<A>(Uc, dc), P.gas, G, flag);
-	if (flag != 0) record_failure(P, flag, mi, A);
-	smax = fmax(smax, s);
-	zero = zero or not (s > 0.0);
-	double out[8];
-	out[0] = G[0];
-	unrotate<A>(G[1], G[2], G[3], out[1], out[2], out[3]);
-	out[4] = G[4];
-	unrotate<A>(G[5], G[6], G[7], out[5], out[6], out[7]);
-	#pragma unroll
-	for (int v = 0; v < 8; v++) P.F[(A * 8 + v) * P.N + c] = out[v];
-}
-
-template <int SOLVER>
-__global__ void __launch_bounds__(THREADS) bounded_faces_kernel(const Stag_Params P)
-{
-	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-	bool zero = false;
-	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
-		int x[3];
-		ext_coords(P, c, x);
-		double Uc[8];
-		#pragma unroll
-		for (int v = 0; v < 8; v++) Uc[v] = __ldg(P.U + v * P.N + c);
-		// a layer cell's -d face past the low wall has no cell on its other side
-		if (not (P.ext[0] and x[0] < 0)) bounded_minus_face<SOLVER, 0>(P, c, x, Uc, s0, zero);
-		if (not (P.ext[1] and x[1] < 0)) bounded_minus_face<SOLVER, 1>(P, c, x, Uc, s1, zero);
-		if (not (P.ext[2] and x[2] < 0)) bounded_minus_face<SOLVER, 2>(P, c, x, Uc, s2, zero);
-	}
-	s0 = warp_max(s0);
-	s1 = warp_max(s1);
-	s2 = warp_max(s2);
-	const bool any_zero = __any_sync(0xffffffffu, zero);
-	if ((threadIdx.x & 31) == 0) {
-		Speed_Max& r = P.red[(P.phase + 1) % 3];
-		atomicMax(&r.smax[0], (unsigned long long)__double_as_longlong(s0));
-		atomicMax(&r.smax[1], (unsigned long long)__double_as_longlong(s1));
-		atomicMax(&r.smax[2], (unsigned long long)__double_as_longlong(s2));
-		if (any_zero) atomicOr(&r.zero, 1u);
-	}
-}
-
-// whether the -D face of cell x is one the step updates: an interior cell's, or a high wall's
-template <int D>
-__device__ __forceinline__ bool updated_face(const Stag_Params& P, const int x[3])
-{
-	#pragma unroll
-	for (int e = 0; e < 3; e++) {
-		const int top = P.n[e] + ((e == D and P.ext[e]) ? 1 : 0);
-		if (x[e] < 0 or x[e] >= top) return false;
-	}
-	return true;
-}
-
-template <int D>
-__device__ __forceinline__ void bounded_face_update(const Stag_Params& P, const long long c, const int x[3],
-                                                    const double dt)
-{
-	if (not updated_face<D>(P, x)) {
-		P.Bo[D * P.N + c] = P.B[D * P.N + c];
-		return;
-	}
-	auto get = [&](const int axis, const int comp, const int ox, const int oy, const int oz) {
-		return P.F[(axis * 8 + 5 + comp) * P.N + ext_index(P, x[0] + ox, x[1] + oy, x[2] + oz)];
-	};
-	P.Bo[D * P.N + c] = P.B[D * P.N + c] + face_dB<D>(P, get, dt) / P.area[D];
-}
-
-__global__ void __launch_bounds__(THREADS) bounded_field_kernel(const Stag_Params P)
-{
-	__shared__ double s_dt;
-	__shared__ int s_skip;
-	if (threadIdx.x == 0) {
-		bool skip;
-		s_dt = step_start(P, skip);
-		s_skip = skip ? 1 : 0;
-	}
-	__syncthreads();
-	const double dt = s_dt;
-	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.N; c += stride) {
-		if (s_skip != 0) {
-			#pragma unroll
-			for (int d = 0; d < 3; d++) P.Bo[d * P.N + c] = P.B[d * P.N + c];
-			continue;
-		}
-		int x[3];
-		ext_coords(P, c, x);
-		bounded_face_update<0>(P, c, x, dt);
-		bounded_face_update<1>(P, c, x, dt);
-		bounded_face_update<2>(P, c, x, dt);
-	}
 }
 
 /*
@@ -788,7 +710,8 @@ __device__ __forceinline__ double wall_sync(const double old, const double updat
 	return p1 + diff2 / 2;
 }
 
-__global__ void __launch_bounds__(THREADS) bounded_cell_kernel(const Stag_Params P)
+// two blocks per SM, as cell_kernel (the loads in flight matter more than a few spilled registers)
+__global__ void __launch_bounds__(THREADS, 2) bounded_cell_kernel(const Stag_Params P)
 {
 	__shared__ double s_dt;
 	__shared__ int s_skip;
@@ -895,18 +818,38 @@ __global__ void __launch_bounds__(THREADS) layer_fill_kernel(const Stag_Params P
 		if (skip) return;
 	}
 	const long long N = P.N;
+	// the layer's cells only, enumerated as the planes below and above the box (along a bounded z),
+	// then the rows in front and behind between them (bounded y), then the columns left and right
+	const long long nz_planes = P.ext[2] ? 2ll * P.E[0] * P.E[1] : 0;
+	const long long ny_rows = P.ext[1] ? 2ll * P.E[0] * P.n[2] : 0;
+	const long long nx_cols = P.ext[0] ? 2ll * P.n[1] * P.n[2] : 0;
+	const long long count = nz_planes + ny_rows + nx_cols;
 	const long long stride = (long long)gridDim.x * blockDim.x;
-	for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < N; c += stride) {
+	for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < count; t += stride) {
 		int x[3], s[3];
-		ext_coords(P, c, x);
-		bool shell[3], any = false;
+		if (t < nz_planes) {
+			const long long r = t % ((long long)P.E[0] * P.E[1]);
+			x[0] = int(r % P.E[0]) - P.ext[0];
+			x[1] = int(r / P.E[0]) - P.ext[1];
+			x[2] = t < nz_planes / 2 ? -1 : P.n[2];
+		} else if (t < nz_planes + ny_rows) {
+			const long long u = t - nz_planes, r = u % ((long long)P.E[0] * P.n[2]);
+			x[0] = int(r % P.E[0]) - P.ext[0];
+			x[1] = u < ny_rows / 2 ? -1 : P.n[1];
+			x[2] = int(r / P.E[0]);
+		} else {
+			const long long u = t - nz_planes - ny_rows, r = u % ((long long)P.n[1] * P.n[2]);
+			x[0] = u < nx_cols / 2 ? -1 : P.n[0];
+			x[1] = int(r % P.n[1]);
+			x[2] = int(r / P.n[1]);
+		}
+		const long long c = ext_index(P, x[0], x[1], x[2]);
+		bool shell[3];
 		#pragma unroll
 		for (int d = 0; d < 3; d++) {
 			shell[d] = x[d] < 0 or x[d] >= P.n[d];
-			any = any or shell[d];
 			s[d] = x[d] < 0 ? 0 : (x[d] >= P.n[d] ? P.n[d] - 1 : x[d]);
 		}
-		if (not any) continue;
 		const long long src = ext_index(P, s[0], s[1], s[2]);
 		double u[8];
 		#pragma unroll
@@ -1039,7 +982,7 @@ template <int SOLVER>
 int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 {
 	constexpr bool USES_BG = SOLVER == PAMHD_RUSANOV or SOLVER == PAMHD_HLL_ATHENA;
-	const dim3 tiles((P.n[0] + STX - 1) / STX, (P.n[1] + STY - 1) / STY, (P.n[2] + P.kchunk - 1) / P.kchunk);
+	const dim3 tiles((P.E[0] + STX - 1) / STX, (P.E[1] + STY - 1) / STY, (P.E[2] + P.kchunk - 1) / P.kchunk);
 	const dim3 block(STX, STY);
 	if (USES_BG and P.bg != nullptr) {
 		faces_kernel<SOLVER, USES_BG><<<tiles, block, SMEM_FACES, stream>>>(P);
@@ -1047,7 +990,7 @@ int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 		faces_kernel<SOLVER, false><<<tiles, block, SMEM_FACES, stream>>>(P);
 	}
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
-	const dim3 field_tiles((P.n[0] + FTX - 1) / FTX, (P.n[1] + FTY - 1) / FTY, (P.n[2] + P.fchunk - 1) / P.fchunk);
+	const dim3 field_tiles((P.E[0] + FTX - 1) / FTX, (P.E[1] + FTY - 1) / FTY, (P.E[2] + P.fchunk - 1) / P.fchunk);
 	field_kernel<<<field_tiles, dim3(FTX, FTY), SMEM_FIELD, stream>>>(P);
 	if (cudaGetLastError() != cudaSuccess) return PAMHD_ERR_CUDA;
 	cell_kernel<<<grid, THREADS, 0, stream>>>(P);
@@ -1058,8 +1001,12 @@ int launch_pair(const Stag_Params& P, const int grid, cudaStream_t stream)
 template <int SOLVER>
 int launch_bounded(const Stag_Params& P, const int grid, cudaStream_t stream)
 {
-	bounded_faces_kernel<SOLVER><<<grid, THREADS, 0, stream>>>(P);
-	bounded_field_kernel<<<grid, THREADS, 0, stream>>>(P);
+	// the tiled face solves and face-field stencil over the grid with its layer, then the cell
+	// update with the walls' copy sync, the layer and the inflow plane
+	const dim3 tiles((P.E[0] + STX - 1) / STX, (P.E[1] + STY - 1) / STY, (P.E[2] + P.kchunk - 1) / P.kchunk);
+	faces_kernel<SOLVER, false><<<tiles, dim3(STX, STY), SMEM_FACES, stream>>>(P);
+	const dim3 field_tiles((P.E[0] + FTX - 1) / FTX, (P.E[1] + FTY - 1) / FTY, (P.E[2] + P.fchunk - 1) / P.fchunk);
+	field_kernel<<<field_tiles, dim3(FTX, FTY), SMEM_FIELD, stream>>>(P);
 	bounded_cell_kernel<<<grid, THREADS, 0, stream>>>(P);
 	layer_fill_kernel<<<grid, THREADS, 0, stream>>>(P, P.Uo, P.Bo, true);
 	if (P.value_dim >= 0) {
@@ -1297,12 +1244,15 @@ int pamhd_gpu_staggered_create(const pamhd_cfg* cfg, pamhd_stag** out)
 	Stag_Params& P = x->base;
 	P = Stag_Params{};
 	// z chunks so that the face tiles fill the SMs about six times over
-	const long long tiles = (long long)((cfg->n[0] + STX - 1) / STX) * ((cfg->n[1] + STY - 1) / STY);
-	const long long chunks = std::max(1ll, std::min((long long)cfg->n[2], 18ll * sms / tiles));
-	P.kchunk = int((cfg->n[2] + chunks - 1) / chunks);
-	const long long ftiles = (long long)((cfg->n[0] + FTX - 1) / FTX) * ((cfg->n[1] + FTY - 1) / FTY);
-	const long long fchunks = std::max(1ll, std::min((long long)cfg->n[2], 12ll * sms / ftiles));
-	P.fchunk = int((cfg->n[2] + fchunks - 1) / fchunks);
+	// (over the grid with its boundary layer on a bounded grid)
+	int E[3];
+	for (int d = 0; d < 3; d++) E[d] = cfg->n[d] + 2 * ext[d];
+	const long long tiles = (long long)((E[0] + STX - 1) / STX) * ((E[1] + STY - 1) / STY);
+	const long long chunks = std::max(1ll, std::min((long long)E[2], 18ll * sms / tiles));
+	P.kchunk = int((E[2] + chunks - 1) / chunks);
+	const long long ftiles = (long long)((E[0] + FTX - 1) / FTX) * ((E[1] + FTY - 1) / FTY);
+	const long long fchunks = std::max(1ll, std::min((long long)E[2], 12ll * sms / ftiles));
+	P.fchunk = int((E[2] + fchunks - 1) / fchunks);
 	if (cudaFuncSetAttribute(field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_FIELD))
 		!= cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
