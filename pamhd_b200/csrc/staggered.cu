@@ -3,7 +3,8 @@ The staggered-field MHD step (the reference's timestep() with face magnetic
 field, mhd/solve.hpp:1837-1924) on uniform grids, behind
 pamhd_gpu_staggered_* of include/pamhd_gpu.h.  Periodic grids take the
 tiled kernels described here; bounded grids (a layer of boundary cells
-outside the walls) the plain kernels described further down.
+outside the walls) the same face and face-field kernels over the grid with
+its layer, and the cell and layer kernels described further down.
 
 Data in HBM, every array x fastest over the n0 x n1 x n2 cells, no ghosts
 (neighbours wrap around):
