@@ -450,9 +450,11 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
     st = torch.cuda.ExternalStream(batch.stream(), device=dev)
     batched_ms = timed(lambda: batch.run(steps))
     run_grid, run_items, graphed = batch.run_info()
-    # boxes whose state the reference scheme rejects keep being stepped (the same work per step);
-    # they are counted, not hidden
+    # a box whose state the reference scheme rejects stops after its failing step (later steps only
+    # copy it): it is counted, not hidden, and the value counts the cell updates the boxes made
     failed = [i for i in range(len(boxes)) if batch.status(i)[0] != 0]
+    taken = [batch.time(i)[1] for i in range(len(boxes))]
+    updates = sum(b["n"] ** 3 * t for b, t in zip(boxes, taken))
     failed_steps = {}
     batch.close()
 
@@ -481,9 +483,9 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
         if ctx.status()[0] != 0:
             failed_steps[len(failed_steps)] = True
         ctx.close()
-    batched = cells * steps / (batched_ms / 1e3)
+    batched = updates / (batched_ms / 1e3)
     healthy_cells = sum(b["n"] ** 3 for i, b in enumerate(boxes) if i not in failed)
-    plain = cells * steps / (plain_ms / 1e3) if sequential else None
+    plain = updates / (plain_ms / 1e3) if sequential else None
     return {
         "workload": f"{len(boxes)} independent SI solar-wind boxes, edges from {{32,48,64,96,128}} "
                     f"({cells} cells), HLL, inflow -x, copy elsewhere, per-box CFL 0.5 timestep, {steps} steps",
@@ -495,16 +497,18 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
                                                              "planes_per_item": run_tiling[1]}},
         "healthy_boxes_value": healthy_cells * steps / (batched_ms / 1e3),
         "healthy_boxes": len(boxes) - len(failed),
-        "per_step_launches": {"value": cells * steps / (per_step_ms / 1e3), "ms": per_step_ms,
+        "per_step_launches": {"value": updates / (per_step_ms / 1e3), "ms": per_step_ms,
                               "tuned": {"tile": f"32x{tiling[0]}", "planes_per_item": tiling[1],
                                         "grid": tiling[2], "by": "autotuner" if tune else "defaults"}},
         "plain_sequential": plain,
         "plain_ms": plain_ms,
         "batched_over_plain": batched / plain if sequential else None,
         "boxes_failed": failed,
+        "boxes_failed_steps": {i: taken[i] for i in failed},
         "boxes_failed_note": "boxes whose state hit the positivity check of the reference scheme within the "
-                             "run (the CPU oracle fails box 24 at step 236, like the GPU); same count in the "
-                             f"sequential run: {len(failed_steps)}",
+                             "run (the CPU oracle fails box 24 at step 236, like the GPU), with the steps each "
+                             "took (the failing one included); they stop there, and value counts the cell "
+                             f"updates made; same count in the sequential run: {len(failed_steps)}",
         "what": "batched: all steps of all boxes in one persistent cooperative launch (a box's step waits only for "
                 "its own previous step; each box its own lagged CFL dt), replayed from a CUDA graph; "
                 "per_step_launches: the same ensemble with one launch per step; plain: each box in its own context, "

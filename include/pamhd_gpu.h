@@ -173,7 +173,12 @@ and its minimize_timestep reads (mhd/solve.hpp:1933-2014), so that a host
 caller can apply its own timestep rule: dt = min over dimensions d of
 CFL * dx_d / max_signal[d].  Faces between two ghost cells of a
 non-periodic side count, as in the reference.
-Returns PAMHD_ERR_PHYSICS if any face met an invalid state.
+Returns PAMHD_ERR_PHYSICS if any face met an invalid state.  The step in
+which a face fails completes (its state is what the faces gave); the grid
+then stops, as the reference aborts there (mhd/solve.hpp:156-181): every
+later step (pamhd_gpu_step, _steps, _step_part) leaves the state, the time
+and the step count as they are (dt 0, max_signal the failing step's) until
+set_state.
 */
 int pamhd_gpu_step(pamhd_ctx* ctx, double max_dt, double* dt_taken, double* max_signal);
 
@@ -375,7 +380,12 @@ step is a dt = 0 priming step for every box.
 int pamhd_gpu_batch_set_state(pamhd_batch* batch, int32_t box, const double* const soa[8]);
 int pamhd_gpu_batch_get_state(pamhd_batch* batch, int32_t box, double* const soa[8]);
 
-/* nsteps steps of every box, each capped so that its time does not pass t_end; no host sync. */
+/*
+nsteps steps of every box, each capped so that its time does not pass t_end;
+no host sync.  A box in which a face failed stops after that step (its state,
+time and step count stay as they are, as pamhd_gpu_step describes) while the
+other boxes go on.
+*/
 int pamhd_gpu_batch_steps(pamhd_batch* batch, int32_t nsteps, double t_end);
 
 /*

@@ -231,7 +231,7 @@ int reset_run_state(pamhd_batch& b)
 	std::vector<Status> s(b.nboxes);
 	for (auto& x: s) {
 		x.flags = 0;
-		x.pad = 0;
+		x.fail_step = 0;
 		x.first = ~0ull;
 	}
 	PAMHD_TRY(check(cudaMemcpyAsync(b.status, s.data(), s.size() * sizeof(Status), cudaMemcpyHostToDevice,
@@ -830,9 +830,13 @@ int pamhd_gpu_batch_dt_history(pamhd_batch* b, const int32_t box, double* dt, co
 	std::vector<double> all(b->hist_len);
 	PAMHD_TRY(check(cudaMemcpyAsync(all.data(), b->dt_hist + (long long)b->hist_len * box,
 	                                b->hist_len * sizeof(double), cudaMemcpyDeviceToHost, b->stream)));
+	// the steps the box took (a box that stopped at a failure holds its count)
+	Clock c;
+	PAMHD_TRY(check(cudaMemcpyAsync(&c, b->clock + 3 * box + b->steps % 3, sizeof c, cudaMemcpyDeviceToHost,
+	                                b->stream)));
 	PAMHD_TRY(check(cudaStreamSynchronize(b->stream)));
-	const long long n = std::min<long long>(std::min<long long>(b->steps, b->hist_len), count);
-	for (long long i = 0; i < n; i++) dt[i] = all[(b->steps - n + i) % b->hist_len];
+	const long long n = std::min<long long>(std::min<long long>(c.steps, b->hist_len), count);
+	for (long long i = 0; i < n; i++) dt[i] = all[(c.steps - n + i) % b->hist_len];
 	if (written != nullptr) *written = int32_t(n);
 	return PAMHD_OK;
 }

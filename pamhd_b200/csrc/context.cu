@@ -93,7 +93,7 @@ int reset_run_state(pamhd_ctx& x)
 	PAMHD_TRY(check(cudaMemsetAsync(x.clock, 0, 3 * sizeof(Clock), x.stream)));
 	Status s;
 	s.flags = 0;
-	s.pad = 0;
+	s.fail_step = 0;
 	s.first = ~0ull;
 	PAMHD_TRY(check(cudaMemcpyAsync(x.status, &s, sizeof s, cudaMemcpyHostToDevice, x.stream)));
 	x.steps = 0;
@@ -515,11 +515,14 @@ int pamhd_gpu_dt_history(pamhd_ctx* x, double* dt, const int32_t count, int32_t*
 	std::vector<double> all(x->hist_len);
 	PAMHD_TRY(check(cudaMemcpyAsync(all.data(), x->dt_hist, x->hist_len * sizeof(double),
 	                                cudaMemcpyDeviceToHost, x->stream)));
+	// the steps the grid took (a grid that stopped at a failure holds its count)
+	Clock c;
+	PAMHD_TRY(check(cudaMemcpyAsync(&c, x->clock + x->steps % 3, sizeof c, cudaMemcpyDeviceToHost, x->stream)));
 	PAMHD_TRY(check(cudaStreamSynchronize(x->stream)));
-	const long long have = std::min<long long>(x->steps, x->hist_len);
+	const long long have = std::min<long long>(c.steps, x->hist_len);
 	const long long n = std::min<long long>(have, count);
 	for (long long i = 0; i < n; i++) {
-		const long long step = x->steps - n + i;
+		const long long step = c.steps - n + i;
 		dt[i] = all[step % x->hist_len];
 	}
 	if (written != nullptr) *written = int32_t(n);

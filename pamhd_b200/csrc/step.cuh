@@ -52,7 +52,7 @@ struct Clock {
 // error state: OR of flags and the first failing face ((key << 8) | flag)
 struct Status {
 	unsigned int flags;
-	unsigned int pad;
+	unsigned int fail_step;        // the cell-centred steps: 1 + the clock's step count of the failing step (0: none)
 	unsigned long long first;
 };
 

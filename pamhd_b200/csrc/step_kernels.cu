@@ -102,12 +102,29 @@ __device__ __forceinline__ double step_dt(const Step_Params& P)
 	return (cap <= smallest) ? cap : smallest;
 }
 
-// block-wide start of a step: every block computes dt; block 0 advances the clock ring
-__device__ __forceinline__ double begin_step(const Step_Params& P, double* s_dt, const bool first_block)
+/*
+Whether the grid stopped in an earlier step: a face failed there (the
+reference aborts at that step, mhd/solve.hpp:156-181).  Such a step leaves
+the state as it is and the clock where it is.  The failing step itself is
+completed (every block of it sees the same answer: the failure is dated by
+the clock's step count).
+*/
+__device__ __forceinline__ bool stopped_before(const Step_Params& P)
+{
+	const unsigned int at = __ldcg(&P.status->fail_step);
+	return at != 0u and (long long)(at - 1u) < __ldcg(&P.clock[P.phase].steps);
+}
+
+// block-wide start of a step: every block computes dt; block 0 advances the clock ring.  *s_stop:
+// the grid stopped in an earlier step (dt 0, the clock held)
+__device__ __forceinline__ double begin_step(const Step_Params& P, double* s_dt, const bool first_block,
+                                             int* s_stop)
 {
 	if (threadIdx.x == 0 and threadIdx.y == 0) {
-		const double dt = step_dt(P);
+		const bool stop = stopped_before(P);
+		const double dt = stop ? 0.0 : step_dt(P);
 		*s_dt = dt;
+		*s_stop = stop ? 1 : 0;
 		if (first_block) {
 			Clock c;
 			c.t = __ldcg(&P.clock[P.phase].t);
@@ -115,11 +132,20 @@ __device__ __forceinline__ double begin_step(const Step_Params& P, double* s_dt,
 			Clock& next = P.clock[(P.phase + 1) % 3];
 			next.t = c.t + dt;
 			next.dt = dt;
-			next.steps = c.steps + 1;
-			if (P.dt_hist != nullptr) P.dt_hist[c.steps % P.hist_len] = dt;
+			next.steps = stop ? c.steps : c.steps + 1;
+			if (P.dt_hist != nullptr and not stop) P.dt_hist[c.steps % P.hist_len] = dt;
 			Speed_Max& z = P.red[(P.phase + 2) % 3];
 			z.smax[0] = z.smax[1] = z.smax[2] = 0ull;
 			z.zero = 0u;
+			if (stop) {
+				// no face is solved: the failing step's maxima stay the latest
+				const Speed_Max& r = P.red[P.phase];
+				Speed_Max& o = P.red[(P.phase + 1) % 3];
+				o.smax[0] = __ldcg(&r.smax[0]);
+				o.smax[1] = __ldcg(&r.smax[1]);
+				o.smax[2] = __ldcg(&r.smax[2]);
+				o.zero = __ldcg(&r.zero);
+			}
 		}
 	}
 	__syncthreads();
@@ -140,6 +166,8 @@ __device__ void record_failure(const Step_Params& P, const uint32_t flag, const 
 		+ nx * ((unsigned long long)(c[1] + P.ext[1]) + ny * (unsigned long long)(c[2] + P.ext[2]));
 	atomicOr(&P.status->flags, flag);
 	atomicMin(&P.status->first, ((lin * 4ull + (unsigned long long)dir) << 8) | flag);
+	// every failure of a step writes the same date
+	P.status->fail_step = (unsigned int)(__ldcg(&P.clock[P.phase].steps) + 1);
 }
 
 __device__ __forceinline__ void flush_speeds(const Step_Params& P, double smax[3], bool zero)
@@ -381,6 +409,37 @@ __device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec
 
 // ------------------------------------------------------------------ the step
 
+// the planes [kb, ke) of block row bz: a z chunk, or with kpart 1 the first (bz 0) or the last
+// (bz 1) plane alone, or with kpart 2 a chunk of the planes between them
+__device__ __forceinline__ void tile_planes(const Step_Params& P, const int bz, int& kb, int& ke)
+{
+	const int nz = P.L.n[2];
+	const int kbase = P.kpart == 2 ? 1 : 0, ktop = P.kpart == 2 ? nz - 1 : nz;
+	kb = P.kpart == 1 ? (bz == 0 ? 0 : nz - 1) : kbase + bz * P.kchunk;
+	ke = P.kpart == 1 ? kb + 1 : min(ktop, kb + P.kchunk);
+}
+
+/*
+A step of a grid that stopped: the tile's cells are copied into the new
+state unchanged, with the ghosts a step writes, so that both states hold
+the failing step's result.  CO: loads at L2 (see load_record).
+*/
+template <int TY, bool CO>
+__device__ void tile_hold(const Step_Params& P, const int bx, const int by, const int bz)
+{
+	int kb, ke;
+	tile_planes(P, bz, kb, ke);
+	const int gx = bx * TX + threadIdx.x, gy = by * TY + threadIdx.y;
+	if (gx >= P.L.n[0] or gy >= P.L.n[1]) return;
+	for (int k = kb; k < ke; k++) {
+		const long long off = P.L.offset(gx, gy, k);
+		double U[8];
+		#pragma unroll
+		for (int v = 0; v < 8; v++) U[v] = CO ? __ldcg(P.in + v * P.L.var + off) : P.in[v * P.L.var + off];
+		write_cell(P, gx, gy, k, U, 0.0);
+	}
+}
+
 /*
 One work item of a step: the tile (bx, by) of 32 x TY columns over the z
 chunk bz, marched plane by plane; the face speeds are folded into
@@ -421,12 +480,9 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 	const bool own = gx < nx and gy < ny;
 	// the +x / +y ghost of a partial tile lies inside the tile's own columns / rows
 	const bool stage = gx <= nx and (TY == 1 ? gy == 0 : gy <= ny);
-	// the planes of this block: a z chunk, or with kpart 1 the first (bz 0) or the last (bz 1)
-	// plane alone, or with kpart 2 a chunk of the planes between them
-	const int nz = P.L.n[2];
-	const int kbase = P.kpart == 2 ? 1 : 0, ktop = P.kpart == 2 ? nz - 1 : nz;
-	const int kb = P.kpart == 1 ? (bz == 0 ? 0 : nz - 1) : kbase + bz * P.kchunk;
-	const int ke = P.kpart == 1 ? kb + 1 : min(ktop, kb + P.kchunk);
+	// the planes of this block
+	int kb, ke;
+	tile_planes(P, bz, kb, ke);
 	const int kfirst = zact ? kb - 1 : kb;
 	const int klast = zact ? ke : ke - 1;
 	const int ri = (ty + T::JO) * T::W + tx + 1;
@@ -552,8 +608,13 @@ __global__ void __launch_bounds__(TX * TY, MINB) step_kernel(const Step_Params P
 {
 	extern __shared__ __align__(16) double smem[];
 	__shared__ double s_dt;
+	__shared__ int s_stop;
 	const bool first_block = blockIdx.x == 0 and blockIdx.y == 0 and blockIdx.z == 0;
-	const double dt = begin_step(P, &s_dt, first_block);
+	const double dt = begin_step(P, &s_dt, first_block, &s_stop);
+	if (s_stop) {
+		tile_hold<TY, false>(P, blockIdx.x, blockIdx.y, blockIdx.z);
+		return;
+	}
 	double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 	bool zero = false;
 	tile_step<SOLVER, TY>(P, smem, dt, blockIdx.x, blockIdx.y, blockIdx.z, s0, s1, s2, zero);
@@ -576,6 +637,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) batch_step_kernel(const Step_Pa
 	extern __shared__ __align__(16) double smem[];
 	__shared__ Step_Params sp;
 	__shared__ double s_dt;
+	__shared__ int s_stop;
 	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
 	for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
 		const int4 w = items[item];
@@ -586,8 +648,12 @@ __global__ void __launch_bounds__(TX * TY, MINB) batch_step_kernel(const Step_Pa
 		}
 		__syncthreads();
 		const bool first = w.y == 0 and w.z == 0 and w.w == 0;
-		const double dt = begin_step(sp, &s_dt, first);
+		const double dt = begin_step(sp, &s_dt, first, &s_stop);
 		const int tiles_x = (sp.L.n[0] + TX - 1) / TX;
+		if (s_stop) {
+			tile_hold<TY, false>(sp, w.y % tiles_x, w.y / tiles_x, w.z);
+			continue;
+		}
 		double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 		bool zero = false;
 		tile_step<SOLVER, TY>(sp, smem, dt, w.y % tiles_x, w.y / tiles_x, w.z, s0, s1, s2, zero);
@@ -679,6 +745,8 @@ blockIdx.y enumerates (ghost dimension d, side, tangential axis e).
 template <int SOLVER>
 __device__ __forceinline__ void boundary_speeds(const Step_Params& P)
 {
+	// a grid that stopped solves no face (the value is the same for every thread)
+	if (stopped_before(P)) return;
 	int combos[12][3];
 	const int nc = boundary_combos(P, combos);
 	double smax[3] = {0.0, 0.0, 0.0};
@@ -824,6 +892,7 @@ __global__ void __launch_bounds__(TX * TY, MINB) batch_run_kernel(
 	__shared__ double s_dt;
 	__shared__ unsigned int s_q;
 	__shared__ int s_go;
+	__shared__ int s_stop;
 	const int tid = threadIdx.y * blockDim.x + threadIdx.x;
 	const int nthreads = blockDim.x * blockDim.y;
 	const unsigned int total = (unsigned int)nsteps * (unsigned int)nitems;
@@ -870,11 +939,15 @@ __global__ void __launch_bounds__(TX * TY, MINB) batch_run_kernel(
 		bool zero = false;
 		if (w.w == 0) {
 			const bool first = w.y == 0 and w.z == 0;
-			const double dt = begin_step(sp, &s_dt, first);
+			const double dt = begin_step(sp, &s_dt, first, &s_stop);
 			const int tiles_x = (sp.L.n[0] + TX - 1) / TX;
-			tile_step<SOLVER, TY, true>(sp, smem, dt, w.y % tiles_x, w.y / tiles_x, w.z, smax[0], smax[1],
-			                            smax[2], zero);
-		} else {
+			if (s_stop) {
+				tile_hold<TY, true>(sp, w.y % tiles_x, w.y / tiles_x, w.z);
+			} else {
+				tile_step<SOLVER, TY, true>(sp, smem, dt, w.y % tiles_x, w.y / tiles_x, w.z, smax[0], smax[1],
+				                            smax[2], zero);
+			}
+		} else if (not stopped_before(sp)) {
 			// ghost-ghost faces: combination w.y, faces [w.z BOUNDARY_CHUNK, (w.z + 1) BOUNDARY_CHUNK)
 			int combos[12][3];
 			const int nc = boundary_combos(sp, combos);

@@ -141,6 +141,43 @@ def test_batch_reports_failing_box():
         assert batch.status(i)[0] == 0
 
 
+@pytest.mark.parametrize("persistent", [False, True])
+def test_failed_box_stops_while_the_others_go_on(persistent):
+    """A box whose face fails stops after that step (its state, time and step count stay, as a
+    reference run aborts there) while the other boxes take every step, bit for bit as in their
+    own contexts; in one launch per step and in the persistent run."""
+    cfgs, U0s = small_ensemble()
+    U0s[2] = U0s[2].copy()
+    U0s[2][4, 1, 2, 3] = 0.0  # negative pressure in box 2: its first step fails
+    batch = pg.Batch(cfgs)
+    for i, U in enumerate(U0s):
+        batch.set_state(i, U)
+    batch.steps(1)
+    with pytest.raises(pg.PhysicsError):
+        batch.sync()
+    held = batch.get_state(2)
+    assert batch.time(2) == (0.0, 1, 0.0)
+    if persistent:
+        batch.run(12)
+    else:
+        batch.steps(12)
+    with pytest.raises(pg.PhysicsError) as e:
+        batch.sync()
+    assert "box 2" in str(e.value)
+    np.testing.assert_array_equal(batch.get_state(2), held)
+    assert batch.time(2) == (0.0, 1, 0.0)
+    np.testing.assert_array_equal(batch.dt_history(2, 20), [0.0])
+    for i in (0, 1, 3, 4):
+        assert batch.status(i)[0] == 0
+        ctx = pg.Context(cfgs[i])
+        ctx.set_state(U0s[i])
+        ctx.steps(13, 1e300)
+        ctx.sync()
+        np.testing.assert_array_equal(batch.get_state(i), ctx.get_state())
+        np.testing.assert_array_equal(batch.dt_history(i, 20), ctx.dt_history(20))
+        assert batch.time(i) == ctx.time()
+
+
 # ---------------------------------------------------------------- the persistent run
 
 

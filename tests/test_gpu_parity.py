@@ -299,6 +299,49 @@ def test_blast_positivity_failure_matches_oracle(port):
     assert fail_g == fail_o
 
 
+def test_steps_after_a_failure_hold_the_grid():
+    """The reference aborts in the step whose face fails (mhd/solve.hpp:156-181): here that step
+    completes and every later one leaves the grid as it left it.  The 64^3 blast loses positivity
+    after some steps; then steps one at a time, in a CUDA graph and split in two parts keep the
+    state, the time, the step count and the dt history, and report the error again; set_state
+    starts over."""
+    n = 64
+    U0 = states.blast_wave(n)
+    cfg = pg.Config(n=(n, n, n), solver=pg.HLLD, cell_length=(1 / n,) * 3, time_step_factor=0.4)
+    g = pg.Context(cfg)
+    g.set_state(U0)
+    failed = None
+    for step in range(120):
+        try:
+            g.step(1e30)
+        except pg.PhysicsError as e:
+            failed = (step, e.flags, e.cell, e.direction)
+            break
+    assert failed is not None and failed[0] > 5
+    held = g.get_state()
+    t, count, _ = g.time()
+    assert count == failed[0] + 1
+    history = g.dt_history(200)
+    assert len(history) == count and history[-1] > 0.0
+    for _ in range(2):
+        with pytest.raises(pg.PhysicsError) as e:
+            g.step(1e30)
+        assert (e.value.flags, e.value.cell, e.value.direction) == failed[1:]
+    g.steps(13, 1e30)
+    with pytest.raises(pg.PhysicsError):
+        g.sync()
+    g.step_part(1, 1e30)
+    g.step_part(2, 1e30)
+    with pytest.raises(pg.PhysicsError):
+        g.sync()
+    np.testing.assert_array_equal(g.get_state(), held)
+    assert g.time() == (t, count, 0.0)
+    np.testing.assert_array_equal(g.dt_history(200), history)
+    g.set_state(U0)
+    assert g.step(1e30) == 0.0 and g.step(1e30) == history[1]
+    assert g.status()[0] == 0
+
+
 @pytest.mark.parametrize("count", [0, 1, 33, 257])
 def test_face_flux_empty_and_ragged_batches(port, count):
     """Batches of no face, one face and counts that leave partial blocks: the same results as
