@@ -103,7 +103,7 @@ long long cells_of(const pamhd_cfg& c)
 std::vector<int> tile_choices(const pamhd_batch& b)
 {
 	if (not b.yact) return {1};
-	return {step_tile_rows(), 8};
+	return {batch_tile_rows(), 8};
 }
 
 // ghost states of a box's VALUE sides at time t: configured values or time-stamped inflow
@@ -437,7 +437,7 @@ int pamhd_gpu_batch_create(const int32_t device, const int32_t nboxes, const pam
 		or cudaMemset(b->dt_hist, 0, size_t(b->hist_len) * nboxes * sizeof(double)) != cudaSuccess) {
 		return fail(PAMHD_ERR_CUDA);
 	}
-	b->ty = b->yact ? step_tile_rows() : 1;
+	b->ty = b->yact ? batch_tile_rows() : 1;
 	for (const int ty: tile_choices(*b)) {
 		if (prepare_batch_kernels(b->solver, ty) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);
 		if (prepare_batch_run_kernels(b->solver, ty) != PAMHD_OK) return fail(PAMHD_ERR_CUDA);

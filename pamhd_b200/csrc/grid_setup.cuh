@@ -12,6 +12,10 @@ constant part of its step parameters.
 
 #include "step.cuh"
 
+#ifndef PAMHD_CHUNK_BLOCKS
+#define PAMHD_CHUNK_BLOCKS 4736   // blocks of a step the z chunking aims at: 32 per SM
+#endif
+
 namespace pamhd_b200 {
 
 inline int validate(const pamhd_cfg& c)
@@ -147,9 +151,9 @@ inline bool grid_params(const pamhd_cfg& c, const Layout& L, Step_Params& P, con
 		if (P.active[d] and not P.periodic[d] and own_side and active_count > 1) needs_boundary_speeds = true;
 	}
 	// z planes per block: enough blocks for several waves on 148 SMs, few redundant z faces
-	const int ty = P.active[1] ? step_tile_rows() : 1;
+	const int ty = P.active[1] ? step_tile_rows(c.solver) : 1;
 	const long long tiles = (long long)((c.n[0] + 31) / 32) * ((c.n[1] + ty - 1) / ty);
-	long long chunks = (2368 + tiles - 1) / tiles;
+	long long chunks = (PAMHD_CHUNK_BLOCKS + tiles - 1) / tiles;
 	chunks = std::max(1LL, std::min(chunks, (long long)std::max(1, c.n[2] / 16)));
 	P.kchunk = int((c.n[2] + chunks - 1) / chunks);
 	if (kchunk_cap > 0) P.kchunk = std::min(P.kchunk, kchunk_cap);

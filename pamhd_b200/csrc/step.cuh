@@ -122,8 +122,8 @@ int launch_face_flux(int solver, long long n, const double* neg, const double* p
                      const Gas& gas, double* flux, double* speed, uint32_t* flags, cudaStream_t stream);
 int launch_totals(const double* state, const Layout& L, double volume, double* partial, int nblocks,
                   cudaStream_t stream);
-int step_smem_bytes(int ty);
-int step_tile_rows();
+int step_tile_rows(int solver);
+int batch_tile_rows();
 int prepare_batch_kernels(int solver, int tile_rows);
 int batch_blocks_per_sm(int solver, int tile_rows, int* blocks);
 int launch_batch_step(const Step_Params* boxes, const int4* items, int nitems, int phase, int grid, int solver,

@@ -37,12 +37,29 @@ constexpr int TX = 32;
 #ifndef PAMHD_MINB
 #define PAMHD_MINB 3
 #endif
-constexpr int TY_3D = PAMHD_TY;     // tile rows of 2-D and 3-D grids
+#ifndef PAMHD_STEP_TY
+#define PAMHD_STEP_TY 8
+#endif
+#ifndef PAMHD_STEP_MINB
+#define PAMHD_STEP_MINB 2
+#endif
+constexpr int TY_3D = PAMHD_TY;     // tile rows of the batched step on 2-D and 3-D grids
 constexpr int MINB = PAMHD_MINB;    // resident blocks per SM asked of the register allocator
-constexpr int NV = 13;  // record: rho, mom xyz, E, B xyz, 1/rho, p, cf x, cf y, cf z
+constexpr int TY_STEP = PAMHD_STEP_TY;  // tile rows of the single-grid step (Roe aside)
+// record of a cell in shared memory: rho, mom xyz, E, B xyz, 1/rho, p, cf x, cf y (the fast
+// speed along z is needed by the column's owner only, which keeps it in a register)
+constexpr int NV = 12;
 enum { R_RINV = 8, R_P = 9, R_CF = 10 };
 
-template <int TY> struct Tile {
+/*
+Rows of a face flux kept in shared memory, in the face frame: rho, the
+normal and the two tangential momenta, E, the two tangential field
+components, and the normal field component only for Rusanov, the one
+solver whose flux of it is not zero (mhd/rusanov.hpp diffuses it).
+*/
+template <int SOLVER> struct Flux_Rows { static constexpr int N = SOLVER == PAMHD_RUSANOV ? 8 : 7; };
+
+template <int TY, int NF = 8> struct Tile {
 	static constexpr int JO = (TY > 1) ? 1 : 0;            // halo rows exist when y is active
 	static constexpr int W = TX + 2;                       // record row width (halo columns)
 	static constexpr int H = TY + 2 * JO;                  // record rows
@@ -50,15 +67,34 @@ template <int TY> struct Tile {
 	static constexpr int REC = NV * CELLS;                 // doubles per plane slot
 	static constexpr int FXN = TY * (TX + 1);              // x faces of a plane
 	static constexpr int FYN = (TY > 1) ? (TY + 1) * TX : 0;
-	static constexpr size_t BYTES = size_t(2 * REC + 8 * FXN + 8 * FYN) * 8 + size_t(2 * CELLS) * 4;
+	// two record slots, the x and y face fluxes, one validity byte per cell and slot
+	static constexpr size_t BYTES = size_t(2 * REC + NF * FXN + NF * FYN) * 8 + size_t(2 * CELLS);
 };
 
-int step_smem_bytes(const int ty)
+template <int SOLVER, int TY> constexpr size_t tile_bytes() { return Tile<TY, Flux_Rows<SOLVER>::N>::BYTES; }
+
+/*
+Tile rows of the single-grid step on 2-D and 3-D grids and the resident
+blocks per SM it is built for: 32 x 8 tiles, two blocks of 256 threads per
+SM at 128 registers (16 warps per SM; a taller tile solves fewer halo
+faces and records per cell); Roe's solver needs more registers than that,
+so it keeps 32 x 4 tiles at three blocks per SM.
+*/
+template <int SOLVER> struct Step_Shape {
+	static constexpr int rows = SOLVER == PAMHD_ROE_ATHENA ? TY_3D : TY_STEP;
+	static constexpr int blocks = SOLVER == PAMHD_ROE_ATHENA ? MINB : PAMHD_STEP_MINB;
+};
+
+template <int SOLVER, int TY> struct Step_Minb {
+	static constexpr int value = (TY > 1 and TY == Step_Shape<SOLVER>::rows) ? Step_Shape<SOLVER>::blocks : MINB;
+};
+
+int step_tile_rows(const int solver)
 {
-	return ty == 1 ? int(Tile<1>::BYTES) : int(Tile<TY_3D>::BYTES);
+	return solver == PAMHD_ROE_ATHENA ? Step_Shape<PAMHD_ROE_ATHENA>::rows : TY_STEP;
 }
 
-int step_tile_rows()
+int batch_tile_rows()
 {
 	return TY_3D;
 }
@@ -293,8 +329,8 @@ persistent launch whose later steps read what other blocks wrote (the
 non-coherent L1 could hold a line of the same buffer from two steps before).
 */
 template <bool CX, bool CY, bool CZ, bool CO>
-__device__ __forceinline__ void load_record(const Step_Params& P, double* rec, uint32_t* bad, const int cells,
-                                            const int ri, const int i, const int j, const int k)
+__device__ __forceinline__ double load_record(const Step_Params& P, double* rec, uint8_t* bad, const int cells,
+                                              const int ri, const int i, const int j, const int k)
 {
 	const long long off = P.L.offset(i, j, k);
 	double U[8];
@@ -307,13 +343,16 @@ __device__ __forceinline__ void load_record(const Step_Params& P, double* rec, u
 	rec[R_P * cells + ri] = d.p;
 	if (CX) rec[(R_CF + 0) * cells + ri] = d.cf[0];
 	if (CY) rec[(R_CF + 1) * cells + ri] = d.cf[1];
-	if (CZ) rec[(R_CF + 2) * cells + ri] = d.cf[2];
-	bad[ri] = d.bad;
+	bad[ri] = uint8_t(d.bad);
+	// the fast speed along z, for the caller's z faces
+	return CZ ? d.cf[2] : 0.0;
 }
 
-// one cell of a record slot seen from a face normal to axis A (rotation by index permutation)
+// one cell of a record slot seen from a face normal to axis A (rotation by index permutation),
+// with its fast speed along A
 template <int A>
-__device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, const int cells, const int ri)
+__device__ __forceinline__ Side side_at(const double* rec, const uint8_t* bad, const int cells, const int ri,
+                                        const double cf)
 {
 	Side s;
 	s.rho = rec[ri];
@@ -322,7 +361,7 @@ __device__ __forceinline__ Side side_at(const double* rec, const uint32_t* bad, 
 	rotate<A>(rec[5 * cells + ri], rec[6 * cells + ri], rec[7 * cells + ri], s.b0, s.b1, s.b2);
 	s.rinv = rec[R_RINV * cells + ri];
 	s.p = rec[R_P * cells + ri];
-	s.cf = rec[(R_CF + A) * cells + ri];
+	s.cf = cf;
 	s.v0 = s.m0 * s.rinv;
 	s.v1 = s.m1 * s.rinv;
 	s.v2 = s.m2 * s.rinv;
@@ -337,12 +376,13 @@ cell).  Each kernel inlines this once, so a z face is computed by the same
 instructions wherever it lies in the tiling.
 */
 template <int SOLVER, int CELLS>
-__device__ __forceinline__ void solve_z(const Step_Params& P, const double* rec_l, const uint32_t* bad_l,
-                                        const double* rec_r, const uint32_t* bad_r, const int ri, double d[8],
-                                        double& smax, bool& zero, const int i, const int j, const int k)
+__device__ __forceinline__ void solve_z(const Step_Params& P, const double* rec_l, const uint8_t* bad_l,
+                                        const double* rec_r, const uint8_t* bad_r, const int ri, const double cf_l,
+                                        const double cf_r, double d[8], double& smax, bool& zero, const int i,
+                                        const int j, const int k)
 {
-	const Side L = side_at<2>(rec_l, bad_l, CELLS, ri);
-	const Side R = side_at<2>(rec_r, bad_r, CELLS, ri);
+	const Side L = side_at<2>(rec_l, bad_l, CELLS, ri, cf_l);
+	const Side R = side_at<2>(rec_r, bad_r, CELLS, ri, cf_r);
 	double F[8];
 	uint32_t flag = 0;
 	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag);
@@ -360,11 +400,11 @@ One x or y face (axis a, 0 or 1, known only at run time) between record
 positions rl and rr of one slot.  The x and y faces of a plane share this
 one inlined solver instance (half the code of one instance per axis, which
 the instruction cache rewards); the rotation into the face frame is a
-choice of record rows to read, and back a choice of rows of `out` to write.
-The unscaled flux goes to out[v][idx] in the xyz frame.
+choice of record rows to read.  The unscaled flux goes to out[r][idx] in
+the face frame, Flux_Rows<SOLVER>::N rows (the caller rotates it back).
 */
 template <int SOLVER, int CELLS>
-__device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec, const uint32_t* bad,
+__device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec, const uint8_t* bad,
                                          const int rl, const int rr, const int a, double* out, const int nout,
                                          const int idx, double& s0, double& s1, bool& zero,
                                          const int i, const int j, const int k)
@@ -398,13 +438,13 @@ __device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec
 	if (a == 0) s0 = fmax(s0, sp); else s1 = fmax(s1, sp);
 	zero = zero or not (sp > 0.0);
 	out[idx] = F[0];
-	out[(1 + a) * nout + idx] = F[1];
-	out[(1 + a1) * nout + idx] = F[2];
-	out[(1 + a2) * nout + idx] = F[3];
+	out[1 * nout + idx] = F[1];
+	out[2 * nout + idx] = F[2];
+	out[3 * nout + idx] = F[3];
 	out[4 * nout + idx] = F[4];
-	out[(5 + a) * nout + idx] = F[5];
-	out[(5 + a1) * nout + idx] = F[6];
-	out[(5 + a2) * nout + idx] = F[7];
+	out[5 * nout + idx] = F[6];
+	out[6 * nout + idx] = F[7];
+	if (Flux_Rows<SOLVER>::N == 8) out[7 * nout + idx] = F[5];
 }
 
 // ------------------------------------------------------------------ the step
@@ -458,11 +498,12 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
                                           const int bx, const int by, const int bz,
                                           double& s0, double& s1, double& s2, bool& zero)
 {
-	using T = Tile<TY>;
+	constexpr int NF = Flux_Rows<SOLVER>::N;
+	using T = Tile<TY, NF>;
 	double* const rec_base = smem;
-	double* const fx = smem + 2 * T::REC;        // [8][TY][TX + 1]
-	double* const fy = fx + 8 * T::FXN;          // [8][TY + 1][TX]
-	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(fy + 8 * T::FYN);
+	double* const fx = smem + 2 * T::REC;        // [NF][TY][TX + 1]
+	double* const fy = fx + NF * T::FXN;         // [NF][TY + 1][TX]
+	uint8_t* const bad_base = reinterpret_cast<uint8_t*>(fy + NF * T::FYN);
 
 	constexpr bool YACT = TY > 1;
 	const bool zact = P.active[2] != 0;
@@ -494,17 +535,20 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 	double Acc[8];
 	#pragma unroll
 	for (int v = 0; v < 8; v++) Acc[v] = 0.0;
+	// the own column's fast speed along z in the previous and the current plane
+	double cfz_prev = 0.0, cfz = 0.0;
 
 	for (int k = kfirst; k <= klast; k++) {
 		const int slot = (k - kfirst) & 1;
 		double* const rec = rec_base + slot * T::REC;
-		uint32_t* const bad = bad_base + slot * T::CELLS;
+		uint8_t* const bad = bad_base + slot * T::CELLS;
 		const double* const prev = rec_base + (slot ^ 1) * T::REC;
-		const uint32_t* const prev_bad = bad_base + (slot ^ 1) * T::CELLS;
+		const uint8_t* const prev_bad = bad_base + (slot ^ 1) * T::CELLS;
 		const bool inner = k >= kb and k < ke;
 
 		// (a) stage the plane: own cells, and the halo for planes with x / y faces
-		if (stage) load_record<true, YACT, true, CO>(P, rec, bad, T::CELLS, ri, gx, gy, k);
+		cfz_prev = cfz;
+		if (stage) cfz = load_record<true, YACT, true, CO>(P, rec, bad, T::CELLS, ri, gx, gy, k);
 		// halo, spread over warps: the rows below / above the tile on warps 0 and 1, the columns
 		// left / right of it on warp 2 (warp 0 when y is inactive)
 		if (inner) {
@@ -567,7 +611,7 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 		// the cell below (U += (F- - F+) dt/dx, then y, then z: solve.hpp:1551-1587)
 		if (zact and k > kfirst and own) {
 			double Fz[8];
-			solve_z<SOLVER, T::CELLS>(P, prev, prev_bad, rec, bad, ri, Fz, s2, zero, gx, gy, k - 1);
+			solve_z<SOLVER, T::CELLS>(P, prev, prev_bad, rec, bad, ri, cfz_prev, cfz, Fz, s2, zero, gx, gy, k - 1);
 			if (k > kb) {
 				#pragma unroll
 				for (int v = 0; v < 8; v++) Acc[v] = Acc[v] - Fz[v] * cz;
@@ -580,17 +624,31 @@ __device__ __forceinline__ void tile_step(const Step_Params& P, double* const sm
 
 		// (c) the own cell: state plus x and y flux differences (plus its -z flux, held in Acc)
 		if (own and inner) {
+			// the flux row of each xyz variable in the x and the y face frames; -1: the normal
+			// field component, whose flux is zero unless the solver keeps an eighth row (adding
+			// 0.0 keeps the bits of adding a zero flux difference)
+			constexpr int XROW[8] = {0, 1, 2, 3, 4, NF == 8 ? 7 : -1, 5, 6};
+			constexpr int YROW[8] = {0, 3, 1, 2, 4, 6, NF == 8 ? 7 : -1, 5};
 			double Un[8];
 			#pragma unroll
 			for (int v = 0; v < 8; v++) {
-				const double* f = fx + v * T::FXN + ty * (TX + 1) + tx;
-				Un[v] = rec[v * T::CELLS + ri] + (f[0] - f[1]) * cx;
+				const double u = rec[v * T::CELLS + ri];
+				if (XROW[v] >= 0) {
+					const double* f = fx + XROW[v] * T::FXN + ty * (TX + 1) + tx;
+					Un[v] = u + (f[0] - f[1]) * cx;
+				} else {
+					Un[v] = u + 0.0;
+				}
 			}
 			if (YACT) {
 				#pragma unroll
 				for (int v = 0; v < 8; v++) {
-					const double* f = fy + v * T::FYN + ty * TX + tx;
-					Un[v] += (f[0] - f[TX]) * cy;
+					if (YROW[v] >= 0) {
+						const double* f = fy + YROW[v] * T::FYN + ty * TX + tx;
+						Un[v] += (f[0] - f[TX]) * cy;
+					} else {
+						Un[v] += 0.0;
+					}
 				}
 			}
 			if (zact) {
@@ -1072,18 +1130,21 @@ __global__ void totals_kernel(const double* __restrict__ state, const Layout L, 
 template <int SOLVER, int TY>
 static int prepare_t()
 {
-	const cudaError_t e = cudaFuncSetAttribute(step_kernel<SOLVER, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                                           int(Tile<TY>::BYTES));
+	const auto kernel = step_kernel<SOLVER, TY, Step_Minb<SOLVER, TY>::value>;
+	cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                     int(tile_bytes<SOLVER, TY>()));
+	// all of the SM's memory as shared memory, so that the blocks the registers allow fit
+	if (e == cudaSuccess) e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
 int prepare_step_kernels(const int solver, const bool y)
 {
 	switch (solver) {
-	case PAMHD_RUSANOV: return y ? prepare_t<PAMHD_RUSANOV, TY_3D>() : prepare_t<PAMHD_RUSANOV, 1>();
-	case PAMHD_HLL_ATHENA: return y ? prepare_t<PAMHD_HLL_ATHENA, TY_3D>() : prepare_t<PAMHD_HLL_ATHENA, 1>();
-	case PAMHD_HLLD_ATHENA: return y ? prepare_t<PAMHD_HLLD_ATHENA, TY_3D>() : prepare_t<PAMHD_HLLD_ATHENA, 1>();
-	case PAMHD_ROE_ATHENA: return y ? prepare_t<PAMHD_ROE_ATHENA, TY_3D>() : prepare_t<PAMHD_ROE_ATHENA, 1>();
+	case PAMHD_RUSANOV: return y ? prepare_t<PAMHD_RUSANOV, Step_Shape<PAMHD_RUSANOV>::rows>() : prepare_t<PAMHD_RUSANOV, 1>();
+	case PAMHD_HLL_ATHENA: return y ? prepare_t<PAMHD_HLL_ATHENA, Step_Shape<PAMHD_HLL_ATHENA>::rows>() : prepare_t<PAMHD_HLL_ATHENA, 1>();
+	case PAMHD_HLLD_ATHENA: return y ? prepare_t<PAMHD_HLLD_ATHENA, Step_Shape<PAMHD_HLLD_ATHENA>::rows>() : prepare_t<PAMHD_HLLD_ATHENA, 1>();
+	case PAMHD_ROE_ATHENA: return y ? prepare_t<PAMHD_ROE_ATHENA, Step_Shape<PAMHD_ROE_ATHENA>::rows>() : prepare_t<PAMHD_ROE_ATHENA, 1>();
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 }
@@ -1091,7 +1152,7 @@ int prepare_step_kernels(const int solver, const bool y)
 template <int SOLVER, int TY>
 static int launch_step_t(const Step_Params& P, cudaStream_t stream)
 {
-	const size_t smem = Tile<TY>::BYTES;
+	const size_t smem = tile_bytes<SOLVER, TY>();
 	const dim3 block(TX, TY);
 	const int nz = P.L.n[2];
 	const int chunks = P.kpart == 1 ? (nz > 1 ? 2 : 1)
@@ -1099,7 +1160,7 @@ static int launch_step_t(const Step_Params& P, cudaStream_t stream)
 	                 : (nz + P.kchunk - 1) / P.kchunk;
 	if (chunks < 1) return PAMHD_OK;  // no planes between the first and the last
 	const dim3 grid((P.L.n[0] + TX - 1) / TX, (P.L.n[1] + TY - 1) / TY, chunks);
-	step_kernel<SOLVER, TY, MINB><<<grid, block, smem, stream>>>(P);
+	step_kernel<SOLVER, TY, Step_Minb<SOLVER, TY>::value><<<grid, block, smem, stream>>>(P);
 	return cudaGetLastError() == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -1107,10 +1168,10 @@ int launch_step(const Step_Params& P, const int solver, cudaStream_t stream)
 {
 	const bool y = P.active[1] != 0;
 	switch (solver) {
-	case PAMHD_RUSANOV: return y ? launch_step_t<PAMHD_RUSANOV, TY_3D>(P, stream) : launch_step_t<PAMHD_RUSANOV, 1>(P, stream);
-	case PAMHD_HLL_ATHENA: return y ? launch_step_t<PAMHD_HLL_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_HLL_ATHENA, 1>(P, stream);
-	case PAMHD_HLLD_ATHENA: return y ? launch_step_t<PAMHD_HLLD_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_HLLD_ATHENA, 1>(P, stream);
-	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, TY_3D>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
+	case PAMHD_RUSANOV: return y ? launch_step_t<PAMHD_RUSANOV, Step_Shape<PAMHD_RUSANOV>::rows>(P, stream) : launch_step_t<PAMHD_RUSANOV, 1>(P, stream);
+	case PAMHD_HLL_ATHENA: return y ? launch_step_t<PAMHD_HLL_ATHENA, Step_Shape<PAMHD_HLL_ATHENA>::rows>(P, stream) : launch_step_t<PAMHD_HLL_ATHENA, 1>(P, stream);
+	case PAMHD_HLLD_ATHENA: return y ? launch_step_t<PAMHD_HLLD_ATHENA, Step_Shape<PAMHD_HLLD_ATHENA>::rows>(P, stream) : launch_step_t<PAMHD_HLLD_ATHENA, 1>(P, stream);
+	case PAMHD_ROE_ATHENA: return y ? launch_step_t<PAMHD_ROE_ATHENA, Step_Shape<PAMHD_ROE_ATHENA>::rows>(P, stream) : launch_step_t<PAMHD_ROE_ATHENA, 1>(P, stream);
 	default: return PAMHD_ERR_ARGUMENT;
 	}
 }
@@ -1126,7 +1187,7 @@ template <int SOLVER, int TY>
 static int prepare_batch_t()
 {
 	const cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
-	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tile<TY>::BYTES));
+	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_bytes<SOLVER, TY>()));
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -1156,7 +1217,7 @@ template <int SOLVER, int TY>
 static cudaError_t occupancy_t(int* blocks)
 {
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
-	                                                     TX * TY, Tile<TY>::BYTES);
+	                                                     TX * TY, tile_bytes<SOLVER, TY>());
 }
 
 template <int SOLVER>
@@ -1187,7 +1248,7 @@ template <int SOLVER, int TY>
 static int prepare_run_t()
 {
 	const cudaError_t e = cudaFuncSetAttribute(batch_run_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
-	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(Tile<TY>::BYTES));
+	                                           cudaFuncAttributeMaxDynamicSharedMemorySize, int(tile_bytes<SOLVER, TY>()));
 	return e == cudaSuccess ? PAMHD_OK : PAMHD_ERR_CUDA;
 }
 
@@ -1195,7 +1256,7 @@ template <int SOLVER, int TY>
 static cudaError_t run_occupancy_t(int* blocks)
 {
 	return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, batch_run_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF>,
-	                                                     TX * TY, Tile<TY>::BYTES);
+	                                                     TX * TY, tile_bytes<SOLVER, TY>());
 }
 
 template <int SOLVER, int TY>
@@ -1207,7 +1268,7 @@ static int launch_run_t(const Step_Params* even, const Step_Params* odd, const i
 	cudaLaunchConfig_t c = {};
 	c.gridDim = dim3(grid);
 	c.blockDim = dim3(TX, TY);
-	c.dynamicSmemBytes = Tile<TY>::BYTES;
+	c.dynamicSmemBytes = tile_bytes<SOLVER, TY>();
 	c.stream = stream;
 	cudaLaunchAttribute a[1];
 	a[0].id = cudaLaunchAttributeCooperative;
@@ -1297,7 +1358,7 @@ template <int SOLVER, int TY>
 static void launch_batch_t(const Step_Params* boxes, const int4* items, const int nitems, const int phase,
                            const int grid, cudaStream_t stream)
 {
-	batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF><<<grid, dim3(TX, TY), Tile<TY>::BYTES, stream>>>(
+	batch_step_kernel<SOLVER, TY, Batch_Build<TY>::MINB_OF><<<grid, dim3(TX, TY), tile_bytes<SOLVER, TY>(), stream>>>(
 		boxes, items, nitems, phase);
 }
 
