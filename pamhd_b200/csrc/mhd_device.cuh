@@ -350,14 +350,25 @@ __device__ __forceinline__ Star_T star_transverse(const Side& X, const double rh
 {
 	const double tmp = rho_sd * sm - bx2_mu;
 	const double it = recip(tmp);
+	const bool keep = fabs(tmp) < thr;
+#if PAMHD_STAR_SELECT2
+	// the degenerate case as factors 0 and 1: the same values (a zero may change sign)
+	const double t1 = keep ? 0.0 : bx * (s_mid - X.v0) * g.inv_mu0 * it;
+	const double t2 = keep ? 1.0 : (rho_sd * sd - bx2_mu) * it;
+	Star_T t;
+	t.w1 = X.v1 - X.b1 * t1;
+	t.w2 = X.v2 - X.b2 * t1;
+	t.b1 = X.b1 * t2;
+	t.b2 = X.b2 * t2;
+#else
 	const double t1 = bx * (s_mid - X.v0) * g.inv_mu0 * it;
 	const double t2 = (rho_sd * sd - bx2_mu) * it;
-	const bool keep = fabs(tmp) < thr;
 	Star_T t;
 	t.w1 = keep ? X.v1 : X.v1 - X.b1 * t1;
 	t.w2 = keep ? X.v2 : X.v2 - X.b2 * t1;
 	t.b1 = keep ? X.b1 : X.b1 * t2;
 	t.b2 = keep ? X.b2 : X.b2 * t2;
+#endif
 	return t;
 }
 
@@ -370,9 +381,19 @@ double-star state) and the reference's region choice (:475-552) selects
 among them, so that the compiler can overlap the two sides' dependency
 chains; values of regions not taken are discarded by selects, never
 multiplied in.
+The side the flux is taken from comes from pick(left): a caller that holds
+the sides' records in shared memory reads that side again instead of
+selecting all of its fields between the two sides held in registers.
 */
+struct Held_Sides {
+	const Side& L;
+	const Side& R;
+	__device__ __forceinline__ Side operator()(const bool left) const { return left ? L : R; }
+};
+
+template <class PICK>
 __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const Gas& g, double F[8],
-                                            uint32_t& /*flag*/)
+                                            uint32_t& /*flag*/, const PICK& pick)
 {
 	const double fast = fmax(L.cf, R.cf);
 	const bool order = L.v0 <= R.v0;
@@ -418,7 +439,7 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	const bool star_r = not star_l and not left and not (ssR > 0.0);
 	const bool dbl = not star_l and not star_r;
 	const bool useL = star_l or (dbl and left);   // the side the flux is taken from
-	const Side& S = useL ? L : R;
+	const Side S = pick(useL);
 	const Star_T& ts = useL ? tl : tr;
 	const double sd = useL ? sdL : sdR, ism = useL ? ismL : ismR, rs = useL ? rsL : rsR;
 	const double pt = useL ? ptL : ptR, s_out = useL ? s_neg : s_pos;
@@ -717,17 +738,31 @@ __device__ __forceinline__ double flux_roe(const Side& L, const Side& R, const G
 	return fmax(fabs(s_neg), fabs(s_pos));
 }
 
-template <int SOLVER>
+__device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const Gas& g, double F[8],
+                                            uint32_t& flag)
+{
+	return flux_hlld(L, R, g, F, flag, Held_Sides{L, R});
+}
+
+// pick: see flux_hlld (the other solvers use the sides held)
+template <int SOLVER, class PICK>
 __device__ __forceinline__ double solve_face(const Side& L, const Side& R, const Gas& g, double F[8],
-                                             uint32_t& flag)
+                                             uint32_t& flag, const PICK& pick)
 {
 	flag = L.bad | R.bad;
 	if (flag & PAMHD_FLAG_DENSITY) flag = PAMHD_FLAG_DENSITY;
 	else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
 	if (SOLVER == PAMHD_RUSANOV) return flux_rusanov<false>(L, R, g, F, flag);
 	if (SOLVER == PAMHD_HLL_ATHENA) return flux_hll<false>(L, R, g, F, flag);
-	if (SOLVER == PAMHD_HLLD_ATHENA) return flux_hlld(L, R, g, F, flag);
+	if (SOLVER == PAMHD_HLLD_ATHENA) return flux_hlld(L, R, g, F, flag, pick);
 	return flux_roe(L, R, g, F, flag);
+}
+
+template <int SOLVER>
+__device__ __forceinline__ double solve_face(const Side& L, const Side& R, const Gas& g, double F[8],
+                                             uint32_t& flag)
+{
+	return solve_face<SOLVER>(L, R, g, F, flag, Held_Sides{L, R});
 }
 
 } // namespace pamhd_b200
