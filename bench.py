@@ -506,9 +506,11 @@ def batched_section(local, steps=500, nboxes=64, tune=True, sequential=True):
         "boxes_failed": failed,
         "boxes_failed_steps": {i: taken[i] for i in failed},
         "boxes_failed_note": "boxes whose state hit the positivity check of the reference scheme within the "
-                             "run (the CPU oracle fails box 24 at step 236, like the GPU), with the steps each "
-                             "took (the failing one included); they stop there, and value counts the cell "
-                             f"updates made; same count in the sequential run: {len(failed_steps)}",
+                             "run, with the steps each took (the failing one included); they stop there, and "
+                             "value counts the cell updates made. The CPU oracle fails the same three boxes; the "
+                             "step differs (box 24: 236 there) because these boxes amplify round-off about 30x "
+                             "per 10 steps (the oracle against itself with a 1e-15 perturbation fails box 36 at "
+                             f"step 111 instead of 146); same count in the sequential run: {len(failed_steps)}",
         "what": "batched: all steps of all boxes in one persistent cooperative launch (a box's step waits only for "
                 "its own previous step; each box its own lagged CFL dt), replayed from a CUDA graph; "
                 "per_step_launches: the same ensemble with one launch per step; plain: each box in its own context, "
