@@ -20,7 +20,8 @@ ghost gradients of VALUE sides, one block per side, fixed order; launched
 only when the grid has a VALUE side).
 
 Driver (pamhd_gpu_adjoint): the forward run stores the state every K
-steps and keeps every state of the last segment; the reverse sweep steps
+steps and keeps every state of the last two segments (they fill the two
+segment buffers, so no recompute is needed for them); the reverse sweep steps
 lambda back through each segment while the segment before it is
 recomputed from its checkpoint on a second stream (same kernels, so the
 same bits), into the other of two segment buffers.  Memory: ceil(N/K)
@@ -435,16 +436,20 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 		W.seg_ready[b] = std::max(W.seg_ready[b], seg_len - 1);
 	}
 	std::vector<double> dts(nsteps);
-	const int last = nck - 1, last_start = last * every;
+	const int last = nck - 1;
+	// the segments from kept on fill the two segment buffers as they are made instead of being
+	// recomputed: the last two (the buffers hold two segments)
+	const int kept = std::max(0, last - 1);
 	for (int n = 0; n < nsteps; n++) {
 		if (n % every == 0) {
 			PAMHD_TRY(check(cudaMemcpyAsync(W.ck.p + state_len * size_t(n / every), x->state[x->cur],
 			                                state_len * sizeof(double), cudaMemcpyDeviceToDevice, x->stream)));
 		}
 		PAMHD_TRY(forward_step(*x, dt_in != nullptr ? dt_in[n] : -1.0));
-		// the states of the last segment are kept as they are made instead of being recomputed
-		if (n >= last_start and n + 1 < nsteps) {
-			PAMHD_TRY(check(cudaMemcpyAsync(W.seg[last & 1].p + state_len * size_t(n - last_start), x->state[x->cur],
+		// state n + 1, inside segment n / every (not the next checkpoint)
+		const int sn = n / every;
+		if (sn >= kept and n + 1 < std::min(nsteps, (sn + 1) * every)) {
+			PAMHD_TRY(check(cudaMemcpyAsync(W.seg[sn & 1].p + state_len * size_t(n - sn * every), x->state[x->cur],
 			                                state_len * sizeof(double), cudaMemcpyDeviceToDevice, x->stream)));
 		}
 	}
@@ -499,8 +504,8 @@ int pamhd_gpu_adjoint(pamhd_ctx* x, const int32_t nsteps, const int32_t every, c
 	int li = 0;
 	for (int s = nck - 1; s >= 0; s--) {
 		const int start = s * every, end = std::min(nsteps, start + every);
-		if (s >= 1) PAMHD_TRY(recompute(s - 1));
-		if (s != last) PAMHD_TRY(check(cudaStreamWaitEvent(x->stream, W.recomputed[s & 1], 0)));
+		if (s >= 1 and s - 1 < kept) PAMHD_TRY(recompute(s - 1));
+		if (s < kept) PAMHD_TRY(check(cudaStreamWaitEvent(x->stream, W.recomputed[s & 1], 0)));
 		std::vector<const double*> states(end - start);
 		for (int i = 0; i < end - start; i++) states[i] = state_of(s, i);
 		for (int n = end - 1; n >= start; n--) {
