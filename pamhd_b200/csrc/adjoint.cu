@@ -247,7 +247,23 @@ int launch_vjp(const Adj_Params& A, const int solver, cudaStream_t stream)
 {
 	long long count = 0;
 	for (int d = 0; d < 3; d++) count += A.active[d] ? A.nf[d] : 0;
-	const int blocks = int(std::min<long long>(65535, (count + 127) / 128));
+	int blocks = int(std::min<long long>(65535, (count + 127) / 128));
+	// no more blocks than fit at once: the loop over faces then ends without a partial last wave
+	{
+		int device = 0, sms = 0, per_sm = 0;
+		cudaError_t e = cudaGetDevice(&device);
+		if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+		if (e == cudaSuccess) {
+			switch (solver) {
+			case PAMHD_RUSANOV: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, faces_vjp_kernel<PAMHD_RUSANOV>, 128, 0); break;
+			case PAMHD_HLL_ATHENA: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, faces_vjp_kernel<PAMHD_HLL_ATHENA>, 128, 0); break;
+			case PAMHD_HLLD_ATHENA: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, faces_vjp_kernel<PAMHD_HLLD_ATHENA>, 128, 0); break;
+			default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, faces_vjp_kernel<PAMHD_ROE_ATHENA>, 128, 0); break;
+			}
+		}
+		if (e != cudaSuccess) return PAMHD_ERR_CUDA;
+		if (per_sm > 0) blocks = std::max(1, std::min(blocks, per_sm * sms));
+	}
 	switch (solver) {
 	case PAMHD_RUSANOV: faces_vjp_kernel<PAMHD_RUSANOV><<<blocks, 128, 0, stream>>>(A); break;
 	case PAMHD_HLL_ATHENA: faces_vjp_kernel<PAMHD_HLL_ATHENA><<<blocks, 128, 0, stream>>>(A); break;
