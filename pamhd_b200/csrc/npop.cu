@@ -406,9 +406,9 @@ cells and marches it in z through a chunk of planes.  Per plane k:
       rows below and above it, are read once into a shared-memory record (the
       13 state values, the two density reciprocals and, per active axis, the
       fast speed of the rotated total state with its check flag);
-  (b) every cell solves its -x and -y faces from the records (the last
-      column its +x face too, the last row its +y face) and its -z face
-      against its own record of plane k - 1, kept in registers;
+  (b) every cell solves its -x and -y faces from the records (the tile's
+      +x faces by four lanes of warp 2, its +y faces by the last row) and
+      its -z face against its own record of plane k - 1, kept in registers;
   (c) the x and y contributions go through shared memory to the cells on
       their other side, and every cell sums its faces' contributions in the
       order -x, +x, -y, +y, -z (the +z one arrives with plane k + 1);
@@ -696,7 +696,13 @@ __global__ void __launch_bounds__(NTX * NTY, 3) npop_fused_kernel(const Npop_Par
 			// (and the last row's +y)
 			if (ax) {
 				record_face<SOLVER, 0>(P, rec, flg, ri - 1, ri, dt, col_mx + kofs, s0, xch + xi, NXF);
-				if (tx == NTX - 1) record_face<SOLVER, 0>(P, rec, flg, ri, ri + 1, dt, col + kofs, s0, xch + xi + 1, NXF);
+				// the last column's +x faces: one lane per row of warp 2 (one extra pass for one warp,
+				// instead of one for every warp with its last lane alone active)
+				if (ty == 2 and tx < NTY) {
+					const int rl = (tx + 1) * NW + NTX;
+					const long long m = wrap_any(gx0 + NTX - 1, nx) + (long long)nx * wrap_any(gy0 + tx, ny);
+					record_face<SOLVER, 0>(P, rec, flg, rl, rl + 1, dt, m + kofs, s0, xch + tx * (NTX + 1) + NTX, NXF);
+				}
 			}
 			if (ay) {
 				record_face<SOLVER, 1>(P, rec, flg, ri - NW, ri, dt, col_my + kofs, s1, ych + yi, NYF);
