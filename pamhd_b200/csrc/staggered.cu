@@ -139,7 +139,7 @@ validity per axis) instead of once per face; every cell then solves its three
 Three record slots rotate over the planes, so one barrier per plane keeps a
 plane's stores apart from the reads of the plane two before it.
 */
-constexpr int STX = 32, STY = 4;
+constexpr int STX = 32, STY = 8;            // 256 threads, two blocks per SM (one for Roe)
 constexpr int SW = STX + 1;                 // a record row: the -x halo at column 0
 constexpr int SCELLS = SW * (STY + 1);      // record rows: the -y halo at row 0
 constexpr int SREC = 13;                    // rho, mom xyz, E, B xyz, 1/rho, p, c_f xyz
@@ -241,7 +241,7 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 template <int SOLVER, bool BG>
-__global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 2 : 3) faces_kernel(const Stag_Params P)
+__global__ void __launch_bounds__(STX * STY, SOLVER == PAMHD_ROE_ATHENA ? 1 : 2) faces_kernel(const Stag_Params P)
 {
 	extern __shared__ __align__(16) double smem[];
 	uint32_t* const bad_base = reinterpret_cast<uint32_t*>(smem + SSLOTS * SSLOT);
