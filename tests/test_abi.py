@@ -99,7 +99,7 @@ def test_any_active_dimensions_pass_the_checks(lib, n):
     dict(n=(0, 4, 4)),
     dict(cell_length=(0.1, -0.1, 0.1)),
     dict(adiabatic_index=0.5),
-    dict(n=(1, 4 * 65535 + 1, 1)),                 # more rows of face tiles than a launch can have
+    dict(n=(1, 8 * 65535 + 1, 1)),                 # more rows of face tiles (8 cells high) than a launch can have
 ])
 def test_staggered_create_rejects_invalid_config(lib, change):
     lib.pamhd_gpu_staggered_create.argtypes = [ctypes.POINTER(pg._Cfg), ctypes.POINTER(ctypes.c_void_p)]
