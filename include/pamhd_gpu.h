@@ -134,6 +134,9 @@ const char* pamhd_gpu_errstr(int code);
 Creates a context: allocates the state (two copies, ping-pong) and the
 reduction buffers on cfg->device.  Replaces the dccrg grid set-up and the
 cell-data allocation of tests/mhd/test.cpp:330-444 for uniform grids.
+Launch limits (PAMHD_ERR_ARGUMENT beyond them): at most 524,280 cells
+along the second active dimension (262,140 with Roe) and 1,048,560 along
+the third.
 */
 int pamhd_gpu_create(const pamhd_cfg* cfg, pamhd_ctx** ctx);
 

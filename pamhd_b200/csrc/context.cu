@@ -207,6 +207,12 @@ int pamhd_gpu_create(const pamhd_cfg* cfg, pamhd_ctx** out)
 	}
 	const pamhd_cfg internal = relabelled(*cfg, map);
 	PAMHD_TRY(validate(internal));
+	// the step's launch: rows of tiles along y and z chunks within a grid dimension's 65535 blocks
+	if (internal.n[1] > 1) {
+		const int rows = step_tile_rows(internal.solver);
+		if ((internal.n[1] + rows - 1) / rows > 65535) return PAMHD_ERR_ARGUMENT;
+	}
+	if (internal.n[2] > 16 * 65535) return PAMHD_ERR_ARGUMENT;
 	pamhd_ctx* x = new (std::nothrow) pamhd_ctx;
 	if (x == nullptr) return PAMHD_ERR_ARGUMENT;
 	x->cfg = internal;

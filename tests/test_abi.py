@@ -61,6 +61,8 @@ def test_cfg_layout_matches_oracle():
     dict(vacuum_permeability=0.0),
     dict(time_step_factor=0.0),
     dict(bc_lo=(0, 0, 0), bc_hi=(1, 0, 0)),  # periodic on one side only
+    dict(n=(2, 8 * 65535 + 1, 1)),           # more rows of 32 x 8 tiles than a launch can have
+    dict(n=(2, 4 * 65535 + 1, 1), solver=4),  # Roe's 32 x 4 tiles
 ])
 def test_create_rejects_invalid_config(lib, change):
     kw = dict(n=(8, 8, 8), solver=pg.HLLD, cell_length=(0.1, 0.1, 0.1))
