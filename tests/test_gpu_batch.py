@@ -89,6 +89,43 @@ def test_batch_box_matches_oracle(port):
         assert (np.abs(a - o).max(axis=1) / scale).max() <= 1e-12 * (1 + step)
 
 
+def test_configured_boxes_match_oracle_in_the_persistent_run(port):
+    """Boxes of the configured ensemble (its seed, its 32^3, 64^3 and 96^3 sizes, their own winds),
+    20 steps in one persistent launch, against the oracle at the per-step bar grown with the step
+    count: the state and every step's dt of each box."""
+    boxes = states.solar_wind_ensemble()
+    picked = []
+    for size in (32, 64, 96):
+        picked.append(next(b for b in boxes if b["n"] == size))
+    cfgs = [wind_cfg(b["n"], b["inflow"]) for b in picked]
+    batch = pg.Batch(cfgs)
+    for i, b in enumerate(picked):
+        batch.set_state(i, states.ensemble_state(b))
+    steps = 20
+    batch.run(steps)
+    batch.sync()
+    for i, b in enumerate(picked):
+        n = b["n"]
+        ora = port.grid(po.make_cfg((n, n, n), po.HLL, (states.EARTH_RADIUS_CELL,) * 3, 5 / 3, states.MU0_SI, 0.5,
+                                    bc_lo=(po.BC_VALUE, po.BC_COPY, po.BC_COPY), bc_hi=(po.BC_COPY,) * 3,
+                                    value_lo=[b["inflow"], None, None]), threads=8)
+        ora.set_state(states.ensemble_state(b))
+        dts = []
+        for _ in range(steps):
+            do, flag, _, _ = ora.step(1e300)
+            assert flag == 0
+            dts.append(do)
+        dg = batch.dt_history(i, steps)
+        assert len(dg) == steps
+        for a, o in zip(dg, dts):
+            assert abs(a - o) <= 1e-12 * max(o, 1e-300) or a == o == 0.0
+        a = batch.get_state(i).reshape(8, -1)
+        o = ora.get_state().reshape(8, -1)
+        scale = np.abs(o).max(axis=1)
+        scale[scale == 0] = 1.0
+        assert (np.abs(a - o).max(axis=1) / scale).max() <= 1e-12 * steps, n
+
+
 def test_tuner_restores_state():
     cfgs, U0s = small_ensemble()
     tuned, plain = pg.Batch(cfgs), pg.Batch(cfgs)
