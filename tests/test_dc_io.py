@@ -121,7 +121,7 @@ def test_reference_reader_reads_our_files(tmp_path):
 @pytest.mark.parametrize("case,vx", [("da_px", 1.0), ("da_mx", -1.0)])
 def test_reference_diff_tool_accepts_our_output(tmp_path, port, case, vx):
     """The oracle's density-advection run, written by this library, against the reference
-    program's own output, judged by the reference's comparison tool (tests/mhd/mhd_diff.py,
+    program's own output, checked by the reference's comparison tool (tests/mhd/mhd_diff.py,
     which also requires every header field to match) at 1e-14."""
     import subprocess
     import states
