@@ -45,9 +45,6 @@ constexpr int TX = 32;
 #endif
 constexpr int TY_3D = PAMHD_TY;     // tile rows of the batched step on 2-D and 3-D grids
 constexpr int MINB = PAMHD_MINB;    // resident blocks per SM asked of the register allocator
-#ifndef PAMHD_RELOAD_SIDE
-#define PAMHD_RELOAD_SIDE 1
-#endif
 constexpr int TY_STEP = PAMHD_STEP_TY;  // tile rows of the single-grid step (Roe aside)
 // record of a cell in shared memory: rho, mom xyz, E, B xyz, 1/rho, p, cf x, cf y (the fast
 // speed along z is needed by the column's owner only, which keeps it in a register)
@@ -388,13 +385,10 @@ __device__ __forceinline__ void solve_z(const Step_Params& P, const double* rec_
 	const Side R = side_at<2>(rec_r, bad_r, CELLS, ri, cf_r);
 	double F[8];
 	uint32_t flag = 0;
-#if PAMHD_RELOAD_SIDE
+	// the side an HLLD flux is taken from, read again from the records (see flux_hlld)
 	const auto pick = [&](const bool left) {
 		return side_at<2>(left ? rec_l : rec_r, left ? bad_l : bad_r, CELLS, ri, left ? cf_l : cf_r);
 	};
-#else
-	const Held_Sides pick{L, R};
-#endif
 	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag, pick);
 	if (flag != 0) record_failure(P, flag, i, j, k, 3);
 	smax = fmax(smax, s);
@@ -443,11 +437,7 @@ __device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec
 	const Side R = side(rr);
 	double F[8];
 	uint32_t flag = 0;
-#if PAMHD_RELOAD_SIDE
 	const auto pick = [&](const bool left) { return side(left ? rl : rr); };
-#else
-	const Held_Sides pick{L, R};
-#endif
 	const double sp = solve_face<SOLVER>(L, R, P.gas, F, flag, pick);
 	if (flag != 0) record_failure(P, flag, i, j, k, a + 1);
 	if (a == 0) s0 = fmax(s0, sp); else s1 = fmax(s1, sp);
