@@ -126,6 +126,31 @@ def test_configured_boxes_match_oracle_in_the_persistent_run(port):
         assert (np.abs(a - o).max(axis=1) / scale).max() <= 1e-12 * steps, n
 
 
+@pytest.mark.parametrize("persistent", [False, True])
+def test_one_dimensional_box_equals_its_context(persistent):
+    """A 1-D grid (the Brio-Wu shock tube, 1000 cells, COPY ends) as a batch of one box, per-step
+    launches or the persistent run, capped at t_end: the same bits, time and step count as the
+    same grid in its own context."""
+    U = states.brio_wu(1000)
+    cfg = pg.Config(n=(1000, 1, 1), solver=pg.HLLD, cell_length=(1e-3, 1.0, 1.0), adiabatic_index=2.0,
+                    time_step_factor=0.5, bc_lo=(pg.BC_COPY, 0, 0), bc_hi=(pg.BC_COPY, 0, 0))
+    batch = pg.Batch([cfg])
+    batch.set_state(0, U)
+    ctx = pg.Context(cfg)
+    ctx.set_state(U)
+    for n in (7, 60, 300):
+        if persistent:
+            batch.run(n, 0.02)
+        else:
+            batch.steps(n, 0.02)
+        batch.sync()
+        ctx.steps(n, 0.02)
+        ctx.sync()
+        np.testing.assert_array_equal(batch.get_state(0), ctx.get_state())
+        assert batch.time(0) == ctx.time()
+    assert ctx.time()[0] == 0.02
+
+
 def test_tuner_restores_state():
     cfgs, U0s = small_ensemble()
     tuned, plain = pg.Batch(cfgs), pg.Batch(cfgs)
