@@ -220,12 +220,46 @@ __device__ __forceinline__ Side side_of(const double U[8], const Derived& d)
 }
 
 /*
+Arithmetic of the HLLD solver.  Ar<false>: plain expressions, as written
+(the files built with -fmad=false round every operation on its own).
+Ar<true>: every operation an explicitly rounded intrinsic, a fused
+multiply-add where the formula has a product added, so that every kernel
+of the cell-centred step (single grid, batched, persistent) computes the
+same bits for the same face, whatever other code it is inlined beside.
+In both, fma(a, b, c) is a b + c and x - y z is written fma(-y, z, x),
+which negates exactly, so Ar<false> keeps the written operation order.
+*/
+template <bool X> struct Ar {
+	static __device__ __forceinline__ double mul(const double a, const double b) { return X ? __dmul_rn(a, b) : a * b; }
+	static __device__ __forceinline__ double add(const double a, const double b) { return X ? __dadd_rn(a, b) : a + b; }
+	static __device__ __forceinline__ double sub(const double a, const double b) { return X ? __dsub_rn(a, b) : a - b; }
+	static __device__ __forceinline__ double fma(const double a, const double b, const double c)
+	{
+		return X ? __fma_rn(a, b, c) : a * b + c;
+	}
+};
+
+/*
 Ideal-MHD flux along the face normal, mhd/common.hpp:146-244, with the
 background field zero (every configuration of the fused step).  pb is the
 magnetic pressure B^2 / (2 mu0).
 */
+template <bool X = false>
 __device__ __forceinline__ void physical_flux(const Side& s, const double pb, const Gas& g, double F[8])
 {
+	if constexpr (X) {
+		using A = Ar<true>;
+		F[0] = s.m0;
+		F[1] = A::add(A::fma(s.m0, s.v0, -A::mul(g.inv_mu0, A::mul(s.b0, s.b0))), A::add(s.p, pb));
+		F[2] = A::fma(s.m1, s.v0, -A::mul(g.inv_mu0, A::mul(s.b0, s.b1)));
+		F[3] = A::fma(s.m2, s.v0, -A::mul(g.inv_mu0, A::mul(s.b0, s.b2)));
+		const double vb = A::fma(s.v2, s.b2, A::fma(s.v1, s.b1, A::mul(s.v0, s.b0)));
+		F[4] = A::fma(s.v0, A::add(A::add(s.E, s.p), pb), -A::mul(A::mul(s.b0, vb), g.inv_mu0));
+		F[5] = 0.0;
+		F[6] = A::fma(s.v0, s.b1, -A::mul(s.b0, s.v1));
+		F[7] = A::fma(s.v0, s.b2, -A::mul(s.b0, s.v2));
+		return;
+	}
 	F[0] = s.m0;
 	F[1] = s.m0 * s.v0 - g.inv_mu0 * (s.b0 * s.b0) + (s.p + pb);
 	F[2] = s.m1 * s.v0 - g.inv_mu0 * (s.b0 * s.b1);
@@ -261,8 +295,13 @@ __device__ __forceinline__ void physical_flux_bg(
 	F[7] = s.v0 * t2 - t0 * s.v2;
 }
 
+template <bool X = false>
 __device__ __forceinline__ double magnetic_pressure(const Side& s, const Gas& g)
 {
+	if constexpr (X) {
+		using A = Ar<true>;
+		return A::mul(A::mul(0.5, g.inv_mu0), A::fma(s.b2, s.b2, A::fma(s.b1, s.b1, A::mul(s.b0, s.b0))));
+	}
 	return 0.5 * g.inv_mu0 * (s.b0 * s.b0 + s.b1 * s.b1 + s.b2 * s.b2);
 }
 
@@ -344,31 +383,22 @@ struct Star_T {
 	double w1, w2, b1, b2;
 };
 
+template <bool EX>
 __device__ __forceinline__ Star_T star_transverse(const Side& X, const double rho_sd, const double sd,
                                                   const double sm, const double s_mid, const double bx,
                                                   const double bx2_mu, const double thr, const Gas& g)
 {
-	const double tmp = rho_sd * sm - bx2_mu;
+	using A = Ar<EX>;
+	const double tmp = A::fma(rho_sd, sm, -bx2_mu);
 	const double it = recip(tmp);
 	const bool keep = fabs(tmp) < thr;
-#if PAMHD_STAR_SELECT2
-	// the degenerate case as factors 0 and 1: the same values (a zero may change sign)
-	const double t1 = keep ? 0.0 : bx * (s_mid - X.v0) * g.inv_mu0 * it;
-	const double t2 = keep ? 1.0 : (rho_sd * sd - bx2_mu) * it;
+	const double t1 = A::mul(A::mul(A::mul(bx, A::sub(s_mid, X.v0)), g.inv_mu0), it);
+	const double t2 = A::mul(A::fma(rho_sd, sd, -bx2_mu), it);
 	Star_T t;
-	t.w1 = X.v1 - X.b1 * t1;
-	t.w2 = X.v2 - X.b2 * t1;
-	t.b1 = X.b1 * t2;
-	t.b2 = X.b2 * t2;
-#else
-	const double t1 = bx * (s_mid - X.v0) * g.inv_mu0 * it;
-	const double t2 = (rho_sd * sd - bx2_mu) * it;
-	Star_T t;
-	t.w1 = keep ? X.v1 : X.v1 - X.b1 * t1;
-	t.w2 = keep ? X.v2 : X.v2 - X.b2 * t1;
-	t.b1 = keep ? X.b1 : X.b1 * t2;
-	t.b2 = keep ? X.b2 : X.b2 * t2;
-#endif
+	t.w1 = keep ? X.v1 : A::fma(-X.b1, t1, X.v1);
+	t.w2 = keep ? X.v2 : A::fma(-X.b2, t1, X.v2);
+	t.b1 = keep ? X.b1 : A::mul(X.b1, t2);
+	t.b2 = keep ? X.b2 : A::mul(X.b2, t2);
 	return t;
 }
 
@@ -391,47 +421,49 @@ struct Held_Sides {
 	__device__ __forceinline__ Side operator()(const bool left) const { return left ? L : R; }
 };
 
-template <class PICK>
+template <bool EX, class PICK>
 __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const Gas& g, double F[8],
                                             uint32_t& /*flag*/, const PICK& pick)
 {
+	using A = Ar<EX>;
 	const double fast = fmax(L.cf, R.cf);
 	const bool order = L.v0 <= R.v0;
-	const double s_neg = (order ? L.v0 : R.v0) - fast;  // eqn 67
-	const double s_pos = (order ? R.v0 : L.v0) + fast;
-	const double pbL = magnetic_pressure(L, g), pbR = magnetic_pressure(R, g);
+	const double s_neg = A::sub(order ? L.v0 : R.v0, fast);  // eqn 67
+	const double s_pos = A::add(order ? R.v0 : L.v0, fast);
+	const double pbL = magnetic_pressure<EX>(L, g), pbR = magnetic_pressure<EX>(R, g);
 
 	if (s_neg >= 0.0) {
-		physical_flux(L, pbL, g, F);
+		physical_flux<EX>(L, pbL, g, F);
 		return fabs(s_pos);
 	}
 	if (s_pos <= 0.0) {
-		physical_flux(R, pbR, g, F);
+		physical_flux<EX>(R, pbR, g, F);
 		return fabs(s_neg);
 	}
 	const double speed = fmax(fabs(s_neg), fabs(s_pos));
 
-	const double bx = 0.5 * (L.b0 + R.b0);
-	const double bx2_mu = bx * bx * g.inv_mu0;
-	const double sdL = s_neg - L.v0, sdR = s_pos - R.v0;       // < 0 and > 0 here
-	const double ptL = L.p + pbL, ptR = R.p + pbR;
-	const double rsdL = L.rho * sdL, rsdR = R.rho * sdR;
+	const double bx = A::mul(0.5, A::add(L.b0, R.b0));
+	const double bx2_mu = A::mul(A::mul(bx, bx), g.inv_mu0);
+	const double sdL = A::sub(s_neg, L.v0), sdR = A::sub(s_pos, R.v0);       // < 0 and > 0 here
+	const double ptL = A::add(L.p, pbL), ptR = A::add(R.p, pbR);
+	const double rsdL = A::mul(L.rho, sdL), rsdR = A::mul(R.rho, sdR);
 	// eqn 38; the denominator is sdR rho_R - sdL rho_L > 0
-	const double s_mid = (sdR * R.m0 - sdL * L.m0 - ptR + ptL) * recip(rsdR - rsdL);
-	const double smL = s_neg - s_mid, smR = s_pos - s_mid;     // < 0 and > 0 for physical states
+	const double s_mid = A::mul(A::add(A::sub(A::fma(sdR, R.m0, -A::mul(sdL, L.m0)), ptR), ptL),
+	                            recip(A::sub(rsdR, rsdL)));
+	const double smL = A::sub(s_neg, s_mid), smR = A::sub(s_pos, s_mid);     // < 0 and > 0 for physical states
 	const double ismL = recip(smL), ismR = recip(smR);
 	// eqn 43, and the square roots of the star densities with their reciprocals
-	const double rsL = rsdL * ismL, rsR = rsdR * ismR;
+	const double rsL = A::mul(rsdL, ismL), rsR = A::mul(rsdR, ismR);
 	const double irL = rsqrt_nr(rsL), irR = rsqrt_nr(rsR);
-	const double sqL = rsL * irL, sqR = rsR * irR;
+	const double sqL = A::mul(rsL, irL), sqR = A::mul(rsR, irR);
 	// eqn 51
-	const double abx = fabs(bx) * g.inv_sqrt_mu0;
-	const double ssL = s_mid - abx * irL, ssR = s_mid + abx * irR;
-	const double ptst = ptL + rsdL * (s_mid - L.v0);
-	const double thr = DBL_EPS * ptst;
+	const double abx = A::mul(fabs(bx), g.inv_sqrt_mu0);
+	const double ssL = A::fma(-abx, irL, s_mid), ssR = A::fma(abx, irR, s_mid);
+	const double ptst = A::fma(rsdL, A::sub(s_mid, L.v0), ptL);
+	const double thr = A::mul(DBL_EPS, ptst);
 	// transverse star velocity and field of both sides, eqns 44-47
-	const Star_T tl = star_transverse(L, rsdL, sdL, smL, s_mid, bx, bx2_mu, thr, g);
-	const Star_T tr = star_transverse(R, rsdR, sdR, smR, s_mid, bx, bx2_mu, thr, g);
+	const Star_T tl = star_transverse<EX>(L, rsdL, sdL, smL, s_mid, bx, bx2_mu, thr, g);
+	const Star_T tr = star_transverse<EX>(R, rsdR, sdR, smR, s_mid, bx, bx2_mu, thr, g);
 
 	// region order of hlld_athena.hpp:475-552: S*_L >= 0, S_M >= 0, S*_R > 0, else
 	const bool left = s_mid >= 0.0;
@@ -445,33 +477,38 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	const double pt = useL ? ptL : ptR, s_out = useL ? s_neg : s_pos;
 
 	// that side's full star state, eqn 48 for the energy
-	const double vb_star = s_mid * bx + ts.w1 * ts.b1 + ts.w2 * ts.b2;
-	const double vb = S.v0 * S.b0 + S.v1 * S.b1 + S.v2 * S.b2;
+	const double vb_star = A::fma(ts.w2, ts.b2, A::fma(ts.w1, ts.b1, A::mul(s_mid, bx)));
+	const double vb = A::fma(S.v2, S.b2, A::fma(S.v1, S.b1, A::mul(S.v0, S.b0)));
 	double us[8];
-	us[0] = rs; us[1] = rs * s_mid; us[2] = rs * ts.w1; us[3] = rs * ts.w2;
-	us[4] = (sd * S.E - pt * S.v0 + ptst * s_mid + bx * g.inv_mu0 * (vb - vb_star)) * ism;
+	us[0] = rs; us[1] = A::mul(rs, s_mid); us[2] = A::mul(rs, ts.w1); us[3] = A::mul(rs, ts.w2);
+	{
+		double e = A::fma(sd, S.E, -A::mul(pt, S.v0));
+		e = A::fma(ptst, s_mid, e);
+		e = A::fma(A::mul(bx, g.inv_mu0), A::sub(vb, vb_star), e);
+		us[4] = A::mul(e, ism);
+	}
 	us[5] = bx; us[6] = ts.b1; us[7] = ts.b2;
 	const double U0[8] = {S.rho, S.m0, S.m1, S.m2, S.E, S.b0, S.b1, S.b2};
-	physical_flux(S, useL ? pbL : pbR, g, F);
+	physical_flux<EX>(S, useL ? pbL : pbR, g, F);
 
 	// double-star state, eqns 59-63 (the star state itself when Bx ~ 0)
-	const double inv_sum = recip(sqL + sqR);
+	const double inv_sum = recip(A::add(sqL, sqR));
 	const double sgn = (bx > 0.0) ? 1.0 : -1.0;
-	const double cv = sgn * g.inv_sqrt_mu0;
-	const double v1 = inv_sum * ((sqL * tl.w1 + sqR * tr.w1) + cv * (tr.b1 - tl.b1));
-	const double v2 = inv_sum * ((sqL * tl.w2 + sqR * tr.w2) + cv * (tr.b2 - tl.b2));
-	const double wb = sgn * sqL * sqR * g.sqrt_mu0;
-	const double b1 = inv_sum * ((sqL * tr.b1 + sqR * tl.b1) + wb * (tr.w1 - tl.w1));
-	const double b2 = inv_sum * ((sqL * tr.b2 + sqR * tl.b2) + wb * (tr.w2 - tl.w2));
-	const double vb2 = s_mid * bx + v1 * b1 + v2 * b2;
+	const double cv = A::mul(sgn, g.inv_sqrt_mu0);
+	const double v1 = A::mul(inv_sum, A::fma(cv, A::sub(tr.b1, tl.b1), A::fma(sqR, tr.w1, A::mul(sqL, tl.w1))));
+	const double v2 = A::mul(inv_sum, A::fma(cv, A::sub(tr.b2, tl.b2), A::fma(sqR, tr.w2, A::mul(sqL, tl.w2))));
+	const double wb = A::mul(A::mul(A::mul(sgn, sqL), sqR), g.sqrt_mu0);
+	const double b1 = A::mul(inv_sum, A::fma(wb, A::sub(tr.w1, tl.w1), A::fma(sqR, tl.b1, A::mul(sqL, tr.b1))));
+	const double b2 = A::mul(inv_sum, A::fma(wb, A::sub(tr.w2, tl.w2), A::fma(sqR, tl.b2, A::mul(sqL, tr.b2))));
+	const double vb2 = A::fma(v2, b2, A::fma(v1, b1, A::mul(s_mid, bx)));
 	const double e2 = left
-		? us[4] - sqL * sgn * (vb_star - vb2) * g.inv_sqrt_mu0
-		: us[4] + sqR * sgn * (vb_star - vb2) * g.inv_sqrt_mu0;
-	const bool two = dbl and not (0.5 * bx * bx < thr);
+		? A::sub(us[4], A::mul(A::mul(A::mul(sqL, sgn), A::sub(vb_star, vb2)), g.inv_sqrt_mu0))
+		: A::add(us[4], A::mul(A::mul(A::mul(sqR, sgn), A::sub(vb_star, vb2)), g.inv_sqrt_mu0));
+	const bool two = dbl and not (A::mul(A::mul(0.5, bx), bx) < thr);
 	double u2[8];
 	u2[0] = us[0]; u2[1] = us[1];
-	u2[2] = two ? rs * v1 : us[2];
-	u2[3] = two ? rs * v2 : us[3];
+	u2[2] = two ? A::mul(rs, v1) : us[2];
+	u2[3] = two ? A::mul(rs, v2) : us[3];
 	u2[4] = two ? e2 : us[4];
 	u2[5] = us[5];
 	u2[6] = two ? b1 : us[6];
@@ -480,11 +517,11 @@ __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const 
 	// single star: F + s_out (U* - U); double star: F + s_in U** - (s_in - s_out) U* - s_out U
 	const double s_in = left ? ssL : ssR;
 	const double c2 = dbl ? s_in : 0.0;
-	const double c1 = dbl ? s_in - s_out : -s_out;
+	const double c1 = dbl ? A::sub(s_in, s_out) : -s_out;
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
 		if (v == 5) continue;
-		F[v] = F[v] + u2[v] * c2 - us[v] * c1 - U0[v] * s_out;
+		F[v] = A::fma(-U0[v], s_out, A::fma(-us[v], c1, A::fma(u2[v], c2, F[v])));
 	}
 	F[5] = 0.0;
 	return speed;
@@ -738,14 +775,15 @@ __device__ __forceinline__ double flux_roe(const Side& L, const Side& R, const G
 	return fmax(fabs(s_neg), fabs(s_pos));
 }
 
+template <bool EX = false>
 __device__ __forceinline__ double flux_hlld(const Side& L, const Side& R, const Gas& g, double F[8],
                                             uint32_t& flag)
 {
-	return flux_hlld(L, R, g, F, flag, Held_Sides{L, R});
+	return flux_hlld<EX>(L, R, g, F, flag, Held_Sides{L, R});
 }
 
-// pick: see flux_hlld (the other solvers use the sides held)
-template <int SOLVER, class PICK>
+// pick: see flux_hlld (the other solvers use the sides held); EX: Ar<true> arithmetic for HLLD
+template <int SOLVER, bool EX = false, class PICK>
 __device__ __forceinline__ double solve_face(const Side& L, const Side& R, const Gas& g, double F[8],
                                              uint32_t& flag, const PICK& pick)
 {
@@ -754,15 +792,15 @@ __device__ __forceinline__ double solve_face(const Side& L, const Side& R, const
 	else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
 	if (SOLVER == PAMHD_RUSANOV) return flux_rusanov<false>(L, R, g, F, flag);
 	if (SOLVER == PAMHD_HLL_ATHENA) return flux_hll<false>(L, R, g, F, flag);
-	if (SOLVER == PAMHD_HLLD_ATHENA) return flux_hlld(L, R, g, F, flag, pick);
+	if (SOLVER == PAMHD_HLLD_ATHENA) return flux_hlld<EX>(L, R, g, F, flag, pick);
 	return flux_roe(L, R, g, F, flag);
 }
 
-template <int SOLVER>
+template <int SOLVER, bool EX = false>
 __device__ __forceinline__ double solve_face(const Side& L, const Side& R, const Gas& g, double F[8],
                                              uint32_t& flag)
 {
-	return solve_face<SOLVER>(L, R, g, F, flag, Held_Sides{L, R});
+	return solve_face<SOLVER, EX>(L, R, g, F, flag, Held_Sides{L, R});
 }
 
 } // namespace pamhd_b200

@@ -389,7 +389,7 @@ __device__ __forceinline__ void solve_z(const Step_Params& P, const double* rec_
 	const auto pick = [&](const bool left) {
 		return side_at<2>(left ? rec_l : rec_r, left ? bad_l : bad_r, CELLS, ri, left ? cf_l : cf_r);
 	};
-	const double s = solve_face<SOLVER>(L, R, P.gas, F, flag, pick);
+	const double s = solve_face<SOLVER, true>(L, R, P.gas, F, flag, pick);
 	if (flag != 0) record_failure(P, flag, i, j, k, 3);
 	smax = fmax(smax, s);
 	zero = zero or not (s > 0.0);
@@ -438,7 +438,7 @@ __device__ __forceinline__ void solve_xy(const Step_Params& P, const double* rec
 	double F[8];
 	uint32_t flag = 0;
 	const auto pick = [&](const bool left) { return side(left ? rl : rr); };
-	const double sp = solve_face<SOLVER>(L, R, P.gas, F, flag, pick);
+	const double sp = solve_face<SOLVER, true>(L, R, P.gas, F, flag, pick);
 	if (flag != 0) record_failure(P, flag, i, j, k, a + 1);
 	if (a == 0) s0 = fmax(s0, sp); else s1 = fmax(s1, sp);
 	zero = zero or not (sp > 0.0);
@@ -792,7 +792,7 @@ __device__ __forceinline__ void boundary_face(const Step_Params& P, const int d,
 	fill(R, UB, db);
 	double F[8];
 	uint32_t flag = 0;
-	const double sp = solve_face<SOLVER>(L, R, P.gas, F, flag);
+	const double sp = solve_face<SOLVER, true>(L, R, P.gas, F, flag);
 	if (flag != 0) record_failure(P, flag, a[0], a[1], a[2], e + 1);
 	smax[e] = fmax(smax[e], sp);
 	zero = zero or not (sp > 0.0);
@@ -1082,7 +1082,7 @@ __global__ void face_flux_kernel(long long n, const double* __restrict__ neg, co
 		double s;
 		if (SOLVER == PAMHD_RUSANOV) s = use_bg ? flux_rusanov<true>(L, R, g, F, flag, b) : flux_rusanov<false>(L, R, g, F, flag);
 		else if (SOLVER == PAMHD_HLL_ATHENA) s = use_bg ? flux_hll<true>(L, R, g, F, flag, b) : flux_hll<false>(L, R, g, F, flag);
-		else if (SOLVER == PAMHD_HLLD_ATHENA) s = flux_hlld(L, R, g, F, flag);
+		else if (SOLVER == PAMHD_HLLD_ATHENA) s = flux_hlld<true>(L, R, g, F, flag);
 		else s = flux_roe(L, R, g, F, flag);
 		for (int v = 0; v < 8; v++) flux[8 * t + v] = flag ? 0.0 : F[v];
 		speed[t] = flag ? 0.0 : s;

@@ -151,6 +151,34 @@ def test_one_dimensional_box_equals_its_context(persistent):
     assert ctx.time()[0] == 0.02
 
 
+def test_box_failing_late_in_a_persistent_run_holds_its_failing_step():
+    """The 64^3 magnetised blast loses positivity after some tens of steps: run as a batch of one
+    box for 80 steps in one persistent launch, it holds the state, time and step count its own
+    context has right after the failing step (later steps of the launch hold the box)."""
+    n = 64
+    U = states.blast_wave(n)
+    cfg = pg.Config(n=(n, n, n), solver=pg.HLLD, cell_length=(1 / n,) * 3, time_step_factor=0.4)
+    ctx = pg.Context(cfg)
+    ctx.set_state(U)
+    failed = None
+    for step in range(80):
+        try:
+            ctx.step(1e30)
+        except pg.PhysicsError:
+            failed = step
+            break
+    assert failed is not None and 5 < failed < 70
+    batch = pg.Batch([cfg])
+    batch.set_state(0, U)
+    batch.run(80)
+    with pytest.raises(pg.PhysicsError):
+        batch.sync()
+    np.testing.assert_array_equal(batch.get_state(0), ctx.get_state())
+    t, count, _ = ctx.time()
+    assert batch.time(0)[:2] == (t, count) and count == failed + 1
+    np.testing.assert_array_equal(batch.dt_history(0, 100), ctx.dt_history(100))
+
+
 def test_tuner_restores_state():
     cfgs, U0s = small_ensemble()
     tuned, plain = pg.Batch(cfgs), pg.Batch(cfgs)
