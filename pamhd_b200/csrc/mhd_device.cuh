@@ -220,7 +220,7 @@ __device__ __forceinline__ Side side_of(const double U[8], const Derived& d)
 }
 
 /*
-Arithmetic of the HLLD solver.  Ar<false>: plain expressions, as written
+Arithmetic of the face solvers (Rusanov, HLL, HLLD).  Ar<false>: plain expressions, as written
 (the files built with -fmad=false round every operation on its own).
 Ar<true>: every operation an explicitly rounded intrinsic, a fused
 multiply-add where the formula has a product added, so that every kernel
@@ -311,26 +311,27 @@ F = (F_L + F_R)/2 - s/2 (U_R - U_L), s = max(|u_L|, |u_R|) + max(c_f,L, c_f,R).
 The field's normal component is diffused like the rest (the reference
 does not zero it).
 */
-template <bool BG>
+template <bool BG, bool EX = false>
 __device__ __forceinline__ double flux_rusanov(const Side& L, const Side& R, const Gas& g, double F[8],
                                                uint32_t& flag, const double* bg = nullptr)
 {
+	using A = Ar<EX and not BG>;
 	const double fast = fmax(L.cf, R.cf);
-	const double s = fmax(fabs(L.v0), fabs(R.v0)) + fast;
+	const double s = A::add(fmax(fabs(L.v0), fabs(R.v0)), fast);
 	double FL[8], FR[8];
 	if (BG) {
 		physical_flux_bg(L, bg[0], bg[1], bg[2], g, FL);
 		physical_flux_bg(R, bg[0], bg[1], bg[2], g, FR);
 	} else {
-		physical_flux(L, magnetic_pressure(L, g), g, FL);
-		physical_flux(R, magnetic_pressure(R, g), g, FR);
+		physical_flux<EX>(L, magnetic_pressure<EX>(L, g), g, FL);
+		physical_flux<EX>(R, magnetic_pressure<EX>(R, g), g, FR);
 	}
-	const double h = 0.5 * s;
+	const double h = A::mul(0.5, s);
 	const double UL[8] = {L.rho, L.m0, L.m1, L.m2, L.E, L.b0, L.b1, L.b2};
 	const double UR[8] = {R.rho, R.m0, R.m1, R.m2, R.E, R.b0, R.b1, R.b2};
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
-		F[v] = 0.5 * (FL[v] + FR[v]) - (UR[v] - UL[v]) * h;
+		F[v] = A::fma(-A::sub(UR[v], UL[v]), h, A::mul(0.5, A::add(FL[v], FR[v])));
 	}
 	if (flag == 0 and (not is_finite(F[0]) or not is_finite(s))) flag = PAMHD_FLAG_FLUX;
 	return s;
@@ -342,16 +343,17 @@ S_L = min(u_L, u_R) - max c_f, S_R = max(u_L, u_R) + max c_f,
 bm = min(S_L, 0), bp = max(S_R, 0); a degenerate fan (bp - bm not a
 positive normal number) gives zero flux and zero speed.
 */
-template <bool BG>
+template <bool BG, bool EX = false>
 __device__ __forceinline__ double flux_hll(const Side& L, const Side& R, const Gas& g, double F[8],
                                            uint32_t& /*flag*/, const double* bg = nullptr)
 {
+	using A = Ar<EX and not BG>;
 	const double fast = fmax(L.cf, R.cf);
 	const bool order = L.v0 <= R.v0;
-	const double s_neg = (order ? L.v0 : R.v0) - fast;
-	const double s_pos = (order ? R.v0 : L.v0) + fast;
+	const double s_neg = A::sub(order ? L.v0 : R.v0, fast);
+	const double s_pos = A::add(order ? R.v0 : L.v0, fast);
 	const double bm = fmin(s_neg, 0.0), bp = fmax(s_pos, 0.0);
-	const double width = bp - bm;
+	const double width = A::sub(bp, bm);
 	if (not (is_normal(width) and width > 0.0)) {
 		#pragma unroll
 		for (int v = 0; v < 8; v++) F[v] = 0.0;
@@ -362,17 +364,17 @@ __device__ __forceinline__ double flux_hll(const Side& L, const Side& R, const G
 		physical_flux_bg(L, bg[0], bg[1], bg[2], g, FL);
 		physical_flux_bg(R, bg[0], bg[1], bg[2], g, FR);
 	} else {
-		physical_flux(L, magnetic_pressure(L, g), g, FL);
-		physical_flux(R, magnetic_pressure(R, g), g, FR);
+		physical_flux<EX>(L, magnetic_pressure<EX>(L, g), g, FL);
+		physical_flux<EX>(R, magnetic_pressure<EX>(R, g), g, FR);
 	}
 	const double UL[8] = {L.rho, L.m0, L.m1, L.m2, L.E, L.b0, L.b1, L.b2};
 	const double UR[8] = {R.rho, R.m0, R.m1, R.m2, R.E, R.b0, R.b1, R.b2};
-	const double w = 0.5 * (bp + bm) * recip(width);
+	const double w = A::mul(A::mul(0.5, A::add(bp, bm)), recip(width));
 	#pragma unroll
 	for (int v = 0; v < 8; v++) {
-		const double a = (v == 5) ? 0.0 : FL[v] - bm * UL[v];
-		const double b = (v == 5) ? 0.0 : FR[v] - bp * UR[v];
-		F[v] = 0.5 * (a + b) + (a - b) * w;
+		const double a = (v == 5) ? 0.0 : A::fma(-bm, UL[v], FL[v]);
+		const double b = (v == 5) ? 0.0 : A::fma(-bp, UR[v], FR[v]);
+		F[v] = A::fma(A::sub(a, b), w, A::mul(0.5, A::add(a, b)));
 	}
 	return fmax(fabs(bp), fabs(bm));
 }
@@ -790,8 +792,8 @@ __device__ __forceinline__ double solve_face(const Side& L, const Side& R, const
 	flag = L.bad | R.bad;
 	if (flag & PAMHD_FLAG_DENSITY) flag = PAMHD_FLAG_DENSITY;
 	else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
-	if (SOLVER == PAMHD_RUSANOV) return flux_rusanov<false>(L, R, g, F, flag);
-	if (SOLVER == PAMHD_HLL_ATHENA) return flux_hll<false>(L, R, g, F, flag);
+	if (SOLVER == PAMHD_RUSANOV) return flux_rusanov<false, EX>(L, R, g, F, flag);
+	if (SOLVER == PAMHD_HLL_ATHENA) return flux_hll<false, EX>(L, R, g, F, flag);
 	if (SOLVER == PAMHD_HLLD_ATHENA) return flux_hlld<EX>(L, R, g, F, flag, pick);
 	return flux_roe(L, R, g, F, flag);
 }

@@ -1080,8 +1080,8 @@ __global__ void face_flux_kernel(long long n, const double* __restrict__ neg, co
 		if (flag & PAMHD_FLAG_DENSITY) flag = PAMHD_FLAG_DENSITY;
 		else if (flag & PAMHD_FLAG_PRESSURE) flag = PAMHD_FLAG_PRESSURE;
 		double s;
-		if (SOLVER == PAMHD_RUSANOV) s = use_bg ? flux_rusanov<true>(L, R, g, F, flag, b) : flux_rusanov<false>(L, R, g, F, flag);
-		else if (SOLVER == PAMHD_HLL_ATHENA) s = use_bg ? flux_hll<true>(L, R, g, F, flag, b) : flux_hll<false>(L, R, g, F, flag);
+		if (SOLVER == PAMHD_RUSANOV) s = use_bg ? flux_rusanov<true>(L, R, g, F, flag, b) : flux_rusanov<false, true>(L, R, g, F, flag);
+		else if (SOLVER == PAMHD_HLL_ATHENA) s = use_bg ? flux_hll<true>(L, R, g, F, flag, b) : flux_hll<false, true>(L, R, g, F, flag);
 		else if (SOLVER == PAMHD_HLLD_ATHENA) s = flux_hlld<true>(L, R, g, F, flag);
 		else s = flux_roe(L, R, g, F, flag);
 		for (int v = 0; v < 8; v++) flux[8 * t + v] = flag ? 0.0 : F[v];
