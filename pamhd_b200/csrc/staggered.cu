@@ -219,7 +219,9 @@ __device__ __forceinline__ void solve_minus_face(const Stag_Params& P, Side L, S
 		s = SOLVER == PAMHD_RUSANOV ? flux_rusanov<true>(L, R, P.gas, G, flag, b)
 		                            : flux_hll<true>(L, R, P.gas, G, flag, b);
 	} else {
-		s = solve_face<SOLVER>(L, R, P.gas, G, flag);
+		// HLLD in explicitly rounded arithmetic (fused multiply-adds: fewer instructions under
+		// -fmad=false); the other solvers as written, in the oracle's operation order
+		s = solve_face<SOLVER, SOLVER == PAMHD_HLLD_ATHENA>(L, R, P.gas, G, flag);
 	}
 	if (flag != 0) record_failure(P, flag, m, A);
 	smax = fmax(smax, s);

@@ -272,7 +272,8 @@ __device__ __forceinline__ void plus_face(const Sub_Params& P, const long long c
 	const Side L = side_of<A>(Uc, dc), R = side_of<A>(Uu, du);
 	double G[8];
 	uint32_t flag = 0;
-	const double s = solve_face<SOLVER>(L, R, P.gas, G, flag);
+	// HLLD in explicitly rounded arithmetic, as in the cell-centred step
+	const double s = solve_face<SOLVER, SOLVER == PAMHD_HLLD_ATHENA>(L, R, P.gas, G, flag);
 	if (flag != 0) {
 		atomicOr(&P.status->flags, flag);
 		atomicMin(&P.status->first, ((unsigned long long)(c * 3 + A) << 8) | flag);
