@@ -179,6 +179,30 @@ def test_box_failing_late_in_a_persistent_run_holds_its_failing_step():
     np.testing.assert_array_equal(batch.dt_history(0, 100), ctx.dt_history(100))
 
 
+@pytest.mark.parametrize("solver", [pg.RUSANOV, pg.HLL, pg.HLLD, 4])
+def test_every_solver_gives_the_context_bits_in_every_batch_kernel(solver):
+    """The 48^3 magnetised blast (periodic) with each solver: a batch of one box, tiles of 4 and of
+    8 rows, per-step launches and the persistent run, against the same grid in its own context
+    (32 x 8 tiles, 32 x 4 for Roe): the same bits after 6 steps."""
+    n = 48
+    U = states.blast_wave(n)
+    cfg = pg.Config(n=(n, n, n), solver=solver, cell_length=(1 / n,) * 3, time_step_factor=0.4)
+    ctx = pg.Context(cfg)
+    ctx.set_state(U)
+    ctx.steps(6, 1e300)
+    ctx.sync()
+    ref = ctx.get_state()
+    for rows in (4, 8):
+        for persistent in (False, True):
+            batch = pg.Batch([cfg])
+            batch.set_state(0, U)
+            batch.set_tiling(rows, 16, 1 << 20)
+            (batch.run if persistent else batch.steps)(6)
+            batch.sync()
+            np.testing.assert_array_equal(batch.get_state(0), ref)
+            assert batch.time(0) == ctx.time()
+
+
 def test_tuner_restores_state():
     cfgs, U0s = small_ensemble()
     tuned, plain = pg.Batch(cfgs), pg.Batch(cfgs)
